@@ -1,0 +1,428 @@
+"""Benchmark of the CIPHER RHS on B200: cell-updates/s, FP32-mixed vs FP64.
+
+Workload (the 3D grain-growth configuration): uniform periodic 128^3 grid,
+2000 seeded Voronoi grains (splitmix64 seed 12345), at most 12 active phases
+per cell, chemicalenergy none, interface energy 1, mobility 1, width 4 cells.
+The input state is a diffuse-interface Voronoi state (phi profiles of width 4
+around every grain boundary, active sets united with the face neighbours'),
+built on the host; the inputs are larger than L2 (about 180 MB mixed and
+270 MB FP64 of state per RHS), so no L2 flush is needed between launches.
+
+A step is one RHS evaluation over all 2,097,152 cells.  One process per GPU;
+ranks run independent replicas (the path has no cross-GPU exchange), so
+`value` = cells * steps * ranks / max-over-ranks device time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cipher|reference]
+
+`--impl reference` times the reference's own RHSFunction (compiled from its
+sources into oracle/_ref) on all host cores, one process per core on a slab
+with a one-cell halo, as `mpiexec -n p` runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s mixed vs FP64 at 1e-6 rel err"
+UNIT = "cell-updates/s"
+WORKLOAD = dict(dim=3, res=(128, 128, 128), ngrains=2000, cap=12, seed=12345, width=4.0)
+WORKLOAD_NAME = "3D grain growth 128^3, 2000 Voronoi grains, P=12, diffuse state (width 4)"
+HBM_PEAK_MEASURED = 6423.4   # GB/s, MEASURED_PEAKS.json hbm_gbs on this pool
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# --------------------------------------------------------------------------- #
+# workload                                                                     #
+# --------------------------------------------------------------------------- #
+
+def build_problem():
+    import cipher_b200 as cb
+    w = WORKLOAD
+    return cb.Problem.grain_growth(w["dim"], list(w["res"]), w["ngrains"], w["cap"], w["seed"])
+
+
+def build_state(problem, mesh):
+    import cipher_b200 as cb
+    return cb.diffuse_state_aos(problem, mesh, WORKLOAD["width"])
+
+
+def algorithmic_bytes(nsum: int, ncells: int, P: int, rb: int) -> int:
+    """Compulsory bytes of one RHS launch: each cell's active count and ids
+    (uint16), its active phi and T read once; all P phi slots and T of F
+    written once (neighbour values are re-reads served on chip)."""
+    reads = 2 * ncells + 2 * nsum + rb * nsum + rb * ncells
+    writes = ncells * (rb * P + rb)
+    return reads + writes
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_PEAK_MEASURED, "measured (pool value recorded with this build)"
+
+
+def traffic_per_launch(kind: str):
+    """DRAM bytes per launch of the RHS kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "rhs_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        e = d[kind]
+        return float(e["dram_bytes_per_launch"]) * float(e.get("scale_to_workload", 1.0))
+    except Exception:
+        return None
+
+
+# --------------------------------------------------------------------------- #
+# clocks (NVML sampled from a thread during each timed region)                #
+# --------------------------------------------------------------------------- #
+
+class ClockSampler:
+    HW = 0x8          # clocks_event_reasons: hw_slowdown
+    HW_THERMAL = 0x40
+    SW_THERMAL = 0x20
+    SW_POWER = 0x4
+
+    def __init__(self, device: int):
+        self.samples = []
+        self.reasons = 0
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        nv = self.nv
+        reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            getattr(nv, "nvmlDeviceGetCurrentClocksThrottleReasons")
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                self.reasons |= reasons(self.h)
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def start(self):
+        if self.nv is None:
+            return
+        self._stop.clear()
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        if self._t is not None:
+            self._stop.set()
+            self._t.join()
+            self._t = None
+
+    def summary(self):
+        if self.nv is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"], "samples": 0}
+        names = []
+        r = self.reasons
+        for bit, name in ((self.HW, "hw_slowdown"), (self.HW_THERMAL, "hw_thermal_slowdown"),
+                          (self.SW_THERMAL, "sw_thermal_slowdown"), (self.SW_POWER, "sw_power_cap")):
+            if r & bit:
+                names.append(name)
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": names, "samples": len(self.samples)}
+
+
+# --------------------------------------------------------------------------- #
+# reference on host cores                                                     #
+# --------------------------------------------------------------------------- #
+
+def _ref_worker(args):
+    lo, hi, Xs, reps, warm = args
+    import cipher_b200 as cb
+    import oracle
+    P = build_problem()
+    M = cb.Mesh(P, slab=(lo, hi))
+    times = []
+    with oracle.RefOracle(P, M) as R:
+        for i in range(warm + reps):
+            _, sec = R.rhs(Xs, with_time=True)
+            if i >= warm:
+                times.append(sec)
+    return times
+
+
+def reference_rate(X_aos: np.ndarray, procs: int, reps: int, warm: int):
+    """cell-updates/s of the reference RHS on `procs` host processes; each
+    step's time is the slowest process's (as an MPI run waits for it)."""
+    import cipher_b200 as cb
+    P = build_problem()
+    nz = P.s.resolution[P.s.dim - 1]
+    procs = max(1, min(procs, nz))
+    bounds = [(nz * k // procs, nz * (k + 1) // procs) for k in range(procs)]
+    jobs = []
+    for lo, hi in bounds:
+        M = cb.Mesh(P, slab=(lo, hi))
+        jobs.append((lo, hi, np.ascontiguousarray(X_aos[M.cell_global()]), reps, warm))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_ref_worker, jobs)
+    per_step = [max(r[k] for r in res) for k in range(reps)]
+    ncells = int(np.prod(WORKLOAD["res"]))
+    return ncells / statistics.mean(per_step), per_step
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# --------------------------------------------------------------------------- #
+# arms                                                                         #
+# --------------------------------------------------------------------------- #
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "metric": METRIC, "unit": UNIT,
+                          "unavailable": "oracle/_ref/libcipher_ref.so was not built (reference sources absent)"}))
+        return
+    import cipher_b200 as cb
+    P = build_problem()
+    M = cb.Mesh(P)
+    X = build_state(P, M)
+    cores = host_cores()
+    rate, per_step = reference_rate(X, cores, args.steps, args.warmup)
+    ms = 1e3 * statistics.mean(per_step)
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_NAME, "parallelism": f"{cores} host processes (slab + halo)"},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"each step one RHSFunction over all {int(np.prod(WORKLOAD['res']))} "
+                                       f"cells split in {cores} slabs"},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def time_launches(fn, steps, stream):
+    """Run fn() `steps` times on `stream`, one CUDA-event pair per launch."""
+    import torch
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for k in range(steps):
+        starts[k].record(stream)
+        fn()
+        ends[k].record(stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    per = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    return t0.elapsed_time(t1), per
+
+
+def run_cipher(args, rank, world, local_rank):
+    import torch
+    import cipher_b200 as cb
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(local_rank)
+    dev = local_rank
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    t_setup = time.time()
+    P = build_problem()
+    M = cb.Mesh(P)
+    X = build_state(P, M)
+    Lay = P.aos
+    Pcap = P.s.pf_size
+    ncells = M.nowned
+    nsum = int(X[:, Lay.as_offset].sum())
+    # the mixed path stores phi and T in FP32; both paths get those values
+    X32 = X.copy()
+    X32[:, Lay.pf_offset:Lay.pf_offset + Pcap] = X32[:, Lay.pf_offset:Lay.pf_offset + Pcap].astype(np.float32)
+    X32[:, Lay.tm_offset] = X32[:, Lay.tm_offset].astype(np.float32)
+    log(f"[rank {rank}] setup {time.time() - t_setup:.1f}s, mean active phases {nsum / ncells:.2f}")
+
+    c64 = cb.Context(P, M, "fp64", device=dev)
+    c32 = cb.Context(P, M, "mixed", device=dev)
+    X64d, F64d = c64.alloc_state(), c64.alloc_state()
+    X32d, F32d = c32.alloc_state(), c32.alloc_state()
+    c64.from_aos(X, X64d)
+    c32.from_aos(X32, X32d)
+    stream = torch.cuda.current_stream()
+
+    # accuracy of the mixed path against FP64 on the same input values
+    Xc, Fc = c64.alloc_state(), c64.alloc_state()
+    c64.from_aos(X32, Xc)
+    c64.rhs(0.0, Xc, Fc)
+    c32.rhs(0.0, X32d, F32d)
+    c64.check()
+    c32.check()
+    Fa, Fb = c64.to_aos(Fc), c32.to_aos(F32d)
+    sl = slice(Lay.pf_offset, Lay.pf_offset + Pcap)
+    rel_err = float(np.abs(Fb[:, sl] - Fa[:, sl]).max() / np.abs(Fa[:, sl]).max())
+    del Xc, Fc, Fa, Fb
+
+    for _ in range(args.warmup):
+        c64.rhs(0.0, X64d, F64d)
+        c32.rhs(0.0, X32d, F32d)
+    barrier()
+
+    clk = ClockSampler(dev)
+    # FP64 timed region
+    barrier()
+    clk.start()
+    tot64, per64 = time_launches(lambda: c64.rhs(0.0, X64d, F64d), args.steps, stream)
+    barrier()
+    # mixed timed region (the headline)
+    barrier()
+    tot32, per32 = time_launches(lambda: c32.rhs(0.0, X32d, F32d), args.steps, stream)
+    barrier()
+    clk.stop()
+    c64.check()
+    c32.check()
+    tot64 = max_over_ranks(tot64)
+    tot32 = max_over_ranks(tot32)
+
+    # end to end through the host-buffer entry point (reference AoS layout,
+    # pinned host memory, copies inside the timed region)
+    hx = torch.from_numpy(X).pin_memory()
+    hf = torch.empty_like(hx).pin_memory()
+    e2e_steps = max(1, min(args.steps, 10))
+    c32.rhs_aos_host(0.0, hx, hf)
+    barrier()
+    clk2 = ClockSampler(dev)
+    clk2.start()
+    tot_e2e, _ = time_launches(lambda: c32.rhs_aos_host(0.0, hx, hf), e2e_steps, stream)
+    clk2.stop()
+    barrier()
+    tot_e2e = max_over_ranks(tot_e2e)
+    aos_bytes = int(X.nbytes)
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    value = ncells * args.steps * world / (tot32 / 1e3)
+    value64 = ncells * args.steps * world / (tot64 / 1e3)
+    peak, peak_src = hbm_peak()
+    avg32 = statistics.mean(per32) / 1e3
+    avg64 = statistics.mean(per64) / 1e3
+    b32 = algorithmic_bytes(nsum, ncells, Pcap, 4)
+    b64 = algorithmic_bytes(nsum, ncells, Pcap, 8)
+    ach32 = b32 / avg32 / 1e9
+    ach64 = b64 / avg64 / 1e9
+    tr32 = traffic_per_launch("mixed")
+    tr64 = traffic_per_launch("fp64")
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            cores = host_cores()
+            rate, per_step = reference_rate(X, cores, 2, 1)
+            cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+                   "sample": f"2 timed RHSFunction calls (after 1 warm-up) over all {ncells} cells, "
+                             f"{cores} processes on z-slabs with a one-cell halo"}
+        else:
+            rate, sec = None, None
+            t0 = time.time()
+            oracle.port_rhs(P, M, X)
+            rate = ncells / (time.time() - t0)
+            cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+                   "sample": f"1 RHS over all {ncells} cells, one thread"}
+
+    c = clk.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": tot32 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_NAME, "cells": ncells, "max_phases": Pcap,
+                   "mean_active_phases": nsum / ncells, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (no flush)"},
+        "fp64": {"value": value64, "unit": UNIT, "ms_per_step": tot64 / args.steps,
+                 "roofline_frac": ach64 / peak},
+        "mixed_speedup_vs_fp64": value / value64,
+        "mixed_rel_err_vs_fp64": rel_err,
+        "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak,
+                     "traffic": tr32, "peak_source": peak_src, "algorithmic_bytes_per_launch": b32,
+                     "kernel": "k_rhs_phasefield<3,12,float>"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": ncells * e2e_steps * world / (tot_e2e / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": aos_bytes, "d2h_bytes_per_step": aos_bytes,
+                "path": "cipher_rhs_aos_host, reference AoS doubles in pinned host memory"},
+        "clocks": {"sm_mhz": c["sm_mhz"], "sm_max_mhz": c["sm_max_mhz"], "reasons": c["reasons"],
+                   "samples": c["samples"]},
+        "gpu_launches": args.steps,
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="cipher", choices=["cipher", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    import cipher_b200.build as b
+    if not os.path.exists(b.LIB):
+        b.build()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_cipher(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,9 @@
+"""cipher_b200 - B200 implementation of CIPHER's time-stepper right-hand side.
+
+The compute path is the CUDA library ``libcipher_b200.so`` (sm_100a) behind
+the C ABI of ``include/cipher_b200.h``; this package is its Python face.
+"""
+from ._lib import CipherError, load  # noqa: F401
+from .api import Context, Mesh, Problem, TSView, diffuse_state_aos, initial_state_aos  # noqa: F401
+
+__all__ = ["CipherError", "Context", "Mesh", "Problem", "TSView", "diffuse_state_aos", "initial_state_aos", "load"]

@@ -1,0 +1,189 @@
+"""ctypes bindings of the C ABI in include/cipher_b200.h and include/cipher_problem.h.
+
+The shared library is built in-tree (``cipher_b200/libcipher_b200.so``); this
+module never falls back to anything else: if the library is missing the import
+of the device API raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcipher_b200.so")
+
+MAXCP = 5
+MAXAP = 15
+MAXTSER = 10
+MAXRK = 4
+MAXRKTAB = 50
+MAXBIN = 10
+MAXSRC = 2
+MAXDIR = 8
+MAXLC = 8
+MAXBC = 6
+
+CHEM_QUADRATIC, CHEM_CALPHADDIS, CHEM_CALPHAD2SL, CHEM_NONE = 0, 1, 2, 3
+INTERP_LINEAR, INTERP_QUADRATIC, INTERP_CUBIC = 0, 1, 2
+BC_NEUMANN, BC_DIRICHLET, BC_NONE = 0, 1, 2
+SOURCE_SINK, SOURCE_RANDOM = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+
+OK = 0
+E_ARG, E_NOMEM, E_CAP, E_NONFINITE, E_CUDA, E_TIMEOUT, E_UNSUPPORTED, E_STEP = range(1, 9)
+
+
+class TSeries(C.Structure):
+    _fields_ = [("n", C.c_int32), ("exp", C.c_int32 * MAXTSER), ("coeff", C.c_double * MAXTSER),
+                ("logcoeff", C.c_double)]
+
+
+class RK(C.Structure):
+    _fields_ = [("n", C.c_int32), ("i", C.c_int32 * MAXRK), ("h", TSeries * MAXRK)]
+
+
+class Mobility(C.Structure):
+    _fields_ = [("m0", C.c_double), ("unary", TSeries * MAXCP), ("binary", RK * MAXBIN)]
+
+
+class Source(C.Structure):
+    _fields_ = [("model", C.c_int32), ("rate", C.c_double * MAXCP), ("ceq", C.c_double * MAXCP),
+                ("amplitude", C.c_double * MAXCP)]
+
+
+class Material(C.Structure):
+    _fields_ = [("model", C.c_int32), ("nsites", C.c_int32), ("molarvolume", C.c_double),
+                ("chempot_ex_kineticcoeff", C.c_double), ("c0", C.c_double * (2 * MAXCP)),
+                ("stoichiometry", C.c_double * 2), ("p", C.c_double), ("q", C.c_double),
+                ("ref", TSeries), ("unary", TSeries * (MAXCP * MAXCP)), ("quad_ceq", TSeries * MAXCP),
+                ("quad_binary", TSeries * MAXCP), ("binary", RK * MAXRKTAB), ("ternary", RK * MAXRKTAB),
+                ("binaryq", RK * MAXRKTAB), ("ternaryq", RK * MAXRKTAB), ("mobilityc", Mobility * MAXCP),
+                ("temperature0", C.c_double), ("specific_heat", TSeries), ("latent_heat", TSeries),
+                ("tconductivity", TSeries), ("nsources", C.c_int32), ("sources", Source * MAXSRC)]
+
+
+class Interface(C.Structure):
+    _fields_ = [("width", C.c_double), ("energy_m0", C.c_double), ("energy_activation", TSeries),
+                ("energy_naniso", C.c_int32), ("energy_aniso_dir", C.c_double * (MAXDIR * 3)),
+                ("energy_aniso_val", C.c_double * MAXDIR), ("mobility_m0", C.c_double),
+                ("mobility_activation", TSeries), ("mobility_naniso", C.c_int32),
+                ("mobility_aniso_dir", C.c_double * (MAXDIR * 3)), ("mobility_aniso_val", C.c_double * MAXDIR),
+                ("has_potential", C.c_int32), ("potential", C.c_double * MAXCP), ("has_mobilityc", C.c_int32),
+                ("mobilityc", C.c_double * MAXCP), ("nsources", C.c_int32), ("sources", Source * MAXSRC)]
+
+
+class BC(C.Structure):
+    _fields_ = [("boundaryid", C.c_int32), ("chem_bctype", C.c_int32), ("thermal_bctype", C.c_int32),
+                ("chem_bcval", C.c_double * MAXCP), ("thermal_bcval", C.c_double),
+                ("chem_bcbool", C.c_int8 * MAXCP)]
+
+
+class ProblemStruct(C.Structure):
+    _fields_ = [("dim", C.c_int32), ("npf", C.c_int32), ("ncp", C.c_int32), ("ndp", C.c_int32),
+                ("nmat", C.c_int32), ("nf", C.c_int32), ("nbcs", C.c_int32), ("pf_size", C.c_int32),
+                ("maxsites", C.c_int32), ("interpolation", C.c_int32), ("gradient_calculation", C.c_int32),
+                ("junctionpenalty", C.c_double), ("nloadcases", C.c_int32), ("currentloadcase", C.c_int32),
+                ("has_temperature_rate", C.c_int32), ("time", C.c_double * MAXLC),
+                ("temperature_rate", C.c_double * MAXLC), ("timestep0", C.c_double), ("mintimestep", C.c_double),
+                ("maxtimestep", C.c_double), ("reltol", C.c_double), ("abstol", C.c_double),
+                ("resolution", C.c_int32 * 3), ("size", C.c_double * 3), ("periodic", C.c_int32 * 3),
+                ("material", C.POINTER(Material)), ("interface", C.POINTER(Interface)),
+                ("interfacelist", C.POINTER(C.c_int32)), ("phasematerialmapping", C.POINTER(C.c_int32)),
+                ("voxelphase", C.POINTER(C.c_int32)), ("bcs", BC * MAXBC), ("centres", C.POINTER(C.c_double))]
+
+
+class MeshStruct(C.Structure):
+    _fields_ = [("dim", C.c_int32), ("ncells", C.c_int32), ("nowned", C.c_int32), ("nfaces", C.c_int32),
+                ("face_cells", C.POINTER(C.c_int32)), ("nbfaces", C.c_int32), ("bface_cell", C.POINTER(C.c_int32)),
+                ("bface_label", C.POINTER(C.c_int32)), ("cellgeom", C.POINTER(C.c_double)),
+                ("cell_global", C.POINTER(C.c_int32)), ("uniform", C.c_int32), ("res", C.c_int32 * 3),
+                ("periodic", C.c_int32 * 3), ("slab_lo", C.c_int32), ("slab_hi", C.c_int32)]
+
+
+class AosLayout(C.Structure):
+    _fields_ = [("as_offset", C.c_int32), ("pf_offset", C.c_int32), ("dp_offset", C.c_int32),
+                ("ex_offset", C.c_int32), ("tm_offset", C.c_int32), ("ndof", C.c_int32),
+                ("as_size", C.c_int32), ("pf_size", C.c_int32), ("dp_size", C.c_int32),
+                ("ex_size", C.c_int32), ("sp_size", C.c_int32), ("sf_size", C.c_int32)]
+
+
+class StateLayout(C.Structure):
+    _fields_ = [("ncells", C.c_int64), ("stride", C.c_int64), ("pf_size", C.c_int32), ("dp_size", C.c_int32),
+                ("ex_size", C.c_int32), ("precision", C.c_int32), ("as_offset", C.c_int64),
+                ("pf_offset", C.c_int64), ("dp_offset", C.c_int64), ("ex_offset", C.c_int64),
+                ("tm_offset", C.c_int64), ("bytes", C.c_int64)]
+
+
+PP = C.POINTER(ProblemStruct)
+MP = C.POINTER(MeshStruct)
+
+# (name, restype, argtypes)
+_SIGNATURES = [
+    ("cipher_strerror", C.c_char_p, [C.c_int]),
+    ("cipher_last_error", C.c_char_p, []),
+    ("cipher_abi_sizes", C.c_int, [C.POINTER(C.c_int64), C.c_int]),
+    ("cipher_problem_new", PP, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+    ("cipher_problem_free", None, [PP]),
+    ("cipher_problem_finalize", C.c_int, [PP]),
+    ("cipher_problem_set_cap", C.c_int, [PP, C.c_int]),
+    ("cipher_problem_aos_layout", AosLayout, [PP]),
+    ("cipher_problem_grain_growth", C.c_int,
+     [C.c_int, C.POINTER(C.c_int32), C.c_int, C.c_int, C.c_uint64, C.c_double, C.c_double, C.c_double,
+      C.c_double, C.c_double, C.POINTER(PP)]),
+    ("cipher_voronoi", C.c_int, [C.c_int, C.POINTER(C.c_int32), C.c_int, C.c_uint64, C.POINTER(C.c_int32),
+                                 C.POINTER(C.c_double)]),
+    ("cipher_rand_uniform", C.c_double, [C.POINTER(C.c_uint64)]),
+    ("cipher_mesh_uniform", C.c_int, [PP, C.c_int, C.c_int, C.POINTER(MP)]),
+    ("cipher_mesh_free", None, [MP]),
+    ("cipher_initial_state_aos", C.c_int, [PP, MP, C.POINTER(C.c_double)]),
+    ("cipher_initial_state_diffuse_aos", C.c_int, [PP, MP, C.c_double, C.POINTER(C.c_double)]),
+    ("cipher_waxpy", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),
+    ("cipher_ctx_create", C.c_int, [PP, MP, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    ("cipher_ctx_destroy", None, [C.c_void_p]),
+    ("cipher_ctx_layout", C.c_int, [C.c_void_p, C.POINTER(StateLayout)]),
+    ("cipher_rhs", C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("cipher_poststep", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("cipher_ctx_check", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("cipher_state_from_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("cipher_state_to_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("cipher_rhs_aos_host", C.c_int,
+     [C.c_void_p, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
+]
+
+EXPORTED = [s[0] for s in _SIGNATURES]
+
+_lib = None
+
+
+class CipherError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        lib = _lib
+        msg = ""
+        if lib is not None:
+            msg = lib.cipher_last_error().decode(errors="replace")
+            name = lib.cipher_strerror(code).decode()
+        else:
+            name = str(code)
+        super().__init__(f"{where}: {name} ({code}) {msg}")
+        self.code = code
+
+
+def load() -> C.CDLL:
+    """Load libcipher_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m cipher_b200.build` (needs nvcc)")
+    lib = C.CDLL(LIB_PATH)
+    for name, res, args in _SIGNATURES:
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int, where: str) -> None:
+    if rc != OK:
+        raise CipherError(rc, where)

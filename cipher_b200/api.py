@@ -1,0 +1,253 @@
+"""Python face of the C ABI: problems, meshes, device contexts.
+
+Mirrors the reference's callback pair: ``Context.RHSFunction(ts, t, X, F)``
+is the RHSFunction of src/cipher.c:27 and ``Context.PostStep(ts)`` its
+PostStep (src/cipher.c:686); both call the CUDA library.  Device buffers are
+torch uint8 tensors of ``layout.bytes`` (torch provides memory and streams;
+the arithmetic is the library's).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+
+
+class Problem:
+    """Owns a ``cipher_problem`` (model parameters + initial voxel map)."""
+
+    def __init__(self, ptr):
+        self._lib = L.load()
+        self.ptr = ptr
+
+    @classmethod
+    def grain_growth(cls, dim: int, res, ngrains: int, cap: int, seed: int, energy: float = 1.0,
+                     mobility: float = 1.0, width: float = 4.0, molarvolume: float = 1e-5,
+                     temperature0: float = 500.0) -> "Problem":
+        lib = L.load()
+        r = (C.c_int32 * 3)(*(list(res) + [1] * (3 - len(res))))
+        out = L.PP()
+        L.check(lib.cipher_problem_grain_growth(dim, r, ngrains, cap, seed, energy, mobility, width,
+                                                molarvolume, temperature0, C.byref(out)),
+                "cipher_problem_grain_growth")
+        return cls(out)
+
+    @property
+    def s(self) -> L.ProblemStruct:
+        return self.ptr.contents
+
+    @property
+    def aos(self) -> L.AosLayout:
+        return self._lib.cipher_problem_aos_layout(self.ptr)
+
+    @property
+    def ndof(self) -> int:
+        return self.aos.ndof
+
+    def voxelphase(self) -> np.ndarray:
+        s = self.s
+        n = int(np.prod([s.resolution[d] for d in range(s.dim)]))
+        return np.ctypeslib.as_array(s.voxelphase, shape=(n,)).copy()
+
+    def close(self):
+        if self.ptr:
+            self._lib.cipher_problem_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Mesh:
+    """Owns a ``cipher_mesh`` (uniform grid, whole domain or a slab + halo)."""
+
+    def __init__(self, problem: Problem, slab=None):
+        self._lib = L.load()
+        s = problem.s
+        lo, hi = (0, s.resolution[s.dim - 1]) if slab is None else slab
+        out = L.MP()
+        L.check(self._lib.cipher_mesh_uniform(problem.ptr, lo, hi, C.byref(out)), "cipher_mesh_uniform")
+        self.ptr = out
+        self.problem = problem
+
+    @property
+    def s(self) -> L.MeshStruct:
+        return self.ptr.contents
+
+    @property
+    def ncells(self) -> int:
+        return self.s.ncells
+
+    @property
+    def nowned(self) -> int:
+        return self.s.nowned
+
+    def cell_global(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self.s.cell_global, shape=(self.ncells,)).copy()
+
+    def close(self):
+        if self.ptr:
+            self._lib.cipher_mesh_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def initial_state_aos(problem: Problem, mesh: Mesh) -> np.ndarray:
+    """SetUpProblem's state (src/init.c:1721-1830) in the reference AoS layout."""
+    lib = L.load()
+    X = np.zeros((mesh.ncells, problem.ndof), dtype=np.float64)
+    L.check(lib.cipher_initial_state_aos(problem.ptr, mesh.ptr, X.ctypes.data_as(C.POINTER(C.c_double))),
+            "cipher_initial_state_aos")
+    return X
+
+
+def diffuse_state_aos(problem: Problem, mesh: Mesh, width: float = 4.0) -> np.ndarray:
+    """Diffuse-interface Voronoi state (see cipher_initial_state_diffuse_aos)."""
+    lib = L.load()
+    X = np.zeros((mesh.ncells, problem.ndof), dtype=np.float64)
+    L.check(lib.cipher_initial_state_diffuse_aos(problem.ptr, mesh.ptr, float(width),
+                                                 X.ctypes.data_as(C.POINTER(C.c_double))),
+            "cipher_initial_state_diffuse_aos")
+    return X
+
+
+@dataclass
+class TSView:
+    """The slice of a PETSc TS the callbacks read: solution, time, step."""
+    X: object = None
+    t: float = 0.0
+    dt: float = 0.0
+    step: int = 0
+
+
+def _ptr(t) -> int:
+    return int(t.data_ptr()) if hasattr(t, "data_ptr") else int(t)
+
+
+def _stream_handle(stream) -> C.c_void_p:
+    if stream is None:
+        import torch
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if hasattr(stream, "cuda_stream"):
+        return C.c_void_p(stream.cuda_stream)
+    return C.c_void_p(int(stream))
+
+
+class Context:
+    """A device context (``cipher_ctx``) for one problem on one GPU."""
+
+    def __init__(self, problem: Problem, mesh: Mesh, precision: str = "fp64", device: int = 0):
+        self._lib = L.load()
+        prec = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}[precision]
+        out = C.c_void_p()
+        L.check(self._lib.cipher_ctx_create(problem.ptr, mesh.ptr, prec, device, C.byref(out)),
+                "cipher_ctx_create")
+        self.ptr = out
+        self.problem, self.mesh, self.precision, self.device = problem, mesh, precision, device
+        lay = L.StateLayout()
+        L.check(self._lib.cipher_ctx_layout(self.ptr, C.byref(lay)), "cipher_ctx_layout")
+        self.layout = lay
+
+    # -- buffers -------------------------------------------------------------
+    def alloc_state(self):
+        import torch
+        return torch.zeros(int(self.layout.bytes), dtype=torch.uint8, device=f"cuda:{self.device}")
+
+    def planes(self, X):
+        """Typed views (as, phi, dp, ex, tm) of a device state tensor."""
+        import torch
+        lay = self.layout
+        S, P = int(lay.stride), int(lay.pf_size)
+        rt = torch.float64 if self.precision == "fp64" else torch.float32
+        rb = 8 if self.precision == "fp64" else 4
+
+        def view(off, n, dt, nb):
+            return X[off:off + n * S * nb].view(dt).view(n, S) if n else X[0:0].view(dt).view(0, S)
+        return (view(int(lay.as_offset), P + 1, torch.int16, 2), view(int(lay.pf_offset), P, rt, rb),
+                view(int(lay.dp_offset), int(lay.dp_size), torch.float64, 8),
+                view(int(lay.ex_offset), int(lay.ex_size), torch.float64, 8),
+                view(int(lay.tm_offset), 1, rt, rb))
+
+    # -- conversions -----------------------------------------------------------
+    def from_aos(self, aos, X, stream=None):
+        """Device state X <- reference AoS array (numpy host or torch device)."""
+        import torch
+        if isinstance(aos, np.ndarray):
+            aos = torch.from_numpy(np.ascontiguousarray(aos, dtype=np.float64)).to(f"cuda:{self.device}")
+        L.check(self._lib.cipher_state_from_aos(self.ptr, C.c_void_p(_ptr(aos)), C.c_void_p(_ptr(X)),
+                                                 _stream_handle(stream)), "cipher_state_from_aos")
+        return X
+
+    def to_aos(self, X, stream=None) -> np.ndarray:
+        import torch
+        out = torch.empty((int(self.layout.ncells), self.problem.ndof), dtype=torch.float64,
+                          device=f"cuda:{self.device}")
+        L.check(self._lib.cipher_state_to_aos(self.ptr, C.c_void_p(_ptr(X)), C.c_void_p(_ptr(out)),
+                                               _stream_handle(stream)), "cipher_state_to_aos")
+        torch.cuda.synchronize(self.device)
+        return out.cpu().numpy()
+
+    # -- the two callbacks -------------------------------------------------------
+    def rhs(self, t: float, X, F, stream=None):
+        L.check(self._lib.cipher_rhs(self.ptr, float(t), C.c_void_p(_ptr(X)), C.c_void_p(_ptr(F)),
+                                     _stream_handle(stream)), "cipher_rhs")
+
+    def poststep(self, X, stream=None):
+        L.check(self._lib.cipher_poststep(self.ptr, C.c_void_p(_ptr(X)), _stream_handle(stream)),
+                "cipher_poststep")
+
+    def waxpy(self, Y, X, a: float, F, stream=None):
+        """Y = X + a*F on the real planes (AS copied from X)."""
+        L.check(self._lib.cipher_waxpy(self.ptr, C.c_void_p(_ptr(Y)), C.c_void_p(_ptr(X)), float(a),
+                                       C.c_void_p(_ptr(F)), _stream_handle(stream)), "cipher_waxpy")
+
+    def check(self, stream=None):
+        L.check(self._lib.cipher_ctx_check(self.ptr, _stream_handle(stream)), "cipher_ctx_check")
+
+    def RHSFunction(self, ts: TSView, ftime: float, X, F) -> int:
+        """Reference-shaped callback: F = RHS(ftime, X); returns 0 like PetscErrorCode."""
+        self.rhs(ftime, X, F)
+        return 0
+
+    def PostStep(self, ts: TSView) -> int:
+        """Reference-shaped callback: active-set update of ts.X in place."""
+        self.poststep(ts.X)
+        return 0
+
+    def rhs_aos_host(self, t: float, X, F=None, stream=None):
+        """Drop-in call on host buffers in the reference AoS layout (numpy
+        arrays, or pinned CPU torch tensors for full-speed copies)."""
+        if hasattr(X, "data_ptr"):
+            xp = C.cast(C.c_void_p(X.data_ptr()), C.POINTER(C.c_double))
+            fp = C.cast(C.c_void_p(F.data_ptr()), C.POINTER(C.c_double))
+        else:
+            X = np.ascontiguousarray(X, dtype=np.float64)
+            if F is None:
+                F = np.empty_like(X)
+            xp = X.ctypes.data_as(C.POINTER(C.c_double))
+            fp = F.ctypes.data_as(C.POINTER(C.c_double))
+        L.check(self._lib.cipher_rhs_aos_host(self.ptr, float(t), xp, fp, _stream_handle(stream)),
+                "cipher_rhs_aos_host")
+        return F
+
+    def close(self):
+        if self.ptr:
+            self._lib.cipher_ctx_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

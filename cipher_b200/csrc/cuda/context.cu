@@ -1,0 +1,485 @@
+/*
+ * context.cu - device context and the C ABI entry points of include/cipher_b200.h.
+ *
+ * A context owns the device copies of the model tables and the scratch the
+ * per-step update needs; state vectors X and F are owned by the caller (the
+ * time stepper), as PETSc's TS owns X and F for the reference's RHSFunction
+ * (src/cipher.c:27, 1107).
+ */
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <cuda_runtime.h>
+#include "cipher_b200.h"
+#include "device_common.cuh"
+#include "kernels.h"
+
+using namespace cipher;
+
+/* ------------------------------------------------------------------ */
+/* errors                                                               */
+/* ------------------------------------------------------------------ */
+
+static thread_local char g_errmsg[512] = "";
+
+static int set_error(int code, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_errmsg, sizeof(g_errmsg), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+static int cuda_fail(cudaError_t e, const char *where)
+{
+    return set_error(CIPHER_E_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+#define CUDA_TRY(call, where)                              \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cuda_fail(e_, where); \
+    } while (0)
+
+extern "C" const char *cipher_strerror(int code)
+{
+    switch (code) {
+    case CIPHER_OK: return "ok";
+    case CIPHER_E_ARG: return "invalid argument";
+    case CIPHER_E_NOMEM: return "out of memory";
+    case CIPHER_E_CAP: return "active-set superset exceeds the phase cap";
+    case CIPHER_E_NONFINITE: return "non-finite value";
+    case CIPHER_E_CUDA: return "CUDA error";
+    case CIPHER_E_TIMEOUT: return "bounded device wait ran out";
+    case CIPHER_E_UNSUPPORTED: return "configuration not supported on the device";
+    case CIPHER_E_STEP: return "time step below the minimum";
+    default: return "unknown error";
+    }
+}
+
+extern "C" const char *cipher_last_error(void) { return g_errmsg; }
+
+/* ------------------------------------------------------------------ */
+/* context                                                              */
+/* ------------------------------------------------------------------ */
+
+struct cipher_ctx {
+    int device, precision, dim;
+    int res[3], per[3];
+    int64_t ncells, stride;
+    int P, npf, ncp, ndp, S, nmat;
+    cipher_state_layout lay;
+    cipher_aos_layout aos;
+    int single;
+    double sig0, mob0, wid0, tj0, ffactor, vol, junctionpenalty;
+    int has_temp_rate;
+    double temp_rate;
+    int32_t *d_itflist;
+    DevInterface *d_itfs;
+    uint16_t *d_pruned;
+    double *d_ex_init;
+    int *d_err;
+    int *h_err;
+    /* buffers of the host-AoS entry point, allocated on first use */
+    double *d_aos_x, *d_aos_f;
+    void *d_X, *d_F;
+};
+
+static int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+
+static int problem_supported(const cipher_problem *p, char *why, size_t len)
+{
+    if (p->gradient_calculation) { snprintf(why, len, "gradient_calculation (anisotropy) is not implemented"); return 0; }
+    if (p->ndp != 0) { snprintf(why, len, "chemistry (ncp > 1) is not implemented on the device yet"); return 0; }
+    if (p->nbcs != 0) { snprintf(why, len, "boundary conditions are not implemented on the device yet"); return 0; }
+    for (int m = 0; m < p->nmat; m++) {
+        const cipher_material *mat = &p->material[m];
+        if (mat->model != CIPHER_CHEM_NONE) { snprintf(why, len, "material %d: chemical model needs ncp > 1", m); return 0; }
+        if (mat->ref.n != 0 || mat->ref.logcoeff != 0.0) { snprintf(why, len, "material %d: non-zero reference energy", m); return 0; }
+        if (mat->tconductivity.n || mat->specific_heat.n || mat->latent_heat.n) {
+            snprintf(why, len, "material %d: thermal model without chemistry reads an unset temperature in the reference", m);
+            return 0;
+        }
+        if (mat->nsources) { snprintf(why, len, "material %d: sources need chemistry", m); return 0; }
+    }
+    for (int i = 0; i < p->nf; i++)
+        if (p->interface[i].has_potential || p->interface[i].nsources || p->interface[i].energy_naniso ||
+            p->interface[i].mobility_naniso) {
+            snprintf(why, len, "interface %d: segregation, sources or anisotropy need chemistry/gradients", i);
+            return 0;
+        }
+    if (p->interpolation != CIPHER_INTERP_CUBIC && p->interpolation != CIPHER_INTERP_QUADRATIC &&
+        p->interpolation != CIPHER_INTERP_LINEAR) { snprintf(why, len, "unknown interpolation"); return 0; }
+    return 1;
+}
+
+static void free_ctx(cipher_ctx *c)
+{
+    if (!c) return;
+    cudaFree(c->d_itflist);
+    cudaFree(c->d_itfs);
+    cudaFree(c->d_pruned);
+    cudaFree(c->d_ex_init);
+    cudaFree(c->d_err);
+    if (c->h_err) cudaFreeHost(c->h_err);
+    cudaFree(c->d_aos_x);
+    cudaFree(c->d_aos_f);
+    cudaFree(c->d_X);
+    cudaFree(c->d_F);
+    free(c);
+}
+
+extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, int precision, int device,
+                                 cipher_ctx **out)
+{
+    if (!out) return set_error(CIPHER_E_ARG, "out is NULL");
+    *out = NULL;
+    if (!p || !m) return set_error(CIPHER_E_ARG, "problem or mesh is NULL");
+    if (precision != CIPHER_PREC_FP64 && precision != CIPHER_PREC_MIXED)
+        return set_error(CIPHER_E_ARG, "unknown precision %d", precision);
+    if (!m->uniform || m->ncells != m->nowned)
+        return set_error(CIPHER_E_UNSUPPORTED, "device path needs a whole-domain uniform mesh");
+    if (p->pf_size < 1 || p->pf_size > CIPHER_MAXAP) return set_error(CIPHER_E_ARG, "bad phase cap %d", p->pf_size);
+    char why[256];
+    if (!problem_supported(p, why, sizeof(why))) return set_error(CIPHER_E_UNSUPPORTED, "%s", why);
+    /* the linear interpolant is not used by the phase-field-only kernel (no chemistry) */
+
+    CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    cipher_ctx *c = (cipher_ctx *)calloc(1, sizeof(cipher_ctx));
+    if (!c) return set_error(CIPHER_E_NOMEM, "host allocation");
+    c->device = device;
+    c->precision = precision;
+    c->dim = p->dim;
+    for (int d = 0; d < 3; d++) {
+        c->res[d] = d < p->dim ? m->res[d] : 1;
+        c->per[d] = d < p->dim ? (m->periodic[d] && m->res[d] > 1) : 0;
+    }
+    c->ncells = m->ncells;
+    c->stride = align_up(c->ncells, 128);
+    c->P = p->pf_size;
+    c->npf = p->npf;
+    c->ncp = p->ncp;
+    c->ndp = p->ndp;
+    c->S = p->maxsites * p->ndp;
+    c->nmat = p->nmat;
+    c->junctionpenalty = p->junctionpenalty;
+    c->has_temp_rate = p->has_temperature_rate;
+    c->temp_rate = p->has_temperature_rate ? p->temperature_rate[p->currentloadcase] : 0.0;
+    c->aos = cipher_problem_aos_layout(p);
+
+    /* geometry exactly as the reference forms it (src/cipher.c:273-275) */
+    {
+        double delta = m->cellgeom[0];
+        double vol = 1.0, b = delta;
+        unsigned e = (unsigned)p->dim;
+        while (e) { if (e & 1u) vol *= b; e >>= 1; b *= b; }
+        c->vol = vol;
+        c->ffactor = 2.0 * (delta < delta ? vol / delta : vol / delta) / (delta + delta);
+    }
+
+    /* state layout */
+    const int64_t rb = precision == CIPHER_PREC_FP64 ? 8 : 4;
+    cipher_state_layout L;
+    memset(&L, 0, sizeof(L));
+    L.ncells = c->ncells;
+    L.stride = c->stride;
+    L.pf_size = c->P;
+    L.dp_size = c->ndp;
+    L.ex_size = c->P * c->S;
+    L.precision = precision;
+    int64_t off = 0;
+    L.as_offset = off; off = align_up(off + (int64_t)(c->P + 1) * c->stride * 2, 256);
+    L.pf_offset = off; off = align_up(off + (int64_t)c->P * c->stride * rb, 256);
+    L.dp_offset = off; off = align_up(off + (int64_t)c->ndp * c->stride * 8, 256);
+    L.ex_offset = off; off = align_up(off + (int64_t)L.ex_size * c->stride * 8, 256);
+    L.tm_offset = off; off = align_up(off + c->stride * rb, 256);
+    L.bytes = off;
+    c->lay = L;
+
+    /* interface tables: one T-independent interface for every pair is the
+     * common case (grain growth) and needs no lookup */
+    int first = -1, single = 1;
+    for (int a = 0; a < p->npf && single; a++)
+        for (int b = a + 1; b < p->npf; b++) {
+            int i = p->interfacelist[a * p->npf + b];
+            if (i < 0 || i >= p->nf) { free_ctx(c); return set_error(CIPHER_E_ARG, "interface index %d out of range", i); }
+            if (first < 0) first = i;
+            else if (i != first) { single = 0; break; }
+        }
+    if (first < 0) first = 0;
+    if (p->interface[first].energy_activation.n || p->interface[first].mobility_activation.n) single = 0;
+    c->single = single;
+    {
+        const cipher_interface *itf = &p->interface[first];
+        c->sig0 = 1.0 * itf->energy_m0;
+        c->mob0 = 1.0 * itf->mobility_m0;
+        c->wid0 = itf->width;
+        double v = c->sig0 / c->wid0, t = 0.0;
+        t = t > v ? t : v;
+        t = t > v ? t : v;
+        t = t > v ? t : v;
+        t *= p->junctionpenalty;
+        c->tj0 = t;
+    }
+    cudaError_t e;
+    if (!single) {
+        for (int a = 0; a < p->npf; a++)
+            for (int b = a + 1; b < p->npf; b++) {
+                int i = p->interfacelist[a * p->npf + b];
+                if (i < 0 || i >= p->nf) { free_ctx(c); return set_error(CIPHER_E_ARG, "interface index out of range"); }
+            }
+        size_t nb = (size_t)p->npf * p->npf * sizeof(int32_t);
+        if ((e = cudaMalloc(&c->d_itflist, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc itflist"); }
+        if ((e = cudaMemcpy(c->d_itflist, p->interfacelist, nb, cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy itflist"); }
+    }
+    {
+        DevInterface *h = (DevInterface *)calloc((size_t)p->nf, sizeof(DevInterface));
+        if (!h) { free_ctx(c); return set_error(CIPHER_E_NOMEM, "host allocation"); }
+        for (int i = 0; i < p->nf; i++) {
+            const cipher_interface *s = &p->interface[i];
+            h[i].width = s->width;
+            h[i].energy_m0 = s->energy_m0;
+            h[i].mobility_m0 = s->mobility_m0;
+            h[i].energy_act = s->energy_activation;
+            h[i].mobility_act = s->mobility_activation;
+            h[i].has_potential = s->has_potential;
+            h[i].has_mobilityc = s->has_mobilityc;
+            memcpy(h[i].potential, s->potential, sizeof(h[i].potential));
+            memcpy(h[i].mobilityc, s->mobilityc, sizeof(h[i].mobilityc));
+        }
+        e = cudaMalloc(&c->d_itfs, (size_t)p->nf * sizeof(DevInterface));
+        if (e == cudaSuccess) e = cudaMemcpy(c->d_itfs, h, (size_t)p->nf * sizeof(DevInterface), cudaMemcpyHostToDevice);
+        free(h);
+        if (e != cudaSuccess) { free_ctx(c); return cuda_fail(e, "interface table"); }
+    }
+    if ((e = cudaMalloc(&c->d_pruned, (size_t)(c->P + 1) * c->stride * sizeof(uint16_t))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc pruned"); }
+    if ((e = cudaMalloc(&c->d_err, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc err"); }
+    if ((e = cudaMemset(c->d_err, 0, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMemset err"); }
+    if ((e = cudaMallocHost(&c->h_err, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMallocHost err"); }
+    *c->h_err = 0;
+    *out = c;
+    return CIPHER_OK;
+}
+
+extern "C" void cipher_ctx_destroy(cipher_ctx *c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    free_ctx(c);
+}
+
+extern "C" int cipher_ctx_layout(const cipher_ctx *c, cipher_state_layout *out)
+{
+    if (!c || !out) return set_error(CIPHER_E_ARG, "NULL argument");
+    *out = c->lay;
+    return CIPHER_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* RHS and PostStep                                                     */
+/* ------------------------------------------------------------------ */
+
+template <typename R>
+static PfArgs<R> pf_args(const cipher_ctx *c, const void *X, void *F)
+{
+    PfArgs<R> a;
+    memset(&a, 0, sizeof(a));
+    const char *x = (const char *)X;
+    char *f = (char *)F;
+    a.ncells = c->ncells;
+    a.stride = c->stride;
+    for (int d = 0; d < 3; d++) { a.res[d] = c->res[d]; a.per[d] = c->per[d]; }
+    a.P = c->P;
+    a.npf = c->npf;
+    a.ffactor = c->ffactor;
+    a.vol = c->vol;
+    a.junctionpenalty = c->junctionpenalty;
+    a.has_temp_rate = c->has_temp_rate;
+    a.temp_rate = c->temp_rate;
+    a.single = c->single;
+    a.sig0 = c->sig0;
+    a.mob0 = c->mob0;
+    a.wid0 = c->wid0;
+    a.tj0 = c->tj0;
+    a.itflist = c->d_itflist;
+    a.itfs = c->d_itfs;
+    a.as = (const uint16_t *)(x + c->lay.as_offset);
+    a.phi = (const R *)(x + c->lay.pf_offset);
+    a.tm = (const R *)(x + c->lay.tm_offset);
+    a.fphi = (R *)(f + c->lay.pf_offset);
+    a.ftm = (R *)(f + c->lay.tm_offset);
+    a.err = c->d_err;
+    return a;
+}
+
+extern "C" int cipher_rhs(cipher_ctx *c, double t, const void *X, void *F, void *stream)
+{
+    (void)t;
+    if (!c || !X || !F) return set_error(CIPHER_E_ARG, "NULL argument");
+    if (X == F) return set_error(CIPHER_E_ARG, "X and F must not alias");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e;
+    if (c->precision == CIPHER_PREC_FP64) e = launch_rhs_phasefield(pf_args<double>(c, X, F), c->dim, s);
+    else e = launch_rhs_phasefield(pf_args<float>(c, X, F), c->dim, s);
+    if (e != cudaSuccess) return cuda_fail(e, "rhs launch");
+    return CIPHER_OK;
+}
+
+template <typename R>
+static PostArgs<R> post_args(const cipher_ctx *c, void *X)
+{
+    PostArgs<R> a;
+    memset(&a, 0, sizeof(a));
+    char *x = (char *)X;
+    a.ncells = c->ncells;
+    a.stride = c->stride;
+    for (int d = 0; d < 3; d++) { a.res[d] = c->res[d]; a.per[d] = c->per[d]; }
+    a.P = c->P;
+    a.S = c->S;
+    a.as = (uint16_t *)(x + c->lay.as_offset);
+    a.phi = (R *)(x + c->lay.pf_offset);
+    a.ex = (double *)(x + c->lay.ex_offset);
+    a.tm = (const R *)(x + c->lay.tm_offset);
+    a.pruned = c->d_pruned;
+    a.ex_init = c->d_ex_init;
+    a.err = c->d_err;
+    return a;
+}
+
+static int read_flags(cipher_ctx *c, cudaStream_t s, int *flags)
+{
+    CUDA_TRY(cudaMemcpyAsync(c->h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, s), "read error flags");
+    CUDA_TRY(cudaStreamSynchronize(s), "stream sync");
+    *flags = *c->h_err;
+    if (*flags) CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), s), "clear error flags");
+    return CIPHER_OK;
+}
+
+extern "C" int cipher_poststep(cipher_ctx *c, void *X, void *stream)
+{
+    if (!c || !X) return set_error(CIPHER_E_ARG, "NULL argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e;
+    if (c->precision == CIPHER_PREC_FP64) e = launch_poststep(post_args<double>(c, X), c->dim, s);
+    else e = launch_poststep(post_args<float>(c, X), c->dim, s);
+    if (e != cudaSuccess) return cuda_fail(e, "poststep launch");
+    int flags = 0;
+    int rc = read_flags(c, s, &flags);
+    if (rc) return rc;
+    if (flags & ERR_CAP) return set_error(CIPHER_E_CAP, "active-set superset exceeds the cap P=%d", c->P);
+    if (flags & ERR_BADSET) return set_error(CIPHER_E_ARG, "state holds an active count outside 1..P");
+    return CIPHER_OK;
+}
+
+/* sync, read and clear the kernels' error flags */
+extern "C" int cipher_ctx_check(cipher_ctx *c, void *stream)
+{
+    if (!c) return set_error(CIPHER_E_ARG, "NULL argument");
+    int flags = 0;
+    int rc = read_flags(c, (cudaStream_t)stream, &flags);
+    if (rc) return rc;
+    if (flags & ERR_CAP) return set_error(CIPHER_E_CAP, "active-set superset exceeds the cap P=%d", c->P);
+    if (flags & ERR_BADSET) return set_error(CIPHER_E_ARG, "state holds an active count outside 1..P");
+    return CIPHER_OK;
+}
+
+namespace cipher {
+cudaError_t launch_waxpy(int precision, int64_t nreal, int64_t ndbl, const void *xr, const void *fr, void *yr,
+                         const double *xd, const double *fd, double *yd, double a, cudaStream_t s);
+}
+
+extern "C" int cipher_waxpy(cipher_ctx *c, void *Y, const void *X, double a, const void *F, void *stream)
+{
+    if (!c || !Y || !X || !F) return set_error(CIPHER_E_ARG, "NULL argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const char *x = (const char *)X, *f = (const char *)F;
+    char *y = (char *)Y;
+    const cipher_state_layout &L = c->lay;
+    if (Y != X)
+        CUDA_TRY(cudaMemcpyAsync(y + L.as_offset, x + L.as_offset, (size_t)(L.pf_offset - L.as_offset),
+                                 cudaMemcpyDeviceToDevice, s), "copy AS");
+    int64_t rb = c->precision == CIPHER_PREC_FP64 ? 8 : 4;
+    int64_t nreal = (int64_t)c->P * c->stride;
+    int64_t ndbl = (L.tm_offset - L.dp_offset) / 8;
+    cudaError_t e = launch_waxpy(c->precision, nreal, ndbl, x + L.pf_offset, f + L.pf_offset, y + L.pf_offset,
+                                 (const double *)(x + L.dp_offset), (const double *)(f + L.dp_offset),
+                                 (double *)(y + L.dp_offset), a, s);
+    if (e != cudaSuccess) return cuda_fail(e, "waxpy launch");
+    e = launch_waxpy(c->precision, c->stride, 0, x + L.tm_offset, f + L.tm_offset, y + L.tm_offset,
+                     nullptr, nullptr, nullptr, a, s);
+    if (e != cudaSuccess) return cuda_fail(e, "waxpy launch");
+    (void)rb;
+    return CIPHER_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* layouts and the host-buffer entry point                             */
+/* ------------------------------------------------------------------ */
+
+static LayoutArgs layout_args(const cipher_ctx *c, void *X)
+{
+    LayoutArgs a;
+    memset(&a, 0, sizeof(a));
+    char *x = (char *)X;
+    a.ncells = c->ncells;
+    a.stride = c->stride;
+    a.P = c->P;
+    a.D = c->ndp;
+    a.E = c->P * c->S;
+    a.ndof = c->aos.ndof;
+    a.as_off = c->aos.as_offset;
+    a.pf_off = c->aos.pf_offset;
+    a.dp_off = c->aos.dp_offset;
+    a.ex_off = c->aos.ex_offset;
+    a.tm_off = c->aos.tm_offset;
+    a.real_bytes = c->precision == CIPHER_PREC_FP64 ? 8 : 4;
+    a.as = (uint16_t *)(x + c->lay.as_offset);
+    a.phi = x + c->lay.pf_offset;
+    a.dp = (double *)(x + c->lay.dp_offset);
+    a.ex = (double *)(x + c->lay.ex_offset);
+    a.tm = x + c->lay.tm_offset;
+    return a;
+}
+
+extern "C" int cipher_state_from_aos(cipher_ctx *c, const double *aos, void *X, void *stream)
+{
+    if (!c || !aos || !X) return set_error(CIPHER_E_ARG, "NULL argument");
+    cudaError_t e = launch_aos_to_soa(layout_args(c, X), aos, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "aos->state launch");
+    return CIPHER_OK;
+}
+
+extern "C" int cipher_state_to_aos(cipher_ctx *c, const void *X, double *aos, void *stream)
+{
+    if (!c || !aos || !X) return set_error(CIPHER_E_ARG, "NULL argument");
+    cudaError_t e = launch_soa_to_aos(layout_args(c, (void *)X), aos, 1, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "state->aos launch");
+    return CIPHER_OK;
+}
+
+extern "C" int cipher_rhs_aos_host(cipher_ctx *c, double t, const double *X_host, double *F_host, void *stream)
+{
+    if (!c || !X_host || !F_host) return set_error(CIPHER_E_ARG, "NULL argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    size_t nb = (size_t)c->ncells * c->aos.ndof * sizeof(double);
+    if (!c->d_aos_x) {
+        CUDA_TRY(cudaMalloc(&c->d_aos_x, nb), "cudaMalloc aos x");
+        CUDA_TRY(cudaMalloc(&c->d_aos_f, nb), "cudaMalloc aos f");
+        CUDA_TRY(cudaMalloc(&c->d_X, (size_t)c->lay.bytes), "cudaMalloc X");
+        CUDA_TRY(cudaMalloc(&c->d_F, (size_t)c->lay.bytes), "cudaMalloc F");
+        CUDA_TRY(cudaMemset(c->d_F, 0, (size_t)c->lay.bytes), "cudaMemset F");
+    }
+    CUDA_TRY(cudaMemcpyAsync(c->d_aos_x, X_host, nb, cudaMemcpyHostToDevice, s), "copy X to device");
+    cudaError_t e = launch_aos_to_soa(layout_args(c, c->d_X), c->d_aos_x, s);
+    if (e != cudaSuccess) return cuda_fail(e, "aos->state launch");
+    int rc = cipher_rhs(c, t, c->d_X, c->d_F, stream);
+    if (rc) return rc;
+    e = launch_soa_to_aos(layout_args(c, c->d_F), c->d_aos_f, 0, s);
+    if (e != cudaSuccess) return cuda_fail(e, "state->aos launch");
+    CUDA_TRY(cudaMemcpyAsync(F_host, c->d_aos_f, nb, cudaMemcpyDeviceToHost, s), "copy F to host");
+    CUDA_TRY(cudaStreamSynchronize(s), "stream sync");
+    return cipher_ctx_check(c, stream);
+}

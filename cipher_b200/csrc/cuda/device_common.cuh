@@ -1,0 +1,76 @@
+/*
+ * device_common.cuh - device-side tables and helpers shared by the RHS and
+ * PostStep kernels.
+ *
+ * Arithmetic that decides bit-exact outputs (phase sets) or that the FP64
+ * path reproduces bit for bit follows the reference's operation order; the
+ * FP64 translation units are compiled with --fmad=false so no multiply-add is
+ * contracted (the reference's x86-64 build has no FMA either).
+ */
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "cipher_problem.h"
+
+#define CIPHER_PI_D 3.14159265358979323846264338327950288419716939937510582
+#define CIPHER_PMAX 16
+
+namespace cipher {
+
+/* one interface, flattened for the device (INTERFACE, src/typedef.h:235-240) */
+struct DevInterface {
+    double width;
+    double energy_m0, mobility_m0;
+    cipher_tseries energy_act, mobility_act;
+    int has_potential, has_mobilityc;
+    double potential[CIPHER_MAXCP];
+    double mobilityc[CIPHER_MAXCP];
+};
+
+/* error flags raised by kernels (bit mask); never a trap */
+enum : int {
+    ERR_CAP = 1,        /* active-set superset above P */
+    ERR_BADSET = 2,     /* n > P or an id >= npf in the input state */
+    ERR_NONFINITE = 4,
+};
+
+/* exponentiation by squaring, as the reference's FastPow (src/utility.c:112-124) */
+__device__ __forceinline__ double ipow(double b, unsigned e)
+{
+    double r = 1.0;
+    while (e) {
+        if (e & 1u) r *= b;
+        e >>= 1;
+        b *= b;
+    }
+    return r;
+}
+
+/* T-series sum (src/utility.c:48-62) */
+__device__ inline double tseries(double T, const cipher_tseries &s)
+{
+    double r = 0.0;
+    for (int i = 0; i < s.n; i++) {
+        int e = s.exp[i];
+        if (e > 0) r += s.coeff[i] * ipow(T, (unsigned)e);
+        else if (e < 0) r += s.coeff[i] / ipow(T, (unsigned)(-e));
+        else r += s.coeff[i];
+    }
+    if (fabs(s.logcoeff) > 0.0) r += s.logcoeff * T * log(T);
+    return r;
+}
+
+/* pair properties sigma, m, w of an interface at temperature T
+ * (src/cipher.c:422-471 without anisotropy) */
+__device__ inline void interface_props(const DevInterface &itf, double T, double &sig, double &mob, double &wid)
+{
+    sig = 1.0;
+    mob = 1.0;
+    sig *= itf.energy_m0;
+    if (itf.energy_act.n) sig *= exp(tseries(T, itf.energy_act) / CIPHER_R_GAS / T);
+    mob *= itf.mobility_m0;
+    if (itf.mobility_act.n) mob *= exp(tseries(T, itf.mobility_act) / CIPHER_R_GAS / T);
+    wid = itf.width;
+}
+
+}  // namespace cipher

@@ -1,0 +1,197 @@
+/*
+ * poststep.cu - per-step active-set update on uniform grids, the part of
+ * PostStep at src/cipher.c:869-974.
+ *
+ *   k_post_prune : project phi of every cell with n > 1 onto the Gibbs
+ *                  simplex (src/utility.c:578-603), write it back, and store
+ *                  the pruned set {id : phi > TOL} in a scratch plane set;
+ *                  cells with n == 1 get phi = 1.
+ *   k_post_union : superset = own pruned set U pruned sets of the face
+ *                  neighbours (sorted merge, src/utility.c:195-230); keep phi
+ *                  and EX of surviving phases, zero phi and initialise EX of
+ *                  new phases, write the superset.  A superset above P raises
+ *                  the cap flag and leaves that cell's set unchanged.
+ *
+ * The projection and the TOL test run in FP64 for both precisions, so the
+ * phase sets are decided by the same arithmetic as the reference.
+ */
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace cipher {
+
+template <int PM, typename R>
+__global__ void __launch_bounds__(256) k_post_prune(const PostArgs<R> a)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.ncells) return;
+    const int64_t S = a.stride;
+    int n = a.as[c];
+    if (n < 1 || n > a.P) {
+        atomicOr(a.err, ERR_BADSET);
+        a.pruned[c] = 0;
+        return;
+    }
+    if (n == 1) {
+        a.phi[c] = (R)1.0;
+        a.pruned[c] = 1;
+        a.pruned[S + c] = a.as[S + c];
+        return;
+    }
+    double phi[PM], s[PM];
+#pragma unroll
+    for (int g = 0; g < PM; g++)
+        if (g < n) { phi[g] = (double)a.phi[(int64_t)g * S + c]; s[g] = phi[g]; }
+    /* sort a copy in descending order (insertion sort; n <= 16) */
+    for (int i = 1; i < n; i++) {
+        double v = s[i];
+        int j = i - 1;
+        while (j >= 0 && s[j] < v) { s[j + 1] = s[j]; j--; }
+        s[j + 1] = v;
+    }
+    double sum = 0.0, tmax = 0.0;
+    bool found = false;
+    for (int i = 0; i < n - 1; i++) {
+        sum += s[i];
+        tmax = (sum - 1.0) / ((double)(i + 1));
+        if (tmax >= s[i + 1]) { found = true; break; }
+    }
+    if (!found) tmax = (sum + s[n - 1] - 1.0) / ((double)n);
+    int np = 0;
+#pragma unroll
+    for (int g = 0; g < PM; g++) {
+        if (g < n) {
+            double v = phi[g] - tmax > 0.0 ? phi[g] - tmax : 0.0;
+            a.phi[(int64_t)g * S + c] = (R)v;
+            if (v > CIPHER_TOL) {
+                a.pruned[(int64_t)(1 + np) * S + c] = a.as[(int64_t)(1 + g) * S + c];
+                np++;
+            }
+        }
+    }
+    a.pruned[c] = (uint16_t)np;
+}
+
+/* out = a U b (sorted); returns the size, or P+1 if it would exceed P */
+template <int PM>
+__device__ __forceinline__ int merge_union(const uint16_t *sa, int na, const uint16_t *pl, int64_t S, int64_t nb,
+                                           int nbn, uint16_t *out, int P)
+{
+    int i = 0, j = 0, n = 0;
+    uint16_t b = nbn > 0 ? pl[S + nb] : 0;
+    while (i < na || j < nbn) {
+        uint16_t v;
+        if (j >= nbn || (i < na && sa[i] < b)) {
+            v = sa[i++];
+        } else if (i >= na || b < sa[i]) {
+            v = b;
+            j++;
+            if (j < nbn) b = pl[(int64_t)(1 + j) * S + nb];
+        } else {
+            v = sa[i++];
+            j++;
+            if (j < nbn) b = pl[(int64_t)(1 + j) * S + nb];
+        }
+        if (n >= P) return P + 1;
+        out[n++] = v;
+    }
+    return n;
+}
+
+template <int DIM, int PM, typename R>
+__global__ void __launch_bounds__(256) k_post_union(const PostArgs<R> a)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.ncells) return;
+    const int64_t S = a.stride;
+    int n = a.as[c];
+    int ns = a.pruned[c];
+    if (n < 1 || n > a.P || ns < 1 || ns > a.P) return;   /* flagged by k_post_prune */
+    uint16_t sup[PM], tmp[PM];
+    for (int k = 0; k < ns; k++) sup[k] = a.pruned[(int64_t)(1 + k) * S + c];
+
+    const int res[3] = {a.res[0], a.res[1], a.res[2]};
+    const int64_t st[3] = {1, (int64_t)res[0], (int64_t)res[0] * res[1]};
+    int co[3];
+    co[0] = (int)(c % res[0]);
+    co[1] = DIM > 1 ? (int)((c / res[0]) % res[1]) : 0;
+    co[2] = DIM > 2 ? (int)(c / ((int64_t)res[0] * res[1])) : 0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+            int64_t nb;
+            if (side == 0) {
+                if (co[d] > 0) nb = c - st[d];
+                else if (a.per[d] && res[d] > 1) nb = c + (int64_t)(res[d] - 1) * st[d];
+                else continue;
+            } else {
+                if (co[d] < res[d] - 1) nb = c + st[d];
+                else if (a.per[d] && res[d] > 1) nb = c - (int64_t)(res[d] - 1) * st[d];
+                else continue;
+            }
+            if (nb == c) continue;
+            int nbn = a.pruned[nb];
+            if (nbn > a.P) nbn = a.P;
+            int m = merge_union<PM>(sup, ns, a.pruned, S, nb, nbn, tmp, a.P);
+            if (m > a.P) {
+                atomicOr(a.err, ERR_CAP);
+                return;
+            }
+            for (int k = 0; k < m; k++) sup[k] = tmp[k];
+            ns = m;
+        }
+    }
+
+    /* old (unpruned) set of this cell: phi survives for phases in the superset */
+    uint16_t old[PM];
+    for (int k = 0; k < n; k++) old[k] = a.as[(int64_t)(1 + k) * S + c];
+    R phiss[PM];
+    int from[PM];
+    for (int g = 0; g < ns; g++) { phiss[g] = (R)0; from[g] = -1; }
+    {
+        int i = 0, j = 0;
+        while (i < n && j < ns) {
+            if (old[i] == sup[j]) { from[j] = i; i++; j++; }
+            else if (old[i] < sup[j]) i++;
+            else j++;
+        }
+    }
+    for (int g = 0; g < ns; g++)
+        if (from[g] >= 0) phiss[g] = a.phi[(int64_t)from[g] * S + c];
+    /* explicit site potentials: survivors keep theirs, new phases start at
+     * SitepotentialExplicit(c0) (src/cipher.c:953-964) */
+    if (a.S > 0) {
+        double exss[PM * 2 * CIPHER_MAXCP];
+        for (int g = 0; g < ns; g++)
+            for (int q = 0; q < a.S; q++)
+                exss[g * a.S + q] = from[g] >= 0 ? a.ex[(int64_t)(from[g] * a.S + q) * S + c]
+                                                 : a.ex_init[(int64_t)sup[g] * a.S + q];
+        for (int g = 0; g < ns; g++)
+            for (int q = 0; q < a.S; q++) a.ex[(int64_t)(g * a.S + q) * S + c] = exss[g * a.S + q];
+    }
+    for (int g = 0; g < ns; g++) a.phi[(int64_t)g * S + c] = phiss[g];
+    a.as[c] = (uint16_t)ns;
+    for (int g = 0; g < ns; g++) a.as[(int64_t)(1 + g) * S + c] = sup[g];
+}
+
+template <typename R>
+static cudaError_t launch_post(const PostArgs<R> &a, int dim, cudaStream_t s)
+{
+    int64_t blocks = (a.ncells + 255) / 256;
+    dim3 grid((unsigned)blocks), block(256);
+    k_post_prune<CIPHER_PMAX, R><<<grid, block, 0, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (dim == 1) k_post_union<1, CIPHER_PMAX, R><<<grid, block, 0, s>>>(a);
+    else if (dim == 2) k_post_union<2, CIPHER_PMAX, R><<<grid, block, 0, s>>>(a);
+    else k_post_union<3, CIPHER_PMAX, R><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_poststep(const PostArgs<double> &a, int dim, cudaStream_t s) { return launch_post(a, dim, s); }
+cudaError_t launch_poststep(const PostArgs<float> &a, int dim, cudaStream_t s) { return launch_post(a, dim, s); }
+
+}  // namespace cipher

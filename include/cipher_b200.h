@@ -1,0 +1,155 @@
+/*
+ * cipher_b200.h - C ABI of the B200 implementation of CIPHER's time-stepper
+ * right-hand side.
+ *
+ * Plain pointers and sizes only.  Device pointers are CUDA global-memory
+ * addresses on the context's device; `stream` is a cudaStream_t passed as
+ * void* (NULL = legacy default stream).  Every entry point returns 0 on
+ * success or one of the CIPHER_E_* codes; cipher_last_error() gives a
+ * message for the calling thread.
+ *
+ * The two hot entry points replace the reference's PETSc callbacks:
+ *   cipher_rhs      <- RHSFunction(TS, PetscReal, Vec X, Vec F, void *ctx)
+ *                      src/cipher.c:20,27-681, registered at src/cipher.c:1107
+ *   cipher_poststep <- PostStep(TS), active-set part src/cipher.c:869-974,
+ *                      registered at src/cipher.c:1108
+ */
+#ifndef CIPHER_B200_H
+#define CIPHER_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+#include "cipher_problem.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* error codes                                                         */
+/* ------------------------------------------------------------------ */
+#define CIPHER_OK             0
+#define CIPHER_E_ARG          1   /* invalid argument */
+#define CIPHER_E_NOMEM        2   /* host or device allocation failed */
+#define CIPHER_E_CAP          3   /* active-set superset above the cap; the
+                                     reference asserts (src/cipher.c:968) */
+#define CIPHER_E_NONFINITE    4   /* NaN/Inf in a state or error norm */
+#define CIPHER_E_CUDA         5   /* CUDA runtime error */
+#define CIPHER_E_TIMEOUT      6   /* a bounded device wait ran out */
+#define CIPHER_E_UNSUPPORTED  7   /* configuration not implemented on device */
+#define CIPHER_E_STEP         8   /* time step fell below the minimum */
+
+const char *cipher_strerror(int code);
+const char *cipher_last_error(void);
+
+/* sizeof of the public structs, for binding generators to check their
+ * mirrors: out[0..8] = tseries, rk, mobility, source, material, interface,
+ * bc, problem, mesh; returns how many were written (at most n) */
+int cipher_abi_sizes(int64_t *out, int n);
+
+/* ------------------------------------------------------------------ */
+/* host: problem description, meshes, initial state                    */
+/* (the reference builds these in SetUpConfig/main/SetUpProblem,        */
+/*  src/init.c:104-1716, src/cipher.c:1148-1231, src/init.c:1721-1830)  */
+/* ------------------------------------------------------------------ */
+
+/* allocate a problem with default parameters (src/init.c:1260-1327 defaults) */
+cipher_problem *cipher_problem_new(int dim, int npf, int ncp, int nmat, int nf);
+void cipher_problem_free(cipher_problem *p);
+/* derive nsites, stoichiometry, maxsites after the tables are filled */
+int cipher_problem_finalize(cipher_problem *p);
+/* P = min(max_phase_neighbours, npf)  (src/init.c:1326-1343) */
+int cipher_problem_set_cap(cipher_problem *p, int max_phase_neighbours);
+cipher_aos_layout cipher_problem_aos_layout(const cipher_problem *p);
+
+/* seeded grain-growth problem: periodic box of res[] cells, ngrains Voronoi
+ * grains (splitmix64 seed), one material with chemicalenergy none, one
+ * interface of the given energy, mobility and width */
+int cipher_problem_grain_growth(int dim, const int32_t *res, int ngrains, int cap, uint64_t seed,
+                                double energy, double mobility, double width,
+                                double molarvolume, double temperature0,
+                                cipher_problem **out);
+/* nearest-centre Voronoi map under the periodic metric, x fastest; the
+ * seeded centres are returned in centres[ngrains*3] when it is not NULL */
+int cipher_voronoi(int dim, const int32_t *res, int ngrains, uint64_t seed, int32_t *voxel, double *centres);
+double cipher_rand_uniform(uint64_t *state);
+
+/* uniform leaf mesh; owned planes [slab_lo, slab_hi) of the slowest axis
+ * plus a one-cell halo (pass 0, res[dim-1] for the whole domain) */
+int cipher_mesh_uniform(const cipher_problem *p, int slab_lo, int slab_hi, cipher_mesh **out);
+void cipher_mesh_free(cipher_mesh *m);
+
+/* SetUpProblem active sets / phi / T in the reference AoS layout (host) */
+int cipher_initial_state_aos(const cipher_problem *p, const cipher_mesh *m, double *X);
+
+/* a diffuse-interface state of a Voronoi problem (host): every grain j whose
+ * bisector with the cell's nearest grain i is closer than width/2 gets
+ * weight f/(1-f), f = (1 - sin(pi d/width))/2, the owner weight 1, phi the
+ * normalised weights; active sets are then united with the face neighbours'
+ * as the per-step update does.  Returns CIPHER_E_CAP if a set exceeds P. */
+int cipher_initial_state_diffuse_aos(const cipher_problem *p, const cipher_mesh *m, double width, double *X);
+
+/* ------------------------------------------------------------------ */
+/* device context                                                      */
+/* ------------------------------------------------------------------ */
+
+typedef struct cipher_ctx cipher_ctx;
+
+enum { CIPHER_PREC_FP64 = 0,    /* plain FP64 drop-in */
+       CIPHER_PREC_MIXED = 1 }; /* FP32 phi/T storage and stencil, FP64 chemistry */
+
+/*
+ * Device state layout (structure of arrays, plane-major, one plane per slot):
+ *   AS  uint16 [P+1][stride]   plane 0 = active count n, planes 1..P = sorted ids
+ *   PF  real   [P][stride]     phase fractions of the active phases
+ *   DP  double [D][stride]     diffusion potentials mu
+ *   EX  double [P*S][stride]   explicit site potentials, slot g*S+s*D+c
+ *   TM  real   [stride]        temperature
+ * real = double (FP64) or float (MIXED).  Offsets are bytes from the state
+ * base pointer; every plane starts on a 256-byte boundary.  The RHS vector F
+ * uses the same layout; its AS region is not written (the reference's F is
+ * identically zero there).
+ */
+typedef struct cipher_state_layout {
+    int64_t ncells;      /* owned cells */
+    int64_t stride;      /* elements per plane (ncells rounded up) */
+    int32_t pf_size, dp_size, ex_size, precision;
+    int64_t as_offset, pf_offset, dp_offset, ex_offset, tm_offset;
+    int64_t bytes;       /* total bytes of one state vector */
+} cipher_state_layout;
+
+/* create a context on `device` for problem p over mesh m (owned cells only;
+ * ghosts are not used on one GPU) */
+int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, int precision, int device,
+                      cipher_ctx **out);
+void cipher_ctx_destroy(cipher_ctx *c);
+int cipher_ctx_layout(const cipher_ctx *c, cipher_state_layout *out);
+
+/* F = RHS(t, X) over all owned cells; X and F are device state vectors */
+int cipher_rhs(cipher_ctx *c, double t, const void *X, void *F, void *stream);
+
+/* per-step active-set update of X in place: Gibbs-simplex projection, prune
+ * phi <= TOL, union with the face neighbours' pruned sets, reorder PF/EX.
+ * Synchronises `stream`; returns CIPHER_E_CAP if a superset exceeds P. */
+int cipher_poststep(cipher_ctx *c, void *X, void *stream);
+
+/* synchronise `stream`, then read and clear the error flags the kernels
+ * raise instead of trapping (bad active counts, cap overflow) */
+int cipher_ctx_check(cipher_ctx *c, void *stream);
+
+/* Y = X + a*F on the PF, DP, EX and TM planes; AS is copied from X
+ * (VecWAXPY on the solution vector).  Y may alias X. */
+int cipher_waxpy(cipher_ctx *c, void *Y, const void *X, double a, const void *F, void *stream);
+
+/* reference AoS layout (ncells x ndof doubles, device) <-> device state */
+int cipher_state_from_aos(cipher_ctx *c, const double *aos, void *X, void *stream);
+int cipher_state_to_aos(cipher_ctx *c, const void *X, double *aos, void *stream);
+
+/* drop-in call with HOST buffers in the reference AoS layout: copies X to the
+ * device, evaluates the RHS and copies F back (synchronous on `stream`) */
+int cipher_rhs_aos_host(cipher_ctx *c, double t, const double *X_host, double *F_host, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CIPHER_B200_H */

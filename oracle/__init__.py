@@ -1,0 +1,168 @@
+"""CPU oracles for CIPHER's RHS and per-step active-set update.
+
+TEST INFRASTRUCTURE ONLY.  Imported by tests/, ``__graft_entry__.smoke()``
+and the CPU-baseline leg of ``bench.py``; the product never imports it.
+
+Two oracles:
+
+* ``port``: this project's C restatement (oracle/port/*.c), built into
+  ``oracle/liboracle_port.so``.
+* ``ref``: the reference's own src/{typedef,utility,material,cipher}.c compiled
+  unmodified against the PETSc shim (oracle/shim) into
+  ``oracle/_ref/libcipher_ref.so``; built where the reference sources exist
+  and shipped as a prebuilt library elsewhere.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "liboracle_port.so")
+REF_LIB = os.path.join(HERE, "_ref", "libcipher_ref.so")
+REF_SRC = "/root/reference/src"
+
+_port = None
+_ref = None
+
+
+def build(ref: bool = True) -> None:
+    """Compile the port (and the reference build when its sources exist)."""
+    targets = ["port"]
+    if ref and os.path.isdir(REF_SRC):
+        targets.append("ref")
+    r = subprocess.run(["make", "-s", "-C", HERE] + targets, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def port():
+    global _port
+    if _port is None:
+        if not os.path.exists(PORT_LIB):
+            build(ref=False)
+        lib = C.CDLL(PORT_LIB)
+        lib.oracle_rhs.restype = C.c_int
+        lib.oracle_rhs.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.oracle_poststep.restype = C.c_int
+        lib.oracle_poststep.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]
+        lib.oracle_initial_state.restype = C.c_int
+        lib.oracle_initial_state.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]
+        lib.or_simplex_projection.restype = None
+        lib.or_simplex_projection.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int]
+        _port = lib
+    return _port
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_LIB):
+            raise FileNotFoundError(f"{REF_LIB} not built (needs the reference sources)")
+        lib = C.CDLL(REF_LIB)
+        lib.ref_create.restype = C.c_int
+        lib.ref_create.argtypes = [C.c_void_p, C.c_void_p]
+        lib.ref_destroy.restype = None
+        lib.ref_destroy.argtypes = []
+        lib.ref_ndof.restype = C.c_int
+        lib.ref_rhs.restype = C.c_int
+        lib.ref_rhs.argtypes = [C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.ref_poststep.restype = C.c_int
+        lib.ref_poststep.argtypes = [C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_double), C.c_int,
+                                     C.POINTER(C.c_double)]
+        _ref = lib
+    return _ref
+
+
+def _addr(obj) -> C.c_void_p:
+    """ctypes pointer of a cipher_b200 Problem/Mesh (or a raw pointer)."""
+    p = getattr(obj, "ptr", obj)
+    return C.cast(p, C.c_void_p)
+
+
+# ---------------------------------------------------------------- port ----
+
+def port_rhs(problem, mesh, X: np.ndarray, t: float = 0.0) -> np.ndarray:
+    """F over owned cells; X holds owned then ghost cells (AoS doubles)."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    F = np.zeros((mesh.nowned, X.shape[1]), dtype=np.float64)
+    rc = port().oracle_rhs(_addr(problem), _addr(mesh), t, _dp(X), _dp(F))
+    if rc:
+        raise RuntimeError(f"oracle_rhs failed ({rc})")
+    return F
+
+
+def port_poststep(problem, mesh, X: np.ndarray) -> int:
+    """Active-set update in place; returns 0, or 3 when a superset exceeds P."""
+    assert X.flags.c_contiguous and X.dtype == np.float64
+    return port().oracle_poststep(_addr(problem), _addr(mesh), _dp(X))
+
+
+def port_initial_state(problem, mesh) -> np.ndarray:
+    X = np.zeros((mesh.ncells, problem.ndof), dtype=np.float64)
+    rc = port().oracle_initial_state(_addr(problem), _addr(mesh), _dp(X))
+    if rc:
+        raise RuntimeError(f"oracle_initial_state failed ({rc})")
+    return X
+
+
+def simplex_projection(v: np.ndarray) -> np.ndarray:
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    out = np.zeros_like(v)
+    port().or_simplex_projection(_dp(out), _dp(v), len(v))
+    return out
+
+
+# ----------------------------------------------------------------- ref ----
+
+class RefOracle:
+    """The reference's RHSFunction/PostStep on one problem (one at a time)."""
+
+    def __init__(self, problem, mesh):
+        self.lib = ref()
+        rc = self.lib.ref_create(_addr(problem), _addr(mesh))
+        if rc:
+            raise RuntimeError(f"ref_create failed ({rc})")
+        self.problem, self.mesh = problem, mesh
+        self.ndof = self.lib.ref_ndof()
+
+    def rhs(self, X: np.ndarray, t: float = 0.0, with_time: bool = False):
+        """X: owned then ghost cells (AoS); returns F over owned cells."""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        nown = self.mesh.nowned
+        own = np.ascontiguousarray(X[:nown])
+        ghost = np.ascontiguousarray(X[nown:]) if X.shape[0] > nown else np.zeros((1, self.ndof))
+        F = np.zeros_like(own)
+        sec = C.c_double(0.0)
+        rc = self.lib.ref_rhs(t, _dp(own), _dp(ghost), _dp(F), C.byref(sec))
+        if rc:
+            raise RuntimeError(f"reference RHSFunction failed ({rc})")
+        return (F, sec.value) if with_time else F
+
+    def poststep(self, X: np.ndarray, t: float = 0.0, dt: float = 0.0, step: int = 1) -> int:
+        assert X.flags.c_contiguous and X.dtype == np.float64
+        d = C.c_double(dt)
+        return self.lib.ref_poststep(_dp(X), t, C.byref(d), step, None)
+
+    def close(self):
+        if self.lib is not None:
+            self.lib.ref_destroy()
+            self.lib = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
