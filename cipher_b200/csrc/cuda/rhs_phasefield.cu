@@ -86,13 +86,21 @@ __global__ void __launch_bounds__(256) k_rhs_phasefield(const PfArgs<R> a)
         return;
     }
     CellSets<PM, R> cs;
+    bool badid = false;
 #pragma unroll
     for (int g = 0; g < PM; g++) {
         if (g < n) {
             cs.ids[g] = a.as[(int64_t)(1 + g) * S + c];
             cs.phi[g] = a.phi[(int64_t)g * S + c];
             cs.lap[g] = (R)0;
+            badid |= cs.ids[g] >= a.npf;
         }
+    }
+    if (badid) {   /* ids index the interface table: never read past it */
+        atomicOr(a.err, ERR_BADSET);
+        for (int g = 0; g < a.P; g++) a.fphi[(int64_t)g * S + c] = (R)0;
+        a.ftm[c] = (R)0;
+        return;
     }
 
     /* neighbours in the reference's face order */
