@@ -296,6 +296,15 @@ static PfArgs<R> pf_args(const cipher_ctx *c, const void *X, void *F)
     a.npf = c->npf;
     a.ffactor = c->ffactor;
     a.vol = c->vol;
+    {
+        int ex;
+        double mant = frexp(c->vol, &ex);
+        if (c->ffactor == 1.0 && c->vol == 1.0) a.geom_mode = 2;        /* GEOM_UNIT */
+        else if (mant == 0.5) a.geom_mode = 1;                          /* GEOM_RECIP */
+        else a.geom_mode = 0;                                           /* GEOM_DIVIDE */
+        a.inv_vol = 1.0 / c->vol;
+        a.face_coef = c->ffactor / c->vol;
+    }
     a.junctionpenalty = c->junctionpenalty;
     a.has_temp_rate = c->has_temp_rate;
     a.temp_rate = c->temp_rate;

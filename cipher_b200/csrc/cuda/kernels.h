@@ -17,6 +17,9 @@ struct PfArgs {
     int per[3];
     int P, npf;
     double ffactor, vol;          /* face factor and cell volume (src/cipher.c:273-275) */
+    int geom_mode;                /* GEOM_DIVIDE / GEOM_RECIP / GEOM_UNIT (pf_gather.cuh) */
+    double inv_vol;               /* 1/vol, exact when vol is a power of two */
+    double face_coef;             /* ffactor/vol, for the mixed path */
     double junctionpenalty;
     int has_temp_rate;
     double temp_rate;

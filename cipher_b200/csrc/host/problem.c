@@ -331,7 +331,8 @@ int cipher_mesh_uniform(const cipher_problem *p, int slab_lo, int slab_hi, ciphe
     if (!m) return CIPHER_E_NOMEM;
     m->dim = dim;
     m->uniform = 1;
-    for (int d = 0; d < 3; d++) { m->res[d] = r[d]; m->periodic[d] = d < dim ? p->periodic[d] : 0; }
+    /* a periodic direction one cell wide would make a cell its own neighbour */
+    for (int d = 0; d < 3; d++) { m->res[d] = r[d]; m->periodic[d] = d < dim ? (p->periodic[d] && r[d] > 1) : 0; }
     m->slab_lo = slab_lo;
     m->slab_hi = slab_hi;
 

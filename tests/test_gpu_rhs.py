@@ -81,7 +81,7 @@ def test_poststep_fp64_bit_exact(case):
 def test_trajectory_fp64_bit_exact():
     """20 forward-Euler steps (device AXPY + RHS + PostStep) stay bit-identical
     to the oracle driven the same way."""
-    P, M, X = _build(3, [14, 12, 10], 25, 12, 17, "sharp")
+    P, M, X = _build(3, [20, 18, 16], 12, 12, 17, "sharp")
     ctx = cb.Context(P, M, "fp64")
     dX, dF = ctx.alloc_state(), ctx.alloc_state()
     ctx.from_aos(X, dX)
@@ -90,10 +90,16 @@ def test_trajectory_fp64_bit_exact():
     for step in range(20):
         ctx.rhs(0.0, dX, dF)
         ctx.waxpy(dX, dX, dt, dF)
-        ctx.poststep(dX)
         Fo = oracle.port_rhs(P, M, Xo)
         Xo = Xo + dt * Fo
-        assert oracle.port_poststep(P, M, Xo) == 0
+        rc = oracle.port_poststep(P, M, Xo)
+        if rc:
+            # a cap overflow must be reported by the device at the same step
+            with pytest.raises(cb.CipherError) as e:
+                ctx.poststep(dX)
+            assert e.value.code == 3 and rc == 3
+            return
+        ctx.poststep(dX)
     Xd = ctx.to_aos(dX)
     n = Xo[:, 0].astype(int)
     assert np.array_equal(Xd[:, 0], Xo[:, 0])
