@@ -143,6 +143,9 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
     if (!m->uniform || m->ncells != m->nowned)
         return set_error(CIPHER_E_UNSUPPORTED, "device path needs a whole-domain uniform mesh");
     if (p->pf_size < 1 || p->pf_size > CIPHER_MAXAP) return set_error(CIPHER_E_ARG, "bad phase cap %d", p->pf_size);
+    /* kernels launch one block row per (y, z) grid line */
+    if ((p->dim > 1 && m->res[1] > 65535) || (p->dim > 2 && m->res[2] > 65535))
+        return set_error(CIPHER_E_UNSUPPORTED, "grid lines above 65535 in y or z");
     char why[256];
     if (!problem_supported(p, why, sizeof(why))) return set_error(CIPHER_E_UNSUPPORTED, "%s", why);
     /* the linear interpolant is not used by the phase-field-only kernel (no chemistry) */

@@ -5,10 +5,13 @@
  * The reference scatters each face's flux into both cells (src/cipher.c:
  * 235-317); here every cell gathers the contributions of its own faces, in
  * the order the reference's face loop reaches them, so each slot receives
- * the same additions in the same order.  Slot arrays stay in registers: the
- * own set is held in fixed-size arrays indexed only by unrolled constants,
- * and a neighbour's phase is matched against all own slots by comparison
- * instead of a merge with data-dependent indices.
+ * the same additions in the same order.  The cell's slots live in shared
+ * memory, one column per thread (SlotColumns), and a face is matched by a
+ * two-pointer merge of the two sorted sets, as SetIntersection does
+ * (src/utility.c:168-190).
+ *
+ * Launch geometry: grid (ceil(res0/block), res1, res2), one thread per cell
+ * of an x-row, so cell coordinates need no integer division.
  */
 #pragma once
 #include <cstdint>
@@ -24,14 +27,48 @@ enum GeomMode : int {
     GEOM_UNIT = 2,      /* ff == 1 and vol == 1: flux itself, exact */
 };
 
-template <int PM, typename R>
-struct CellPF {
-    uint16_t ids[PM];
-    R phi[PM];
-    R lap[PM];
-    int n;
-    uint16_t maxid;
+/* a thread's slot columns in shared memory: element g at base[g*st] */
+template <typename R>
+struct SlotColumns {
+    R *phi, *aj, *lap, *cap;
+    uint16_t *ids;
+    uint8_t *nz;                 /* slots with phi != 0, ascending */
+    int st;
+    __device__ __forceinline__ R &PHI(int g) const { return phi[g * st]; }
+    __device__ __forceinline__ R &AJ(int g) const { return aj[g * st]; }
+    __device__ __forceinline__ R &LAP(int g) const { return lap[g * st]; }
+    __device__ __forceinline__ R &CAP(int g) const { return cap[g * st]; }
+    __device__ __forceinline__ uint16_t &ID(int g) const { return ids[g * st]; }
+    __device__ __forceinline__ uint8_t &NZ(int g) const { return nz[g * st]; }
 };
+
+/* carve the columns of thread `tid` out of a block's dynamic shared memory;
+ * layout: R phi,aj,lap,cap [PM][bd] | uint16 ids [PM][bd] | uint8 nz [PM][bd] */
+template <typename R>
+__device__ __forceinline__ SlotColumns<R> slot_columns(unsigned char *smem, int PM, int bd, int tid, bool with_aj_cap)
+{
+    SlotColumns<R> sc;
+    R *base = (R *)smem;
+    int k = 0;
+    sc.st = bd;
+    sc.phi = base + (size_t)(k++) * PM * bd + tid;
+    sc.lap = base + (size_t)(k++) * PM * bd + tid;
+    if (with_aj_cap) {
+        sc.aj = base + (size_t)(k++) * PM * bd + tid;
+        sc.cap = base + (size_t)(k++) * PM * bd + tid;
+    } else {
+        sc.aj = sc.cap = nullptr;
+    }
+    uint16_t *ib = (uint16_t *)(base + (size_t)k * PM * bd);
+    sc.ids = ib + tid;
+    sc.nz = (uint8_t *)(ib + (size_t)PM * bd) + tid;
+    return sc;
+}
+
+__host__ __device__ constexpr size_t slot_columns_bytes(int PM, int bd, int rbytes, bool with_aj_cap)
+{
+    return (size_t)PM * bd * ((with_aj_cap ? 4 : 2) * rbytes + 2 + 1) + 16;
+}
 
 template <typename R, bool EXACT>
 __device__ __forceinline__ R face_term(const PfArgs<R> &a, R flux)
@@ -46,94 +83,116 @@ __device__ __forceinline__ R face_term(const PfArgs<R> &a, R flux)
 }
 
 /* contributions of the face shared with neighbour nb (src/cipher.c:277-288) */
-template <int PM, typename R, bool EXACT>
-__device__ __forceinline__ void gather_face(const PfArgs<R> &a, CellPF<PM, R> &cp, int64_t nb, bool cell_is_L)
+template <typename R, bool EXACT>
+__device__ __forceinline__ void gather_face(const PfArgs<R> &a, const SlotColumns<R> &sc, int n, int64_t nb,
+                                            bool cell_is_L)
 {
     const int64_t S = a.stride;
     int nn = a.as[nb];
     if (nn > a.P) nn = a.P;                 /* that cell's own thread raises the flag */
-    if (nn < 1 || cp.n < 1) return;
-    uint16_t b0 = a.as[S + nb];
+    if (nn < 1) return;
+    uint16_t b = a.as[S + nb];
+    uint16_t v = sc.ID(0);
     /* the phase flux is gated on the L cell only (src/cipher.c:277) */
-    bool gate = cell_is_L ? (cp.n > 1 || cp.ids[0] > 1) : (nn > 1 || b0 > 1);
+    bool gate = cell_is_L ? (n > 1 || v > 1) : (nn > 1 || b > 1);
     if (!gate) return;
-    for (int j = 0; j < nn; j++) {
-        uint16_t nid = j == 0 ? b0 : a.as[(int64_t)(1 + j) * S + nb];
-        if (nid > cp.maxid) break;          /* both sets are sorted */
-        int mi = -1;
-#pragma unroll
-        for (int i = 0; i < PM; i++)
-            if (i < cp.n && cp.ids[i] == nid) mi = i;
-        if (mi < 0) continue;
-        R pn = a.phi[(int64_t)j * S + nb];
-#pragma unroll
-        for (int i = 0; i < PM; i++) {
-            if (i == mi) {
-                if (cell_is_L) cp.lap[i] += face_term<R, EXACT>(a, pn - cp.phi[i]);
-                else cp.lap[i] -= face_term<R, EXACT>(a, cp.phi[i] - pn);
-            }
+    int i = 0, j = 0;
+    while (true) {
+        if (v == b) {
+            R pn = a.phi[(int64_t)j * S + nb];
+            if (cell_is_L) sc.LAP(i) += face_term<R, EXACT>(a, pn - sc.PHI(i));
+            else sc.LAP(i) -= face_term<R, EXACT>(a, sc.PHI(i) - pn);
+            if (++i >= n || ++j >= nn) break;
+            v = sc.ID(i);
+            b = a.as[(int64_t)(1 + j) * S + nb];
+        } else if (v < b) {
+            if (++i >= n) break;
+            v = sc.ID(i);
+        } else {
+            if (++j >= nn) break;
+            b = a.as[(int64_t)(1 + j) * S + nb];
         }
     }
 }
 
-/* load the cell's set and phase fractions, then gather its faces in the
- * reference's face order (non-wrapped faces from below in descending
- * direction, own faces in ascending direction, wrapped faces from above in
- * ascending direction).  Returns false for an invalid cell (flag raised). */
-template <int DIM, int PM, typename R, bool EXACT>
-__device__ __forceinline__ bool load_and_gather(const PfArgs<R> &a, int64_t c, bool live, CellPF<PM, R> &cp)
+/* cell index and coordinates of this thread */
+struct CellIndex {
+    int64_t c;
+    int x, y, z;
+    bool live;
+};
+
+__device__ __forceinline__ CellIndex cell_index(const int *res)
 {
-    const int64_t S = a.stride;
-    int n = live ? (int)a.as[c] : 0;
+    CellIndex ci;
+    ci.x = blockIdx.x * blockDim.x + threadIdx.x;
+    ci.y = blockIdx.y;
+    ci.z = blockIdx.z;
+    ci.live = ci.x < res[0];
+    ci.c = (int64_t)ci.x + (int64_t)res[0] * ((int64_t)ci.y + (int64_t)res[1] * ci.z);
+    return ci;
+}
+
+/* load the cell's set and phase fractions into its columns, then gather its
+ * faces in the reference's face order (non-wrapped faces from below in
+ * descending direction, own faces in ascending direction, wrapped faces
+ * from above in ascending direction).  Returns the active count (0 for a
+ * dead or invalid cell; an invalid one raises ERR_BADSET). */
+template <int DIM, typename R, bool EXACT>
+__device__ __forceinline__ int load_and_gather(const PfArgs<R> &a, const CellIndex &ci, const SlotColumns<R> &sc)
+{
+    const int64_t S = a.stride, c = ci.c;
+    int n = ci.live ? (int)a.as[c] : 0;
     bool ok = true;
-    if (live && (n < 1 || n > a.P)) { ok = false; n = 0; }
-    uint16_t maxid = 0;
-#pragma unroll
-    for (int g = 0; g < PM; g++) {
-        if (g < n) {
-            cp.ids[g] = a.as[(int64_t)(1 + g) * S + c];
-            cp.phi[g] = a.phi[(int64_t)g * S + c];
-            if (cp.ids[g] >= a.npf) ok = false;
-            maxid = cp.ids[g];
-        } else {
-            cp.ids[g] = 0xFFFF;
-            cp.phi[g] = (R)0;
-        }
-        cp.lap[g] = (R)0;
+    if (ci.live && (n < 1 || n > a.P)) { ok = false; n = 0; }
+    int nz = 0;
+    for (int g = 0; g < n; g++) {
+        uint16_t id = a.as[(int64_t)(1 + g) * S + c];
+        R p = a.phi[(int64_t)g * S + c];
+        sc.ID(g) = id;
+        sc.PHI(g) = p;
+        sc.LAP(g) = (R)0;
+        if (p != (R)0) sc.NZ(nz++) = (uint8_t)g;
+        if (id >= a.npf) ok = false;
     }
     if (!ok) {
         atomicOr(a.err, ERR_BADSET);
-        n = 0;
+        return 0;
     }
-    cp.n = n;
-    cp.maxid = maxid;
-    if (n == 0) return ok;
-
+    if (n == 0) return 0;
+    (void)nz;
     const int res0 = a.res[0], res1 = a.res[1], res2 = a.res[2];
     const int64_t st1 = res0, st2 = (int64_t)res0 * res1;
-    int co0 = (int)(c % res0);
-    int co1 = DIM > 1 ? (int)((c / res0) % res1) : 0;
-    int co2 = DIM > 2 ? (int)(c / st2) : 0;
+    const int co0 = ci.x, co1 = ci.y, co2 = ci.z;
     /* faces whose L cell lies below without wrapping, descending direction */
-    if (DIM > 2 && co2 > 0) gather_face<PM, R, EXACT>(a, cp, c - st2, false);
-    if (DIM > 1 && co1 > 0) gather_face<PM, R, EXACT>(a, cp, c - st1, false);
-    if (co0 > 0) gather_face<PM, R, EXACT>(a, cp, c - 1, false);
+    if (DIM > 2 && co2 > 0) gather_face<R, EXACT>(a, sc, n, c - st2, false);
+    if (DIM > 1 && co1 > 0) gather_face<R, EXACT>(a, sc, n, c - st1, false);
+    if (co0 > 0) gather_face<R, EXACT>(a, sc, n, c - 1, false);
     /* own faces, ascending direction */
-    if (co0 < res0 - 1) gather_face<PM, R, EXACT>(a, cp, c + 1, true);
-    else if (a.per[0]) gather_face<PM, R, EXACT>(a, cp, c - (res0 - 1), true);
+    if (co0 < res0 - 1) gather_face<R, EXACT>(a, sc, n, c + 1, true);
+    else if (a.per[0]) gather_face<R, EXACT>(a, sc, n, c - (res0 - 1), true);
     if (DIM > 1) {
-        if (co1 < res1 - 1) gather_face<PM, R, EXACT>(a, cp, c + st1, true);
-        else if (a.per[1]) gather_face<PM, R, EXACT>(a, cp, c - (int64_t)(res1 - 1) * st1, true);
+        if (co1 < res1 - 1) gather_face<R, EXACT>(a, sc, n, c + st1, true);
+        else if (a.per[1]) gather_face<R, EXACT>(a, sc, n, c - (int64_t)(res1 - 1) * st1, true);
     }
     if (DIM > 2) {
-        if (co2 < res2 - 1) gather_face<PM, R, EXACT>(a, cp, c + st2, true);
-        else if (a.per[2]) gather_face<PM, R, EXACT>(a, cp, c - (int64_t)(res2 - 1) * st2, true);
+        if (co2 < res2 - 1) gather_face<R, EXACT>(a, sc, n, c + st2, true);
+        else if (a.per[2]) gather_face<R, EXACT>(a, sc, n, c - (int64_t)(res2 - 1) * st2, true);
     }
     /* faces whose L cell wraps around from above, ascending direction */
-    if (co0 == 0 && a.per[0]) gather_face<PM, R, EXACT>(a, cp, c + (res0 - 1), false);
-    if (DIM > 1 && co1 == 0 && a.per[1]) gather_face<PM, R, EXACT>(a, cp, c + (int64_t)(res1 - 1) * st1, false);
-    if (DIM > 2 && co2 == 0 && a.per[2]) gather_face<PM, R, EXACT>(a, cp, c + (int64_t)(res2 - 1) * st2, false);
-    return ok;
+    if (co0 == 0 && a.per[0]) gather_face<R, EXACT>(a, sc, n, c + (res0 - 1), false);
+    if (DIM > 1 && co1 == 0 && a.per[1]) gather_face<R, EXACT>(a, sc, n, c + (int64_t)(res1 - 1) * st1, false);
+    if (DIM > 2 && co2 == 0 && a.per[2]) gather_face<R, EXACT>(a, sc, n, c + (int64_t)(res2 - 1) * st2, false);
+    return n;
+}
+
+/* number of phi != 0 slots recorded by load_and_gather */
+template <typename R>
+__device__ __forceinline__ int count_nonzero(const SlotColumns<R> &sc, int n)
+{
+    int nz = 0;
+    for (int g = 0; g < n; g++) nz += sc.PHI(g) != (R)0;
+    return nz;
 }
 
 }  // namespace cipher

@@ -26,123 +26,92 @@ namespace cipher {
 
 constexpr int kMixedBlock = 128;
 
-template <int DIM, int PM>
+template <int DIM>
 __global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_single(const PfArgs<float> a)
 {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = c < a.ncells;
-    const int64_t S = a.stride;
-    CellPF<PM, float> cp;
-    load_and_gather<DIM, PM, float, false>(a, c, live, cp);
-    const int n = cp.n;
-    float pf[PM];
-#pragma unroll
-    for (int g = 0; g < PM; g++) pf[g] = 0.0f;
-
+    extern __shared__ __align__(16) unsigned char smem[];
+    const CellIndex ci = cell_index(a.res);
+    const SlotColumns<float> sc = slot_columns<float>(smem, a.P, blockDim.x, threadIdx.x, false);
+    const int n = load_and_gather<DIM, float, false>(a, ci, sc);
+    if (!ci.live) return;
+    const int64_t S = a.stride, c = ci.c;
+    uint32_t act = 0;
+    double nact = 0.0, Ca = 0.0;
+    const double mob = a.mob0;
     if (n > 1) {
         const float sig = (float)a.sig0, inv_w = (float)(1.0 / a.wid0);
         const float w_pi2 = (float)(a.wid0 / (CIPHER_PI_D * CIPHER_PI_D));
         const float tjh = (float)(0.5 * a.tj0);
-        const double mob = a.mob0;
         float A = 0.0f, S1 = 0.0f, S2 = 0.0f;
-#pragma unroll
-        for (int k = 0; k < PM; k++)
-            if (k < n) {
-                A += cp.phi[k] * inv_w + cp.lap[k] * w_pi2;
-                S1 += cp.phi[k];
-                S2 += cp.phi[k] * cp.phi[k];
-            }
-        float cap[PM];
+        for (int k = 0; k < n; k++) {
+            const float p = sc.PHI(k);
+            A += p * inv_w + sc.LAP(k) * w_pi2;
+            S1 += p;
+            S2 += p * p;
+        }
+        /* capillary force, stored over the consumed Laplacian */
         double C = 0.0;
-#pragma unroll
-        for (int k = 0; k < PM; k++) {
-            if (k < n) {
-                float ak = cp.phi[k] * inv_w + cp.lap[k] * w_pi2;
-                float o1 = S1 - cp.phi[k];
-                float o2 = S2 - cp.phi[k] * cp.phi[k];
-                cap[k] = 8.0f * (-sig * (A - ak) - tjh * (o1 * o1 - o2)) + cp.lap[k];
-                C += (double)cap[k];
-            } else {
-                cap[k] = 0.0f;
-            }
+        for (int k = 0; k < n; k++) {
+            const float p = sc.PHI(k), l = sc.LAP(k);
+            const float ak = p * inv_w + l * w_pi2;
+            const float o1 = S1 - p, o2 = S2 - p * p;
+            const float cap = 8.0f * (-sig * (A - ak) - tjh * (o1 * o1 - o2)) + l;
+            sc.LAP(k) = cap;
+            C += (double)cap;
         }
-        uint32_t act = 0;
-        double nact = 0.0, Ca = 0.0;
-#pragma unroll
-        for (int k = 0; k < PM; k++) {
-            if (k < n) {
-                double u = mob * ((double)n * (double)cap[k] - C);
-                double p = (double)cp.phi[k];
-                bool on = (p > CIPHER_TOL && p < 1.0 - CIPHER_TOL) || (p < CIPHER_TOL && u > 0.0) ||
-                          (p > 1.0 - CIPHER_TOL && u < 0.0);
-                if (on) { act |= 1u << k; nact += 1.0; Ca += (double)cap[k]; }
-            }
+        for (int k = 0; k < n; k++) {
+            const double cap = (double)sc.LAP(k);
+            const double u = mob * ((double)n * cap - C);
+            const double p = (double)sc.PHI(k);
+            const bool on = (p > CIPHER_TOL && p < 1.0 - CIPHER_TOL) || (p < CIPHER_TOL && u > 0.0) ||
+                            (p > 1.0 - CIPHER_TOL && u < 0.0);
+            if (on) { act |= 1u << k; nact += 1.0; Ca += cap; }
         }
-#pragma unroll
-        for (int k = 0; k < PM; k++)
-            if (k < n && (act >> k & 1u)) pf[k] = (float)(mob * (nact * (double)cap[k] - Ca) / nact);
     }
-    if (!live) return;
-#pragma unroll
-    for (int g = 0; g < PM; g++)
-        if (g < a.P) a.fphi[(int64_t)g * S + c] = pf[g];
+    for (int m = 0; m < a.P; m++) {
+        float v = 0.0f;
+        if (m < n && (act >> m & 1u)) v = (float)(mob * (nact * (double)sc.LAP(m) - Ca) / nact);
+        a.fphi[(int64_t)m * S + c] = v;
+    }
     double tr = 0.0;
     if (a.has_temp_rate) tr += a.temp_rate;
     a.ftm[c] = (float)tr;
-}
-
-template <int DIM, int PM>
-__global__ void __launch_bounds__(64) k_rhs_pf_mixed_multi(const PfArgs<float> a)
-{
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = c < a.ncells;
-    CellPF<PM, float> cp;
-    load_and_gather<DIM, PM, float, false>(a, c, live, cp);
-    const int bd = blockDim.x, tid = threadIdx.x;
-    float *base = (float *)smem;
-    SlotColumns<float> sc;
-    sc.st = bd;
-    sc.phi = base + tid;
-    sc.aj = base + (size_t)PM * bd + tid;
-    sc.lap = base + (size_t)2 * PM * bd + tid;
-    sc.cap = base + (size_t)3 * PM * bd + tid;
-    sc.ids = (uint16_t *)(base + (size_t)4 * PM * bd) + tid;
-    const double T = (!live || cp.n == 0) ? 0.0 : (double)a.tm[c];
-    cell_rates_ordered<PM, float>(a, cp, sc, c, live, T);
-    if (!live) return;
-    double tr = 0.0;
-    if (a.has_temp_rate) tr += a.temp_rate;
-    a.ftm[c] = (float)tr;
-}
-
-template <int DIM, int PM>
-static void launch_one(const PfArgs<float> &a, cudaStream_t s)
-{
-    if (a.single) {
-        int64_t blocks = (a.ncells + kMixedBlock - 1) / kMixedBlock;
-        k_rhs_pf_mixed_single<DIM, PM><<<(unsigned)blocks, kMixedBlock, 0, s>>>(a);
-    } else {
-        int64_t blocks = (a.ncells + 63) / 64;
-        size_t sm = (size_t)64 * PM * (4 * 4 + 2);
-        k_rhs_pf_mixed_multi<DIM, PM><<<(unsigned)blocks, 64, sm, s>>>(a);
-    }
 }
 
 template <int DIM>
-static void launch_pm(const PfArgs<float> &a, cudaStream_t s)
+__global__ void __launch_bounds__(64) k_rhs_pf_mixed_multi(const PfArgs<float> a)
 {
-    if (a.P <= 4) launch_one<DIM, 4>(a, s);
-    else if (a.P <= 8) launch_one<DIM, 8>(a, s);
-    else if (a.P <= 12) launch_one<DIM, 12>(a, s);
-    else launch_one<DIM, 16>(a, s);
+    extern __shared__ __align__(16) unsigned char smem[];
+    const CellIndex ci = cell_index(a.res);
+    const SlotColumns<float> sc = slot_columns<float>(smem, a.P, blockDim.x, threadIdx.x, true);
+    const int n = load_and_gather<DIM, float, false>(a, ci, sc);
+    const double T = n == 0 ? 0.0 : (double)a.tm[ci.c];
+    cell_rates_ordered<float, false>(a, sc, n, ci.c, ci.live, T);
+    if (!ci.live) return;
+    double tr = 0.0;
+    if (a.has_temp_rate) tr += a.temp_rate;
+    a.ftm[ci.c] = (float)tr;
+}
+
+template <int DIM>
+static void launch_dim(const PfArgs<float> &a, cudaStream_t s)
+{
+    if (a.single) {
+        dim3 grid((unsigned)((a.res[0] + kMixedBlock - 1) / kMixedBlock), (unsigned)a.res[1], (unsigned)a.res[2]);
+        size_t sm = slot_columns_bytes(a.P, kMixedBlock, 4, false);
+        k_rhs_pf_mixed_single<DIM><<<grid, kMixedBlock, sm, s>>>(a);
+    } else {
+        dim3 grid((unsigned)((a.res[0] + 63) / 64), (unsigned)a.res[1], (unsigned)a.res[2]);
+        size_t sm = slot_columns_bytes(a.P, 64, 4, true);
+        k_rhs_pf_mixed_multi<DIM><<<grid, 64, sm, s>>>(a);
+    }
 }
 
 cudaError_t launch_rhs_phasefield(const PfArgs<float> &a, int dim, cudaStream_t s)
 {
-    if (dim == 1) launch_pm<1>(a, s);
-    else if (dim == 2) launch_pm<2>(a, s);
-    else launch_pm<3>(a, s);
+    if (dim == 1) launch_dim<1>(a, s);
+    else if (dim == 2) launch_dim<2>(a, s);
+    else launch_dim<3>(a, s);
     return cudaGetLastError();
 }
 

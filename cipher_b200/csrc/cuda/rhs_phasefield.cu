@@ -22,60 +22,36 @@ namespace cipher {
 
 constexpr int kFp64Block = 64;
 
-template <int PM>
-__host__ __device__ constexpr size_t slot_smem_bytes(int block, int rbytes)
-{
-    return (size_t)block * PM * (4 * rbytes + 2);
-}
-
-template <int DIM, int PM>
+template <int DIM, bool SINGLE>
 __global__ void __launch_bounds__(kFp64Block) k_rhs_pf_fp64(const PfArgs<double> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = c < a.ncells;
-    CellPF<PM, double> cp;
-    load_and_gather<DIM, PM, double, true>(a, c, live, cp);
-    const int bd = blockDim.x, tid = threadIdx.x;
-    double *base = (double *)smem;
-    SlotColumns<double> sc;
-    sc.st = bd;
-    sc.phi = base + tid;
-    sc.aj = base + (size_t)PM * bd + tid;
-    sc.lap = base + (size_t)2 * PM * bd + tid;
-    sc.cap = base + (size_t)3 * PM * bd + tid;
-    sc.ids = (uint16_t *)(base + (size_t)4 * PM * bd) + tid;
-    const double T = (a.single || !live || cp.n == 0) ? 0.0 : a.tm[c];
-    cell_rates_ordered<PM, double>(a, cp, sc, c, live, T);
-    if (!live) return;
+    const CellIndex ci = cell_index(a.res);
+    const SlotColumns<double> sc = slot_columns<double>(smem, a.P, blockDim.x, threadIdx.x, true);
+    const int n = load_and_gather<DIM, double, true>(a, ci, sc);
+    const double T = (SINGLE || n == 0) ? 0.0 : a.tm[ci.c];
+    cell_rates_ordered<double, SINGLE>(a, sc, n, ci.c, ci.live, T);
+    if (!ci.live) return;
     /* temperature: no conductivity, latent or specific heat (src/cipher.c:558-568) */
     double tr = 0.0;
     if (a.has_temp_rate) tr += a.temp_rate;
-    a.ftm[c] = tr;
-}
-
-template <int DIM, int PM>
-static void launch_one(const PfArgs<double> &a, cudaStream_t s)
-{
-    int64_t blocks = (a.ncells + kFp64Block - 1) / kFp64Block;
-    size_t sm = slot_smem_bytes<PM>(kFp64Block, 8);
-    k_rhs_pf_fp64<DIM, PM><<<(unsigned)blocks, kFp64Block, sm, s>>>(a);
+    a.ftm[ci.c] = tr;
 }
 
 template <int DIM>
-static void launch_pm(const PfArgs<double> &a, cudaStream_t s)
+static void launch_dim(const PfArgs<double> &a, cudaStream_t s)
 {
-    if (a.P <= 4) launch_one<DIM, 4>(a, s);
-    else if (a.P <= 8) launch_one<DIM, 8>(a, s);
-    else if (a.P <= 12) launch_one<DIM, 12>(a, s);
-    else launch_one<DIM, 16>(a, s);
+    dim3 grid((unsigned)((a.res[0] + kFp64Block - 1) / kFp64Block), (unsigned)a.res[1], (unsigned)a.res[2]);
+    size_t sm = slot_columns_bytes(a.P, kFp64Block, 8, true);
+    if (a.single) k_rhs_pf_fp64<DIM, true><<<grid, kFp64Block, sm, s>>>(a);
+    else k_rhs_pf_fp64<DIM, false><<<grid, kFp64Block, sm, s>>>(a);
 }
 
 cudaError_t launch_rhs_phasefield(const PfArgs<double> &a, int dim, cudaStream_t s)
 {
-    if (dim == 1) launch_pm<1>(a, s);
-    else if (dim == 2) launch_pm<2>(a, s);
-    else launch_pm<3>(a, s);
+    if (dim == 1) launch_dim<1>(a, s);
+    else if (dim == 2) launch_dim<2>(a, s);
+    else launch_dim<3>(a, s);
     return cudaGetLastError();
 }
 
