@@ -82,35 +82,44 @@ __device__ __forceinline__ R face_term(const PfArgs<R> &a, R flux)
     }
 }
 
-/* contributions of the face shared with neighbour nb (src/cipher.c:277-288) */
-template <typename R, bool EXACT>
-__device__ __forceinline__ void gather_face(const PfArgs<R> &a, const SlotColumns<R> &sc, int n, int64_t nb,
+/* contributions of the face shared with neighbour nb whose active count nn
+ * was already loaded (src/cipher.c:277-288).  The neighbour's ids and phase
+ * fractions are loaded up front (independent loads, registers), then merged
+ * against the cell's own sorted set in its columns. */
+template <int PM, typename R, bool EXACT>
+__device__ __forceinline__ void gather_face(const PfArgs<R> &a, const SlotColumns<R> &sc, int n, int64_t nb, int nn,
                                             bool cell_is_L)
 {
     const int64_t S = a.stride;
-    int nn = a.as[nb];
     if (nn > a.P) nn = a.P;                 /* that cell's own thread raises the flag */
     if (nn < 1) return;
-    uint16_t b = a.as[S + nb];
-    uint16_t v = sc.ID(0);
+    uint16_t nid[PM];
+    R nph[PM];
+#pragma unroll
+    for (int j = 0; j < PM; j++) {
+        if (j < nn) {
+            nid[j] = a.as[(int64_t)(1 + j) * S + nb];
+            nph[j] = a.phi[(int64_t)j * S + nb];
+        }
+    }
     /* the phase flux is gated on the L cell only (src/cipher.c:277) */
-    bool gate = cell_is_L ? (n > 1 || v > 1) : (nn > 1 || b > 1);
+    const bool gate = cell_is_L ? (n > 1 || sc.ID(0) > 1) : (nn > 1 || nid[0] > 1);
     if (!gate) return;
-    int i = 0, j = 0;
-    while (true) {
+    int i = 0;
+    uint16_t v = sc.ID(0);
+#pragma unroll
+    for (int j = 0; j < PM; j++) {
+        if (j >= nn) break;
+        const uint16_t b = nid[j];
+        while (v < b) {
+            if (++i >= n) return;
+            v = sc.ID(i);
+        }
         if (v == b) {
-            R pn = a.phi[(int64_t)j * S + nb];
-            if (cell_is_L) sc.LAP(i) += face_term<R, EXACT>(a, pn - sc.PHI(i));
-            else sc.LAP(i) -= face_term<R, EXACT>(a, sc.PHI(i) - pn);
-            if (++i >= n || ++j >= nn) break;
+            if (cell_is_L) sc.LAP(i) += face_term<R, EXACT>(a, nph[j] - sc.PHI(i));
+            else sc.LAP(i) -= face_term<R, EXACT>(a, sc.PHI(i) - nph[j]);
+            if (++i >= n) return;
             v = sc.ID(i);
-            b = a.as[(int64_t)(1 + j) * S + nb];
-        } else if (v < b) {
-            if (++i >= n) break;
-            v = sc.ID(i);
-        } else {
-            if (++j >= nn) break;
-            b = a.as[(int64_t)(1 + j) * S + nb];
         }
     }
 }
@@ -138,21 +147,42 @@ __device__ __forceinline__ CellIndex cell_index(const int *res)
  * descending direction, own faces in ascending direction, wrapped faces
  * from above in ascending direction).  Returns the active count (0 for a
  * dead or invalid cell; an invalid one raises ERR_BADSET). */
-template <int DIM, typename R, bool EXACT>
+template <int DIM, int PM, typename R, bool EXACT>
 __device__ __forceinline__ int load_and_gather(const PfArgs<R> &a, const CellIndex &ci, const SlotColumns<R> &sc)
 {
     const int64_t S = a.stride, c = ci.c;
+    const int res0 = a.res[0], res1 = a.res[1], res2 = a.res[2];
+    const int64_t st1 = res0, st2 = (int64_t)res0 * res1;
+    const int co0 = ci.x, co1 = ci.y, co2 = ci.z;
+    /* the neighbours in the reference's face order, at fixed positions:
+     * [0, DIM)       below without wrap, descending direction
+     * [DIM, 2 DIM)   own faces (L = this cell), ascending direction
+     * [2 DIM, 3 DIM) wrapped from above, ascending direction
+     * -1 marks an absent face */
+    const int co[3] = {co0, co1, co2};
+    const int rs[3] = {res0, res1, res2};
+    const int64_t st[3] = {1, st1, st2};
+    int64_t nb[3 * DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        const int e = DIM - 1 - d;                     /* descending direction */
+        nb[d] = co[e] > 0 ? c - st[e] : -1;
+        nb[DIM + d] = co[d] < rs[d] - 1 ? c + st[d] : (a.per[d] ? c - (int64_t)(rs[d] - 1) * st[d] : -1);
+        nb[2 * DIM + d] = (co[d] == 0 && a.per[d]) ? c + (int64_t)(rs[d] - 1) * st[d] : -1;
+    }
+
+    /* own set and every neighbour's count: independent loads issued together */
     int n = ci.live ? (int)a.as[c] : 0;
+    int nn[3 * DIM];
+#pragma unroll
+    for (int f = 0; f < 3 * DIM; f++) nn[f] = (ci.live && nb[f] >= 0) ? (int)a.as[nb[f]] : 0;
     bool ok = true;
     if (ci.live && (n < 1 || n > a.P)) { ok = false; n = 0; }
-    int nz = 0;
     for (int g = 0; g < n; g++) {
         uint16_t id = a.as[(int64_t)(1 + g) * S + c];
-        R p = a.phi[(int64_t)g * S + c];
         sc.ID(g) = id;
-        sc.PHI(g) = p;
+        sc.PHI(g) = a.phi[(int64_t)g * S + c];
         sc.LAP(g) = (R)0;
-        if (p != (R)0) sc.NZ(nz++) = (uint8_t)g;
         if (id >= a.npf) ok = false;
     }
     if (!ok) {
@@ -160,29 +190,9 @@ __device__ __forceinline__ int load_and_gather(const PfArgs<R> &a, const CellInd
         return 0;
     }
     if (n == 0) return 0;
-    (void)nz;
-    const int res0 = a.res[0], res1 = a.res[1], res2 = a.res[2];
-    const int64_t st1 = res0, st2 = (int64_t)res0 * res1;
-    const int co0 = ci.x, co1 = ci.y, co2 = ci.z;
-    /* faces whose L cell lies below without wrapping, descending direction */
-    if (DIM > 2 && co2 > 0) gather_face<R, EXACT>(a, sc, n, c - st2, false);
-    if (DIM > 1 && co1 > 0) gather_face<R, EXACT>(a, sc, n, c - st1, false);
-    if (co0 > 0) gather_face<R, EXACT>(a, sc, n, c - 1, false);
-    /* own faces, ascending direction */
-    if (co0 < res0 - 1) gather_face<R, EXACT>(a, sc, n, c + 1, true);
-    else if (a.per[0]) gather_face<R, EXACT>(a, sc, n, c - (res0 - 1), true);
-    if (DIM > 1) {
-        if (co1 < res1 - 1) gather_face<R, EXACT>(a, sc, n, c + st1, true);
-        else if (a.per[1]) gather_face<R, EXACT>(a, sc, n, c - (int64_t)(res1 - 1) * st1, true);
-    }
-    if (DIM > 2) {
-        if (co2 < res2 - 1) gather_face<R, EXACT>(a, sc, n, c + st2, true);
-        else if (a.per[2]) gather_face<R, EXACT>(a, sc, n, c - (int64_t)(res2 - 1) * st2, true);
-    }
-    /* faces whose L cell wraps around from above, ascending direction */
-    if (co0 == 0 && a.per[0]) gather_face<R, EXACT>(a, sc, n, c + (res0 - 1), false);
-    if (DIM > 1 && co1 == 0 && a.per[1]) gather_face<R, EXACT>(a, sc, n, c + (int64_t)(res1 - 1) * st1, false);
-    if (DIM > 2 && co2 == 0 && a.per[2]) gather_face<R, EXACT>(a, sc, n, c + (int64_t)(res2 - 1) * st2, false);
+#pragma unroll
+    for (int f = 0; f < 3 * DIM; f++)
+        if (nb[f] >= 0) gather_face<PM, R, EXACT>(a, sc, n, nb[f], nn[f], f >= DIM && f < 2 * DIM);
     return n;
 }
 

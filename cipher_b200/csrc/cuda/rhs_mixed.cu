@@ -26,13 +26,13 @@ namespace cipher {
 
 constexpr int kMixedBlock = 128;
 
-template <int DIM>
+template <int DIM, int PM>
 __global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_single(const PfArgs<float> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const CellIndex ci = cell_index(a.res);
     const SlotColumns<float> sc = slot_columns<float>(smem, a.P, blockDim.x, threadIdx.x, false);
-    const int n = load_and_gather<DIM, float, false>(a, ci, sc);
+    const int n = load_and_gather<DIM, PM, float, false>(a, ci, sc);
     if (!ci.live) return;
     const int64_t S = a.stride, c = ci.c;
     uint32_t act = 0;
@@ -78,13 +78,13 @@ __global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_single(const PfArg
     a.ftm[c] = (float)tr;
 }
 
-template <int DIM>
+template <int DIM, int PM>
 __global__ void __launch_bounds__(64) k_rhs_pf_mixed_multi(const PfArgs<float> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const CellIndex ci = cell_index(a.res);
     const SlotColumns<float> sc = slot_columns<float>(smem, a.P, blockDim.x, threadIdx.x, true);
-    const int n = load_and_gather<DIM, float, false>(a, ci, sc);
+    const int n = load_and_gather<DIM, PM, float, false>(a, ci, sc);
     const double T = n == 0 ? 0.0 : (double)a.tm[ci.c];
     cell_rates_ordered<float, false>(a, sc, n, ci.c, ci.live, T);
     if (!ci.live) return;
@@ -93,18 +93,27 @@ __global__ void __launch_bounds__(64) k_rhs_pf_mixed_multi(const PfArgs<float> a
     a.ftm[ci.c] = (float)tr;
 }
 
-template <int DIM>
-static void launch_dim(const PfArgs<float> &a, cudaStream_t s)
+template <int DIM, int PM>
+static void launch_pm(const PfArgs<float> &a, cudaStream_t s)
 {
     if (a.single) {
         dim3 grid((unsigned)((a.res[0] + kMixedBlock - 1) / kMixedBlock), (unsigned)a.res[1], (unsigned)a.res[2]);
         size_t sm = slot_columns_bytes(a.P, kMixedBlock, 4, false);
-        k_rhs_pf_mixed_single<DIM><<<grid, kMixedBlock, sm, s>>>(a);
+        k_rhs_pf_mixed_single<DIM, PM><<<grid, kMixedBlock, sm, s>>>(a);
     } else {
         dim3 grid((unsigned)((a.res[0] + 63) / 64), (unsigned)a.res[1], (unsigned)a.res[2]);
         size_t sm = slot_columns_bytes(a.P, 64, 4, true);
-        k_rhs_pf_mixed_multi<DIM><<<grid, 64, sm, s>>>(a);
+        k_rhs_pf_mixed_multi<DIM, PM><<<grid, 64, sm, s>>>(a);
     }
+}
+
+template <int DIM>
+static void launch_dim(const PfArgs<float> &a, cudaStream_t s)
+{
+    if (a.P <= 4) launch_pm<DIM, 4>(a, s);
+    else if (a.P <= 8) launch_pm<DIM, 8>(a, s);
+    else if (a.P <= 12) launch_pm<DIM, 12>(a, s);
+    else launch_pm<DIM, 16>(a, s);
 }
 
 cudaError_t launch_rhs_phasefield(const PfArgs<float> &a, int dim, cudaStream_t s)
