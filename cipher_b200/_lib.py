@@ -114,6 +114,11 @@ class StateLayout(C.Structure):
                 ("tm_offset", C.c_int64), ("bytes", C.c_int64)]
 
 
+class GridDesc(C.Structure):
+    _fields_ = [("dim", C.c_int32), ("res", C.c_int32 * 3), ("periodic", C.c_int32 * 3),
+                ("ex_per_phase", C.c_int32), ("layout", StateLayout), ("ex_init", C.c_void_p)]
+
+
 PP = C.POINTER(ProblemStruct)
 MP = C.POINTER(MeshStruct)
 
@@ -144,6 +149,7 @@ _SIGNATURES = [
     ("cipher_rhs", C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_poststep", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_ctx_check", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("cipher_poststep_noalloc", C.c_int, [C.POINTER(GridDesc), C.c_void_p, C.c_void_p]),
     ("cipher_state_from_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_state_to_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_rhs_aos_host", C.c_int,

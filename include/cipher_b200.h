@@ -137,6 +137,28 @@ int cipher_poststep(cipher_ctx *c, void *X, void *stream);
  * raise instead of trapping (bad active counts, cap overflow) */
 int cipher_ctx_check(cipher_ctx *c, void *stream);
 
+/* grid and state description for the allocation-free entry point */
+typedef struct cipher_grid_desc {
+    int32_t dim;
+    int32_t res[3];
+    int32_t periodic[3];
+    int32_t ex_per_phase;        /* S: explicit site potentials per phase */
+    cipher_state_layout layout;  /* offsets of the state planes (see above) */
+    const double *ex_init;       /* device [npf*S] potentials of new phases, or NULL when S == 0 */
+} cipher_grid_desc;
+
+/* The per-step active-set update of cipher_poststep for callers that cannot
+ * allocate device memory (an embedding application that owns the device
+ * heap, a service with a fixed footprint, code where allocation after
+ * start-up is forbidden).  No counterpart in the reference: CIPHER's PostStep
+ * allocates its work vectors through PETSc.  Needs no context and calls no
+ * allocator; its scratch is a fixed 8 MiB device array inside the library,
+ * so grids with (P+1)*stride above 4 Mi entries are rejected (CIPHER_E_ARG).
+ * The first call on a device looks the array up and must precede any stream
+ * capture; calls that overlap on the GPU share the array and race.
+ * Synchronises `stream`; returns CIPHER_E_CAP when a superset exceeds P. */
+int cipher_poststep_noalloc(const cipher_grid_desc *g, void *X, void *stream);
+
 /* Y = X + a*F on the PF, DP, EX and TM planes; AS is copied from X
  * (VecWAXPY on the solution vector).  Y may alias X. */
 int cipher_waxpy(cipher_ctx *c, void *Y, const void *X, double a, const void *F, void *stream);
