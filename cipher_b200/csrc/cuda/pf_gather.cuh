@@ -27,18 +27,19 @@ enum GeomMode : int {
     GEOM_UNIT = 2,      /* ff == 1 and vol == 1: flux itself, exact */
 };
 
-/* a thread's slot columns in shared memory: element g at base[g*st] */
+/* a thread's slot columns in shared memory: phi and ids at base[g*pst]
+ * (a staged tile plane or a private column), the rest at base[g*st] */
 template <typename R>
 struct SlotColumns {
     R *phi, *aj, *lap, *cap;
     uint16_t *ids;
     uint8_t *nz;                 /* slots with phi != 0, ascending */
-    int st;
-    __device__ __forceinline__ R &PHI(int g) const { return phi[g * st]; }
+    int st, pst;
+    __device__ __forceinline__ R &PHI(int g) const { return phi[g * pst]; }
     __device__ __forceinline__ R &AJ(int g) const { return aj[g * st]; }
     __device__ __forceinline__ R &LAP(int g) const { return lap[g * st]; }
     __device__ __forceinline__ R &CAP(int g) const { return cap[g * st]; }
-    __device__ __forceinline__ uint16_t &ID(int g) const { return ids[g * st]; }
+    __device__ __forceinline__ uint16_t &ID(int g) const { return ids[g * pst]; }
     __device__ __forceinline__ uint8_t &NZ(int g) const { return nz[g * st]; }
 };
 
@@ -51,6 +52,7 @@ __device__ __forceinline__ SlotColumns<R> slot_columns(unsigned char *smem, int 
     R *base = (R *)smem;
     int k = 0;
     sc.st = bd;
+    sc.pst = bd;
     sc.phi = base + (size_t)(k++) * PM * bd + tid;
     sc.lap = base + (size_t)(k++) * PM * bd + tid;
     if (with_aj_cap) {
