@@ -114,23 +114,22 @@ __device__ __forceinline__ void tile_face(const PfArgs<R> &a, const TilePlane<R>
     /* the phase flux is gated on the L cell only (src/cipher.c:277) */
     const bool gate = cell_is_L ? (n > 1 || v > 1) : (nn > 1 || b > 1);
     if (!gate) return;
+    /* branch-free two-pointer merge: both pointers advance by predicate, so
+     * the lanes of a warp stay converged whatever their sets look like */
+    const uint16_t *oi = own.ids + h0, *ni = nbp.ids + hn;
+    const R *op = own.phi + h0, *np = nbp.phi + hn;
     int i = 0, j = 0;
     while (true) {
         if (v == b) {
-            const R pn = nbp.phi[j * HC + hn];
-            const R po = own.phi[i * HC + h0];
+            const R pn = np[j * HC], po = op[i * HC];
             if (cell_is_L) lap[i * lst] += face_term<R, EXACT>(a, pn - po);
             else lap[i * lst] -= face_term<R, EXACT>(a, po - pn);
-            if (++i >= n || ++j >= nn) break;
-            v = own.ids[i * HC + h0];
-            b = nbp.ids[j * HC + hn];
-        } else if (v < b) {
-            if (++i >= n) break;
-            v = own.ids[i * HC + h0];
-        } else {
-            if (++j >= nn) break;
-            b = nbp.ids[j * HC + hn];
         }
+        i += v <= b;
+        j += v >= b;
+        if (i >= n || j >= nn) break;
+        v = oi[i * HC];
+        b = ni[j * HC];
     }
 }
 
