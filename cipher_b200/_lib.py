@@ -10,7 +10,9 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libcipher_b200.so")
+# CIPHER_B200_LIB selects another build of the same library (for example a
+# build with different launch parameters); default: the in-tree build
+LIB_PATH = os.environ.get("CIPHER_B200_LIB") or os.path.join(HERE, "libcipher_b200.so")
 
 MAXCP = 5
 MAXAP = 15

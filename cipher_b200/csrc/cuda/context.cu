@@ -146,6 +146,9 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
     /* kernels launch one block row per (y, z) grid line */
     if ((p->dim > 1 && m->res[1] > 65535) || (p->dim > 2 && m->res[2] > 65535))
         return set_error(CIPHER_E_UNSUPPORTED, "grid lines above 65535 in y or z");
+    /* kernels index cells with 32-bit integers */
+    if ((int64_t)m->ncells > 2147483647LL - 1024)
+        return set_error(CIPHER_E_UNSUPPORTED, "more than 2^31 cells on one context");
     char why[256];
     if (!problem_supported(p, why, sizeof(why))) return set_error(CIPHER_E_UNSUPPORTED, "%s", why);
     /* the linear interpolant is not used by the phase-field-only kernel (no chemistry) */

@@ -85,44 +85,36 @@ __device__ __forceinline__ R face_term(const PfArgs<R> &a, R flux)
 }
 
 /* contributions of the face shared with neighbour nb whose active count nn
- * was already loaded (src/cipher.c:277-288).  The neighbour's ids and phase
- * fractions are loaded up front (independent loads, registers), then merged
- * against the cell's own sorted set in its columns. */
-template <int PM, typename R, bool EXACT>
+ * was already loaded (src/cipher.c:277-288).  Branch-free two-pointer merge
+ * of the two sorted sets (SetIntersection, src/utility.c:168-190): both
+ * pointers advance by predicate, so a warp's lanes stay converged; the
+ * neighbour's entries are read through the read-only cache. */
+template <typename R, bool EXACT>
 __device__ __forceinline__ void gather_face(const PfArgs<R> &a, const SlotColumns<R> &sc, int n, int64_t nb, int nn,
                                             bool cell_is_L)
 {
     const int64_t S = a.stride;
-    if (nn > a.P) nn = a.P;                 /* that cell's own thread raises the flag */
     if (nn < 1) return;
-    uint16_t nid[PM];
-    R nph[PM];
-#pragma unroll
-    for (int j = 0; j < PM; j++) {
-        if (j < nn) {
-            nid[j] = a.as[(int64_t)(1 + j) * S + nb];
-            nph[j] = a.phi[(int64_t)j * S + nb];
-        }
-    }
-    /* the phase flux is gated on the L cell only (src/cipher.c:277) */
-    const bool gate = cell_is_L ? (n > 1 || sc.ID(0) > 1) : (nn > 1 || nid[0] > 1);
-    if (!gate) return;
-    int i = 0;
+    const uint16_t *nid = a.as + S + nb;
+    const R *nph = a.phi + nb;
+    uint16_t b = __ldg(nid);
     uint16_t v = sc.ID(0);
-#pragma unroll
-    for (int j = 0; j < PM; j++) {
-        if (j >= nn) break;
-        const uint16_t b = nid[j];
-        while (v < b) {
-            if (++i >= n) return;
-            v = sc.ID(i);
-        }
+    /* the phase flux is gated on the L cell only (src/cipher.c:277) */
+    const bool gate = cell_is_L ? (n > 1 || v > 1) : (nn > 1 || b > 1);
+    if (!gate) return;
+    int i = 0, j = 0;
+    while (true) {
         if (v == b) {
-            if (cell_is_L) sc.LAP(i) += face_term<R, EXACT>(a, nph[j] - sc.PHI(i));
-            else sc.LAP(i) -= face_term<R, EXACT>(a, sc.PHI(i) - nph[j]);
-            if (++i >= n) return;
-            v = sc.ID(i);
+            const R pn = __ldg(nph + (int64_t)j * S);
+            if (cell_is_L) sc.LAP(i) += face_term<R, EXACT>(a, pn - sc.PHI(i));
+            else sc.LAP(i) -= face_term<R, EXACT>(a, sc.PHI(i) - pn);
         }
+        const bool ai = v <= b, aj = v >= b;
+        i += ai;
+        j += aj;
+        if (i >= n || j >= nn) break;
+        v = sc.ID(i);
+        if (aj) b = __ldg(nid + (int64_t)j * S);
     }
 }
 
@@ -144,46 +136,52 @@ __device__ __forceinline__ CellIndex cell_index(const int *res)
     return ci;
 }
 
-/* load the cell's set and phase fractions into its columns, then gather its
- * faces in the reference's face order (non-wrapped faces from below in
- * descending direction, own faces in ascending direction, wrapped faces
- * from above in ascending direction).  Returns the active count (0 for a
- * dead or invalid cell; an invalid one raises ERR_BADSET). */
-template <int DIM, int PM, typename R, bool EXACT>
+/* neighbour at fixed face position f: [0,DIM) below without wrap
+ * (descending d), [DIM,2DIM) own faces (ascending d), [2DIM,3DIM) wrapped
+ * around from above (ascending d); -1 when the face is absent.  This is the
+ * order in which the reference's face loop reaches the cell's faces. */
+template <int DIM, typename R>
+__device__ __forceinline__ int64_t face_nb(const PfArgs<R> &a, const CellIndex &ci, int f)
+{
+    const int co[3] = {ci.x, ci.y, ci.z};
+    const int64_t st[3] = {1, (int64_t)a.res[0], (int64_t)a.res[0] * a.res[1]};
+    if (f < DIM) {
+        const int e = DIM - 1 - f;
+        return co[e] > 0 ? ci.c - st[e] : -1;
+    }
+    if (f < 2 * DIM) {
+        const int d = f - DIM;
+        if (co[d] < a.res[d] - 1) return ci.c + st[d];
+        return (a.per[d] && a.res[d] > 1) ? ci.c - (int64_t)(a.res[d] - 1) * st[d] : -1;
+    }
+    const int d = f - 2 * DIM;
+    return (co[d] == 0 && a.per[d] && a.res[d] > 1) ? ci.c + (int64_t)(a.res[d] - 1) * st[d] : -1;
+}
+
+/* load the cell's set into its columns and gather its faces in the
+ * reference's face order.  Returns the active count (0 for a dead or
+ * invalid cell; an invalid one raises ERR_BADSET). */
+template <int DIM, typename R, bool EXACT>
 __device__ __forceinline__ int load_and_gather(const PfArgs<R> &a, const CellIndex &ci, const SlotColumns<R> &sc)
 {
     const int64_t S = a.stride, c = ci.c;
-    const int res0 = a.res[0], res1 = a.res[1], res2 = a.res[2];
-    const int64_t st1 = res0, st2 = (int64_t)res0 * res1;
-    const int co0 = ci.x, co1 = ci.y, co2 = ci.z;
-    /* the neighbours in the reference's face order, at fixed positions:
-     * [0, DIM)       below without wrap, descending direction
-     * [DIM, 2 DIM)   own faces (L = this cell), ascending direction
-     * [2 DIM, 3 DIM) wrapped from above, ascending direction
-     * -1 marks an absent face */
-    const int co[3] = {co0, co1, co2};
-    const int rs[3] = {res0, res1, res2};
-    const int64_t st[3] = {1, st1, st2};
-    int64_t nb[3 * DIM];
+    int n = ci.live ? (int)__ldg(&a.as[c]) : 0;
+    /* the neighbours' counts, packed 4 bits per face position (clamped to P;
+     * a neighbour's own thread flags an invalid count) */
+    uint64_t nnp = 0;
 #pragma unroll
-    for (int d = 0; d < DIM; d++) {
-        const int e = DIM - 1 - d;                     /* descending direction */
-        nb[d] = co[e] > 0 ? c - st[e] : -1;
-        nb[DIM + d] = co[d] < rs[d] - 1 ? c + st[d] : (a.per[d] ? c - (int64_t)(rs[d] - 1) * st[d] : -1);
-        nb[2 * DIM + d] = (co[d] == 0 && a.per[d]) ? c + (int64_t)(rs[d] - 1) * st[d] : -1;
+    for (int f = 0; f < 3 * DIM; f++) {
+        const int64_t nb = ci.live ? face_nb<DIM, R>(a, ci, f) : -1;
+        int k = nb >= 0 ? (int)__ldg(&a.as[nb]) : 0;
+        k = k > a.P ? a.P : k;
+        nnp |= (uint64_t)k << (4 * f);
     }
-
-    /* own set and every neighbour's count: independent loads issued together */
-    int n = ci.live ? (int)a.as[c] : 0;
-    int nn[3 * DIM];
-#pragma unroll
-    for (int f = 0; f < 3 * DIM; f++) nn[f] = (ci.live && nb[f] >= 0) ? (int)a.as[nb[f]] : 0;
     bool ok = true;
     if (ci.live && (n < 1 || n > a.P)) { ok = false; n = 0; }
     for (int g = 0; g < n; g++) {
-        uint16_t id = a.as[(int64_t)(1 + g) * S + c];
+        const uint16_t id = __ldg(&a.as[(int64_t)(1 + g) * S + c]);
         sc.ID(g) = id;
-        sc.PHI(g) = a.phi[(int64_t)g * S + c];
+        sc.PHI(g) = __ldg(&a.phi[(int64_t)g * S + c]);
         sc.LAP(g) = (R)0;
         if (id >= a.npf) ok = false;
     }
@@ -193,8 +191,10 @@ __device__ __forceinline__ int load_and_gather(const PfArgs<R> &a, const CellInd
     }
     if (n == 0) return 0;
 #pragma unroll
-    for (int f = 0; f < 3 * DIM; f++)
-        if (nb[f] >= 0) gather_face<PM, R, EXACT>(a, sc, n, nb[f], nn[f], f >= DIM && f < 2 * DIM);
+    for (int f = 0; f < 3 * DIM; f++) {
+        const int nn = (int)(nnp >> (4 * f) & 15u);
+        if (nn) gather_face<R, EXACT>(a, sc, n, face_nb<DIM, R>(a, ci, f), nn, f >= DIM && f < 2 * DIM);
+    }
     return n;
 }
 

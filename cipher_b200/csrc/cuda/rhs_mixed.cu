@@ -14,8 +14,6 @@
  * makes the cell terms O(n) instead of O(n^3).  Several interfaces use the
  * reference-order evaluation of pf_cell.cuh in FP32.  Accuracy against the
  * FP64 oracle on the same inputs: max|dF|/max|F| <= 1e-6 (tested).
- *
- * Data movement: z-marching shared-memory tiles (rhs_tile.cuh).
  */
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -23,152 +21,90 @@
 #include "kernels.h"
 #include "pf_gather.cuh"
 #include "pf_cell.cuh"
-#include "rhs_tile.cuh"
 
 namespace cipher {
 
-constexpr int kMX = 32, kMY = 4, kMZC = 8;
+constexpr int kMixedBlock = 128;
 
-/* closed-form cell terms for one interface; writes all P slots of F */
-__device__ __forceinline__ void mixed_single_cell(const PfArgs<float> &a, const TilePlane<float> &mid, int HC, int h0,
-                                                  int n, const float *lap, int lst, int64_t c)
+template <int DIM>
+__global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_single(const PfArgs<float> a)
 {
-    const int64_t S = a.stride;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const CellIndex ci = cell_index(a.res);
+    const SlotColumns<float> sc = slot_columns<float>(smem, a.P, blockDim.x, threadIdx.x, false);
+    const int n = load_and_gather<DIM, float, false>(a, ci, sc);
+    if (!ci.live) return;
+    const int64_t S = a.stride, c = ci.c;
     uint32_t act = 0;
     double nact = 0.0, Ca = 0.0;
     const double mob = a.mob0;
-    float cap[CIPHER_PMAX];
     if (n > 1) {
         const float sig = (float)a.sig0, inv_w = (float)(1.0 / a.wid0);
         const float w_pi2 = (float)(a.wid0 / (CIPHER_PI_D * CIPHER_PI_D));
         const float tjh = (float)(0.5 * a.tj0);
         float A = 0.0f, S1 = 0.0f, S2 = 0.0f;
         for (int k = 0; k < n; k++) {
-            const float p = mid.phi[k * HC + h0];
-            A += p * inv_w + lap[k * lst] * w_pi2;
+            const float p = sc.PHI(k);
+            A += p * inv_w + sc.LAP(k) * w_pi2;
             S1 += p;
             S2 += p * p;
         }
+        /* capillary force, stored over the consumed Laplacian */
         double C = 0.0;
-#pragma unroll
-        for (int k = 0; k < CIPHER_PMAX; k++) {
-            if (k < n) {
-                const float p = mid.phi[k * HC + h0], l = lap[k * lst];
-                const float ak = p * inv_w + l * w_pi2;
-                const float o1 = S1 - p, o2 = S2 - p * p;
-                cap[k] = 8.0f * (-sig * (A - ak) - tjh * (o1 * o1 - o2)) + l;
-                C += (double)cap[k];
-            }
+        for (int k = 0; k < n; k++) {
+            const float p = sc.PHI(k), l = sc.LAP(k);
+            const float ak = p * inv_w + l * w_pi2;
+            const float o1 = S1 - p, o2 = S2 - p * p;
+            const float cap = 8.0f * (-sig * (A - ak) - tjh * (o1 * o1 - o2)) + l;
+            sc.LAP(k) = cap;
+            C += (double)cap;
         }
-#pragma unroll
-        for (int k = 0; k < CIPHER_PMAX; k++) {
-            if (k < n) {
-                const double u = mob * ((double)n * (double)cap[k] - C);
-                const double p = (double)mid.phi[k * HC + h0];
-                const bool on = (p > CIPHER_TOL && p < 1.0 - CIPHER_TOL) || (p < CIPHER_TOL && u > 0.0) ||
-                                (p > 1.0 - CIPHER_TOL && u < 0.0);
-                if (on) { act |= 1u << k; nact += 1.0; Ca += (double)cap[k]; }
-            }
+        for (int k = 0; k < n; k++) {
+            const double cap = (double)sc.LAP(k);
+            const double u = mob * ((double)n * cap - C);
+            const double p = (double)sc.PHI(k);
+            const bool on = (p > CIPHER_TOL && p < 1.0 - CIPHER_TOL) || (p < CIPHER_TOL && u > 0.0) ||
+                            (p > 1.0 - CIPHER_TOL && u < 0.0);
+            if (on) { act |= 1u << k; nact += 1.0; Ca += cap; }
         }
     }
-#pragma unroll
-    for (int m = 0; m < CIPHER_PMAX; m++) {
-        if (m >= a.P) break;
+    for (int m = 0; m < a.P; m++) {
         float v = 0.0f;
-        if (m < n && (act >> m & 1u)) v = (float)(mob * (nact * (double)cap[m] - Ca) / nact);
+        if (m < n && (act >> m & 1u)) v = (float)(mob * (nact * (double)sc.LAP(m) - Ca) / nact);
         a.fphi[(int64_t)m * S + c] = v;
     }
+    double tr = 0.0;
+    if (a.has_temp_rate) tr += a.temp_rate;
+    a.ftm[c] = (float)tr;
 }
 
-template <int DIM, bool SINGLE>
-__global__ void __launch_bounds__(kMX * kMY) k_rhs_tile_mixed(const PfArgs<float> a)
+template <int DIM>
+__global__ void __launch_bounds__(64) k_rhs_pf_mixed_multi(const PfArgs<float> a)
 {
-    using T = TileShape<kMX, kMY>;
     extern __shared__ __align__(16) unsigned char smem[];
-    const int P = a.P;
-    const size_t pb = tile_plane_bytes<float, T::HC>(P);
-    auto plane = [&](int slot) { return tile_plane<float, T::HC>(smem + (size_t)slot * pb, P); };
-    unsigned char *cols = smem + 3 * pb;
-    const int tid = threadIdx.x, tx = tid % kMX, ty = tid / kMX;
-    const int x0 = blockIdx.x * kMX, y0 = blockIdx.y * kMY, zs = blockIdx.z * kMZC;
-    const int ze = min(zs + kMZC, a.res[2]);
-    const int gx = x0 + tx, gy = y0 + ty;
-    const bool col_live = gx < a.res[0] && gy < a.res[1];
-    /* private columns: lap [P][NT] (+ aj, cap [P][NT], nz for several interfaces) */
-    float *lap = (float *)cols + tid;
-    SlotColumns<float> sc;
-    if (!SINGLE) {
-        float *fb = (float *)cols;
-        sc.lap = fb + tid;
-        sc.aj = fb + (size_t)P * T::NT + tid;
-        sc.cap = fb + (size_t)2 * P * T::NT + tid;
-        sc.nz = (uint8_t *)(fb + (size_t)3 * P * T::NT) + tid;
-        sc.st = T::NT;
-        sc.pst = T::HC;
-    }
-    if (DIM == 3) {
-        load_tile_plane<DIM, kMX, kMY, float>(a, plane(0), x0, y0, zs - 1, true);
-        load_tile_plane<DIM, kMX, kMY, float>(a, plane(2), x0, y0, zs + 1, zs + 1 < a.res[2] || a.per[2]);
-    }
-    load_tile_plane<DIM, kMX, kMY, float>(a, plane(1), x0, y0, zs, true);
-    const int h0 = (ty + 1) * T::HX + tx + 1;
-    for (int z = zs; z < ze; z++) {
-        const int i = z - zs;
-        const TilePlane<float> lo = plane(i % 3), mid = plane((i + 1) % 3), hi = plane((i + 2) % 3);
-        __syncthreads();
-        if (col_live) {
-            const int64_t c = (int64_t)gx + (int64_t)a.res[0] * ((int64_t)gy + (int64_t)a.res[1] * z);
-            int n = mid.cnt[h0];
-            bool ok = n >= 1 && n <= P;
-            for (int g = 0; ok && g < n; g++) ok = mid.ids[g * T::HC + h0] < a.npf;
-            if (!ok) {
-                atomicOr(a.err, ERR_BADSET);
-                for (int m = 0; m < P; m++) a.fphi[(int64_t)m * a.stride + c] = 0.0f;
-                a.ftm[c] = 0.0f;
-            } else {
-                if (SINGLE) {
-                    tile_gather<DIM, kMX, kMY, float, false>(a, lo, mid, hi, tx, ty, gx, gy, z, n, lap, T::NT);
-                    mixed_single_cell(a, mid, T::HC, h0, n, lap, T::NT, c);
-                } else {
-                    tile_gather<DIM, kMX, kMY, float, false>(a, lo, mid, hi, tx, ty, gx, gy, z, n, sc.lap, T::NT);
-                    sc.phi = mid.phi + h0;
-                    sc.ids = mid.ids + h0;
-                    cell_rates_ordered<float, false>(a, sc, n, c, true, (double)a.tm[c]);
-                }
-                double tr = 0.0;
-                if (a.has_temp_rate) tr += a.temp_rate;
-                a.ftm[c] = (float)tr;
-            }
-        }
-        __syncthreads();
-        if (DIM == 3 && z + 1 < ze) {
-            const int zn = z + 2;
-            load_tile_plane<DIM, kMX, kMY, float>(a, plane(i % 3), x0, y0, zn, zn < a.res[2] || a.per[2]);
-        }
-    }
-}
-
-template <int DIM, bool SINGLE>
-static void launch_tile(const PfArgs<float> &a, cudaStream_t s)
-{
-    using T = TileShape<kMX, kMY>;
-    dim3 grid((unsigned)((a.res[0] + kMX - 1) / kMX), (unsigned)((a.res[1] + kMY - 1) / kMY),
-              (unsigned)((a.res[2] + kMZC - 1) / kMZC));
-    size_t cols = SINGLE ? (size_t)a.P * T::NT * 4 : (size_t)a.P * T::NT * (3 * 4 + 1);
-    size_t sm = 3 * tile_plane_bytes<float, T::HC>(a.P) + cols;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_rhs_tile_mixed<DIM, SINGLE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attr_set = true;
-    }
-    k_rhs_tile_mixed<DIM, SINGLE><<<grid, T::NT, sm, s>>>(a);
+    const CellIndex ci = cell_index(a.res);
+    const SlotColumns<float> sc = slot_columns<float>(smem, a.P, blockDim.x, threadIdx.x, true);
+    const int n = load_and_gather<DIM, float, false>(a, ci, sc);
+    const double T = n == 0 ? 0.0 : (double)a.tm[ci.c];
+    cell_rates_ordered<float, false>(a, sc, n, ci.c, ci.live, T);
+    if (!ci.live) return;
+    double tr = 0.0;
+    if (a.has_temp_rate) tr += a.temp_rate;
+    a.ftm[ci.c] = (float)tr;
 }
 
 template <int DIM>
 static void launch_dim(const PfArgs<float> &a, cudaStream_t s)
 {
-    if (a.single) launch_tile<DIM, true>(a, s);
-    else launch_tile<DIM, false>(a, s);
+    if (a.single) {
+        dim3 grid((unsigned)((a.res[0] + kMixedBlock - 1) / kMixedBlock), (unsigned)a.res[1], (unsigned)a.res[2]);
+        size_t sm = slot_columns_bytes(a.P, kMixedBlock, 4, false);
+        k_rhs_pf_mixed_single<DIM><<<grid, kMixedBlock, sm, s>>>(a);
+    } else {
+        dim3 grid((unsigned)((a.res[0] + 63) / 64), (unsigned)a.res[1], (unsigned)a.res[2]);
+        size_t sm = slot_columns_bytes(a.P, 64, 4, true);
+        k_rhs_pf_mixed_multi<DIM><<<grid, 64, sm, s>>>(a);
+    }
 }
 
 cudaError_t launch_rhs_phasefield(const PfArgs<float> &a, int dim, cudaStream_t s)
