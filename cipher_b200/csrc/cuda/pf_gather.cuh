@@ -10,8 +10,9 @@
  * two-pointer merge of the two sorted sets, as SetIntersection does
  * (src/utility.c:168-190).
  *
- * Launch geometry: grid (ceil(res0/block), res1, res2), one thread per cell
- * of an x-row, so cell coordinates need no integer division.
+ * Launch geometry: blocks of BX x BY cells in (x, y), grid
+ * (ceil(res0/BX), ceil(res1/BY), res2): cell coordinates need no integer
+ * division by the grid size and a warp covers 32 consecutive x cells.
  */
 #pragma once
 #include <cstdint>
@@ -34,6 +35,8 @@ struct SlotColumns {
     R *phi, *aj, *lap, *cap;
     uint16_t *ids;
     uint8_t *nz;                 /* slots with phi != 0, ascending */
+    R *nph;                      /* scratch: the neighbour being merged */
+    uint16_t *nids;
     int st, pst;
     __device__ __forceinline__ R &PHI(int g) const { return phi[g * pst]; }
     __device__ __forceinline__ R &AJ(int g) const { return aj[g * st]; }
@@ -41,10 +44,12 @@ struct SlotColumns {
     __device__ __forceinline__ R &CAP(int g) const { return cap[g * st]; }
     __device__ __forceinline__ uint16_t &ID(int g) const { return ids[g * pst]; }
     __device__ __forceinline__ uint8_t &NZ(int g) const { return nz[g * st]; }
+    __device__ __forceinline__ R &NPH(int g) const { return nph[g * st]; }
+    __device__ __forceinline__ uint16_t &NID(int g) const { return nids[g * st]; }
 };
 
 /* carve the columns of thread `tid` out of a block's dynamic shared memory;
- * layout: R phi,aj,lap,cap [PM][bd] | uint16 ids [PM][bd] | uint8 nz [PM][bd] */
+ * layout: R phi,lap,nph[,aj,cap] [PM][bd] | uint16 ids,nids [PM][bd] | uint8 nz [PM][bd] */
 template <typename R>
 __device__ __forceinline__ SlotColumns<R> slot_columns(unsigned char *smem, int PM, int bd, int tid, bool with_aj_cap)
 {
@@ -55,6 +60,7 @@ __device__ __forceinline__ SlotColumns<R> slot_columns(unsigned char *smem, int 
     sc.pst = bd;
     sc.phi = base + (size_t)(k++) * PM * bd + tid;
     sc.lap = base + (size_t)(k++) * PM * bd + tid;
+    sc.nph = base + (size_t)(k++) * PM * bd + tid;
     if (with_aj_cap) {
         sc.aj = base + (size_t)(k++) * PM * bd + tid;
         sc.cap = base + (size_t)(k++) * PM * bd + tid;
@@ -63,13 +69,14 @@ __device__ __forceinline__ SlotColumns<R> slot_columns(unsigned char *smem, int 
     }
     uint16_t *ib = (uint16_t *)(base + (size_t)k * PM * bd);
     sc.ids = ib + tid;
-    sc.nz = (uint8_t *)(ib + (size_t)PM * bd) + tid;
+    sc.nids = ib + (size_t)PM * bd + tid;
+    sc.nz = (uint8_t *)(ib + (size_t)2 * PM * bd) + tid;
     return sc;
 }
 
 __host__ __device__ constexpr size_t slot_columns_bytes(int PM, int bd, int rbytes, bool with_aj_cap)
 {
-    return (size_t)PM * bd * ((with_aj_cap ? 4 : 2) * rbytes + 2 + 1) + 16;
+    return (size_t)PM * bd * ((with_aj_cap ? 5 : 3) * rbytes + 2 * 2 + 1) + 16;
 }
 
 template <typename R, bool EXACT>
@@ -89,15 +96,34 @@ __device__ __forceinline__ R face_term(const PfArgs<R> &a, R flux)
  * of the two sorted sets (SetIntersection, src/utility.c:168-190): both
  * pointers advance by predicate, so a warp's lanes stay converged; the
  * neighbour's entries are read through the read-only cache. */
-template <typename R, bool EXACT>
+template <int PM, typename R, bool EXACT>
 __device__ __forceinline__ void gather_face(const PfArgs<R> &a, const SlotColumns<R> &sc, int n, int64_t nb, int nn,
                                             bool cell_is_L)
 {
     const int64_t S = a.stride;
     if (nn < 1) return;
-    const uint16_t *nid = a.as + S + nb;
-    const R *nph = a.phi + nb;
-    uint16_t b = __ldg(nid);
+    /* the neighbour's set, staged in the scratch columns four slots at a
+     * time: each group's loads issue back to back, so a face costs about
+     * one memory latency per four slots instead of one per slot */
+    for (int j0 = 0; j0 < nn; j0 += 4) {
+        uint16_t ti[4];
+        R tp[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (j0 + k < nn) {
+                ti[k] = __ldg(a.as + (int64_t)(1 + j0 + k) * S + nb);
+                tp[k] = __ldg(a.phi + (int64_t)(j0 + k) * S + nb);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (j0 + k < nn) {
+                sc.NID(j0 + k) = ti[k];
+                sc.NPH(j0 + k) = tp[k];
+            }
+        }
+    }
+    uint16_t b = sc.NID(0);
     uint16_t v = sc.ID(0);
     /* the phase flux is gated on the L cell only (src/cipher.c:277) */
     const bool gate = cell_is_L ? (n > 1 || v > 1) : (nn > 1 || b > 1);
@@ -105,16 +131,15 @@ __device__ __forceinline__ void gather_face(const PfArgs<R> &a, const SlotColumn
     int i = 0, j = 0;
     while (true) {
         if (v == b) {
-            const R pn = __ldg(nph + (int64_t)j * S);
+            const R pn = sc.NPH(j);
             if (cell_is_L) sc.LAP(i) += face_term<R, EXACT>(a, pn - sc.PHI(i));
             else sc.LAP(i) -= face_term<R, EXACT>(a, sc.PHI(i) - pn);
         }
-        const bool ai = v <= b, aj = v >= b;
-        i += ai;
-        j += aj;
+        i += v <= b;
+        j += v >= b;
         if (i >= n || j >= nn) break;
         v = sc.ID(i);
-        if (aj) b = __ldg(nid + (int64_t)j * S);
+        b = sc.NID(j);
     }
 }
 
@@ -125,13 +150,15 @@ struct CellIndex {
     bool live;
 };
 
+/* blocks of BX x BY cells in (x, y); grid (ceil(res0/BX), ceil(res1/BY), res2) */
+template <int BX, int BY>
 __device__ __forceinline__ CellIndex cell_index(const int *res)
 {
     CellIndex ci;
-    ci.x = blockIdx.x * blockDim.x + threadIdx.x;
-    ci.y = blockIdx.y;
+    ci.x = blockIdx.x * BX + (int)threadIdx.x % BX;
+    ci.y = blockIdx.y * BY + (int)threadIdx.x / BX;
     ci.z = blockIdx.z;
-    ci.live = ci.x < res[0];
+    ci.live = ci.x < res[0] && ci.y < res[1];
     ci.c = (int64_t)ci.x + (int64_t)res[0] * ((int64_t)ci.y + (int64_t)res[1] * ci.z);
     return ci;
 }
@@ -161,7 +188,7 @@ __device__ __forceinline__ int64_t face_nb(const PfArgs<R> &a, const CellIndex &
 /* load the cell's set into its columns and gather its faces in the
  * reference's face order.  Returns the active count (0 for a dead or
  * invalid cell; an invalid one raises ERR_BADSET). */
-template <int DIM, typename R, bool EXACT>
+template <int DIM, int PM, typename R, bool EXACT>
 __device__ __forceinline__ int load_and_gather(const PfArgs<R> &a, const CellIndex &ci, const SlotColumns<R> &sc)
 {
     const int64_t S = a.stride, c = ci.c;
@@ -178,12 +205,25 @@ __device__ __forceinline__ int load_and_gather(const PfArgs<R> &a, const CellInd
     }
     bool ok = true;
     if (ci.live && (n < 1 || n > a.P)) { ok = false; n = 0; }
-    for (int g = 0; g < n; g++) {
-        const uint16_t id = __ldg(&a.as[(int64_t)(1 + g) * S + c]);
-        sc.ID(g) = id;
-        sc.PHI(g) = __ldg(&a.phi[(int64_t)g * S + c]);
-        sc.LAP(g) = (R)0;
-        if (id >= a.npf) ok = false;
+    for (int g0 = 0; g0 < n; g0 += 4) {
+        uint16_t ti[4];
+        R tp[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (g0 + k < n) {
+                ti[k] = __ldg(&a.as[(int64_t)(1 + g0 + k) * S + c]);
+                tp[k] = __ldg(&a.phi[(int64_t)(g0 + k) * S + c]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (g0 + k < n) {
+                sc.ID(g0 + k) = ti[k];
+                sc.PHI(g0 + k) = tp[k];
+                sc.LAP(g0 + k) = (R)0;
+                if (ti[k] >= a.npf) ok = false;
+            }
+        }
     }
     if (!ok) {
         atomicOr(a.err, ERR_BADSET);
@@ -193,7 +233,7 @@ __device__ __forceinline__ int load_and_gather(const PfArgs<R> &a, const CellInd
 #pragma unroll
     for (int f = 0; f < 3 * DIM; f++) {
         const int nn = (int)(nnp >> (4 * f) & 15u);
-        if (nn) gather_face<R, EXACT>(a, sc, n, face_nb<DIM, R>(a, ci, f), nn, f >= DIM && f < 2 * DIM);
+        if (nn) gather_face<PM, R, EXACT>(a, sc, n, face_nb<DIM, R>(a, ci, f), nn, f >= DIM && f < 2 * DIM);
     }
     return n;
 }

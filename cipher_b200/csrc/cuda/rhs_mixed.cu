@@ -22,17 +22,22 @@
 #include "pf_gather.cuh"
 #include "pf_cell.cuh"
 
+#ifndef CIPHER_MIXED_BX
+#define CIPHER_MIXED_BX 32
+#define CIPHER_MIXED_BY 4
+#endif
+
 namespace cipher {
 
-constexpr int kMixedBlock = 128;
+constexpr int kBX = CIPHER_MIXED_BX, kBY = CIPHER_MIXED_BY, kMixedBlock = kBX * kBY;
 
-template <int DIM>
+template <int DIM, int PM>
 __global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_single(const PfArgs<float> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const CellIndex ci = cell_index(a.res);
+    const CellIndex ci = cell_index<kBX, kBY>(a.res);
     const SlotColumns<float> sc = slot_columns<float>(smem, a.P, blockDim.x, threadIdx.x, false);
-    const int n = load_and_gather<DIM, float, false>(a, ci, sc);
+    const int n = load_and_gather<DIM, PM, float, false>(a, ci, sc);
     if (!ci.live) return;
     const int64_t S = a.stride, c = ci.c;
     uint32_t act = 0;
@@ -78,13 +83,13 @@ __global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_single(const PfArg
     a.ftm[c] = (float)tr;
 }
 
-template <int DIM>
-__global__ void __launch_bounds__(64) k_rhs_pf_mixed_multi(const PfArgs<float> a)
+template <int DIM, int PM>
+__global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_multi(const PfArgs<float> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const CellIndex ci = cell_index(a.res);
+    const CellIndex ci = cell_index<kBX, kBY>(a.res);
     const SlotColumns<float> sc = slot_columns<float>(smem, a.P, blockDim.x, threadIdx.x, true);
-    const int n = load_and_gather<DIM, float, false>(a, ci, sc);
+    const int n = load_and_gather<DIM, PM, float, false>(a, ci, sc);
     const double T = n == 0 ? 0.0 : (double)a.tm[ci.c];
     cell_rates_ordered<float, false>(a, sc, n, ci.c, ci.live, T);
     if (!ci.live) return;
@@ -93,18 +98,26 @@ __global__ void __launch_bounds__(64) k_rhs_pf_mixed_multi(const PfArgs<float> a
     a.ftm[ci.c] = (float)tr;
 }
 
+template <int DIM, int PM>
+static void launch_pm(const PfArgs<float> &a, cudaStream_t s)
+{
+    dim3 grid((unsigned)((a.res[0] + kBX - 1) / kBX), (unsigned)((a.res[1] + kBY - 1) / kBY), (unsigned)a.res[2]);
+    if (a.single) {
+        size_t sm = slot_columns_bytes(a.P, kMixedBlock, 4, false);
+        k_rhs_pf_mixed_single<DIM, PM><<<grid, kMixedBlock, sm, s>>>(a);
+    } else {
+        size_t sm = slot_columns_bytes(a.P, kMixedBlock, 4, true);
+        k_rhs_pf_mixed_multi<DIM, PM><<<grid, kMixedBlock, sm, s>>>(a);
+    }
+}
+
 template <int DIM>
 static void launch_dim(const PfArgs<float> &a, cudaStream_t s)
 {
-    if (a.single) {
-        dim3 grid((unsigned)((a.res[0] + kMixedBlock - 1) / kMixedBlock), (unsigned)a.res[1], (unsigned)a.res[2]);
-        size_t sm = slot_columns_bytes(a.P, kMixedBlock, 4, false);
-        k_rhs_pf_mixed_single<DIM><<<grid, kMixedBlock, sm, s>>>(a);
-    } else {
-        dim3 grid((unsigned)((a.res[0] + 63) / 64), (unsigned)a.res[1], (unsigned)a.res[2]);
-        size_t sm = slot_columns_bytes(a.P, 64, 4, true);
-        k_rhs_pf_mixed_multi<DIM><<<grid, 64, sm, s>>>(a);
-    }
+    if (a.P <= 4) launch_pm<DIM, 4>(a, s);
+    else if (a.P <= 8) launch_pm<DIM, 8>(a, s);
+    else if (a.P <= 12) launch_pm<DIM, 12>(a, s);
+    else launch_pm<DIM, 16>(a, s);
 }
 
 cudaError_t launch_rhs_phasefield(const PfArgs<float> &a, int dim, cudaStream_t s)

@@ -20,15 +20,15 @@
 
 namespace cipher {
 
-constexpr int kFp64Block = 64;
+constexpr int kBX = 32, kBY = 2, kFp64Block = kBX * kBY;
 
-template <int DIM, bool SINGLE>
+template <int DIM, int PM, bool SINGLE>
 __global__ void __launch_bounds__(kFp64Block) k_rhs_pf_fp64(const PfArgs<double> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const CellIndex ci = cell_index(a.res);
+    const CellIndex ci = cell_index<kBX, kBY>(a.res);
     const SlotColumns<double> sc = slot_columns<double>(smem, a.P, blockDim.x, threadIdx.x, true);
-    const int n = load_and_gather<DIM, double, true>(a, ci, sc);
+    const int n = load_and_gather<DIM, PM, double, true>(a, ci, sc);
     const double T = (SINGLE || n == 0) ? 0.0 : a.tm[ci.c];
     cell_rates_ordered<double, SINGLE>(a, sc, n, ci.c, ci.live, T);
     if (!ci.live) return;
@@ -38,13 +38,22 @@ __global__ void __launch_bounds__(kFp64Block) k_rhs_pf_fp64(const PfArgs<double>
     a.ftm[ci.c] = tr;
 }
 
+template <int DIM, int PM>
+static void launch_pm(const PfArgs<double> &a, cudaStream_t s)
+{
+    dim3 grid((unsigned)((a.res[0] + kBX - 1) / kBX), (unsigned)((a.res[1] + kBY - 1) / kBY), (unsigned)a.res[2]);
+    size_t sm = slot_columns_bytes(a.P, kFp64Block, 8, true);
+    if (a.single) k_rhs_pf_fp64<DIM, PM, true><<<grid, kFp64Block, sm, s>>>(a);
+    else k_rhs_pf_fp64<DIM, PM, false><<<grid, kFp64Block, sm, s>>>(a);
+}
+
 template <int DIM>
 static void launch_dim(const PfArgs<double> &a, cudaStream_t s)
 {
-    dim3 grid((unsigned)((a.res[0] + kFp64Block - 1) / kFp64Block), (unsigned)a.res[1], (unsigned)a.res[2]);
-    size_t sm = slot_columns_bytes(a.P, kFp64Block, 8, true);
-    if (a.single) k_rhs_pf_fp64<DIM, true><<<grid, kFp64Block, sm, s>>>(a);
-    else k_rhs_pf_fp64<DIM, false><<<grid, kFp64Block, sm, s>>>(a);
+    if (a.P <= 4) launch_pm<DIM, 4>(a, s);
+    else if (a.P <= 8) launch_pm<DIM, 8>(a, s);
+    else if (a.P <= 12) launch_pm<DIM, 12>(a, s);
+    else launch_pm<DIM, 16>(a, s);
 }
 
 cudaError_t launch_rhs_phasefield(const PfArgs<double> &a, int dim, cudaStream_t s)
