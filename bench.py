@@ -61,10 +61,21 @@ def build_state(problem, mesh):
     return cb.diffuse_state_aos(problem, mesh, WORKLOAD["width"])
 
 
-def algorithmic_bytes(nsum: int, ncells: int, P: int, rb: int) -> int:
-    """Compulsory bytes of one RHS launch: each cell's active count and ids
-    (uint16), its active phi and T read once; all P phi slots and T of F
-    written once (neighbour values are re-reads served on chip)."""
+def survey_bytes_per_cell(P: int, D: int, S: int, rb: int) -> int:
+    """Compulsory bytes of one cell-update in the state format: the active
+    set (P+1 uint16), the P phi slots, D chemical potentials, P*S site
+    potentials and T read once; the P phi, D, P*S and T rates written once
+    (phi and T in `rb` bytes, chemistry fields in FP64; neighbour values are
+    re-reads served on chip)."""
+    reads = 2 * (P + 1) + rb * P + 8 * D + 8 * P * S + rb
+    writes = rb * P + 8 * D + 8 * P * S + rb
+    return reads + writes
+
+
+def state_exact_bytes(nsum: int, ncells: int, P: int, rb: int) -> int:
+    """Bytes of one phase-field RHS launch that the sparse state actually
+    holds: each cell's count, its active ids and active phi, and T read once;
+    all P phi slots and T of F written once."""
     reads = 2 * ncells + 2 * nsum + rb * nsum + rb * ncells
     writes = ncells * (rb * P + rb)
     return reads + writes
@@ -352,8 +363,10 @@ def run_cipher(args, rank, world, local_rank):
     peak, peak_src = hbm_peak()
     avg32 = statistics.mean(per32) / 1e3
     avg64 = statistics.mean(per64) / 1e3
-    b32 = algorithmic_bytes(nsum, ncells, Pcap, 4)
-    b64 = algorithmic_bytes(nsum, ncells, Pcap, 8)
+    b32 = survey_bytes_per_cell(Pcap, 0, 0, 4) * ncells
+    b64 = survey_bytes_per_cell(Pcap, 0, 0, 8) * ncells
+    e32 = state_exact_bytes(nsum, ncells, Pcap, 4)
+    e64 = state_exact_bytes(nsum, ncells, Pcap, 8)
     ach32 = b32 / avg32 / 1e9
     ach64 = b64 / avg64 / 1e9
     tr32 = traffic_per_launch("mixed")
@@ -385,12 +398,15 @@ def run_cipher(args, rank, world, local_rank):
                    "mean_active_phases": nsum / ncells, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (no flush)"},
         "fp64": {"value": value64, "unit": UNIT, "ms_per_step": tot64 / args.steps,
-                 "roofline_frac": ach64 / peak},
+                 "roofline_frac": ach64 / peak, "algorithmic_bytes_per_launch": b64,
+                 "state_exact_roofline_frac": e64 / avg64 / 1e9 / peak},
         "mixed_speedup_vs_fp64": value / value64,
         "mixed_rel_err_vs_fp64": rel_err,
         "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak,
                      "traffic": tr32, "peak_source": peak_src, "algorithmic_bytes_per_launch": b32,
-                     "kernel": "k_rhs_phasefield<3,12,float>"},
+                     "bytes_per_cell_update": b32 // ncells, "fp64_format_frac": b64 / avg32 / 1e9 / peak,
+                     "state_exact_bytes_per_launch": e32, "state_exact_frac": e32 / avg32 / 1e9 / peak,
+                     "kernel": "k_rhs_pf_mixed_single<3,12>"},
         "cpu_baseline": cpu,
         "e2e": {"value": ncells * e2e_steps * world / (tot_e2e / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": aos_bytes, "d2h_bytes_per_step": aos_bytes,
