@@ -30,6 +30,9 @@ INTERP_LINEAR, INTERP_QUADRATIC, INTERP_CUBIC = 0, 1, 2
 BC_NEUMANN, BC_DIRICHLET, BC_NONE = 0, 1, 2
 SOURCE_SINK, SOURCE_RANDOM = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
+ALLOY_SEGREGATION, ALLOY_ITF_MOBILITY, ALLOY_ACTIVATION, ALLOY_THERMAL = 0x01, 0x02, 0x04, 0x08
+ALLOY_SOURCES, ALLOY_WALLS, ALLOY_TEMP_RATE, ALLOY_MIXED_MODELS = 0x10, 0x20, 0x40, 0x80
+ALLOY_ALL = 0x7F
 
 OK = 0
 E_ARG, E_NOMEM, E_CAP, E_NONFINITE, E_CUDA, E_TIMEOUT, E_UNSUPPORTED, E_STEP = range(1, 9)
@@ -140,6 +143,8 @@ _SIGNATURES = [
     ("cipher_voronoi", C.c_int, [C.c_int, C.POINTER(C.c_int32), C.c_int, C.c_uint64, C.POINTER(C.c_int32),
                                  C.POINTER(C.c_double)]),
     ("cipher_rand_uniform", C.c_double, [C.POINTER(C.c_uint64)]),
+    ("cipher_problem_alloy", C.c_int,
+     [C.c_int, C.POINTER(C.c_int32), C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint, C.POINTER(PP)]),
     ("cipher_mesh_uniform", C.c_int, [PP, C.c_int, C.c_int, C.POINTER(MP)]),
     ("cipher_mesh_free", None, [MP]),
     ("cipher_initial_state_aos", C.c_int, [PP, MP, C.POINTER(C.c_double)]),
@@ -151,6 +156,7 @@ _SIGNATURES = [
     ("cipher_rhs", C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_poststep", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_ctx_check", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("cipher_chem_init", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_poststep_noalloc", C.c_int, [C.POINTER(GridDesc), C.c_void_p, C.c_void_p]),
     ("cipher_state_from_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_state_to_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

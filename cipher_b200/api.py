@@ -35,6 +35,19 @@ class Problem:
                 "cipher_problem_grain_growth")
         return cls(out)
 
+    @classmethod
+    def alloy(cls, dim: int, res, model: str = "calphad2sl", ncp: int = 4, nprecip: int = 20, cap: int = 15,
+              seed: int = 1, features: int = 0) -> "Problem":
+        """Seeded alloy problem (cipher_problem_alloy): two matrix grains with
+        `nprecip` precipitates; `features` is a mask of the ALLOY_* bits."""
+        lib = L.load()
+        mid = {"quadratic": L.CHEM_QUADRATIC, "calphaddis": L.CHEM_CALPHADDIS, "calphad2sl": L.CHEM_CALPHAD2SL}[model]
+        r = (C.c_int32 * 3)(*(list(res) + [1] * (3 - len(res))))
+        out = L.PP()
+        L.check(lib.cipher_problem_alloy(dim, r, mid, ncp, nprecip, cap, seed, features, C.byref(out)),
+                "cipher_problem_alloy")
+        return cls(out)
+
     @property
     def s(self) -> L.ProblemStruct:
         return self.ptr.contents
@@ -214,6 +227,11 @@ class Context:
 
     def check(self, stream=None):
         L.check(self._lib.cipher_ctx_check(self.ptr, _stream_handle(stream)), "cipher_ctx_check")
+
+    def chem_init(self, X, stream=None):
+        """EX and mu of an initial state from the materials' c0 (SetUpProblem)."""
+        L.check(self._lib.cipher_chem_init(self.ptr, C.c_void_p(_ptr(X)), _stream_handle(stream)),
+                "cipher_chem_init")
 
     def RHSFunction(self, ts: TSView, ftime: float, X, F) -> int:
         """Reference-shaped callback: F = RHS(ftime, X); returns 0 like PetscErrorCode."""

@@ -73,12 +73,18 @@ struct cipher_ctx {
     int P, npf, ncp, ndp, S, nmat;
     cipher_state_layout lay;
     cipher_aos_layout aos;
+    int general;                  /* 1: chemistry / heat / boundary kernels (rhs_general.cu) */
     int single;
-    double sig0, mob0, wid0, tj0, ffactor, vol, junctionpenalty;
+    double sig0, mob0, wid0, tj0, ffactor, vol, junctionpenalty, delta;
     int has_temp_rate;
     double temp_rate;
+    int interp, nbcs;
+    DevBC bcs[CIPHER_MAXBC];
     int32_t *d_itflist;
     DevInterface *d_itfs;
+    cipher_material *d_mat;
+    int32_t *d_pmm;
+    double *d_comp, *d_mob, *d_tcond;
     uint16_t *d_pruned;
     double *d_ex_init;
     int *d_err;
@@ -90,29 +96,47 @@ struct cipher_ctx {
 
 static int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 
+/* problems the general kernels take: everything the reference's RHS does on
+ * a uniform grid except gradient-based anisotropy and random sources (which
+ * call rand() inside the RHS) */
 static int problem_supported(const cipher_problem *p, char *why, size_t len)
 {
     if (p->gradient_calculation) { snprintf(why, len, "gradient_calculation (anisotropy) is not implemented"); return 0; }
-    if (p->ndp != 0) { snprintf(why, len, "chemistry (ncp > 1) is not implemented on the device yet"); return 0; }
-    if (p->nbcs != 0) { snprintf(why, len, "boundary conditions are not implemented on the device yet"); return 0; }
+    if (p->ncp < 1 || p->ncp > CIPHER_MAXCP || p->ndp != p->ncp - 1) { snprintf(why, len, "bad component count"); return 0; }
+    if (p->nbcs < 0 || p->nbcs > CIPHER_MAXBC) { snprintf(why, len, "bad boundary condition count"); return 0; }
     for (int m = 0; m < p->nmat; m++) {
         const cipher_material *mat = &p->material[m];
-        if (mat->model != CIPHER_CHEM_NONE) { snprintf(why, len, "material %d: chemical model needs ncp > 1", m); return 0; }
-        if (mat->ref.n != 0 || mat->ref.logcoeff != 0.0) { snprintf(why, len, "material %d: non-zero reference energy", m); return 0; }
-        if (mat->tconductivity.n || mat->specific_heat.n || mat->latent_heat.n) {
+        if (mat->model < CIPHER_CHEM_QUADRATIC || mat->model > CIPHER_CHEM_NONE) { snprintf(why, len, "material %d: unknown model", m); return 0; }
+        if (p->ndp == 0 && mat->model != CIPHER_CHEM_NONE) { snprintf(why, len, "material %d: chemical model needs ncp > 1", m); return 0; }
+        if (p->ndp == 0 && (mat->tconductivity.n || mat->specific_heat.n || mat->latent_heat.n)) {
             snprintf(why, len, "material %d: thermal model without chemistry reads an unset temperature in the reference", m);
             return 0;
         }
-        if (mat->nsources) { snprintf(why, len, "material %d: sources need chemistry", m); return 0; }
+        if (mat->model == CIPHER_CHEM_CALPHAD2SL && p->maxsites < 2) { snprintf(why, len, "material %d: two sublattices need maxsites 2", m); return 0; }
+        for (int s = 0; s < mat->nsources; s++)
+            if (mat->sources[s].model != CIPHER_SOURCE_SINK) { snprintf(why, len, "material %d: random sources are not reproducible", m); return 0; }
     }
     for (int i = 0; i < p->nf; i++)
-        if (p->interface[i].has_potential || p->interface[i].nsources || p->interface[i].energy_naniso ||
-            p->interface[i].mobility_naniso) {
-            snprintf(why, len, "interface %d: segregation, sources or anisotropy need chemistry/gradients", i);
-            return 0;
-        }
+        for (int s = 0; s < p->interface[i].nsources; s++)
+            if (p->interface[i].sources[s].model != CIPHER_SOURCE_SINK) { snprintf(why, len, "interface %d: random sources are not reproducible", i); return 0; }
     if (p->interpolation != CIPHER_INTERP_CUBIC && p->interpolation != CIPHER_INTERP_QUADRATIC &&
         p->interpolation != CIPHER_INTERP_LINEAR) { snprintf(why, len, "unknown interpolation"); return 0; }
+    return 1;
+}
+
+/* problems the phase-field-only kernels take: no chemistry, no heat, no
+ * boundary faces, no reference energies (grain growth) */
+static int phasefield_only(const cipher_problem *p)
+{
+    if (p->ndp != 0 || p->nbcs != 0) return 0;
+    if (p->interpolation == CIPHER_INTERP_LINEAR) return 0;
+    for (int m = 0; m < p->nmat; m++) {
+        const cipher_material *mat = &p->material[m];
+        if (mat->model != CIPHER_CHEM_NONE || mat->ref.n != 0 || mat->ref.logcoeff != 0.0) return 0;
+        if (mat->tconductivity.n || mat->specific_heat.n || mat->latent_heat.n || mat->nsources) return 0;
+    }
+    for (int i = 0; i < p->nf; i++)
+        if (p->interface[i].has_potential || p->interface[i].nsources) return 0;
     return 1;
 }
 
@@ -121,6 +145,11 @@ static void free_ctx(cipher_ctx *c)
     if (!c) return;
     cudaFree(c->d_itflist);
     cudaFree(c->d_itfs);
+    cudaFree(c->d_mat);
+    cudaFree(c->d_pmm);
+    cudaFree(c->d_comp);
+    cudaFree(c->d_mob);
+    cudaFree(c->d_tcond);
     cudaFree(c->d_pruned);
     cudaFree(c->d_ex_init);
     cudaFree(c->d_err);
@@ -151,7 +180,9 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
         return set_error(CIPHER_E_UNSUPPORTED, "more than 2^31 cells on one context");
     char why[256];
     if (!problem_supported(p, why, sizeof(why))) return set_error(CIPHER_E_UNSUPPORTED, "%s", why);
-    /* the linear interpolant is not used by the phase-field-only kernel (no chemistry) */
+    for (int a = 0; a < p->npf; a++)
+        if (p->phasematerialmapping[a] < 0 || p->phasematerialmapping[a] >= p->nmat)
+            return set_error(CIPHER_E_ARG, "phase %d maps to material %d", a, p->phasematerialmapping[a]);
 
     CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
     cipher_ctx *c = (cipher_ctx *)calloc(1, sizeof(cipher_ctx));
@@ -172,6 +203,19 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
     c->S = p->maxsites * p->ndp;
     c->nmat = p->nmat;
     c->junctionpenalty = p->junctionpenalty;
+    c->general = !phasefield_only(p);
+    c->interp = p->interpolation;
+    c->delta = m->cellgeom[0];
+    c->nbcs = p->nbcs;
+    for (int b = 0; b < p->nbcs; b++) {
+        const cipher_bc *bc = &p->bcs[b];
+        DevBC &d = c->bcs[b];
+        d.label = bc->boundaryid;
+        d.chem_type = bc->chem_bctype;
+        d.thermal_type = bc->thermal_bctype;
+        d.thermal_val = bc->thermal_bcval;
+        for (int k = 0; k < CIPHER_MAXCP; k++) { d.chem_val[k] = bc->chem_bcval[k]; d.chem_on[k] = bc->chem_bcbool[k]; }
+    }
     c->has_temp_rate = p->has_temperature_rate;
     c->temp_rate = p->has_temperature_rate ? p->temperature_rate[p->currentloadcase] : 0.0;
     c->aos = cipher_problem_aos_layout(p);
@@ -231,7 +275,7 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
         c->tj0 = t;
     }
     cudaError_t e;
-    if (!single) {
+    if (!single || c->general) {
         for (int a = 0; a < p->npf; a++)
             for (int b = a + 1; b < p->npf; b++) {
                 int i = p->interfacelist[a * p->npf + b];
@@ -255,11 +299,27 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
             h[i].has_mobilityc = s->has_mobilityc;
             memcpy(h[i].potential, s->potential, sizeof(h[i].potential));
             memcpy(h[i].mobilityc, s->mobilityc, sizeof(h[i].mobilityc));
+            h[i].nsources = s->nsources;
+            memcpy(h[i].sources, s->sources, sizeof(h[i].sources));
         }
         e = cudaMalloc(&c->d_itfs, (size_t)p->nf * sizeof(DevInterface));
         if (e == cudaSuccess) e = cudaMemcpy(c->d_itfs, h, (size_t)p->nf * sizeof(DevInterface), cudaMemcpyHostToDevice);
         free(h);
         if (e != cudaSuccess) { free_ctx(c); return cuda_fail(e, "interface table"); }
+    }
+    if (c->general) {
+        size_t nb = (size_t)p->nmat * sizeof(cipher_material);
+        if ((e = cudaMalloc(&c->d_mat, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc materials"); }
+        if ((e = cudaMemcpy(c->d_mat, p->material, nb, cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy materials"); }
+        nb = (size_t)p->npf * sizeof(int32_t);
+        if ((e = cudaMalloc(&c->d_pmm, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc phase map"); }
+        if ((e = cudaMemcpy(c->d_pmm, p->phasematerialmapping, nb, cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy phase map"); }
+        if (c->ndp) {
+            nb = (size_t)c->ncp * c->stride * sizeof(double);
+            if ((e = cudaMalloc(&c->d_comp, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc composition"); }
+            if ((e = cudaMalloc(&c->d_mob, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc mobility"); }
+            if ((e = cudaMalloc(&c->d_tcond, (size_t)c->stride * sizeof(double))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc conductivity"); }
+        }
     }
     if ((e = cudaMalloc(&c->d_pruned, (size_t)(c->P + 1) * c->stride * sizeof(uint16_t))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc pruned"); }
     if ((e = cudaMalloc(&c->d_err, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc err"); }
@@ -330,6 +390,63 @@ static PfArgs<R> pf_args(const cipher_ctx *c, const void *X, void *F)
     return a;
 }
 
+template <typename R>
+static GenArgs<R> gen_args(const cipher_ctx *c, const void *X, void *F)
+{
+    GenArgs<R> a;
+    memset(&a, 0, sizeof(a));
+    const char *x = (const char *)X;
+    char *f = (char *)F;
+    a.ncells = c->ncells;
+    a.stride = c->stride;
+    for (int d = 0; d < 3; d++) { a.res[d] = c->res[d]; a.per[d] = c->per[d]; }
+    a.P = c->P;
+    a.npf = c->npf;
+    a.ncp = c->ncp;
+    a.ndp = c->ndp;
+    a.SP = c->S;
+    a.interp = c->interp;
+    a.ffactor = c->ffactor;
+    a.vol = c->vol;
+    {
+        int ex;
+        double mant = frexp(c->vol, &ex);
+        if (c->ffactor == 1.0 && c->vol == 1.0) a.geom_mode = 2;
+        else if (mant == 0.5) a.geom_mode = 1;
+        else a.geom_mode = 0;
+        a.inv_vol = 1.0 / c->vol;
+    }
+    a.delta = c->delta;
+    a.junctionpenalty = c->junctionpenalty;
+    a.has_temp_rate = c->has_temp_rate;
+    a.temp_rate = c->temp_rate;
+    a.itflist = c->d_itflist;
+    a.itfs = c->d_itfs;
+    a.chem.mat = c->d_mat;
+    a.chem.pmm = c->d_pmm;
+    a.chem.ncp = c->ncp;
+    a.chem.ndp = c->ndp;
+    a.chem.nmat = c->nmat;
+    a.nbcs = c->nbcs;
+    for (int b = 0; b < c->nbcs; b++) a.bcs[b] = c->bcs[b];
+    a.as = (const uint16_t *)(x + c->lay.as_offset);
+    a.phi = (const R *)(x + c->lay.pf_offset);
+    a.dp = (const double *)(x + c->lay.dp_offset);
+    a.ex = (const double *)(x + c->lay.ex_offset);
+    a.tm = (const R *)(x + c->lay.tm_offset);
+    a.comp = c->d_comp;
+    a.mob = c->d_mob;
+    a.tcond = c->d_tcond;
+    if (f) {
+        a.fphi = (R *)(f + c->lay.pf_offset);
+        a.fdp = (double *)(f + c->lay.dp_offset);
+        a.fex = (double *)(f + c->lay.ex_offset);
+        a.ftm = (R *)(f + c->lay.tm_offset);
+    }
+    a.err = c->d_err;
+    return a;
+}
+
 extern "C" int cipher_rhs(cipher_ctx *c, double t, const void *X, void *F, void *stream)
 {
     (void)t;
@@ -337,8 +454,13 @@ extern "C" int cipher_rhs(cipher_ctx *c, double t, const void *X, void *F, void 
     if (X == F) return set_error(CIPHER_E_ARG, "X and F must not alias");
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e;
-    if (c->precision == CIPHER_PREC_FP64) e = launch_rhs_phasefield(pf_args<double>(c, X, F), c->dim, s);
-    else e = launch_rhs_phasefield(pf_args<float>(c, X, F), c->dim, s);
+    if (c->general) {
+        if (c->precision == CIPHER_PREC_FP64) e = launch_rhs_general(gen_args<double>(c, X, F), c->dim, s);
+        else e = launch_rhs_general(gen_args<float>(c, X, F), c->dim, s);
+    } else {
+        if (c->precision == CIPHER_PREC_FP64) e = launch_rhs_phasefield(pf_args<double>(c, X, F), c->dim, s);
+        else e = launch_rhs_phasefield(pf_args<float>(c, X, F), c->dim, s);
+    }
     if (e != cudaSuccess) return cuda_fail(e, "rhs launch");
     return CIPHER_OK;
 }
@@ -360,6 +482,11 @@ static PostArgs<R> post_args(const cipher_ctx *c, void *X)
     a.tm = (const R *)(x + c->lay.tm_offset);
     a.pruned = c->d_pruned;
     a.ex_init = c->d_ex_init;
+    a.chem.mat = c->d_mat;
+    a.chem.pmm = c->d_pmm;
+    a.chem.ncp = c->ncp;
+    a.chem.ndp = c->ndp;
+    a.chem.nmat = c->nmat;
     a.err = c->d_err;
     return a;
 }
@@ -386,6 +513,22 @@ extern "C" int cipher_poststep(cipher_ctx *c, void *X, void *stream)
     if (rc) return rc;
     if (flags & ERR_CAP) return set_error(CIPHER_E_CAP, "active-set superset exceeds the cap P=%d", c->P);
     if (flags & ERR_BADSET) return set_error(CIPHER_E_ARG, "state holds an active count outside 1..P");
+    return CIPHER_OK;
+}
+
+/* explicit site potentials and chemical potentials of an initial state
+ * whose sets, phi and T are filled (src/init.c:1790-1823) */
+extern "C" int cipher_chem_init(cipher_ctx *c, void *X, void *stream)
+{
+    if (!c || !X) return set_error(CIPHER_E_ARG, "NULL argument");
+    if (!c->ndp) return CIPHER_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    char *x = (char *)X;
+    double *ex = (double *)(x + c->lay.ex_offset), *dp = (double *)(x + c->lay.dp_offset);
+    cudaError_t e;
+    if (c->precision == CIPHER_PREC_FP64) e = launch_chem_init(gen_args<double>(c, X, nullptr), ex, dp, s);
+    else e = launch_chem_init(gen_args<float>(c, X, nullptr), ex, dp, s);
+    if (e != cudaSuccess) return cuda_fail(e, "chem init launch");
     return CIPHER_OK;
 }
 

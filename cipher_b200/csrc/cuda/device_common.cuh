@@ -25,6 +25,16 @@ struct DevInterface {
     int has_potential, has_mobilityc;
     double potential[CIPHER_MAXCP];
     double mobilityc[CIPHER_MAXCP];
+    int nsources;
+    cipher_source sources[CIPHER_MAXSRC];
+};
+
+/* material tables on the device: the host structs of cipher_problem.h
+ * copied unchanged, and the phase -> material map */
+struct ChemTables {
+    const cipher_material *mat;      /* [nmat] */
+    const int32_t *pmm;              /* [npf] */
+    int ncp, ndp, nmat;
 };
 
 /* error flags raised by kernels (bit mask); never a trap */

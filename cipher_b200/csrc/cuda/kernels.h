@@ -38,6 +38,53 @@ struct PfArgs {
 cudaError_t launch_rhs_phasefield(const PfArgs<double> &a, int dim, cudaStream_t s);
 cudaError_t launch_rhs_phasefield(const PfArgs<float> &a, int dim, cudaStream_t s);
 
+/* one boundary condition, flattened (BOUNDARYCONDITIONS, src/typedef.h:243-248) */
+struct DevBC {
+    int label, chem_type, thermal_type;
+    double chem_val[CIPHER_MAXCP];
+    int chem_on[CIPHER_MAXCP];
+    double thermal_val;
+};
+
+/* arguments of the general RHS on a uniform grid: chemistry, heat,
+ * boundary faces, several interfaces and materials */
+template <typename R>
+struct GenArgs {
+    int64_t ncells, stride;
+    int res[3];
+    int per[3];
+    int P, npf, ncp, ndp, SP;     /* SP = site potentials per phase (maxsites*ndp) */
+    int interp;
+    double ffactor, vol, inv_vol;
+    int geom_mode;
+    double delta;                 /* cell size (cellgeom) */
+    double junctionpenalty;
+    int has_temp_rate;
+    double temp_rate;
+    const int32_t *itflist;
+    const DevInterface *itfs;
+    ChemTables chem;
+    int nbcs;
+    DevBC bcs[CIPHER_MAXBC];
+    const uint16_t *as;
+    const R *phi;
+    const double *dp;
+    const double *ex;
+    const R *tm;
+    double *comp, *mob, *tcond;   /* per-cell scratch: [ncp][stride], [ncp][stride], [stride] */
+    R *fphi;
+    double *fdp, *fex;
+    R *ftm;
+    int *err;
+};
+
+cudaError_t launch_rhs_general(const GenArgs<double> &a, int dim, cudaStream_t s);
+cudaError_t launch_rhs_general(const GenArgs<float> &a, int dim, cudaStream_t s);
+/* EX of every listed phase and mu of the majority phase from the materials'
+ * c0 at the cell temperature (src/init.c:1790-1823) */
+cudaError_t launch_chem_init(const GenArgs<double> &a, double *ex, double *dp, cudaStream_t s);
+cudaError_t launch_chem_init(const GenArgs<float> &a, double *ex, double *dp, cudaStream_t s);
+
 /* per-step active-set update on a uniform grid (src/cipher.c:869-974) */
 template <typename R>
 struct PostArgs {
@@ -51,6 +98,7 @@ struct PostArgs {
     const R *tm;
     uint16_t *pruned;             /* scratch: pruned sets, [P+1][stride] */
     const double *ex_init;        /* [npf*S] explicit potential of c0 at T0 per phase, or NULL */
+    ChemTables chem;              /* with chem.mat set, new phases get SitepotentialExplicit(c0, T) */
     int *err;
 };
 

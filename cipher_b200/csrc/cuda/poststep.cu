@@ -9,7 +9,8 @@
  *   k_post_union : superset = own pruned set U pruned sets of the face
  *                  neighbours (sorted merge, src/utility.c:195-230); keep phi
  *                  and EX of surviving phases, zero phi and initialise EX of
- *                  new phases, write the superset.  A superset above P raises
+ *                  new phases (SitepotentialExplicit of the material's c0 at
+ *                  the cell temperature), write the superset.  A superset above P raises
  *                  the cap flag and leaves that cell's set unchanged.
  *
  * The projection and the TOL test run in FP64 for both precisions, so the
@@ -19,6 +20,7 @@
 #include <cuda_runtime.h>
 #include "device_common.cuh"
 #include "kernels.h"
+#include "models.cuh"
 
 namespace cipher {
 
@@ -165,10 +167,20 @@ __global__ void __launch_bounds__(256) k_post_union(const PostArgs<R> a)
      * SitepotentialExplicit(c0) (src/cipher.c:953-964) */
     if (a.S > 0) {
         double exss[PM * 2 * CIPHER_MAXCP];
-        for (int g = 0; g < ns; g++)
-            for (int q = 0; q < a.S; q++)
-                exss[g * a.S + q] = from[g] >= 0 ? a.ex[(int64_t)(from[g] * a.S + q) * S + c]
-                                                 : a.ex_init[(int64_t)sup[g] * a.S + q];
+        const double T = (double)a.tm[c];
+        for (int g = 0; g < ns; g++) {
+            if (from[g] >= 0) {
+                for (int q = 0; q < a.S; q++) exss[g * a.S + q] = a.ex[(int64_t)(from[g] * a.S + q) * S + c];
+            } else if (a.chem.mat) {
+                /* slots past the phase's own sites are never read; they start at 0 */
+                const cipher_material &mat = material_of(a.chem, sup[g]);
+                for (int q = 0; q < a.S; q++) exss[g * a.S + q] = 0.0;
+                sitepot_explicit(a.chem, sup[g], mat.c0, T, &exss[g * a.S]);
+            } else {
+                for (int q = 0; q < a.S; q++)
+                    exss[g * a.S + q] = a.ex_init ? a.ex_init[(int64_t)sup[g] * a.S + q] : 0.0;
+            }
+        }
         for (int g = 0; g < ns; g++)
             for (int q = 0; q < a.S; q++) a.ex[(int64_t)(g * a.S + q) * S + c] = exss[g * a.S + q];
     }

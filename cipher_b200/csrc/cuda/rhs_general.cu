@@ -1,0 +1,581 @@
+/*
+ * rhs_general.cu - RHS of the coupled phase-field / chemistry / heat
+ * equations on uniform grids: every problem the device accepts that the
+ * phase-field-only kernels do not cover (chemical models, segregation
+ * potentials, interface mobility factors, solute sources, heat conduction,
+ * latent and specific heat, boundary faces, several interfaces).
+ *
+ * Replaces RHSFunction (src/cipher.c:27-681) in two launches:
+ *   k_chem_cell : per cell (src/cipher.c:148-233): site fractions of every
+ *                 active phase at the cell's potentials, the interpolated
+ *                 composition, lattice mobility (with the interface factors)
+ *                 and conductivity, stored in scratch planes that the face
+ *                 terms of both neighbours read;
+ *   k_rhs_general: per cell: the cell's faces gathered in the reference's
+ *                 face order (phase, mu and heat fluxes, 235-317), its
+ *                 boundary faces (319-389), then the cell terms (391-664):
+ *                 capillary and chemical driving forces, active set and
+ *                 constrained rate, dT/dt, dEX/dt and dmu/dt.
+ * Site fractions of the cell's own phases are recomputed in the second
+ * kernel instead of stored: the same arithmetic gives the same bits, and a
+ * few exponentials per phase cost less than 8*P*S bytes written and read.
+ *
+ * All arithmetic is FP64 in the reference's operation order (this unit is
+ * compiled with --fmad=false); phi and T are read and written in the state's
+ * storage type R (double, or float for the mixed layout).
+ */
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "device_common.cuh"
+#include "kernels.h"
+#include "models.cuh"
+
+namespace cipher {
+
+constexpr int kGenBlock = 128;
+
+/* phase interpolant h and its transposed derivative (src/utility.c:470-557) */
+__device__ inline void interpolant(int kind, const double *phi, int n, double *h)
+{
+    if (kind == CIPHER_INTERP_LINEAR) {
+        for (int g = 0; g < n; g++) h[g] = phi[g];
+        return;
+    }
+    if (n == 1) { h[0] = 1.0; return; }
+    double sum = 0.0;
+    for (int g = 0; g < n; g++) {
+        h[g] = kind == CIPHER_INTERP_QUADRATIC ? phi[g] * phi[g] : phi[g] * phi[g] * (3.0 - 2.0 * phi[g]);
+        sum += h[g];
+    }
+    for (int g = 0; g < n; g++) h[g] /= sum;
+}
+
+template <int PM>
+__device__ inline void interpolant_dT(int kind, double *v, const double *phi, int n)
+{
+    if (kind == CIPHER_INTERP_LINEAR) return;
+    if (n == 1) { v[0] = 0.0; return; }
+    double avg = 0.0, sum = 0.0;
+    for (int g = 0; g < n; g++) {
+        double w = kind == CIPHER_INTERP_QUADRATIC ? phi[g] * phi[g] : phi[g] * phi[g] * (3.0 - 2.0 * phi[g]);
+        sum += w;
+        avg += w * v[g];
+    }
+    for (int g = 0; g < n; g++) {
+        if (kind == CIPHER_INTERP_QUADRATIC) v[g] = 2.0 * phi[g] * (v[g] - avg / sum) / sum;
+        else v[g] = 6.0 * phi[g] * (1.0 - phi[g]) * (v[g] - avg / sum) / sum;
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ const DevInterface &pair_itf(const GenArgs<R> &a, int ia, int ib)
+{
+    return a.itfs[a.itflist[ia * a.npf + ib]];
+}
+
+/* implicit site potentials of slot g: stoichiometry*(mu - ci) - EX */
+template <typename R>
+__device__ __forceinline__ void slot_potential(const GenArgs<R> &a, const cipher_material &mat, const double *mu,
+                                               const double *ci, int64_t c, int g, double *pot)
+{
+    const int64_t S = a.stride;
+    for (int s = 0; s < mat.nsites; s++)
+        for (int d = 0; d < a.ndp; d++)
+            pot[s * a.ndp + d] = mat.stoichiometry[s] * (mu[d] - ci[d]) -
+                                 a.ex[(int64_t)(g * a.SP + s * a.ndp + d) * S + c];
+}
+
+/* segregation potential of the cell, sum_{k<j} h_k h_j V_kj (src/cipher.c:160-172) */
+template <typename R>
+__device__ __forceinline__ void segregation(const GenArgs<R> &a, const uint16_t *ids, const double *h, int n,
+                                            double *ci)
+{
+    for (int d = 0; d < CIPHER_MAXCP; d++) ci[d] = 0.0;
+    for (int k = 0; k < n; k++)
+        for (int j = k + 1; j < n; j++) {
+            const DevInterface &itf = pair_itf(a, ids[k], ids[j]);
+            if (itf.has_potential)
+                for (int d = 0; d < a.ndp; d++) ci[d] += h[k] * h[j] * itf.potential[d];
+        }
+}
+
+/* read a cell's set; returns n, or 0 (and raises ERR_BADSET) if invalid */
+template <int PM, typename R>
+__device__ __forceinline__ int load_set(const GenArgs<R> &a, int64_t c, uint16_t *ids, double *phi)
+{
+    const int64_t S = a.stride;
+    int n = a.as[c];
+    if (n < 1 || n > a.P || n > PM) {
+        atomicOr(a.err, ERR_BADSET);
+        return 0;
+    }
+    for (int g = 0; g < n; g++) {
+        ids[g] = a.as[(int64_t)(1 + g) * S + c];
+        phi[g] = (double)a.phi[(int64_t)g * S + c];
+        if (ids[g] >= a.npf) {
+            atomicOr(a.err, ERR_BADSET);
+            return 0;
+        }
+    }
+    return n;
+}
+
+/* ------------------------------------------------------------------ */
+/* per-cell composition, mobility and conductivity                      */
+/* ------------------------------------------------------------------ */
+
+template <int PM, typename R>
+__global__ void __launch_bounds__(kGenBlock) k_chem_cell(const GenArgs<R> a)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.ncells) return;
+    const int64_t S = a.stride;
+    const int ncp = a.ncp, ndp = a.ndp;
+    uint16_t ids[PM];
+    double phi[PM], h[PM];
+    const int n = load_set<PM>(a, c, ids, phi);
+    double mu[CIPHER_MAXCP], ci[CIPHER_MAXCP], mm[CIPHER_MAXCP], cc[CIPHER_MAXCP];
+    for (int d = 0; d < CIPHER_MAXCP; d++) { mm[d] = 0.0; cc[d] = 0.0; }
+    double tc = 0.0;
+    if (n > 0) {
+        const double T = (double)a.tm[c];
+        for (int d = 0; d < ndp; d++) mu[d] = a.dp[(int64_t)d * S + c];
+        interpolant(a.interp, phi, n, h);
+        segregation(a, ids, h, n, ci);
+        for (int g = 0; g < n; g++) {
+            const cipher_material &mat = material_of(a.chem, ids[g]);
+            double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP], me[CIPHER_MAXCP];
+            slot_potential(a, mat, mu, ci, c, g, pot);
+            sitefrac(a.chem, ids[g], pot, T, y);
+            mobility(a.chem, ids[g], y, T, me);
+            for (int d = 0; d < ncp; d++) mm[d] += h[g] * me[d];
+            for (int s = 0; s < mat.nsites; s++)
+                for (int d = 0; d < ncp; d++) cc[d] += h[g] * mat.stoichiometry[s] * y[s * ncp + d];
+            if (mat.tconductivity.n) tc += h[g] * tseries(T, mat.tconductivity);
+        }
+        for (int k = 0; k < n; k++)
+            for (int j = k + 1; j < n; j++) {
+                const DevInterface &itf = pair_itf(a, ids[k], ids[j]);
+                if (itf.has_mobilityc)
+                    for (int d = 0; d < ncp; d++) mm[d] *= exp(itf.mobilityc[d] / CIPHER_R_GAS / T);
+            }
+    }
+    for (int d = 0; d < ncp; d++) {
+        a.comp[(int64_t)d * S + c] = cc[d];
+        a.mob[(int64_t)d * S + c] = mm[d];
+    }
+    a.tcond[c] = tc;
+}
+
+/* ------------------------------------------------------------------ */
+/* the RHS                                                              */
+/* ------------------------------------------------------------------ */
+
+/* neighbour at face position f in the reference's face order: [0,DIM)
+ * below without wrap (descending d), [DIM,2DIM) own faces (ascending d),
+ * [2DIM,3DIM) wrapped around from above (ascending d); -1 if absent */
+__device__ __forceinline__ int64_t gen_face_nb(const int *res, const int *per, int64_t c, const int *co, int f,
+                                               const int DIM)
+{
+    const int64_t st[3] = {1, (int64_t)res[0], (int64_t)res[0] * res[1]};
+    if (f < DIM) {
+        const int e = DIM - 1 - f;
+        return co[e] > 0 ? c - st[e] : -1;
+    }
+    if (f < 2 * DIM) {
+        const int d = f - DIM;
+        if (co[d] < res[d] - 1) return c + st[d];
+        return (per[d] && res[d] > 1) ? c - (int64_t)(res[d] - 1) * st[d] : -1;
+    }
+    const int d = f - 2 * DIM;
+    return (co[d] == 0 && per[d] && res[d] > 1) ? c + (int64_t)(res[d] - 1) * st[d] : -1;
+}
+
+/* ff*x/vol as the reference forms it (src/cipher.c:281-282) */
+template <typename R>
+__device__ __forceinline__ double face_div(const GenArgs<R> &a, double x)
+{
+    if (a.geom_mode == 2) return x;
+    if (a.geom_mode == 1) return (a.ffactor * x) * a.inv_vol;
+    return (a.ffactor * x) / a.vol;
+}
+
+template <int PM, typename R>
+__global__ void __launch_bounds__(kGenBlock) k_rhs_general(const GenArgs<R> a, const int DIM)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.ncells) return;
+    const int64_t S = a.stride;
+    const int ncp = a.ncp, ndp = a.ndp, SP = a.SP;
+    const double PI = CIPHER_PI_D;
+    int co[3];
+    co[0] = (int)(c % a.res[0]);
+    co[1] = DIM > 1 ? (int)((c / a.res[0]) % a.res[1]) : 0;
+    co[2] = DIM > 2 ? (int)(c / ((int64_t)a.res[0] * a.res[1])) : 0;
+
+    uint16_t ids[PM];
+    double phi[PM], h[PM], lap[PM], pf[PM];
+    const int n = load_set<PM>(a, c, ids, phi);
+    if (n == 0) return;
+    const double T = (double)a.tm[c];
+    double mu[CIPHER_MAXCP], ldp[CIPHER_MAXCP];
+    for (int d = 0; d < ndp; d++) { mu[d] = a.dp[(int64_t)d * S + c]; ldp[d] = 0.0; }
+    double ltm = 0.0;
+    for (int g = 0; g < n; g++) lap[g] = 0.0;
+
+    /* ---- faces in the reference's face order (src/cipher.c:235-317) ---- */
+#pragma unroll 1
+    for (int f = 0; f < 3 * DIM; f++) {
+        const int64_t nb = gen_face_nb(a.res, a.per, c, co, f, DIM);
+        if (nb < 0) continue;
+        const bool self_L = f >= DIM && f < 2 * DIM;
+        const int64_t cl = self_L ? c : nb, cr = self_L ? nb : c;
+        const int nn = a.as[nb];
+        if (nn < 1 || nn > a.P) continue;          /* that cell's own thread raises the flag */
+        /* phase flux, gated on the L cell only (src/cipher.c:277) */
+        const bool gate = self_L ? (n > 1 || ids[0] > 1) : (nn > 1 || a.as[S + nb] > 1);
+        if (gate) {
+            int i = 0, j = 0;
+            while (i < n && j < nn) {
+                const uint16_t b = a.as[(int64_t)(1 + j) * S + nb];
+                if (ids[i] == b) {
+                    const double pn = (double)a.phi[(int64_t)j * S + nb];
+                    if (self_L) lap[i] += face_div(a, pn - phi[i]);
+                    else lap[i] -= face_div(a, phi[i] - pn);
+                    i++;
+                    j++;
+                } else if (ids[i] < b) {
+                    i++;
+                } else {
+                    j++;
+                }
+            }
+        }
+        /* chemical-potential flux with the Andersson-Agren frame (material.c:1125-1137) */
+        if (ndp) {
+            double me[CIPHER_MAXCP], ca[CIPHER_MAXCP], MB[(CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1)];
+            double dmu[CIPHER_MAXCP], fl[CIPHER_MAXCP];
+            for (int d = 0; d < ncp; d++) {
+                const double ml = a.mob[(int64_t)d * S + cl], mr = a.mob[(int64_t)d * S + cr];
+                const double cL = a.comp[(int64_t)d * S + cl], cR = a.comp[(int64_t)d * S + cr];
+                if (fabs(ml) > 1e-32 && fabs(mr) > 1e-32) me[d] = 2.0 * ml * mr / (ml + mr);
+                else me[d] = 0.0;
+                ca[d] = 2.0 * cL * cR / (cL + cR);
+            }
+            for (int i = 0; i < ndp; i++)
+                for (int j = 0; j < ndp; j++) {
+                    double acc = 0.0;
+                    for (int k = 0; k < ncp; k++)
+                        acc += ((j == k ? 1.0 : 0.0) - ca[j]) * ((k == i ? 1.0 : 0.0) - ca[i]) * me[k];
+                    MB[i * ndp + j] = acc;
+                }
+            for (int d = 0; d < ndp; d++) dmu[d] = a.dp[(int64_t)d * S + cr] - a.dp[(int64_t)d * S + cl];
+            matvec(fl, MB, dmu, ndp);
+            for (int d = 0; d < ndp; d++) {
+                if (self_L) ldp[d] += face_div(a, fl[d]);
+                else ldp[d] -= face_div(a, fl[d]);
+            }
+        }
+        /* heat flux */
+        if (a.tcond) {
+            const double tl = a.tcond[cl], tr = a.tcond[cr];
+            if (fabs(tl) > 1e-32 && fabs(tr) > 1e-32) {
+                const double ft = 2.0 * tl * tr / (tl + tr) * ((double)a.tm[cr] - (double)a.tm[cl]);
+                if (self_L) ltm += face_div(a, ft);
+                else ltm -= face_div(a, ft);
+            }
+        }
+    }
+
+    /* ---- boundary faces (src/cipher.c:319-389) ---- */
+    if (a.nbcs) {
+        const double dc = a.delta;
+        const double cf = 1.0 / ipow(dc, 2);
+        const double tcc = a.tcond ? a.tcond[c] : 0.0;
+        for (int b = 0; b < a.nbcs; b++) {
+            const DevBC &bc = a.bcs[b];
+#pragma unroll 1
+            for (int q = 0; q < 2 * DIM; q++) {
+                const int d = q >> 1;
+                if (a.per[d]) continue;
+                const bool on = (q & 1) ? co[d] == a.res[d] - 1 : co[d] == 0;
+                if (!on || bc.label != 2 * d + 1 + (q & 1)) continue;
+                double fd[CIPHER_MAXCP];
+                for (int k = 0; k < CIPHER_MAXCP; k++) fd[k] = 0.0;
+                if (bc.chem_type != CIPHER_BC_NONE) {
+                    if (bc.chem_type == CIPHER_BC_NEUMANN) {
+                        for (int k = 0; k < ndp; k++) if (bc.chem_on[k]) fd[k] = bc.chem_val[k] * dc;
+                    } else {
+                        for (int k = 0; k < ndp; k++)
+                            if (bc.chem_on[k]) fd[k] = a.mob[(int64_t)k * S + c] * (bc.chem_val[k] - mu[k]);
+                    }
+                }
+                double fluxt = 0.0;
+                if (bc.thermal_type == CIPHER_BC_NEUMANN) fluxt = tcc * bc.thermal_val * dc;
+                else if (bc.thermal_type == CIPHER_BC_DIRICHLET) fluxt = tcc * (bc.thermal_val - T);
+                if (bc.chem_type != CIPHER_BC_NONE)
+                    for (int k = 0; k < ndp; k++) ldp[k] += cf * fd[k];
+                if (bc.thermal_type != CIPHER_BC_NONE) ltm += cf * fluxt;
+            }
+        }
+    }
+
+    /* ---- cell terms (src/cipher.c:391-664) ---- */
+    interpolant(a.interp, phi, n, h);
+    double ci[CIPHER_MAXCP];
+    if (ndp) segregation(a, ids, h, n, ci);
+
+    /* pass over the phases: driving force, dEX/dt and the tangent sum */
+    double chem[PM], yw[PM * (CIPHER_MAXCP - 1)];
+    double cbar[CIPHER_MAXCP], dcdm[(CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1)];
+    for (int d = 0; d < CIPHER_MAXCP; d++) cbar[d] = 0.0;
+    for (int q = 0; q < (CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1); q++) dcdm[q] = 0.0;
+    for (int g = 0; g < n; g++) {
+        const cipher_material &mat = material_of(a.chem, ids[g]);
+        double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP];
+        if (ndp) {
+            slot_potential(a, mat, mu, ci, c, g, pot);
+            sitefrac(a.chem, ids[g], pot, T, y);
+        }
+        if (n > 1) {
+            chem[g] = chemenergy(a.chem, ids[g], y, mu, T);
+            for (int s = 0; s < mat.nsites; s++)
+                for (int d = 0; d < ndp; d++) cbar[d] += h[g] * mat.stoichiometry[s] * y[s * ncp + d];
+        }
+        if (ndp) {
+            for (int d = 0; d < ndp; d++) {
+                double w = 0.0;
+                for (int s = 0; s < mat.nsites; s++) w += mat.stoichiometry[s] * y[s * ncp + d];
+                yw[g * (CIPHER_MAXCP - 1) + d] = w;
+            }
+            /* explicit potential relaxation (src/cipher.c:570-581) */
+            double spx[2 * CIPHER_MAXCP];
+            sitepot_explicit(a.chem, ids[g], y, T, spx);
+            for (int s = 0; s < mat.nsites; s++)
+                for (int d = 0; d < ndp; d++) {
+                    const int64_t pl = (int64_t)(g * SP + s * ndp + d) * S + c;
+                    a.fex[pl] = mat.chempot_ex_kineticcoeff * (spx[s * ndp + d] - a.ex[pl]);
+                }
+            for (int q = mat.nsites * ndp; q < SP; q++) a.fex[(int64_t)(g * SP + q) * S + c] = 0.0;
+            double tpot[2 * 16], tex[2 * 16], tT[2 * CIPHER_MAXCP];
+            sitefrac_tangent(a.chem, ids[g], y, pot, T, tpot, tex, tT);
+            for (int s = 0; s < mat.nsites; s++)
+                for (int q = 0; q < ndp * ndp; q++)
+                    dcdm[q] += h[g] * mat.stoichiometry[s] * mat.stoichiometry[s] * tpot[s * ndp * ndp + q];
+        }
+    }
+    for (int q = n * SP; q < a.P * SP; q++) a.fex[(int64_t)q * S + c] = 0.0;
+
+    for (int g = 0; g < PM; g++) pf[g] = 0.0;
+    if (n > 1) {
+        /* capillary force with the triple-junction penalty (src/cipher.c:474-497) */
+        double cap[PM], unc[PM];
+        for (int g = 0; g < n; g++) cap[g] = 0.0;
+        for (int k = 0; k < n; k++) {
+            for (int j = k + 1; j < n; j++) {
+                double skj, mkj, wkj;
+                interface_props(pair_itf(a, ids[k], ids[j]), T, skj, mkj, wkj);
+                cap[k] -= skj * (phi[j] / wkj + lap[j] * wkj / PI / PI);
+                cap[j] -= skj * (phi[k] / wkj + lap[k] * wkj / PI / PI);
+                for (int i = j + 1; i < n; i++) {
+                    double s_, m_, w_, tj = 0.0, v;
+                    v = skj / wkj; tj = tj > v ? tj : v;
+                    interface_props(pair_itf(a, ids[k], ids[i]), T, s_, m_, w_);
+                    v = s_ / w_; tj = tj > v ? tj : v;
+                    interface_props(pair_itf(a, ids[j], ids[i]), T, s_, m_, w_);
+                    v = s_ / w_; tj = tj > v ? tj : v;
+                    tj *= a.junctionpenalty;
+                    cap[k] -= tj * phi[j] * phi[i];
+                    cap[j] -= tj * phi[k] * phi[i];
+                    cap[i] -= tj * phi[k] * phi[j];
+                }
+            }
+            cap[k] *= 8.0;
+            cap[k] += lap[k];
+        }
+        /* chemical driving force (src/cipher.c:499-522) */
+        for (int k = 0; k < n; k++)
+            for (int j = k + 1; j < n; j++) {
+                const DevInterface &itf = pair_itf(a, ids[k], ids[j]);
+                if (itf.has_potential) {
+                    double v = 0.0;
+                    for (int d = 0; d < ndp; d++) v += itf.potential[d] * cbar[d];
+                    chem[k] += v * h[j];
+                    chem[j] += v * h[k];
+                }
+            }
+        interpolant_dT<PM>(a.interp, chem, phi, n);
+        /* active set and constrained rate (src/cipher.c:524-555) */
+        double nact = 0.0;
+        uint32_t act = 0;
+        for (int g = 0; g < n; g++) unc[g] = 0.0;
+        for (int k = 0; k < n; k++) {
+            for (int j = k + 1; j < n; j++) {
+                double s_, m_, w_;
+                interface_props(pair_itf(a, ids[k], ids[j]), T, s_, m_, w_);
+                const double r = m_ * ((cap[k] - cap[j]) - (chem[k] - chem[j]) * 8.0 * sqrt(h[k] * h[j]) / PI);
+                unc[k] += r;
+                unc[j] -= r;
+            }
+            const bool on = (phi[k] > CIPHER_TOL && phi[k] < 1.0 - CIPHER_TOL) || (phi[k] < CIPHER_TOL && unc[k] > 0.0) ||
+                            (phi[k] > 1.0 - CIPHER_TOL && unc[k] < 0.0);
+            if (on) { act |= 1u << k; nact += 1.0; }
+        }
+        for (int k = 0; k < n; k++) {
+            if (!(act >> k & 1u)) continue;
+            for (int j = k + 1; j < n; j++) {
+                if (!(act >> j & 1u)) continue;
+                double s_, m_, w_;
+                interface_props(pair_itf(a, ids[k], ids[j]), T, s_, m_, w_);
+                const double r = m_ * ((cap[k] - cap[j]) - (chem[k] - chem[j]) * 8.0 * sqrt(h[k] * h[j]) / PI);
+                pf[k] += r;
+                pf[j] -= r;
+            }
+            pf[k] /= nact;
+        }
+    }
+    for (int g = 0; g < a.P; g++) a.fphi[(int64_t)g * S + c] = (R)(g < PM ? pf[g] : 0.0);
+
+    /* temperature rate (src/cipher.c:558-568) */
+    double cp = 0.0, tr = ltm;
+    for (int g = 0; g < n; g++) {
+        const cipher_material &mat = material_of(a.chem, ids[g]);
+        if (mat.specific_heat.n) cp += h[g] * tseries(T, mat.specific_heat);
+        if (mat.latent_heat.n) tr += pf[g] * tseries(T, mat.latent_heat);
+    }
+    if (cp != 0.0) tr /= cp;
+    if (a.has_temp_rate) tr += a.temp_rate;
+    a.ftm[c] = (R)tr;
+
+    if (!ndp) return;
+    /* composition rate and dmu/dt (src/cipher.c:583-662) */
+    const int DN = CIPHER_MAXCP - 1;
+    double cpv[PM * (CIPHER_MAXCP - 1)];
+    for (int q = 0; q < n * DN; q++) cpv[q] = 0.0;
+    for (int k = 0; k < n; k++)
+        for (int j = k + 1; j < n; j++) {
+            const DevInterface &itf = pair_itf(a, ids[k], ids[j]);
+            if (itf.has_potential)
+                for (int d = 0; d < ndp; d++) {
+                    cpv[k * DN + d] += itf.potential[d] * h[j];
+                    cpv[j * DN + d] += itf.potential[d] * h[k];
+                }
+        }
+    for (int g = 0; g < n; g++) {
+        double tmp[CIPHER_MAXCP];
+        for (int d = 0; d < ndp; d++) tmp[d] = cpv[g * DN + d];
+        matvec(&cpv[g * DN], dcdm, tmp, ndp);
+    }
+    double wdp[CIPHER_MAXCP];
+    for (int d = 0; d < CIPHER_MAXCP; d++) wdp[d] = 0.0;
+    if (n > 1) {
+        for (int d = 0; d < ndp; d++) {
+            double wpf[PM];
+            for (int g = 0; g < n; g++) wpf[g] = yw[g * DN + d] - cpv[g * DN + d];
+            interpolant_dT<PM>(a.interp, wpf, phi, n);
+            for (int g = 0; g < n; g++) wdp[d] -= pf[g] * wpf[g];
+        }
+    }
+    /* solute sources (material.c:295-351; sink model) */
+    double src[CIPHER_MAXCP], comp[CIPHER_MAXCP];
+    for (int d = 0; d < ncp; d++) { src[d] = 0.0; comp[d] = a.comp[(int64_t)d * S + c]; }
+    for (int k = 0; k < n; k++) {
+        const cipher_material &mat = material_of(a.chem, ids[k]);
+        for (int s = 0; s < mat.nsources; s++) {
+            double tmp[CIPHER_MAXCP];
+            for (int d = 0; d < ncp; d++) tmp[d] = mat.sources[s].rate[d] * (mat.sources[s].ceq[d] - comp[d]);
+            for (int d = 0; d < ncp; d++) src[d] += h[k] * h[k] * tmp[d];
+        }
+        for (int j = k + 1; j < n; j++) {
+            const DevInterface &itf = pair_itf(a, ids[k], ids[j]);
+            for (int s = 0; s < itf.nsources; s++) {
+                double tmp[CIPHER_MAXCP];
+                for (int d = 0; d < ncp; d++) tmp[d] = itf.sources[s].rate[d] * (itf.sources[s].ceq[d] - comp[d]);
+                for (int d = 0; d < ncp; d++) src[d] += 2.0 * h[k] * h[j] * tmp[d];
+            }
+        }
+    }
+    for (int d = 0; d < ndp; d++) wdp[d] += (ldp[d] + src[d]);
+    for (int g = 0; g < n; g++) {
+        const cipher_material &mat = material_of(a.chem, ids[g]);
+        double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP];
+        double tpot[2 * 16], tex[2 * 16], tT[2 * CIPHER_MAXCP];
+        slot_potential(a, mat, mu, ci, c, g, pot);
+        sitefrac(a.chem, ids[g], pot, T, y);
+        sitefrac_tangent(a.chem, ids[g], y, pot, T, tpot, tex, tT);
+        for (int s = 0; s < mat.nsites; s++) {
+            double dex[CIPHER_MAXCP];
+            for (int d = 0; d < ndp; d++) dex[d] = a.fex[(int64_t)(g * SP + s * ndp + d) * S + c];
+            matvec(&cpv[g * DN], &tex[s * ndp * ndp], dex, ndp);
+            for (int d = 0; d < ndp; d++)
+                wdp[d] -= h[g] * mat.stoichiometry[s] * (cpv[g * DN + d] + tT[s * ndp + d] * tr);
+        }
+    }
+    double dmdc[(CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1)], out[CIPHER_MAXCP];
+    invert_small(dmdc, dcdm, ndp);
+    matvec(out, dmdc, wdp, ndp);
+    for (int d = 0; d < ndp; d++) a.fdp[(int64_t)d * S + c] = out[d];
+}
+
+/* ------------------------------------------------------------------ */
+/* chemistry of the initial state                                       */
+/* ------------------------------------------------------------------ */
+
+template <int PM, typename R>
+__global__ void __launch_bounds__(kGenBlock) k_chem_init(const GenArgs<R> a, double *ex, double *dp)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.ncells) return;
+    const int64_t S = a.stride;
+    uint16_t ids[PM];
+    double phi[PM];
+    const int n = load_set<PM>(a, c, ids, phi);
+    if (n == 0) return;
+    const double T = (double)a.tm[c];
+    int own = 0;
+    for (int g = 1; g < n; g++)
+        if (phi[g] > phi[own]) own = g;
+    for (int q = 0; q < a.P * a.SP; q++) ex[(int64_t)q * S + c] = 0.0;
+    for (int g = 0; g < n; g++) {
+        const cipher_material &mat = material_of(a.chem, ids[g]);
+        double sp[2 * CIPHER_MAXCP];
+        sitepot_explicit(a.chem, ids[g], mat.c0, T, sp);
+        for (int q = 0; q < mat.nsites * a.ndp; q++) ex[(int64_t)(g * a.SP + q) * S + c] = sp[q];
+    }
+    const cipher_material &mo = material_of(a.chem, ids[own]);
+    double sp[2 * CIPHER_MAXCP], mu[CIPHER_MAXCP];
+    sitepot_total(a.chem, ids[own], mo.c0, T, sp);
+    for (int d = 0; d < a.ndp; d++) mu[d] = 0.0;
+    for (int s = 0; s < mo.nsites; s++)
+        for (int d = 0; d < a.ndp; d++) mu[d] += sp[s * a.ndp + d];
+    for (int d = 0; d < a.ndp; d++) dp[(int64_t)d * S + c] = mu[d];
+}
+
+/* ------------------------------------------------------------------ */
+/* launchers                                                            */
+/* ------------------------------------------------------------------ */
+
+template <typename R>
+static cudaError_t launch_gen(const GenArgs<R> &a, int dim, cudaStream_t s)
+{
+    const unsigned blocks = (unsigned)((a.ncells + kGenBlock - 1) / kGenBlock);
+    if (a.ndp) k_chem_cell<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a);
+    k_rhs_general<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a, dim);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rhs_general(const GenArgs<double> &a, int dim, cudaStream_t s) { return launch_gen(a, dim, s); }
+cudaError_t launch_rhs_general(const GenArgs<float> &a, int dim, cudaStream_t s) { return launch_gen(a, dim, s); }
+
+template <typename R>
+static cudaError_t launch_init(const GenArgs<R> &a, double *ex, double *dp, cudaStream_t s)
+{
+    const unsigned blocks = (unsigned)((a.ncells + kGenBlock - 1) / kGenBlock);
+    k_chem_init<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a, ex, dp);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_chem_init(const GenArgs<double> &a, double *ex, double *dp, cudaStream_t s) { return launch_init(a, ex, dp, s); }
+cudaError_t launch_chem_init(const GenArgs<float> &a, double *ex, double *dp, cudaStream_t s) { return launch_init(a, ex, dp, s); }
+
+}  // namespace cipher

@@ -69,6 +69,25 @@ int cipher_problem_grain_growth(int dim, const int32_t *res, int ngrains, int ca
                                 double energy, double mobility, double width,
                                 double molarvolume, double temperature0,
                                 cipher_problem **out);
+/* feature bits of cipher_problem_alloy */
+#define CIPHER_ALLOY_SEGREGATION   0x01u  /* segregation potentials on grain and phase boundaries */
+#define CIPHER_ALLOY_ITF_MOBILITY  0x02u  /* interface factors on the solute mobilities */
+#define CIPHER_ALLOY_ACTIVATION    0x04u  /* T-dependent interface energy and mobility */
+#define CIPHER_ALLOY_THERMAL       0x08u  /* specific heat, latent heat, conductivity */
+#define CIPHER_ALLOY_SOURCES       0x10u  /* solute sinks in the precipitates and on grain boundaries */
+#define CIPHER_ALLOY_WALLS         0x20u  /* x not periodic; chemical and thermal BCs on both walls */
+#define CIPHER_ALLOY_TEMP_RATE     0x40u  /* imposed cooling rate */
+#define CIPHER_ALLOY_MIXED_MODELS  0x80u  /* matrix calphaddis, precipitates calphad2sl */
+
+/* seeded alloy problem: two matrix grains (Voronoi) with nprecip spherical
+ * precipitates, ncp components, free-energy model `model` (quadratic,
+ * calphaddis or calphad2sl: matrix 1:1, precipitates 2:1 sublattices) with
+ * random coefficients, T = 700 K, interface width 4 cells, plus the
+ * CIPHER_ALLOY_* features.  No counterpart in the reference (which reads
+ * its tables from YAML); it fills the same tables. */
+int cipher_problem_alloy(int dim, const int32_t *res, int model, int ncp, int nprecip, int cap, uint64_t seed,
+                         unsigned features, cipher_problem **out);
+
 /* nearest-centre Voronoi map under the periodic metric, x fastest; the
  * seeded centres are returned in centres[ngrains*3] when it is not NULL */
 int cipher_voronoi(int dim, const int32_t *res, int ngrains, uint64_t seed, int32_t *voxel, double *centres);
@@ -136,6 +155,13 @@ int cipher_poststep(cipher_ctx *c, void *X, void *stream);
 /* synchronise `stream`, then read and clear the error flags the kernels
  * raise instead of trapping (bad active counts, cap overflow) */
 int cipher_ctx_check(cipher_ctx *c, void *stream);
+
+/* chemistry of an initial state whose sets, phi and T are filled (device):
+ * EX of every listed phase = SitepotentialExplicit(c0, T), mu = the summed
+ * Sitepotential(c0, T) of the phase with the largest phi (the voxel's own
+ * phase in a sharp state), as SetUpProblem does (src/init.c:1790-1823).
+ * No-op without chemistry. */
+int cipher_chem_init(cipher_ctx *c, void *X, void *stream);
 
 /* grid and state description for the allocation-free entry point */
 typedef struct cipher_grid_desc {

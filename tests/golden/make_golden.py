@@ -1,7 +1,7 @@
 """Generate the golden fixtures from the reference's own code.
 
-Each fixture is a small seeded grain-growth problem built with the library's
-host builders; the reference's RHSFunction and PostStep (compiled unmodified
+Each fixture is a small seeded grain-growth or alloy problem built with the
+library's host builders; the reference's RHSFunction and PostStep (compiled unmodified
 through the PETSc shim into oracle/_ref/libcipher_ref.so) produce the outputs:
 
   X      state in the reference AoS layout (owned cells)
@@ -33,6 +33,39 @@ CASES = [
 ]
 
 
+# alloy cases: (name, dim, res, model, ncp, nprecip, cap, seed, features, steps).  The
+# state is the SetUpProblem state of the restatement (the reference's init.c
+# needs libyaml), then `steps` explicit steps taken with the reference's own
+# RHSFunction and PostStep; F and Xpost come from the reference.
+ALLOY_CASES = [
+    ("alloy2sl_2d", 2, [16, 12], "calphad2sl", 4, 4, 8, 21, 0, 3),
+    ("alloydis_all_2d", 2, [16, 12], "calphaddis", 3, 4, 8, 22, 0xFF, 2),
+    ("alloyquad_all_3d", 3, [8, 8, 6], "quadratic", 3, 3, 8, 23, 0x7F, 2),
+]
+MODEL_ID = {"quadratic": 0, "calphaddis": 1, "calphad2sl": 2}
+
+
+def build_alloy(dim, res, model, ncp, nprecip, cap, seed, features):
+    P = cb.Problem.alloy(dim, res, model, ncp, nprecip, cap, seed, features)
+    M = cb.Mesh(P)
+    return P, M
+
+
+def evolve_with_reference(P, M, R, X, steps):
+    """explicit steps with the reference's RHS and PostStep; dt keeps the
+    largest phase-fraction change at 0.05 and mu changes at 2 %"""
+    A = P.aos
+    for _ in range(steps):
+        F = R.rhs(X)
+        fphi = np.abs(F[:, A.pf_offset:A.pf_offset + A.pf_size]).max()
+        fdp = np.abs(F[:, A.dp_offset:A.dp_offset + A.dp_size]).max()
+        mu = np.abs(X[:, A.dp_offset:A.dp_offset + A.dp_size]).max()
+        dt = min(0.05 / max(fphi, 1e-300), 0.02 * mu / max(fdp, 1e-300))
+        X = X + dt * F
+        assert R.poststep(X) == 0
+    return X
+
+
 def build_case(dim, res, ngrains, cap, seed, kind):
     P = cb.Problem.grain_growth(dim, res, ngrains, cap, seed)
     M = cb.Mesh(P)
@@ -53,6 +86,17 @@ def main():
                             meta=np.array([dim] + list(res) + [0] * (3 - len(res)) + [ng, cap, seed,
                                                                                         int(kind == "sharp")]))
         print(name, X.shape, "max|F|", np.abs(F).max())
+    for name, dim, res, model, ncp, npr, cap, seed, feats, steps in ALLOY_CASES:
+        P, M = build_alloy(dim, res, model, ncp, npr, cap, seed, feats)
+        X0 = oracle.port_initial_state(P, M)
+        with oracle.RefOracle(P, M) as R:
+            X = evolve_with_reference(P, M, R, X0, steps)
+            F = R.rhs(X)
+            Xp = X.copy()
+            assert R.poststep(Xp) == 0
+        meta = [dim] + list(res) + [0] * (3 - len(res)) + [MODEL_ID[model], ncp, npr, cap, seed, feats, steps]
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), X=X, F=F, Xpost=Xp, meta=np.array(meta))
+        print(name, X.shape, "max|F|", np.abs(F).max(), "mean n", X[:, 0].mean())
 
 
 if __name__ == "__main__":

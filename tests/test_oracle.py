@@ -18,25 +18,38 @@ import oracle
 GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
 
 
-def _case(meta):
+MODELS = {0: "quadratic", 1: "calphaddis", 2: "calphad2sl"}
+
+
+def _case(meta, X_fixture=None):
+    """Rebuild a fixture's problem and mesh; grain-growth fixtures (8 meta
+    entries) also rebuild their state, alloy fixtures (11) carry theirs."""
     dim = int(meta[0])
     res = [int(v) for v in meta[1:1 + dim]]
-    ng, cap, seed, sharp = (int(v) for v in meta[4:8])
-    P = cb.Problem.grain_growth(dim, res, ng, cap, seed)
+    if len(meta) == 8:
+        ng, cap, seed, sharp = (int(v) for v in meta[4:8])
+        P = cb.Problem.grain_growth(dim, res, ng, cap, seed)
+        M = cb.Mesh(P)
+        X = cb.initial_state_aos(P, M) if sharp else cb.diffuse_state_aos(P, M, 4.0)
+        return P, M, X
+    model, ncp, npr, cap, seed, feats = (int(v) for v in meta[4:10])
+    P = cb.Problem.alloy(dim, res, MODELS[model], ncp, npr, cap, seed, feats)
     M = cb.Mesh(P)
-    X = cb.initial_state_aos(P, M) if sharp else cb.diffuse_state_aos(P, M, 4.0)
-    return P, M, X
+    return P, M, X_fixture
 
 
 def test_golden_fixtures_exist():
-    assert len(GOLDEN) >= 4
+    assert len(GOLDEN) >= 7
+    assert sum(1 for p in GOLDEN if os.path.basename(p).startswith("alloy")) >= 3
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
 def test_port_matches_reference_golden(path):
     g = np.load(path)
-    P, M, X = _case(g["meta"])
-    # the host builders are deterministic: the same input state is rebuilt
+    P, M, X = _case(g["meta"], g["X"])
+    # the host builders are deterministic: the same problem (and, for grain
+    # growth, the same input state) is rebuilt
+    assert P.ndof == g["X"].shape[1]
     assert np.array_equal(X, g["X"])
     F = oracle.port_rhs(P, M, X)
     assert np.array_equal(F, g["F"]), np.abs(F - g["F"]).max()
@@ -136,3 +149,30 @@ def test_poststep_cap_overflow_detected():
     X[c, L.as_offset + 1:L.as_offset + 9] = ids
     X[c, L.pf_offset:L.pf_offset + 8] = 0.125
     assert oracle.port_poststep(P, M, X) == 3
+
+
+@needs_ref
+@pytest.mark.parametrize("model,feats,dim,res", [
+    ("calphad2sl", 0, 2, [20, 16]),
+    ("calphaddis", 0xFF, 2, [16, 16]),
+    ("quadratic", 0x7F, 3, [8, 8, 8]),
+    ("calphad2sl", 0x0B, 3, [8, 10, 6]),
+])
+def test_port_matches_reference_alloy_evolution(model, feats, dim, res):
+    """chemistry, heat, sources, walls: RHS and PostStep bit-exact over steps"""
+    P = cb.Problem.alloy(dim, res, model, 4, 5, 8, 31, feats)
+    M = cb.Mesh(P)
+    A = P.aos
+    X = oracle.port_initial_state(P, M)
+    with oracle.RefOracle(P, M) as R:
+        for _ in range(4):
+            F = oracle.port_rhs(P, M, X)
+            assert np.array_equal(F, R.rhs(X))
+            fphi = np.abs(F[:, A.pf_offset:A.pf_offset + A.pf_size]).max()
+            fdp = np.abs(F[:, A.dp_offset:A.dp_offset + A.dp_size]).max()
+            mu = np.abs(X[:, A.dp_offset:A.dp_offset + A.dp_size]).max()
+            X = X + min(0.05 / max(fphi, 1e-300), 0.02 * mu / max(fdp, 1e-300)) * F
+            Xr = X.copy()
+            assert oracle.port_poststep(P, M, X) == 0
+            assert R.poststep(Xr) == 0
+            assert np.array_equal(X, Xr)
