@@ -124,6 +124,18 @@ class GridDesc(C.Structure):
                 ("ex_per_phase", C.c_int32), ("layout", StateLayout), ("ex_init", C.c_void_p)]
 
 
+class TSOpts(C.Structure):
+    _fields_ = [("scheme", C.c_int32), ("poststep", C.c_int32), ("dt0", C.c_double), ("dtmin", C.c_double),
+                ("dtmax", C.c_double), ("reltol", C.c_double), ("abstol", C.c_double), ("max_steps", C.c_int64)]
+
+
+class TSStats(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("rejected", C.c_int64), ("rhs_calls", C.c_int64), ("t", C.c_double),
+                ("dt", C.c_double), ("last_norm", C.c_double)]
+
+
+TS_RK1FE, TS_RK2A, TS_RK3BS = 0, 1, 2
+
 PP = C.POINTER(ProblemStruct)
 MP = C.POINTER(MeshStruct)
 
@@ -158,6 +170,13 @@ _SIGNATURES = [
     ("cipher_ctx_check", C.c_int, [C.c_void_p, C.c_void_p]),
     ("cipher_chem_init", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_poststep_noalloc", C.c_int, [C.POINTER(GridDesc), C.c_void_p, C.c_void_p]),
+    ("cipher_ts_default_opts", C.c_int, [PP, C.POINTER(TSOpts)]),
+    ("cipher_ts_create", C.c_int, [C.c_void_p, C.POINTER(TSOpts), C.POINTER(C.c_void_p)]),
+    ("cipher_ts_destroy", None, [C.c_void_p]),
+    ("cipher_ts_step", C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.POINTER(C.c_int), C.c_void_p]),
+    ("cipher_ts_solve", C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.POINTER(TSStats), C.c_void_p]),
+    ("cipher_ts_get_stats", C.c_int, [C.c_void_p, C.POINTER(TSStats)]),
+    ("cipher_ts_set_dt", C.c_int, [C.c_void_p, C.c_double]),
     ("cipher_state_from_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_state_to_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_rhs_aos_host", C.c_int,

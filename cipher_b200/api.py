@@ -269,3 +269,58 @@ class Context:
             self.close()
         except Exception:
             pass
+
+
+def ts_options(problem: Problem, scheme: str = "2a", **kw) -> L.TSOpts:
+    """Stepper options from the problem (timestep0, step limits, tolerances),
+    overridden by keyword (dt0, dtmin, dtmax, reltol, abstol, max_steps, poststep)."""
+    lib = L.load()
+    o = L.TSOpts()
+    L.check(lib.cipher_ts_default_opts(problem.ptr, C.byref(o)), "cipher_ts_default_opts")
+    o.scheme = {"1fe": L.TS_RK1FE, "2a": L.TS_RK2A, "3bs": L.TS_RK3BS}[scheme]
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class TimeStepper:
+    """Explicit RK stepper with embedded error control on device states
+    (cipher_ts_*): the role PETSc's TSRK + TSADAPTDSP play for the reference."""
+
+    def __init__(self, ctx: Context, opts: L.TSOpts):
+        self._lib = L.load()
+        self.ctx, self.opts = ctx, opts
+        out = C.c_void_p()
+        L.check(self._lib.cipher_ts_create(ctx.ptr, C.byref(opts), C.byref(out)), "cipher_ts_create")
+        self.ptr = out
+
+    def step(self, X, t_end: float, stream=None) -> bool:
+        acc = C.c_int(0)
+        L.check(self._lib.cipher_ts_step(self.ptr, C.c_void_p(_ptr(X)), float(t_end), C.byref(acc),
+                                         _stream_handle(stream)), "cipher_ts_step")
+        return bool(acc.value)
+
+    def solve(self, X, t0: float, t_end: float, stream=None) -> L.TSStats:
+        st = L.TSStats()
+        L.check(self._lib.cipher_ts_solve(self.ptr, C.c_void_p(_ptr(X)), float(t0), float(t_end), C.byref(st),
+                                          _stream_handle(stream)), "cipher_ts_solve")
+        return st
+
+    def stats(self) -> L.TSStats:
+        st = L.TSStats()
+        L.check(self._lib.cipher_ts_get_stats(self.ptr, C.byref(st)), "cipher_ts_get_stats")
+        return st
+
+    def set_dt(self, dt: float):
+        L.check(self._lib.cipher_ts_set_dt(self.ptr, float(dt)), "cipher_ts_set_dt")
+
+    def close(self):
+        if self.ptr:
+            self._lib.cipher_ts_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -33,6 +33,16 @@ static int set_error(int code, const char *fmt, ...)
     return code;
 }
 
+/* the same, for the other units of the library */
+int cipher_set_error(int code, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_errmsg, sizeof(g_errmsg), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
 static int cuda_fail(cudaError_t e, const char *where)
 {
     return set_error(CIPHER_E_CUDA, "%s: %s", where, cudaGetErrorString(e));

@@ -189,6 +189,48 @@ int cipher_poststep_noalloc(const cipher_grid_desc *g, void *X, void *stream);
  * (VecWAXPY on the solution vector).  Y may alias X. */
 int cipher_waxpy(cipher_ctx *c, void *Y, const void *X, double a, const void *F, void *stream);
 
+/* ------------------------------------------------------------------ */
+/* time stepper on device states                                       */
+/* (the reference's PETSc TS: InitializeTS src/cipher.c:1097-1115 and   */
+/*  the time loop src/cipher.c:1589-1606)                              */
+/* ------------------------------------------------------------------ */
+
+enum { CIPHER_TS_RK1FE = 0,     /* forward Euler, fixed step */
+       CIPHER_TS_RK2A = 1,      /* Heun 2 with embedded Euler (PETSc -ts_rk_type 2a, the reference's examples) */
+       CIPHER_TS_RK3BS = 2 };   /* Bogacki-Shampine 3(2) */
+
+typedef struct cipher_ts_opts {
+    int32_t scheme;          /* CIPHER_TS_* */
+    int32_t poststep;        /* 1: cipher_poststep after every accepted step (TSSetPostStep) */
+    double dt0, dtmin, dtmax;/* first step and step limits (TSAdaptSetStepLimits) */
+    double reltol, abstol;   /* TSSetTolerances */
+    int64_t max_steps;       /* accepted steps per solve call; 0 = no limit */
+} cipher_ts_opts;
+
+typedef struct cipher_ts_stats {
+    int64_t steps, rejected, rhs_calls;
+    double t, dt, last_norm; /* time reached, next step size, last weighted error norm */
+} cipher_ts_stats;
+
+typedef struct cipher_ts cipher_ts;
+
+/* options from the problem: scheme 2a, PostStep on, dt0 = timestep0,
+ * limits mintimestep/maxtimestep, tolerances reltol/abstol */
+int cipher_ts_default_opts(const cipher_problem *p, cipher_ts_opts *o);
+/* stage and candidate buffers are allocated here (ns+1 state vectors) */
+int cipher_ts_create(cipher_ctx *c, const cipher_ts_opts *o, cipher_ts **out);
+void cipher_ts_destroy(cipher_ts *ts);
+/* one attempted step of X from the stepper's time, shortened to end at
+ * t_end (TS_EXACTFINALTIME_MATCHSTEP); *accepted tells whether X advanced.
+ * Synchronises `stream` (the error norm decides acceptance on the host). */
+int cipher_ts_step(cipher_ts *ts, void *X, double t_end, int *accepted, void *stream);
+/* steps X from t0 to t_end (or max_steps accepted steps); the step size
+ * carries over between calls as the reference's solparams.timestep does */
+int cipher_ts_solve(cipher_ts *ts, void *X, double t0, double t_end, cipher_ts_stats *stats, void *stream);
+int cipher_ts_get_stats(const cipher_ts *ts, cipher_ts_stats *st);
+/* next step size (clamped to the limits); resets the controller history */
+int cipher_ts_set_dt(cipher_ts *ts, double dt);
+
 /* reference AoS layout (ncells x ndof doubles, device) <-> device state */
 int cipher_state_from_aos(cipher_ctx *c, const double *aos, void *X, void *stream);
 int cipher_state_to_aos(cipher_ctx *c, const void *X, double *aos, void *stream);

@@ -55,6 +55,16 @@ def port():
         lib.oracle_poststep.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]
         lib.oracle_initial_state.restype = C.c_int
         lib.oracle_initial_state.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]
+        lib.oracle_ts_create.restype = C.c_void_p
+        lib.oracle_ts_create.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.oracle_ts_destroy.restype = None
+        lib.oracle_ts_destroy.argtypes = [C.c_void_p]
+        lib.oracle_ts_step.restype = C.c_int
+        lib.oracle_ts_step.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_int)]
+        lib.oracle_ts_solve.restype = C.c_int
+        lib.oracle_ts_solve.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_double, C.c_double, C.c_void_p]
+        lib.oracle_ts_get_stats.restype = None
+        lib.oracle_ts_get_stats.argtypes = [C.c_void_p, C.c_void_p]
         lib.or_simplex_projection.restype = None
         lib.or_simplex_projection.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int]
         _port = lib
@@ -123,6 +133,48 @@ def simplex_projection(v: np.ndarray) -> np.ndarray:
     out = np.zeros_like(v)
     port().or_simplex_projection(_dp(out), _dp(v), len(v))
     return out
+
+
+class PortTS:
+    """The CPU restatement of the library's RK stepper over the oracle RHS.
+    `opts` and the returned stats are cipher_b200._lib.TSOpts / TSStats."""
+
+    def __init__(self, problem, mesh, opts):
+        self.lib = port()
+        self.ptr = self.lib.oracle_ts_create(_addr(problem), _addr(mesh), C.cast(C.pointer(opts), C.c_void_p))
+        if not self.ptr:
+            raise RuntimeError("oracle_ts_create failed")
+        self.problem, self.mesh = problem, mesh
+
+    def step(self, X: np.ndarray, t_end: float) -> bool:
+        assert X.flags.c_contiguous and X.dtype == np.float64
+        acc = C.c_int(0)
+        rc = self.lib.oracle_ts_step(self.ptr, _dp(X), t_end, C.byref(acc))
+        if rc:
+            raise RuntimeError(f"oracle_ts_step failed ({rc})")
+        return bool(acc.value)
+
+    def solve(self, X: np.ndarray, t0: float, t_end: float, stats):
+        assert X.flags.c_contiguous and X.dtype == np.float64
+        rc = self.lib.oracle_ts_solve(self.ptr, _dp(X), t0, t_end, C.cast(C.pointer(stats), C.c_void_p))
+        if rc:
+            raise RuntimeError(f"oracle_ts_solve failed ({rc})")
+        return stats
+
+    def stats(self, stats):
+        self.lib.oracle_ts_get_stats(self.ptr, C.cast(C.pointer(stats), C.c_void_p))
+        return stats
+
+    def close(self):
+        if self.ptr:
+            self.lib.oracle_ts_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ----------------------------------------------------------------- ref ----

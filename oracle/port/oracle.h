@@ -21,6 +21,7 @@ void or_interpolant(int kind, const double *phi, int n, double *h);
 void or_interpolant_dT(int kind, double *v, const double *phi, int n);
 void or_simplex_projection(double *out, const double *in, int n);
 
+cipher_aos_layout or_aos_layout(const cipher_problem *p);
 const cipher_material *or_material(const cipher_problem *p, int phase);
 double or_chemenergy(const cipher_problem *p, int phase, const double *y, const double *mu, double T);
 void or_sitepot_explicit(const cipher_problem *p, int phase, const double *y, double T, double *out);

@@ -36,6 +36,8 @@ static cipher_aos_layout or_layout(const cipher_problem *p)
     return L;
 }
 
+cipher_aos_layout or_aos_layout(const cipher_problem *p) { return or_layout(p); }
+
 static void decode_set(const double *as, uint16_t *ids, int *n)
 {
     *n = (int)round(as[0]);
