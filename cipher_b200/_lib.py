@@ -135,6 +135,7 @@ class TSStats(C.Structure):
 
 
 TS_RK1FE, TS_RK2A, TS_RK3BS = 0, 1, 2
+BATCH_RUNNING, BATCH_FINISHED, BATCH_FAILED = 0, 1, 2
 
 PP = C.POINTER(ProblemStruct)
 MP = C.POINTER(MeshStruct)
@@ -177,6 +178,17 @@ _SIGNATURES = [
     ("cipher_ts_solve", C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.POINTER(TSStats), C.c_void_p]),
     ("cipher_ts_get_stats", C.c_int, [C.c_void_p, C.POINTER(TSStats)]),
     ("cipher_ts_set_dt", C.c_int, [C.c_void_p, C.c_double]),
+    ("cipher_batch_create", C.c_int, [C.c_int, C.c_int, C.POINTER(TSOpts), C.POINTER(C.c_void_p)]),
+    ("cipher_batch_destroy", None, [C.c_void_p]),
+    ("cipher_batch_footprint", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int64)]),
+    ("cipher_batch_attach", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                      C.POINTER(C.c_int)]),
+    ("cipher_batch_detach", C.c_int, [C.c_void_p, C.c_int]),
+    ("cipher_batch_step", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    ("cipher_batch_flush", C.c_int, [C.c_void_p]),
+    ("cipher_batch_slot_stats", C.c_int, [C.c_void_p, C.c_int, C.POINTER(TSStats), C.POINTER(C.c_int),
+                                          C.POINTER(C.c_int)]),
+    ("cipher_batch_set_graphs", C.c_int, [C.c_void_p, C.c_int]),
     ("cipher_state_from_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_state_to_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_rhs_aos_host", C.c_int,

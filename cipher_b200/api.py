@@ -324,3 +324,60 @@ class TimeStepper:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """Many independent domains stepped together (cipher_batch_*): each with
+    its own step size and error control, all in one graph launch per step."""
+
+    def __init__(self, opts: L.TSOpts, precision: str = "fp64", device: int = 0, graphs: bool = True):
+        self._lib = L.load()
+        out = C.c_void_p()
+        prec = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}[precision]
+        L.check(self._lib.cipher_batch_create(device, prec, C.byref(opts), C.byref(out)), "cipher_batch_create")
+        self.ptr = out
+        self._keep = {}
+        if not graphs:
+            L.check(self._lib.cipher_batch_set_graphs(self.ptr, 0), "cipher_batch_set_graphs")
+
+    def footprint(self, ctx: Context) -> int:
+        v = C.c_int64()
+        L.check(self._lib.cipher_batch_footprint(self.ptr, ctx.ptr, C.byref(v)), "cipher_batch_footprint")
+        return int(v.value)
+
+    def attach(self, ctx: Context, X, t0: float, t_end: float) -> int:
+        slot = C.c_int()
+        L.check(self._lib.cipher_batch_attach(self.ptr, ctx.ptr, C.c_void_p(_ptr(X)), float(t0), float(t_end),
+                                              C.byref(slot)), "cipher_batch_attach")
+        self._keep[slot.value] = (ctx, X)
+        return slot.value
+
+    def detach(self, slot: int):
+        L.check(self._lib.cipher_batch_detach(self.ptr, int(slot)), "cipher_batch_detach")
+        self._keep.pop(slot, None)
+
+    def step(self) -> int:
+        running = C.c_int()
+        L.check(self._lib.cipher_batch_step(self.ptr, C.byref(running)), "cipher_batch_step")
+        return running.value
+
+    def flush(self):
+        L.check(self._lib.cipher_batch_flush(self.ptr), "cipher_batch_flush")
+
+    def stats(self, slot: int):
+        st, status, err = L.TSStats(), C.c_int(), C.c_int()
+        L.check(self._lib.cipher_batch_slot_stats(self.ptr, int(slot), C.byref(st), C.byref(status), C.byref(err)),
+                "cipher_batch_slot_stats")
+        return st, status.value, err.value
+
+    def close(self):
+        if self.ptr:
+            self._lib.cipher_batch_destroy(self.ptr)
+            self.ptr = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -9,6 +9,7 @@ Usage: ``python -m cipher_b200.build`` (or ``cipher_b200.build.build()``).
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -75,6 +76,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     nvcc = _nvcc()
     headers = _headers()
     objs = []
+    jobs = []
     cu_dir = os.path.join(CSRC, "cuda")
     for f in sorted(os.listdir(cu_dir)):
         if not f.endswith(".cu"):
@@ -86,7 +88,12 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
             flags = NVCC_COMMON + ([] if f in FAST_SOURCES else NVCC_EXACT)
             if ptxas_info:
                 flags = flags + ["-Xptxas", "-v"]
-            _run([nvcc] + ARCH + flags + ["-c", src, "-o", obj], verbose or ptxas_info)
+            jobs.append([nvcc] + ARCH + flags + ["-c", src, "-o", obj])
+    # the translation units are independent: compile them concurrently
+    workers = max(1, min(len(jobs), os.cpu_count() or 1))
+    with concurrent.futures.ThreadPoolExecutor(max_workers=workers) as pool:
+        for fut in [pool.submit(_run, cmd, verbose or ptxas_info) for cmd in jobs]:
+            fut.result()
     host_dir = os.path.join(CSRC, "host")
     cc = shutil.which("gcc") or "cc"
     for f in sorted(os.listdir(host_dir)):

@@ -501,6 +501,63 @@ static PostArgs<R> post_args(const cipher_ctx *c, void *X)
     return a;
 }
 
+/* ------------------------------------------------------------------ */
+/* internal accessors for the batch driver (batch.cu)                   */
+/* ------------------------------------------------------------------ */
+
+namespace cipher {
+CtxInfo ctx_info(const cipher_ctx *c)
+{
+    CtxInfo i;
+    i.device = c->device;
+    i.precision = c->precision;
+    i.dim = c->dim;
+    i.general = c->general;
+    i.single = c->single;
+    i.P = c->P;
+    i.ncells = c->ncells;
+    i.res[0] = c->res[0]; i.res[1] = c->res[1]; i.res[2] = c->res[2];
+    return i;
+}
+PfArgs<double> ctx_pf_args_d(const cipher_ctx *c, const void *X, void *F, int *err)
+{
+    PfArgs<double> a = pf_args<double>(c, X, F);
+    a.err = err;
+    return a;
+}
+PfArgs<float> ctx_pf_args_f(const cipher_ctx *c, const void *X, void *F, int *err)
+{
+    PfArgs<float> a = pf_args<float>(c, X, F);
+    a.err = err;
+    return a;
+}
+PostArgs<double> ctx_post_args_d(const cipher_ctx *c, void *X, uint16_t *pruned, int *err)
+{
+    PostArgs<double> a = post_args<double>(c, X);
+    a.pruned = pruned;
+    a.err = err;
+    return a;
+}
+PostArgs<float> ctx_post_args_f(const cipher_ctx *c, void *X, uint16_t *pruned, int *err)
+{
+    PostArgs<float> a = post_args<float>(c, X);
+    a.pruned = pruned;
+    a.err = err;
+    return a;
+}
+cudaError_t ctx_rhs_general(const cipher_ctx *c, const void *X, void *F, int *err, cudaStream_t s)
+{
+    if (c->precision == CIPHER_PREC_FP64) {
+        GenArgs<double> a = gen_args<double>(c, X, F);
+        a.err = err;
+        return launch_rhs_general(a, c->dim, s);
+    }
+    GenArgs<float> a = gen_args<float>(c, X, F);
+    a.err = err;
+    return launch_rhs_general(a, c->dim, s);
+}
+}  // namespace cipher
+
 static int read_flags(cipher_ctx *c, cudaStream_t s, int *flags)
 {
     CUDA_TRY(cudaMemcpyAsync(c->h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, s), "read error flags");

@@ -38,6 +38,23 @@ struct PfArgs {
 cudaError_t launch_rhs_phasefield(const PfArgs<double> &a, int dim, cudaStream_t s);
 cudaError_t launch_rhs_phasefield(const PfArgs<float> &a, int dim, cudaStream_t s);
 
+/* many independent domains in one launch: domain i owns tiles
+ * [tile_start[i], tile_start[i+1]) of the global tile list; a tile is
+ * BX x BY cells of one (y, z) row range of that domain */
+template <typename R>
+struct BatchTiles {
+    const PfArgs<R> *args;        /* [n] device */
+    const int64_t *tile_start;    /* [n+1] device */
+    const int *active;            /* [n] device: 0 skips the domain */
+    int n;
+    int64_t total;                /* tile_start[n] */
+    int pmax;                     /* largest P of the batch (shared-memory columns) */
+};
+
+/* grid: persistent (a multiple of the SM count); by = tile rows (1, 2, 4) */
+cudaError_t launch_rhs_pf_batched(const BatchTiles<double> &b, int dim, int single, int by, int grid, cudaStream_t s);
+cudaError_t launch_rhs_pf_batched(const BatchTiles<float> &b, int dim, int single, int by, int grid, cudaStream_t s);
+
 /* one boundary condition, flattened (BOUNDARYCONDITIONS, src/typedef.h:243-248) */
 struct DevBC {
     int label, chem_type, thermal_type;
@@ -105,6 +122,19 @@ struct PostArgs {
 cudaError_t launch_poststep(const PostArgs<double> &a, int dim, cudaStream_t s);
 cudaError_t launch_poststep(const PostArgs<float> &a, int dim, cudaStream_t s);
 
+/* batched PostStep: domain i owns blocks [block_start[i], block_start[i+1])
+ * of 256 cells; domains whose `active` entry is 0 are skipped */
+template <typename R>
+struct BatchPost {
+    const PostArgs<R> *args;      /* [n] device */
+    const int64_t *block_start;   /* [n+1] device */
+    const int *active;            /* [n] device */
+    int n;
+    int64_t total;
+};
+cudaError_t launch_poststep_batched(const BatchPost<double> &b, int dim, cudaStream_t s);
+cudaError_t launch_poststep_batched(const BatchPost<float> &b, int dim, cudaStream_t s);
+
 /* reference AoS (ncells x ndof doubles) <-> plane-major device state */
 struct LayoutArgs {
     int64_t ncells, stride;
@@ -120,4 +150,21 @@ struct LayoutArgs {
 cudaError_t launch_aos_to_soa(const LayoutArgs &a, const double *aos, cudaStream_t s);
 cudaError_t launch_soa_to_aos(const LayoutArgs &a, double *aos, int include_as, cudaStream_t s);
 
+/* what the batch driver needs to know of a context (context.cu) */
+struct CtxInfo {
+    int device, precision, dim, general, single, P;
+    int64_t ncells;
+    int res[3];
+};
+
+}  // namespace cipher
+
+struct cipher_ctx;
+namespace cipher {
+CtxInfo ctx_info(const cipher_ctx *c);
+PfArgs<double> ctx_pf_args_d(const cipher_ctx *c, const void *X, void *F, int *err);
+PfArgs<float> ctx_pf_args_f(const cipher_ctx *c, const void *X, void *F, int *err);
+PostArgs<double> ctx_post_args_d(const cipher_ctx *c, void *X, uint16_t *pruned, int *err);
+PostArgs<float> ctx_post_args_f(const cipher_ctx *c, void *X, uint16_t *pruned, int *err);
+cudaError_t ctx_rhs_general(const cipher_ctx *c, const void *X, void *F, int *err, cudaStream_t s);
 }  // namespace cipher

@@ -163,6 +163,35 @@ __device__ __forceinline__ CellIndex cell_index(const int *res)
     return ci;
 }
 
+/* cell of this thread in tile t of a batch; `inst` receives the domain.
+ * Domains are found by binary search of the tile prefix (uniform across
+ * the block, so no divergence). */
+template <int BX, int BY, typename R>
+__device__ __forceinline__ CellIndex batch_cell_index(const BatchTiles<R> &b, int64_t t, int &inst)
+{
+    int lo = 0, hi = b.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&b.tile_start[mid]) <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    inst = lo;
+    const int *res = b.args[lo].res;
+    const int r0 = res[0], r1 = res[1];
+    const int64_t local = t - __ldg(&b.tile_start[lo]);
+    const int tx = (r0 + BX - 1) / BX, ty = (r1 + BY - 1) / BY;
+    const int bx = (int)(local % tx);
+    const int by = (int)((local / tx) % ty);
+    const int bz = (int)(local / ((int64_t)tx * ty));
+    CellIndex ci;
+    ci.x = bx * BX + (int)threadIdx.x % BX;
+    ci.y = by * BY + (int)threadIdx.x / BX;
+    ci.z = bz;
+    ci.live = ci.x < r0 && ci.y < r1;
+    ci.c = (int64_t)ci.x + (int64_t)r0 * ((int64_t)ci.y + (int64_t)r1 * ci.z);
+    return ci;
+}
+
 /* neighbour at fixed face position f: [0,DIM) below without wrap
  * (descending d), [DIM,2DIM) own faces (ascending d), [2DIM,3DIM) wrapped
  * around from above (ascending d); -1 when the face is absent.  This is the

@@ -25,10 +25,8 @@
 namespace cipher {
 
 template <int PM, typename R>
-__global__ void __launch_bounds__(256) k_post_prune(const PostArgs<R> a)
+__device__ __forceinline__ void post_prune_cell(const PostArgs<R> &a, int64_t c)
 {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.ncells) return;
     const int64_t S = a.stride;
     int n = a.as[c];
     if (n < 1 || n > a.P) {
@@ -76,6 +74,14 @@ __global__ void __launch_bounds__(256) k_post_prune(const PostArgs<R> a)
     a.pruned[c] = (uint16_t)np;
 }
 
+template <int PM, typename R>
+__global__ void __launch_bounds__(256) k_post_prune(const PostArgs<R> a)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.ncells) return;
+    post_prune_cell<PM, R>(a, c);
+}
+
 /* out = a U b (sorted); returns the size, or P+1 if it would exceed P */
 template <int PM>
 __device__ __forceinline__ int merge_union(const uint16_t *sa, int na, const uint16_t *pl, int64_t S, int64_t nb,
@@ -103,10 +109,8 @@ __device__ __forceinline__ int merge_union(const uint16_t *sa, int na, const uin
 }
 
 template <int DIM, int PM, typename R>
-__global__ void __launch_bounds__(256) k_post_union(const PostArgs<R> a)
+__device__ __forceinline__ void post_union_cell(const PostArgs<R> &a, int64_t c)
 {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.ncells) return;
     const int64_t S = a.stride;
     int n = a.as[c];
     int ns = a.pruned[c];
@@ -188,6 +192,66 @@ __global__ void __launch_bounds__(256) k_post_union(const PostArgs<R> a)
     a.as[c] = (uint16_t)ns;
     for (int g = 0; g < ns; g++) a.as[(int64_t)(1 + g) * S + c] = sup[g];
 }
+
+template <int DIM, int PM, typename R>
+__global__ void __launch_bounds__(256) k_post_union(const PostArgs<R> a)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.ncells) return;
+    post_union_cell<DIM, PM, R>(a, c);
+}
+
+/* batched: block k of the list belongs to the domain whose range holds k */
+template <typename R>
+__device__ __forceinline__ int batch_post_domain(const BatchPost<R> &b, int64_t k)
+{
+    int lo = 0, hi = b.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&b.block_start[mid]) <= k) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int PM, typename R>
+__global__ void __launch_bounds__(256) k_post_prune_batched(const BatchPost<R> b)
+{
+    const int inst = batch_post_domain(b, blockIdx.x);
+    if (!b.active[inst]) return;
+    const PostArgs<R> &a = b.args[inst];
+    const int64_t c = (int64_t)(blockIdx.x - b.block_start[inst]) * blockDim.x + threadIdx.x;
+    if (c >= a.ncells) return;
+    post_prune_cell<PM, R>(a, c);
+}
+
+template <int DIM, int PM, typename R>
+__global__ void __launch_bounds__(256) k_post_union_batched(const BatchPost<R> b)
+{
+    const int inst = batch_post_domain(b, blockIdx.x);
+    if (!b.active[inst]) return;
+    const PostArgs<R> &a = b.args[inst];
+    const int64_t c = (int64_t)(blockIdx.x - b.block_start[inst]) * blockDim.x + threadIdx.x;
+    if (c >= a.ncells) return;
+    post_union_cell<DIM, PM, R>(a, c);
+}
+
+template <typename R>
+static cudaError_t launch_post_batched(const BatchPost<R> &b, int dim, cudaStream_t s)
+{
+    if (b.total < 1) return cudaSuccess;
+    dim3 grid((unsigned)b.total), block(256);
+    k_post_prune_batched<CIPHER_PMAX, R><<<grid, block, 0, s>>>(b);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (dim == 1) k_post_union_batched<1, CIPHER_PMAX, R><<<grid, block, 0, s>>>(b);
+    else if (dim == 2) k_post_union_batched<2, CIPHER_PMAX, R><<<grid, block, 0, s>>>(b);
+    else k_post_union_batched<3, CIPHER_PMAX, R><<<grid, block, 0, s>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_poststep_batched(const BatchPost<double> &b, int dim, cudaStream_t s) { return launch_post_batched(b, dim, s); }
+cudaError_t launch_poststep_batched(const BatchPost<float> &b, int dim, cudaStream_t s) { return launch_post_batched(b, dim, s); }
 
 template <typename R>
 static cudaError_t launch_post(const PostArgs<R> &a, int dim, cudaStream_t s)

@@ -16,6 +16,9 @@
  * FP64 oracle on the same inputs: max|dF|/max|F| <= 1e-6 (tested).
  */
 #include <cstdint>
+#include <mutex>
+#include <utility>
+#include <vector>
 #include <cuda_runtime.h>
 #include "device_common.cuh"
 #include "kernels.h"
@@ -31,12 +34,12 @@ namespace cipher {
 
 constexpr int kBX = CIPHER_MIXED_BX, kBY = CIPHER_MIXED_BY, kMixedBlock = kBX * kBY;
 
+/* one cell of the mixed RHS, single interface (shared by the single-domain
+ * and the batched kernels) */
 template <int DIM, int PM>
-__global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_single(const PfArgs<float> a)
+__device__ __forceinline__ void pf_mixed_single_cell(const PfArgs<float> &a, const CellIndex &ci,
+                                                     const SlotColumns<float> &sc)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const CellIndex ci = cell_index<kBX, kBY>(a.res);
-    const SlotColumns<float> sc = slot_columns<float>(smem, a.P, blockDim.x, threadIdx.x, false);
     const int n = load_and_gather<DIM, PM, float, false>(a, ci, sc);
     if (!ci.live) return;
     const int64_t S = a.stride, c = ci.c;
@@ -84,11 +87,19 @@ __global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_single(const PfArg
 }
 
 template <int DIM, int PM>
-__global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_multi(const PfArgs<float> a)
+__global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_single(const PfArgs<float> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const CellIndex ci = cell_index<kBX, kBY>(a.res);
-    const SlotColumns<float> sc = slot_columns<float>(smem, a.P, blockDim.x, threadIdx.x, true);
+    const SlotColumns<float> sc = slot_columns<float>(smem, a.P, blockDim.x, threadIdx.x, false);
+    pf_mixed_single_cell<DIM, PM>(a, ci, sc);
+}
+
+/* one cell of the mixed RHS, several interfaces (reference-order cell terms in FP32) */
+template <int DIM, int PM>
+__device__ __forceinline__ void pf_mixed_multi_cell(const PfArgs<float> &a, const CellIndex &ci,
+                                                    const SlotColumns<float> &sc)
+{
     const int n = load_and_gather<DIM, PM, float, false>(a, ci, sc);
     const double T = n == 0 ? 0.0 : (double)a.tm[ci.c];
     cell_rates_ordered<float, false>(a, sc, n, ci.c, ci.live, T);
@@ -96,6 +107,30 @@ __global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_multi(const PfArgs
     double tr = 0.0;
     if (a.has_temp_rate) tr += a.temp_rate;
     a.ftm[ci.c] = (float)tr;
+}
+
+template <int DIM, int PM>
+__global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_multi(const PfArgs<float> a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const CellIndex ci = cell_index<kBX, kBY>(a.res);
+    const SlotColumns<float> sc = slot_columns<float>(smem, a.P, blockDim.x, threadIdx.x, true);
+    pf_mixed_multi_cell<DIM, PM>(a, ci, sc);
+}
+
+/* batched: a persistent grid walks the tiles of every domain of the batch */
+template <int DIM, int PM, bool SINGLE, int BY>
+__global__ void __launch_bounds__(kBX * BY) k_rhs_pf_mixed_batched(const BatchTiles<float> b)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const SlotColumns<float> sc = slot_columns<float>(smem, b.pmax, blockDim.x, threadIdx.x, !SINGLE);
+    for (int64_t t = blockIdx.x; t < b.total; t += gridDim.x) {
+        int inst;
+        const CellIndex ci = batch_cell_index<kBX, BY>(b, t, inst);
+        if (!b.active[inst]) continue;
+        if (SINGLE) pf_mixed_single_cell<DIM, PM>(b.args[inst], ci, sc);
+        else pf_mixed_multi_cell<DIM, PM>(b.args[inst], ci, sc);
+    }
 }
 
 template <int DIM, int PM>
@@ -118,6 +153,57 @@ static void launch_dim(const PfArgs<float> &a, cudaStream_t s)
     else if (a.P <= 8) launch_pm<DIM, 8>(a, s);
     else if (a.P <= 12) launch_pm<DIM, 12>(a, s);
     else launch_pm<DIM, 16>(a, s);
+}
+
+/* dynamic shared memory above the default 48 KB needs the kernel's opt-in;
+ * it is set once per kernel and size (before any graph capture: the batch
+ * driver's tile tuning launches every shape it later captures) */
+template <typename K>
+static cudaError_t allow_smem(K kernel, size_t bytes)
+{
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    static std::mutex mu;
+    static std::vector<std::pair<const void *, size_t>> done;
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto &d : done)
+        if (d.first == (const void *)kernel && d.second >= bytes) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) done.push_back({(const void *)kernel, bytes});
+    return e;
+}
+
+template <int DIM, int PM, bool SINGLE>
+static cudaError_t launch_batched_by(const BatchTiles<float> &b, int by, int grid, cudaStream_t s)
+{
+    const size_t sm = slot_columns_bytes(b.pmax, kBX * by, 4, !SINGLE);
+    cudaError_t e;
+    if (by == 1) {
+        if ((e = allow_smem(k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 1>, sm)) != cudaSuccess) return e;
+        k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 1><<<grid, kBX, sm, s>>>(b);
+    } else if (by == 2) {
+        if ((e = allow_smem(k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 2>, sm)) != cudaSuccess) return e;
+        k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 2><<<grid, kBX * 2, sm, s>>>(b);
+    } else {
+        if ((e = allow_smem(k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 4>, sm)) != cudaSuccess) return e;
+        k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 4><<<grid, kBX * 4, sm, s>>>(b);
+    }
+    return cudaGetLastError();
+}
+
+template <int DIM>
+static cudaError_t launch_batched_dim(const BatchTiles<float> &b, int single, int by, int grid, cudaStream_t s)
+{
+    if (b.pmax <= 4) return single ? launch_batched_by<DIM, 4, true>(b, by, grid, s) : launch_batched_by<DIM, 4, false>(b, by, grid, s);
+    if (b.pmax <= 8) return single ? launch_batched_by<DIM, 8, true>(b, by, grid, s) : launch_batched_by<DIM, 8, false>(b, by, grid, s);
+    if (b.pmax <= 12) return single ? launch_batched_by<DIM, 12, true>(b, by, grid, s) : launch_batched_by<DIM, 12, false>(b, by, grid, s);
+    return single ? launch_batched_by<DIM, 16, true>(b, by, grid, s) : launch_batched_by<DIM, 16, false>(b, by, grid, s);
+}
+
+cudaError_t launch_rhs_pf_batched(const BatchTiles<float> &b, int dim, int single, int by, int grid, cudaStream_t s)
+{
+    if (dim == 1) return launch_batched_dim<1>(b, single, by, grid, s);
+    if (dim == 2) return launch_batched_dim<2>(b, single, by, grid, s);
+    return launch_batched_dim<3>(b, single, by, grid, s);
 }
 
 cudaError_t launch_rhs_phasefield(const PfArgs<float> &a, int dim, cudaStream_t s)

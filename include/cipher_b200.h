@@ -231,6 +231,40 @@ int cipher_ts_get_stats(const cipher_ts *ts, cipher_ts_stats *st);
 /* next step size (clamped to the limits); resets the controller history */
 int cipher_ts_set_dt(cipher_ts *ts, double dt);
 
+/* ------------------------------------------------------------------ */
+/* many independent domains stepped together                           */
+/* (no counterpart in the reference, which runs one domain per job)    */
+/* ------------------------------------------------------------------ */
+
+enum { CIPHER_BATCH_RUNNING = 0, CIPHER_BATCH_FINISHED = 1, CIPHER_BATCH_FAILED = 2 };
+
+typedef struct cipher_batch cipher_batch;
+
+/* a batch of domains of one precision and dimension on `device`, stepped
+ * with the options `o` (each domain with its own step size and error
+ * control, exactly as cipher_ts steps it alone) */
+int cipher_batch_create(int device, int precision, const cipher_ts_opts *o, cipher_batch **out);
+void cipher_batch_destroy(cipher_batch *b);
+/* device bytes a domain of context c takes in the batch besides its state */
+int cipher_batch_footprint(const cipher_batch *b, const cipher_ctx *c, int64_t *bytes);
+/* add the domain of context c with device state X (the caller keeps both
+ * alive until detach), to be stepped from t0 to t_end; allocates the
+ * domain's stage buffers.  Membership changes rebuild the batch's launch
+ * tables, tile shapes (timed once per domain class) and CUDA graph. */
+int cipher_batch_attach(cipher_batch *b, cipher_ctx *c, void *X, double t0, double t_end, int *slot);
+/* remove a domain; its X is brought up to date first */
+int cipher_batch_detach(cipher_batch *b, int slot);
+/* one attempted step of every running domain (one graph launch, one host
+ * synchronisation); *running = domains that have not reached t_end.  A
+ * domain's X is current after cipher_batch_flush, detach, or once no
+ * domain runs; a failed domain (cap overflow, bad set, non-finite error)
+ * stops and reports its code through cipher_batch_slot_stats. */
+int cipher_batch_step(cipher_batch *b, int *running);
+int cipher_batch_flush(cipher_batch *b);
+int cipher_batch_slot_stats(const cipher_batch *b, int slot, cipher_ts_stats *st, int *status, int *error);
+/* 1 (default): replay each step from a CUDA graph; 0: launch directly */
+int cipher_batch_set_graphs(cipher_batch *b, int on);
+
 /* reference AoS layout (ncells x ndof doubles, device) <-> device state */
 int cipher_state_from_aos(cipher_ctx *c, const double *aos, void *X, void *stream);
 int cipher_state_to_aos(cipher_ctx *c, const void *X, double *aos, void *stream);

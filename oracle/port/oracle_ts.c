@@ -229,6 +229,7 @@ int oracle_ts_step(oracle_ts *t, double *X, double t_end, int *accepted)
         if (t->dt <= t->o.dtmin) { t->st.rejected++; *accepted = 0; return 4; }
         double dt = t->dt * 0.1;
         t->dt = dt < t->o.dtmin ? t->o.dtmin : dt;
+        t->st.rejected++;
     } else {
         acc = enorm <= 1.0 || h <= t->o.dtmin || !t->eorder;
         double dtn = t->eorder ? ts_dsp_next(t, h, enorm, acc) : t->dt;
