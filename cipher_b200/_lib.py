@@ -134,6 +134,18 @@ class TSStats(C.Structure):
                 ("dt", C.c_double), ("last_norm", C.c_double)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int32), ("precision", C.c_int32), ("max_active", C.c_int32),
+                ("hbm_budget", C.c_int64), ("ts", TSOpts)]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("state", C.c_int32), ("status", C.c_int32), ("error", C.c_int32), ("stats", TSStats),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_finish", C.c_double),
+                ("ncells", C.c_int64), ("ndof", C.c_int32), ("footprint", C.c_int64)]
+
+
+INIT_SHARP, INIT_DIFFUSE = 0, 1
 TS_RK1FE, TS_RK2A, TS_RK3BS = 0, 1, 2
 BATCH_RUNNING, BATCH_FINISHED, BATCH_FAILED = 0, 1, 2
 
@@ -189,6 +201,13 @@ _SIGNATURES = [
     ("cipher_batch_slot_stats", C.c_int, [C.c_void_p, C.c_int, C.POINTER(TSStats), C.POINTER(C.c_int),
                                           C.POINTER(C.c_int)]),
     ("cipher_batch_set_graphs", C.c_int, [C.c_void_p, C.c_int]),
+    ("cipher_server_create", C.c_int, [C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]),
+    ("cipher_server_destroy", None, [C.c_void_p]),
+    ("cipher_server_submit", C.c_int, [C.c_void_p, PP, C.c_int, C.c_double, C.c_double, C.POINTER(C.c_int64)]),
+    ("cipher_server_poll", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("cipher_server_result", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(ServerResult), C.POINTER(C.c_double)]),
+    ("cipher_server_release", C.c_int, [C.c_void_p, C.c_int64]),
+    ("cipher_server_usage", C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     ("cipher_state_from_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_state_to_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_rhs_aos_host", C.c_int,

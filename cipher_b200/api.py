@@ -381,3 +381,65 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class Server:
+    """Continuous-batching request loop (cipher_server_*): requests are
+    admitted in arrival order while they fit the HBM budget and stepped
+    together; each result equals the request solved alone."""
+
+    def __init__(self, opts: L.TSOpts, precision: str = "fp64", device: int = 0, hbm_budget: int = 8 << 30,
+                 max_active: int = 256):
+        self._lib = L.load()
+        so = L.ServerOpts()
+        so.device = device
+        so.precision = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}[precision]
+        so.max_active = max_active
+        so.hbm_budget = hbm_budget
+        so.ts = opts
+        out = C.c_void_p()
+        L.check(self._lib.cipher_server_create(C.byref(so), C.byref(out)), "cipher_server_create")
+        self.ptr = out
+
+    def submit(self, problem: Problem, t_end: float, init: str = "diffuse", width: float = 4.0) -> int:
+        """queue a request; the server takes ownership of the problem"""
+        rid = C.c_int64()
+        kind = {"sharp": L.INIT_SHARP, "diffuse": L.INIT_DIFFUSE}[init]
+        L.check(self._lib.cipher_server_submit(self.ptr, problem.ptr, kind, float(width), float(t_end),
+                                               C.byref(rid)), "cipher_server_submit")
+        problem.ptr = None          # owned by the server now
+        return rid.value
+
+    def poll(self):
+        q, a, d = C.c_int(), C.c_int(), C.c_int()
+        L.check(self._lib.cipher_server_poll(self.ptr, C.byref(q), C.byref(a), C.byref(d)), "cipher_server_poll")
+        return q.value, a.value, d.value
+
+    def result(self, rid: int, with_state: bool = False):
+        r = L.ServerResult()
+        L.check(self._lib.cipher_server_result(self.ptr, int(rid), C.byref(r), None), "cipher_server_result")
+        X = None
+        if with_state and r.state == 2:
+            X = np.empty((int(r.ncells), int(r.ndof)), dtype=np.float64)
+            L.check(self._lib.cipher_server_result(self.ptr, int(rid), C.byref(r),
+                                                   X.ctypes.data_as(C.POINTER(C.c_double))), "cipher_server_result")
+        return r, X
+
+    def release(self, rid: int):
+        L.check(self._lib.cipher_server_release(self.ptr, int(rid)), "cipher_server_release")
+
+    def usage(self):
+        u, p = C.c_int64(), C.c_int64()
+        L.check(self._lib.cipher_server_usage(self.ptr, C.byref(u), C.byref(p)), "cipher_server_usage")
+        return u.value, p.value
+
+    def close(self):
+        if self.ptr:
+            self._lib.cipher_server_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

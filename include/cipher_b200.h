@@ -265,6 +265,50 @@ int cipher_batch_slot_stats(const cipher_batch *b, int slot, cipher_ts_stats *st
 /* 1 (default): replay each step from a CUDA graph; 0: launch directly */
 int cipher_batch_set_graphs(cipher_batch *b, int on);
 
+/* ------------------------------------------------------------------ */
+/* serving: continuous batching of many simulations on one GPU          */
+/* (no counterpart in the reference)                                   */
+/* ------------------------------------------------------------------ */
+
+enum { CIPHER_INIT_SHARP = 0,     /* SetUpProblem state (+ chemistry from c0) */
+       CIPHER_INIT_DIFFUSE = 1 }; /* diffuse Voronoi state of the given width */
+
+typedef struct cipher_server_opts {
+    int32_t device, precision;
+    int32_t max_active;          /* domains stepped together at most */
+    int64_t hbm_budget;          /* device bytes the admitted requests may hold */
+    cipher_ts_opts ts;           /* stepper options of every request */
+} cipher_server_opts;
+
+typedef struct cipher_server_result_t {
+    int32_t state;               /* 0 queued, 1 running, 2 done */
+    int32_t status, error;       /* CIPHER_BATCH_* and the error code of a failed request */
+    cipher_ts_stats stats;
+    double t_submit, t_admit, t_finish;  /* CLOCK_MONOTONIC seconds */
+    int64_t ncells;
+    int32_t ndof;
+    int64_t footprint;           /* device bytes charged against the budget */
+} cipher_server_result_t;
+
+typedef struct cipher_server cipher_server;
+
+int cipher_server_create(const cipher_server_opts *o, cipher_server **out);
+void cipher_server_destroy(cipher_server *s);
+/* queue a request; the server takes ownership of p (freed on release or
+ * destroy) and builds its mesh, context and initial state on admission */
+int cipher_server_submit(cipher_server *s, cipher_problem *p, int init_kind, double width, double t_end, int64_t *id);
+/* admit queued requests in arrival order while they fit the budget, take
+ * one batched step of every running request, retire the finished ones
+ * (their final state is copied to host memory and their device memory
+ * freed) */
+int cipher_server_poll(cipher_server *s, int *queued, int *active, int *done);
+/* a request's state and timings; X (ncells x ndof doubles, reference AoS
+ * layout) receives the final state of a finished request when not NULL */
+int cipher_server_result(const cipher_server *s, int64_t id, cipher_server_result_t *res, double *X);
+int cipher_server_release(cipher_server *s, int64_t id);
+/* device bytes held by admitted requests now and at most so far */
+int cipher_server_usage(const cipher_server *s, int64_t *used, int64_t *peak);
+
 /* reference AoS layout (ncells x ndof doubles, device) <-> device state */
 int cipher_state_from_aos(cipher_ctx *c, const double *aos, void *X, void *stream);
 int cipher_state_to_aos(cipher_ctx *c, const void *X, double *aos, void *stream);
