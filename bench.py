@@ -258,6 +258,196 @@ def time_launches(fn, steps, stream):
     return t0.elapsed_time(t1), per
 
 
+# --------------------------------------------------------------------------- #
+# the other configurations (reported beside the headline)                     #
+# --------------------------------------------------------------------------- #
+
+def bytes_per_cell_update(P: int, D: int, S: int, rb: int) -> int:
+    return survey_bytes_per_cell(P, D, S, rb)
+
+
+def run_chemistry(dev: int, steps: int, peak: float):
+    """config 2 shape on a uniform grid: 512^2, calphad2sl, 4 components,
+    2 matrix grains + 20 precipitates, P = 15; the state is the SetUpProblem
+    state advanced by 20 accepted device steps (interfaces start to spread)"""
+    import torch
+    import cipher_b200 as cb
+    from cipher_b200 import workloads as W
+    P = W.alloy_2d()
+    M = cb.Mesh(P)
+    A = P.aos
+    X0 = cb.initial_state_aos(P, M)
+    c64 = cb.Context(P, M, "fp64", device=dev)
+    X = c64.alloc_state()
+    c64.from_aos(X0, X)
+    c64.chem_init(X)
+    ts = cb.TimeStepper(c64, cb.ts_options(P, "2a", dt0=1e-6, dtmin=1e-12, dtmax=1e-2, reltol=1e-3, abstol=1e-3,
+                                           max_steps=20))
+    ts.solve(X, 0.0, 1.0)
+    Xa = c64.to_aos(X)
+    Xr = Xa.copy()
+    Xr[:, A.pf_offset:A.pf_offset + A.pf_size] = Xr[:, A.pf_offset:A.pf_offset + A.pf_size].astype(np.float32)
+    Xr[:, A.tm_offset] = Xr[:, A.tm_offset].astype(np.float32)
+    c32 = cb.Context(P, M, "mixed", device=dev)
+    out = {"workload": "2D alloy 512^2, calphad2sl 4 components (D=3, S=6), 2 grains + 20 precipitates, P=15, "
+                       "uniform grid, state after 20 accepted steps",
+           "cells": M.ncells, "mean_active_phases": float(Xa[:, 0].mean())}
+    stream = torch.cuda.current_stream()
+    F = {}
+    for name, ctx, Xin in (("fp64", c64, Xr), ("mixed", c32, Xr)):
+        dX, dF = ctx.alloc_state(), ctx.alloc_state()
+        ctx.from_aos(Xin, dX)
+        for _ in range(3):
+            ctx.rhs(0.0, dX, dF)
+        torch.cuda.synchronize()
+        tot, per = time_launches(lambda: ctx.rhs(0.0, dX, dF), steps, stream)
+        ctx.check()
+        F[name] = ctx.to_aos(dF)
+        rb = 8 if name == "fp64" else 4
+        B = bytes_per_cell_update(A.pf_size, A.dp_size, A.sp_size, rb)
+        ms = tot / steps
+        out[name] = {"value": M.ncells / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+                     "bytes_per_cell_update": B, "roofline_frac": B * M.ncells / (ms / 1e3) / 1e9 / peak,
+                     "kernels": ["k_chem_cell", "k_rhs_general"]}
+    errs = {}
+    for nm, off, size in (("pf", A.pf_offset, A.pf_size), ("dp", A.dp_offset, A.dp_size),
+                          ("ex", A.ex_offset, A.ex_size), ("tm", A.tm_offset, 1)):
+        a, b = F["mixed"][:, off:off + size], F["fp64"][:, off:off + size]
+        errs[nm] = float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+    out["mixed_rel_err_vs_fp64"] = errs
+    out["mixed_speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
+
+
+def run_batched(dev: int, n_domains: int, t_end: float, n_alone: int):
+    """config 3: independent 2D grain-growth domains of uneven size stepped
+    together to t_end (one graph launch per step) vs a sample solved one at
+    a time with the single stepper"""
+    import cipher_b200 as cb
+    from cipher_b200 import workloads as W
+    specs = W.batch_domains(n_domains)
+    probe = W.batch_problem(specs[0])
+    opts = cb.ts_options(probe, "2a")
+    doms = []
+    for sp in specs:
+        P = W.batch_problem(sp)
+        M = cb.Mesh(P)
+        ctx = cb.Context(P, M, "fp64", device=dev)
+        X = ctx.alloc_state()
+        ctx.from_aos(cb.initial_state_aos(P, M), X)
+        doms.append((P, M, ctx, X))
+    b = cb.Batch(opts, "fp64", device=dev)
+    slots = [b.attach(ctx, X, 0.0, t_end) for _, _, ctx, X in doms]
+    b.step()                      # builds the tables, tunes the tile shapes, captures the graph
+    t0 = time.perf_counter()
+    nsteps = 1
+    while b.step() > 0:
+        nsteps += 1
+    b.flush()
+    t_batch = time.perf_counter() - t0
+    cells = sum(M.ncells for _, M, _, _ in doms)
+    upd, failed = 0, 0
+    for (P, M, _, _), sl in zip(doms, slots):
+        st, status, _ = b.stats(sl)
+        upd += M.ncells * st.rhs_calls
+        failed += status != L_BATCH_FINISHED()
+    # one at a time: every (n/n_alone)-th domain, solved alone from t = 0
+    stride = max(1, n_domains // n_alone)
+    t_alone, alone_upd, n_al = 0.0, 0, 0
+    for k in range(0, n_domains, stride):
+        P = W.batch_problem(specs[k])
+        M = cb.Mesh(P)
+        ctx = cb.Context(P, M, "fp64", device=dev)
+        X = ctx.alloc_state()
+        ctx.from_aos(cb.initial_state_aos(P, M), X)
+        ts = cb.TimeStepper(ctx, opts)
+        t1 = time.perf_counter()
+        st = ts.solve(X, 0.0, t_end)
+        t_alone += time.perf_counter() - t1
+        alone_upd += M.ncells * st.rhs_calls
+        n_al += 1
+    b.close()
+    return {"workload": f"{n_domains} 2D grain-growth domains, side 2^U[5,8] (32..256), 8-128 grains, P=8, "
+                        f"SetUpProblem start, RK 2a at rtol=atol=1e-4 to t={t_end}",
+            "domains": n_domains, "cells": cells, "batched_steps": nsteps, "failed": failed,
+            "batched": {"solves_per_s": n_domains / t_batch, "seconds": t_batch,
+                        "cell_updates_per_s": upd / t_batch},
+            "one_at_a_time": {"solves_per_s": n_al / t_alone, "seconds_per_solve": t_alone / n_al,
+                              "cell_updates_per_s": alone_upd / t_alone, "sample": n_al},
+            "speedup_solves_per_s": (n_domains / t_batch) / (n_al / t_alone)}
+
+
+def L_BATCH_FINISHED():
+    from cipher_b200 import _lib as L
+    return L.BATCH_FINISHED
+
+
+def run_serving(dev: int, rate: float, duration: float):
+    """config 4: Poisson arrivals served with continuous batching vs the same
+    trace served one request at a time (each solved alone, FIFO)"""
+    import cipher_b200 as cb
+    from cipher_b200 import workloads as W
+    trace = W.serving_trace(rate, duration)
+    opts = cb.ts_options(W.trace_problem(trace[0][1], trace[0][2]), "2a", dt0=1e-6, dtmin=1e-12, dtmax=1.0,
+                         reltol=1e-4, abstol=1e-4)
+    srv = cb.Server(opts, "fp64", device=dev, hbm_budget=16 << 30, max_active=512)
+    # warm the kernels and the tile tuner on one request of each kind
+    for kind in ("gg", "alloy"):
+        ex = next(t for t in trace if t[1] == kind)
+        rid = srv.submit(W.trace_problem(ex[1], ex[2]), ex[4], ex[3])
+        while srv.result(rid)[0].state != 2:
+            srv.poll()
+        srv.release(rid)
+    ids, k = [], 0
+    t0 = time.perf_counter()
+    mono0 = time.monotonic()
+    while True:
+        now = time.perf_counter() - t0
+        while k < len(trace) and trace[k][0] <= now:
+            a, kind, args, init, te = trace[k]
+            ids.append((srv.submit(W.trace_problem(kind, args), te, init), a))
+            k += 1
+        queued, active, _ = srv.poll()
+        if queued == 0 and active == 0:
+            if k == len(trace):
+                break
+            time.sleep(max(0.0, min(1e-3, trace[k][0] - (time.perf_counter() - t0))))
+    wall = time.perf_counter() - t0
+    lat, failed = [], 0
+    for rid, a in ids:
+        r, _ = srv.result(rid)
+        failed += r.status != L_BATCH_FINISHED()
+        lat.append(r.t_finish - (mono0 + a) if r.t_finish > 0 else float("nan"))
+    used, peak_b = srv.usage()
+    srv.close()
+    # the same trace one request at a time: each solved alone, FIFO from its arrival
+    solve = []
+    for a, kind, args, init, te in trace:
+        P = W.trace_problem(kind, args)
+        M = cb.Mesh(P)
+        ctx = cb.Context(P, M, "fp64", device=dev)
+        X = ctx.alloc_state()
+        X0 = cb.initial_state_aos(P, M)
+        t1 = time.perf_counter()
+        ctx.from_aos(X0, X)
+        ctx.chem_init(X)
+        cb.TimeStepper(ctx, opts).solve(X, 0.0, te)
+        solve.append(time.perf_counter() - t1)
+    fin, lat1 = 0.0, []
+    for (a, *_), sv in zip(trace, solve):
+        start = max(a, fin)
+        fin = start + sv
+        lat1.append(fin - a)
+    pct = lambda v, q: float(np.percentile(np.asarray(v), q))
+    return {"workload": f"Poisson({rate}/s) arrivals for {duration} s: 3/4 grain growth 64^2-256^2 to t=5, "
+                        f"1/4 binary two-phase calphaddis 64^2-128^2 to t=0.02; RK 2a, rtol=atol=1e-4",
+            "requests": len(trace), "failed": failed,
+            "served": {"solves_per_s": len(trace) / wall, "p50_s": pct(lat, 50), "p99_s": pct(lat, 99),
+                       "peak_hbm_bytes": peak_b},
+            "one_at_a_time": {"solves_per_s": len(trace) / fin, "p50_s": pct(lat1, 50), "p99_s": pct(lat1, 99),
+                              "mean_solve_s": float(np.mean(solve))}}
+
+
 def run_cipher(args, rank, world, local_rank):
     import torch
     import cipher_b200 as cb
@@ -415,6 +605,16 @@ def run_cipher(args, rank, world, local_rank):
                    "samples": c["samples"]},
         "gpu_launches": args.steps,
     }
+    if not args.no_extra and world == 1:
+        for key, fn in (("chemistry", lambda: run_chemistry(dev, 20, peak)),
+                        ("batched", lambda: run_batched(dev, 256, 50.0, 16)),
+                        ("serving", lambda: run_serving(dev, 50.0, 4.0))):
+            t1 = time.time()
+            try:
+                line[key] = fn()
+            except Exception as exc:       # a failed extra leg must not lose the headline line
+                line[key] = {"error": f"{type(exc).__name__}: {exc}"}
+            log(f"{key}: {time.time() - t1:.1f}s")
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -427,6 +627,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="cipher", choices=["cipher", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the chemistry, batched and serving legs reported beside the headline")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
