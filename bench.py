@@ -629,6 +629,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the chemistry, batched and serving legs reported beside the headline")
+    ap.add_argument("--only", choices=["chemistry", "batched", "serving"],
+                    help="run one of the legs beside the headline alone (for profiling) and print its object")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -636,7 +638,15 @@ def main():
     import cipher_b200.build as b
     if not os.path.exists(b.LIB):
         b.build()
-    if args.impl == "reference":
+    if args.only:
+        import torch
+        torch.cuda.set_device(local_rank)
+        peak, _ = hbm_peak()
+        fn = {"chemistry": lambda: run_chemistry(local_rank, args.steps, peak),
+              "batched": lambda: run_batched(local_rank, 256, 50.0, 16),
+              "serving": lambda: run_serving(local_rank, 50.0, 4.0)}[args.only]
+        print(json.dumps({args.only: fn()}), flush=True)
+    elif args.impl == "reference":
         run_reference(args, rank, world)
     else:
         run_cipher(args, rank, world, local_rank)
