@@ -93,6 +93,8 @@ struct cipher_ctx {
     int32_t *d_itflist;
     DevInterface *d_itfs;
     cipher_material *d_mat;
+    cipher_material *d_mat_spec;  /* the materials specialised at one temperature */
+    double *d_tspec;
     int32_t *d_pmm;
     double *d_comp, *d_mob, *d_tcond;
     uint16_t *d_pruned;
@@ -156,6 +158,8 @@ static void free_ctx(cipher_ctx *c)
     cudaFree(c->d_itflist);
     cudaFree(c->d_itfs);
     cudaFree(c->d_mat);
+    cudaFree(c->d_mat_spec);
+    cudaFree(c->d_tspec);
     cudaFree(c->d_pmm);
     cudaFree(c->d_comp);
     cudaFree(c->d_mob);
@@ -321,6 +325,12 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
         size_t nb = (size_t)p->nmat * sizeof(cipher_material);
         if ((e = cudaMalloc(&c->d_mat, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc materials"); }
         if ((e = cudaMemcpy(c->d_mat, p->material, nb, cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy materials"); }
+        if ((e = cudaMalloc(&c->d_mat_spec, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc materials"); }
+        if ((e = cudaMalloc(&c->d_tspec, sizeof(double))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc materials"); }
+        {
+            const double nan = std::nan("");
+            if ((e = cudaMemcpy(c->d_tspec, &nan, sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy"); }
+        }
         nb = (size_t)p->npf * sizeof(int32_t);
         if ((e = cudaMalloc(&c->d_pmm, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc phase map"); }
         if ((e = cudaMemcpy(c->d_pmm, p->phasematerialmapping, nb, cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy phase map"); }
@@ -437,6 +447,8 @@ static GenArgs<R> gen_args(const cipher_ctx *c, const void *X, void *F)
     a.chem.ncp = c->ncp;
     a.chem.ndp = c->ndp;
     a.chem.nmat = c->nmat;
+    a.chem.spec = c->d_mat_spec;
+    a.chem.tspec = c->d_tspec;
     a.nbcs = c->nbcs;
     for (int b = 0; b < c->nbcs; b++) a.bcs[b] = c->bcs[b];
     a.as = (const uint16_t *)(x + c->lay.as_offset);

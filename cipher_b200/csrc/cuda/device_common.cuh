@@ -35,7 +35,20 @@ struct ChemTables {
     const cipher_material *mat;      /* [nmat] */
     const int32_t *pmm;              /* [npf] */
     int ncp, ndp, nmat;
+    /* the CALPHAD materials with every T-series replaced by its value at
+     * *tspec (rhs_general.cu: k_specialise), or NULL */
+    const cipher_material *spec;
+    const double *tspec;
 };
+
+/* the tables a cell at temperature T reads: the specialised copy when it
+ * was made for exactly this T (same values, computed by the same tseries) */
+__device__ __forceinline__ ChemTables chem_at(const ChemTables &t, double T)
+{
+    ChemTables r = t;
+    if (t.spec && T == *t.tspec) r.mat = t.spec;
+    return r;
+}
 
 /* error flags raised by kernels (bit mask); never a trap */
 enum : int {

@@ -139,15 +139,16 @@ __global__ void __launch_bounds__(kGenBlock) k_chem_cell(const GenArgs<R> a)
     double tc = 0.0;
     if (n > 0) {
         const double T = (double)a.tm[c];
+        const ChemTables ch = chem_at(a.chem, T);
         for (int d = 0; d < ndp; d++) mu[d] = a.dp[(int64_t)d * S + c];
         interpolant(a.interp, phi, n, h);
         segregation(a, ids, h, n, ci);
         for (int g = 0; g < n; g++) {
-            const cipher_material &mat = material_of(a.chem, ids[g]);
+            const cipher_material &mat = material_of(ch, ids[g]);
             double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP], me[CIPHER_MAXCP];
             slot_potential(a, mat, mu, ci, c, g, pot);
-            sitefrac(a.chem, ids[g], pot, T, y);
-            mobility(a.chem, ids[g], y, T, me);
+            sitefrac(ch, ids[g], pot, T, y);
+            mobility(ch, ids[g], y, T, me);
             for (int d = 0; d < ncp; d++) mm[d] += h[g] * me[d];
             for (int s = 0; s < mat.nsites; s++)
                 for (int d = 0; d < ncp; d++) cc[d] += h[g] * mat.stoichiometry[s] * y[s * ncp + d];
@@ -218,6 +219,7 @@ __global__ void __launch_bounds__(kGenBlock) k_rhs_general(const GenArgs<R> a, c
     const int n = load_set<PM>(a, c, ids, phi);
     if (n == 0) return;
     const double T = (double)a.tm[c];
+    const ChemTables ch = chem_at(a.chem, T);
     double mu[CIPHER_MAXCP], ldp[CIPHER_MAXCP];
     for (int d = 0; d < ndp; d++) { mu[d] = a.dp[(int64_t)d * S + c]; ldp[d] = 0.0; }
     double ltm = 0.0;
@@ -330,15 +332,18 @@ __global__ void __launch_bounds__(kGenBlock) k_rhs_general(const GenArgs<R> a, c
     double cbar[CIPHER_MAXCP], dcdm[(CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1)];
     for (int d = 0; d < CIPHER_MAXCP; d++) cbar[d] = 0.0;
     for (int q = 0; q < (CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1); q++) dcdm[q] = 0.0;
+    /* tangent of the last phase evaluated: reused by the composition rate
+     * below when the cell has a single phase (same arguments, same bits) */
+    double tpot[2 * 16], tex[2 * 16], tT[2 * CIPHER_MAXCP];
     for (int g = 0; g < n; g++) {
-        const cipher_material &mat = material_of(a.chem, ids[g]);
+        const cipher_material &mat = material_of(ch, ids[g]);
         double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP];
         if (ndp) {
             slot_potential(a, mat, mu, ci, c, g, pot);
-            sitefrac(a.chem, ids[g], pot, T, y);
+            sitefrac(ch, ids[g], pot, T, y);
         }
         if (n > 1) {
-            chem[g] = chemenergy(a.chem, ids[g], y, mu, T);
+            chem[g] = chemenergy(ch, ids[g], y, mu, T);
             for (int s = 0; s < mat.nsites; s++)
                 for (int d = 0; d < ndp; d++) cbar[d] += h[g] * mat.stoichiometry[s] * y[s * ncp + d];
         }
@@ -350,15 +355,14 @@ __global__ void __launch_bounds__(kGenBlock) k_rhs_general(const GenArgs<R> a, c
             }
             /* explicit potential relaxation (src/cipher.c:570-581) */
             double spx[2 * CIPHER_MAXCP];
-            sitepot_explicit(a.chem, ids[g], y, T, spx);
+            sitepot_explicit(ch, ids[g], y, T, spx);
             for (int s = 0; s < mat.nsites; s++)
                 for (int d = 0; d < ndp; d++) {
                     const int64_t pl = (int64_t)(g * SP + s * ndp + d) * S + c;
                     a.fex[pl] = mat.chempot_ex_kineticcoeff * (spx[s * ndp + d] - a.ex[pl]);
                 }
             for (int q = mat.nsites * ndp; q < SP; q++) a.fex[(int64_t)(g * SP + q) * S + c] = 0.0;
-            double tpot[2 * 16], tex[2 * 16], tT[2 * CIPHER_MAXCP];
-            sitefrac_tangent(a.chem, ids[g], y, pot, T, tpot, tex, tT);
+            sitefrac_tangent(ch, ids[g], y, pot, T, tpot, tex, tT);
             for (int s = 0; s < mat.nsites; s++)
                 for (int q = 0; q < ndp * ndp; q++)
                     dcdm[q] += h[g] * mat.stoichiometry[s] * mat.stoichiometry[s] * tpot[s * ndp * ndp + q];
@@ -439,7 +443,7 @@ __global__ void __launch_bounds__(kGenBlock) k_rhs_general(const GenArgs<R> a, c
     /* temperature rate (src/cipher.c:558-568) */
     double cp = 0.0, tr = ltm;
     for (int g = 0; g < n; g++) {
-        const cipher_material &mat = material_of(a.chem, ids[g]);
+        const cipher_material &mat = material_of(ch, ids[g]);
         if (mat.specific_heat.n) cp += h[g] * tseries(T, mat.specific_heat);
         if (mat.latent_heat.n) tr += pf[g] * tseries(T, mat.latent_heat);
     }
@@ -480,7 +484,7 @@ __global__ void __launch_bounds__(kGenBlock) k_rhs_general(const GenArgs<R> a, c
     double src[CIPHER_MAXCP], comp[CIPHER_MAXCP];
     for (int d = 0; d < ncp; d++) { src[d] = 0.0; comp[d] = a.comp[(int64_t)d * S + c]; }
     for (int k = 0; k < n; k++) {
-        const cipher_material &mat = material_of(a.chem, ids[k]);
+        const cipher_material &mat = material_of(ch, ids[k]);
         for (int s = 0; s < mat.nsources; s++) {
             double tmp[CIPHER_MAXCP];
             for (int d = 0; d < ncp; d++) tmp[d] = mat.sources[s].rate[d] * (mat.sources[s].ceq[d] - comp[d]);
@@ -497,12 +501,13 @@ __global__ void __launch_bounds__(kGenBlock) k_rhs_general(const GenArgs<R> a, c
     }
     for (int d = 0; d < ndp; d++) wdp[d] += (ldp[d] + src[d]);
     for (int g = 0; g < n; g++) {
-        const cipher_material &mat = material_of(a.chem, ids[g]);
-        double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP];
-        double tpot[2 * 16], tex[2 * 16], tT[2 * CIPHER_MAXCP];
-        slot_potential(a, mat, mu, ci, c, g, pot);
-        sitefrac(a.chem, ids[g], pot, T, y);
-        sitefrac_tangent(a.chem, ids[g], y, pot, T, tpot, tex, tT);
+        const cipher_material &mat = material_of(ch, ids[g]);
+        if (n > 1) {
+            double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP];
+            slot_potential(a, mat, mu, ci, c, g, pot);
+            sitefrac(ch, ids[g], pot, T, y);
+            sitefrac_tangent(ch, ids[g], y, pot, T, tpot, tex, tT);
+        }
         for (int s = 0; s < mat.nsites; s++) {
             double dex[CIPHER_MAXCP];
             for (int d = 0; d < ndp; d++) dex[d] = a.fex[(int64_t)(g * SP + s * ndp + d) * S + c];
@@ -552,6 +557,73 @@ __global__ void __launch_bounds__(kGenBlock) k_chem_init(const GenArgs<R> a, dou
 }
 
 /* ------------------------------------------------------------------ */
+/* materials specialised at one temperature                             */
+/* ------------------------------------------------------------------ */
+
+/* T-series slot k of a material (0 <= k < kSpecSlots), or NULL.  Quadratic
+ * materials keep their unary and quadratic series, whose T-derivatives the
+ * tangent needs. */
+constexpr int kSpecSlots = 1 + CIPHER_MAXCP * CIPHER_MAXCP + 4 * CIPHER_MAXRKTAB * CIPHER_MAXRK +
+                           CIPHER_MAXCP * (CIPHER_MAXCP + CIPHER_MAXBIN * CIPHER_MAXRK) + 3;
+
+__device__ inline cipher_tseries *spec_slot(cipher_material &m, int k)
+{
+    if (k == 0) return &m.ref;
+    k -= 1;
+    if (k < CIPHER_MAXCP * CIPHER_MAXCP) return m.model == CIPHER_CHEM_QUADRATIC ? nullptr : &m.unary[k];
+    k -= CIPHER_MAXCP * CIPHER_MAXCP;
+    if (k < 4 * CIPHER_MAXRKTAB * CIPHER_MAXRK) {
+        const int tab = k / (CIPHER_MAXRKTAB * CIPHER_MAXRK), e = k % (CIPHER_MAXRKTAB * CIPHER_MAXRK);
+        cipher_rk *rk = tab == 0 ? m.binary : tab == 1 ? m.ternary : tab == 2 ? m.binaryq : m.ternaryq;
+        return &rk[e / CIPHER_MAXRK].h[e % CIPHER_MAXRK];
+    }
+    k -= 4 * CIPHER_MAXRKTAB * CIPHER_MAXRK;
+    if (k < CIPHER_MAXCP * (CIPHER_MAXCP + CIPHER_MAXBIN * CIPHER_MAXRK)) {
+        cipher_mobility &mob = m.mobilityc[k / (CIPHER_MAXCP + CIPHER_MAXBIN * CIPHER_MAXRK)];
+        const int e = k % (CIPHER_MAXCP + CIPHER_MAXBIN * CIPHER_MAXRK);
+        if (e < CIPHER_MAXCP) return &mob.unary[e];
+        const int b = e - CIPHER_MAXCP;
+        return &mob.binary[b / CIPHER_MAXRK].h[b % CIPHER_MAXRK];
+    }
+    k -= CIPHER_MAXCP * (CIPHER_MAXCP + CIPHER_MAXBIN * CIPHER_MAXRK);
+    if (k == 0) return &m.specific_heat;
+    if (k == 1) return &m.latent_heat;
+    if (k == 2) return &m.tconductivity;
+    return nullptr;
+}
+
+/* one block per material: copy it, then replace each T-series s by the
+ * constant series {n = 1, T^0: tseries(T, s)} at T = the first cell's
+ * temperature.  A constant series evaluates to 0.0 + v = v, so every model
+ * function returns the same bits from either copy; cells at another
+ * temperature keep reading the original. */
+template <typename R>
+__global__ void __launch_bounds__(256) k_specialise(const cipher_material *mat, cipher_material *spec, const R *tm,
+                                                    double *tspec)
+{
+    const double T = (double)tm[0];
+    const double *src = (const double *)&mat[blockIdx.x];
+    double *dst = (double *)&spec[blockIdx.x];
+    for (size_t i = threadIdx.x; i < sizeof(cipher_material) / sizeof(double); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    cipher_material &m = spec[blockIdx.x];
+    const cipher_material &o = mat[blockIdx.x];
+    for (int k = threadIdx.x; k < kSpecSlots; k += blockDim.x) {
+        cipher_tseries *ts = spec_slot(m, k);
+        if (!ts) continue;
+        /* the matching slot of the original: same offset */
+        const cipher_tseries *os = (const cipher_tseries *)((const char *)&o + ((const char *)ts - (const char *)&m));
+        if (os->n == 0 && os->logcoeff == 0.0) continue;
+        const double v = tseries(T, *os);
+        ts->n = 1;
+        ts->exp[0] = 0;
+        ts->coeff[0] = v;
+        ts->logcoeff = 0.0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *tspec = T;
+}
+
+/* ------------------------------------------------------------------ */
 /* launchers                                                            */
 /* ------------------------------------------------------------------ */
 
@@ -559,6 +631,9 @@ template <typename R>
 static cudaError_t launch_gen(const GenArgs<R> &a, int dim, cudaStream_t s)
 {
     const unsigned blocks = (unsigned)((a.ncells + kGenBlock - 1) / kGenBlock);
+    if (a.chem.spec)
+        k_specialise<R><<<a.chem.nmat, 256, 0, s>>>(a.chem.mat, (cipher_material *)a.chem.spec, a.tm,
+                                                     (double *)a.chem.tspec);
     if (a.ndp) k_chem_cell<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a);
     k_rhs_general<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a, dim);
     return cudaGetLastError();
