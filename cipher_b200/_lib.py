@@ -116,7 +116,8 @@ class StateLayout(C.Structure):
     _fields_ = [("ncells", C.c_int64), ("stride", C.c_int64), ("pf_size", C.c_int32), ("dp_size", C.c_int32),
                 ("ex_size", C.c_int32), ("precision", C.c_int32), ("as_offset", C.c_int64),
                 ("pf_offset", C.c_int64), ("dp_offset", C.c_int64), ("ex_offset", C.c_int64),
-                ("tm_offset", C.c_int64), ("bytes", C.c_int64)]
+                ("tm_offset", C.c_int64), ("bytes", C.c_int64), ("map_offset", C.c_int64),
+                ("map_planes", C.c_int32)]
 
 
 class GridDesc(C.Structure):
@@ -182,6 +183,7 @@ _SIGNATURES = [
     ("cipher_poststep", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_ctx_check", C.c_int, [C.c_void_p, C.c_void_p]),
     ("cipher_chem_init", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("cipher_state_refresh", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_poststep_noalloc", C.c_int, [C.POINTER(GridDesc), C.c_void_p, C.c_void_p]),
     ("cipher_ts_default_opts", C.c_int, [PP, C.POINTER(TSOpts)]),
     ("cipher_ts_create", C.c_int, [C.c_void_p, C.POINTER(TSOpts), C.POINTER(C.c_void_p)]),

@@ -256,6 +256,7 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
     L.precision = precision;
     int64_t off = 0;
     L.as_offset = off; off = align_up(off + (int64_t)(c->P + 1) * c->stride * 2, 256);
+    L.map_offset = off; L.map_planes = 2 * c->dim; off = align_up(off + (int64_t)L.map_planes * c->stride * 8, 256);
     L.pf_offset = off; off = align_up(off + (int64_t)c->P * c->stride * rb, 256);
     L.dp_offset = off; off = align_up(off + (int64_t)c->ndp * c->stride * 8, 256);
     L.ex_offset = off; off = align_up(off + (int64_t)L.ex_size * c->stride * 8, 256);
@@ -402,6 +403,7 @@ static PfArgs<R> pf_args(const cipher_ctx *c, const void *X, void *F)
     a.itflist = c->d_itflist;
     a.itfs = c->d_itfs;
     a.as = (const uint16_t *)(x + c->lay.as_offset);
+    a.maps = (const uint64_t *)(x + c->lay.map_offset);
     a.phi = (const R *)(x + c->lay.pf_offset);
     a.tm = (const R *)(x + c->lay.tm_offset);
     a.fphi = (R *)(f + c->lay.pf_offset);
@@ -499,6 +501,8 @@ static PostArgs<R> post_args(const cipher_ctx *c, void *X)
     a.P = c->P;
     a.S = c->S;
     a.as = (uint16_t *)(x + c->lay.as_offset);
+    a.maps = (uint64_t *)(x + c->lay.map_offset);
+    a.npf = c->npf;
     a.phi = (R *)(x + c->lay.pf_offset);
     a.ex = (double *)(x + c->lay.ex_offset);
     a.tm = (const R *)(x + c->lay.tm_offset);
@@ -681,11 +685,27 @@ static LayoutArgs layout_args(const cipher_ctx *c, void *X)
     return a;
 }
 
+static cudaError_t build_maps(const cipher_ctx *c, void *X, cudaStream_t s)
+{
+    if (c->precision == CIPHER_PREC_FP64) return launch_build_maps(post_args<double>(c, X), c->dim, s);
+    return launch_build_maps(post_args<float>(c, X), c->dim, s);
+}
+
 extern "C" int cipher_state_from_aos(cipher_ctx *c, const double *aos, void *X, void *stream)
 {
     if (!c || !aos || !X) return set_error(CIPHER_E_ARG, "NULL argument");
     cudaError_t e = launch_aos_to_soa(layout_args(c, X), aos, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "aos->state launch");
+    e = build_maps(c, X, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "face map launch");
+    return CIPHER_OK;
+}
+
+extern "C" int cipher_state_refresh(cipher_ctx *c, void *X, void *stream)
+{
+    if (!c || !X) return set_error(CIPHER_E_ARG, "NULL argument");
+    cudaError_t e = build_maps(c, X, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "face map launch");
     return CIPHER_OK;
 }
 
@@ -712,6 +732,8 @@ extern "C" int cipher_rhs_aos_host(cipher_ctx *c, double t, const double *X_host
     CUDA_TRY(cudaMemcpyAsync(c->d_aos_x, X_host, nb, cudaMemcpyHostToDevice, s), "copy X to device");
     cudaError_t e = launch_aos_to_soa(layout_args(c, c->d_X), c->d_aos_x, s);
     if (e != cudaSuccess) return cuda_fail(e, "aos->state launch");
+    e = build_maps(c, c->d_X, s);
+    if (e != cudaSuccess) return cuda_fail(e, "face map launch");
     int rc = cipher_rhs(c, t, c->d_X, c->d_F, stream);
     if (rc) return rc;
     e = launch_soa_to_aos(layout_args(c, c->d_F), c->d_aos_f, 0, s);

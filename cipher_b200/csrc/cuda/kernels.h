@@ -28,6 +28,7 @@ struct PfArgs {
     const int32_t *itflist;
     const DevInterface *itfs;
     const uint16_t *as;
+    const uint64_t *maps;         /* [2*dim][stride] face maps (cipher_b200.h) */
     const R *phi;
     const R *tm;
     R *fphi;
@@ -114,6 +115,8 @@ struct PostArgs {
     double *ex;
     const R *tm;
     uint16_t *pruned;             /* scratch: pruned sets, [P+1][stride] */
+    uint64_t *maps;               /* face maps rebuilt after the union, or NULL */
+    int npf;
     const double *ex_init;        /* [npf*S] explicit potential of c0 at T0 per phase, or NULL */
     ChemTables chem;              /* with chem.mat set, new phases get SitepotentialExplicit(c0, T) */
     int *err;
@@ -121,6 +124,9 @@ struct PostArgs {
 
 cudaError_t launch_poststep(const PostArgs<double> &a, int dim, cudaStream_t s);
 cudaError_t launch_poststep(const PostArgs<float> &a, int dim, cudaStream_t s);
+/* the face maps of a state from its sets (also part of launch_poststep) */
+cudaError_t launch_build_maps(const PostArgs<double> &a, int dim, cudaStream_t s);
+cudaError_t launch_build_maps(const PostArgs<float> &a, int dim, cudaStream_t s);
 
 /* batched PostStep: domain i owns blocks [block_start[i], block_start[i+1])
  * of 256 cells; domains whose `active` entry is 0 are skipped */

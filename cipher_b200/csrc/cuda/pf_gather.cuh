@@ -6,9 +6,11 @@
  * 235-317); here every cell gathers the contributions of its own faces, in
  * the order the reference's face loop reaches them, so each slot receives
  * the same additions in the same order.  The cell's slots live in shared
- * memory, one column per thread (SlotColumns), and a face is matched by a
- * two-pointer merge of the two sorted sets, as SetIntersection does
- * (src/utility.c:168-190).
+ * memory, one column per thread (SlotColumns).  Which neighbour slot holds
+ * each own phase (SetIntersection, src/utility.c:168-190, with the gate of
+ * src/cipher.c:277) is read from the state's face maps, built from the sets
+ * when they change (poststep.cu: build_maps_cell), so the RHS does no set
+ * merging at all.
  *
  * Launch geometry: blocks of BX x BY cells in (x, y), grid
  * (ceil(res0/BX), ceil(res1/BY), res2): cell coordinates need no integer
@@ -28,28 +30,24 @@ enum GeomMode : int {
     GEOM_UNIT = 2,      /* ff == 1 and vol == 1: flux itself, exact */
 };
 
-/* a thread's slot columns in shared memory: phi and ids at base[g*pst]
- * (a staged tile plane or a private column), the rest at base[g*st] */
+/* a thread's slot columns in shared memory, one entry per slot g at
+ * base[g*st] */
 template <typename R>
 struct SlotColumns {
     R *phi, *aj, *lap, *cap;
     uint16_t *ids;
     uint8_t *nz;                 /* slots with phi != 0, ascending */
-    R *nph;                      /* scratch: the neighbour being merged */
-    uint16_t *nids;
-    int st, pst;
-    __device__ __forceinline__ R &PHI(int g) const { return phi[g * pst]; }
+    int st;
+    __device__ __forceinline__ R &PHI(int g) const { return phi[g * st]; }
     __device__ __forceinline__ R &AJ(int g) const { return aj[g * st]; }
     __device__ __forceinline__ R &LAP(int g) const { return lap[g * st]; }
     __device__ __forceinline__ R &CAP(int g) const { return cap[g * st]; }
-    __device__ __forceinline__ uint16_t &ID(int g) const { return ids[g * pst]; }
+    __device__ __forceinline__ uint16_t &ID(int g) const { return ids[g * st]; }
     __device__ __forceinline__ uint8_t &NZ(int g) const { return nz[g * st]; }
-    __device__ __forceinline__ R &NPH(int g) const { return nph[g * st]; }
-    __device__ __forceinline__ uint16_t &NID(int g) const { return nids[g * st]; }
 };
 
 /* carve the columns of thread `tid` out of a block's dynamic shared memory;
- * layout: R phi,lap,nph[,aj,cap] [PM][bd] | uint16 ids,nids [PM][bd] | uint8 nz [PM][bd] */
+ * layout: R phi,lap[,aj,cap] [PM][bd] | uint16 ids [PM][bd] | uint8 nz [PM][bd] */
 template <typename R>
 __device__ __forceinline__ SlotColumns<R> slot_columns(unsigned char *smem, int PM, int bd, int tid, bool with_aj_cap)
 {
@@ -57,10 +55,8 @@ __device__ __forceinline__ SlotColumns<R> slot_columns(unsigned char *smem, int 
     R *base = (R *)smem;
     int k = 0;
     sc.st = bd;
-    sc.pst = bd;
     sc.phi = base + (size_t)(k++) * PM * bd + tid;
     sc.lap = base + (size_t)(k++) * PM * bd + tid;
-    sc.nph = base + (size_t)(k++) * PM * bd + tid;
     if (with_aj_cap) {
         sc.aj = base + (size_t)(k++) * PM * bd + tid;
         sc.cap = base + (size_t)(k++) * PM * bd + tid;
@@ -69,14 +65,13 @@ __device__ __forceinline__ SlotColumns<R> slot_columns(unsigned char *smem, int 
     }
     uint16_t *ib = (uint16_t *)(base + (size_t)k * PM * bd);
     sc.ids = ib + tid;
-    sc.nids = ib + (size_t)PM * bd + tid;
-    sc.nz = (uint8_t *)(ib + (size_t)2 * PM * bd) + tid;
+    sc.nz = (uint8_t *)(ib + (size_t)PM * bd) + tid;
     return sc;
 }
 
 __host__ __device__ constexpr size_t slot_columns_bytes(int PM, int bd, int rbytes, bool with_aj_cap)
 {
-    return (size_t)PM * bd * ((with_aj_cap ? 5 : 3) * rbytes + 2 * 2 + 1) + 16;
+    return (size_t)PM * bd * ((with_aj_cap ? 4 : 2) * rbytes + 2 + 1) + 16;
 }
 
 template <typename R, bool EXACT>
@@ -88,58 +83,6 @@ __device__ __forceinline__ R face_term(const PfArgs<R> &a, R flux)
         return ((R)a.ffactor * flux) / (R)a.vol;
     } else {
         return (R)a.face_coef * flux;
-    }
-}
-
-/* contributions of the face shared with neighbour nb whose active count nn
- * was already loaded (src/cipher.c:277-288).  Branch-free two-pointer merge
- * of the two sorted sets (SetIntersection, src/utility.c:168-190): both
- * pointers advance by predicate, so a warp's lanes stay converged; the
- * neighbour's entries are read through the read-only cache. */
-template <int PM, typename R, bool EXACT>
-__device__ __forceinline__ void gather_face(const PfArgs<R> &a, const SlotColumns<R> &sc, int n, int64_t nb, int nn,
-                                            bool cell_is_L)
-{
-    const int64_t S = a.stride;
-    if (nn < 1) return;
-    /* the neighbour's set, staged in the scratch columns four slots at a
-     * time: each group's loads issue back to back, so a face costs about
-     * one memory latency per four slots instead of one per slot */
-    for (int j0 = 0; j0 < nn; j0 += 4) {
-        uint16_t ti[4];
-        R tp[4];
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            if (j0 + k < nn) {
-                ti[k] = __ldg(a.as + (int64_t)(1 + j0 + k) * S + nb);
-                tp[k] = __ldg(a.phi + (int64_t)(j0 + k) * S + nb);
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            if (j0 + k < nn) {
-                sc.NID(j0 + k) = ti[k];
-                sc.NPH(j0 + k) = tp[k];
-            }
-        }
-    }
-    uint16_t b = sc.NID(0);
-    uint16_t v = sc.ID(0);
-    /* the phase flux is gated on the L cell only (src/cipher.c:277) */
-    const bool gate = cell_is_L ? (n > 1 || v > 1) : (nn > 1 || b > 1);
-    if (!gate) return;
-    int i = 0, j = 0;
-    while (true) {
-        if (v == b) {
-            const R pn = sc.NPH(j);
-            if (cell_is_L) sc.LAP(i) += face_term<R, EXACT>(a, pn - sc.PHI(i));
-            else sc.LAP(i) -= face_term<R, EXACT>(a, sc.PHI(i) - pn);
-        }
-        i += v <= b;
-        j += v >= b;
-        if (i >= n || j >= nn) break;
-        v = sc.ID(i);
-        b = sc.NID(j);
     }
 }
 
@@ -214,55 +157,79 @@ __device__ __forceinline__ int64_t face_nb(const PfArgs<R> &a, const CellIndex &
     return (co[d] == 0 && a.per[d] && a.res[d] > 1) ? ci.c + (int64_t)(a.res[d] - 1) * st[d] : -1;
 }
 
-/* load the cell's set into its columns and gather its faces in the
- * reference's face order.  Returns the active count (0 for a dead or
- * invalid cell; an invalid one raises ERR_BADSET). */
-template <int DIM, int PM, typename R, bool EXACT>
+/* face-map direction of face position f: 2d for the lower neighbour along
+ * d (without or with wrap), 2d+1 for the upper one */
+template <int DIM>
+__device__ __forceinline__ int face_dir(int f)
+{
+    if (f < DIM) return 2 * (DIM - 1 - f);
+    if (f < 2 * DIM) return 2 * (f - DIM) + 1;
+    return 2 * (f - 2 * DIM);
+}
+
+/* load the cell's phase fractions (and ids when IDS) into its columns and
+ * gather its faces in the reference's face order through the face maps.
+ * Returns the active count (0 for a dead or invalid cell; an invalid count
+ * raises ERR_BADSET). */
+template <int DIM, int PM, typename R, bool EXACT, bool IDS>
 __device__ __forceinline__ int load_and_gather(const PfArgs<R> &a, const CellIndex &ci, const SlotColumns<R> &sc)
 {
     const int64_t S = a.stride, c = ci.c;
     int n = ci.live ? (int)__ldg(&a.as[c]) : 0;
-    /* the neighbours' counts, packed 4 bits per face position (clamped to P;
-     * a neighbour's own thread flags an invalid count) */
-    uint64_t nnp = 0;
-#pragma unroll
-    for (int f = 0; f < 3 * DIM; f++) {
-        const int64_t nb = ci.live ? face_nb<DIM, R>(a, ci, f) : -1;
-        int k = nb >= 0 ? (int)__ldg(&a.as[nb]) : 0;
-        k = k > a.P ? a.P : k;
-        nnp |= (uint64_t)k << (4 * f);
-    }
-    bool ok = true;
-    if (ci.live && (n < 1 || n > a.P)) { ok = false; n = 0; }
-    for (int g0 = 0; g0 < n; g0 += 4) {
-        uint16_t ti[4];
-        R tp[4];
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            if (g0 + k < n) {
-                ti[k] = __ldg(&a.as[(int64_t)(1 + g0 + k) * S + c]);
-                tp[k] = __ldg(&a.phi[(int64_t)(g0 + k) * S + c]);
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            if (g0 + k < n) {
-                sc.ID(g0 + k) = ti[k];
-                sc.PHI(g0 + k) = tp[k];
-                sc.LAP(g0 + k) = (R)0;
-                if (ti[k] >= a.npf) ok = false;
-            }
-        }
-    }
-    if (!ok) {
+    if (ci.live && (n < 1 || n > a.P)) {
         atomicOr(a.err, ERR_BADSET);
         return 0;
     }
     if (n == 0) return 0;
+    /* the face maps first: independent loads, one per face */
+    uint64_t w[3 * DIM];
 #pragma unroll
     for (int f = 0; f < 3 * DIM; f++) {
-        const int nn = (int)(nnp >> (4 * f) & 15u);
-        if (nn) gather_face<PM, R, EXACT>(a, sc, n, face_nb<DIM, R>(a, ci, f), nn, f >= DIM && f < 2 * DIM);
+        const int64_t nb = face_nb<DIM, R>(a, ci, f);
+        w[f] = nb >= 0 ? __ldg(&a.maps[(int64_t)face_dir<DIM>(f) * S + c]) : ~0ull;
+    }
+    for (int g0 = 0; g0 < n; g0 += 4) {
+        R tp[4];
+        uint16_t ti[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (g0 + k < n) {
+                tp[k] = __ldg(&a.phi[(int64_t)(g0 + k) * S + c]);
+                if (IDS) ti[k] = __ldg(&a.as[(int64_t)(1 + g0 + k) * S + c]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (g0 + k < n) {
+                sc.PHI(g0 + k) = tp[k];
+                sc.LAP(g0 + k) = (R)0;
+                if (IDS) sc.ID(g0 + k) = ti[k];
+            }
+        }
+    }
+#pragma unroll
+    for (int f = 0; f < 3 * DIM; f++) {
+        if (w[f] == ~0ull) continue;
+        const int64_t nb = face_nb<DIM, R>(a, ci, f);
+        const bool cell_is_L = f >= DIM && f < 2 * DIM;
+        /* the matched neighbour slots four at a time: loads issue together */
+        for (int i0 = 0; i0 < n; i0 += 4) {
+            R pn[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int j = (int)((w[f] >> (4 * (i0 + k))) & 15u);
+                pn[k] = (i0 + k < n && j < a.P) ? __ldg(&a.phi[(int64_t)j * S + nb]) : (R)0;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int i = i0 + k;
+                const int j = (int)((w[f] >> (4 * i)) & 15u);
+                if (i < n && j < a.P) {
+                    if (cell_is_L) sc.LAP(i) += face_term<R, EXACT>(a, pn[k] - sc.PHI(i));
+                    else sc.LAP(i) -= face_term<R, EXACT>(a, sc.PHI(i) - pn[k]);
+                }
+            }
+        }
     }
     return n;
 }

@@ -201,6 +201,92 @@ __global__ void __launch_bounds__(256) k_post_union(const PostArgs<R> a)
     post_union_cell<DIM, PM, R>(a, c);
 }
 
+/* face maps of cell c (cipher_b200.h, MAP): for each direction q = 2d+side
+ * the neighbour's slot of every own phase, 15 where the neighbour lacks it
+ * or where the face's L cell fails the phase-flux gate of src/cipher.c:277
+ * (the L cell is the lower one of the face, as the reference enumerates
+ * faces (c, c+e_d)).  Invalid sets raise ERR_BADSET. */
+template <int DIM, typename R>
+__device__ __forceinline__ void build_maps_cell(const PostArgs<R> &a, int64_t c)
+{
+    const int64_t S = a.stride;
+    const int res[3] = {a.res[0], a.res[1], a.res[2]};
+    const int64_t st[3] = {1, (int64_t)res[0], (int64_t)res[0] * res[1]};
+    int co[3];
+    co[0] = (int)(c % res[0]);
+    co[1] = DIM > 1 ? (int)((c / res[0]) % res[1]) : 0;
+    co[2] = DIM > 2 ? (int)(c / ((int64_t)res[0] * res[1])) : 0;
+    const int n = a.as[c];
+    bool ok = n >= 1 && n <= a.P;
+    uint16_t own[CIPHER_PMAX];
+    if (ok)
+        for (int k = 0; k < n; k++) {
+            own[k] = a.as[(int64_t)(1 + k) * S + c];
+            if (a.npf > 0 && own[k] >= a.npf) ok = false;
+        }
+    if (!ok) atomicOr(a.err, ERR_BADSET);
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+            int64_t nb = -1;
+            if (side == 0) {
+                if (co[d] > 0) nb = c - st[d];
+                else if (a.per[d] && res[d] > 1) nb = c + (int64_t)(res[d] - 1) * st[d];
+            } else {
+                if (co[d] < res[d] - 1) nb = c + st[d];
+                else if (a.per[d] && res[d] > 1) nb = c - (int64_t)(res[d] - 1) * st[d];
+            }
+            uint64_t w = ~0ull;
+            if (ok && nb >= 0) {
+                const int nn = a.as[nb];
+                if (nn >= 1 && nn <= a.P) {
+                    const bool gate = side == 1 ? (n > 1 || own[0] > 1) : (nn > 1 || a.as[S + nb] > 1);
+                    if (gate) {
+                        int i = 0, j = 0;
+                        while (i < n && j < nn) {
+                            const uint16_t b = a.as[(int64_t)(1 + j) * S + nb];
+                            if (own[i] == b) {
+                                w &= ~(0xFull << (4 * i));
+                                w |= (uint64_t)j << (4 * i);
+                                i++;
+                                j++;
+                            } else if (own[i] < b) {
+                                i++;
+                            } else {
+                                j++;
+                            }
+                        }
+                    }
+                }
+            }
+            a.maps[(int64_t)(2 * d + side) * S + c] = w;
+        }
+    }
+}
+
+template <int DIM, typename R>
+__global__ void __launch_bounds__(256) k_build_maps(const PostArgs<R> a)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.ncells) return;
+    build_maps_cell<DIM, R>(a, c);
+}
+
+template <typename R>
+static cudaError_t launch_maps(const PostArgs<R> &a, int dim, cudaStream_t s)
+{
+    if (!a.maps) return cudaSuccess;
+    const int64_t blocks = (a.ncells + 255) / 256;
+    if (dim == 1) k_build_maps<1, R><<<(unsigned)blocks, 256, 0, s>>>(a);
+    else if (dim == 2) k_build_maps<2, R><<<(unsigned)blocks, 256, 0, s>>>(a);
+    else k_build_maps<3, R><<<(unsigned)blocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_build_maps(const PostArgs<double> &a, int dim, cudaStream_t s) { return launch_maps(a, dim, s); }
+cudaError_t launch_build_maps(const PostArgs<float> &a, int dim, cudaStream_t s) { return launch_maps(a, dim, s); }
+
 /* batched: block k of the list belongs to the domain whose range holds k */
 template <typename R>
 __device__ __forceinline__ int batch_post_domain(const BatchPost<R> &b, int64_t k)
@@ -236,6 +322,18 @@ __global__ void __launch_bounds__(256) k_post_union_batched(const BatchPost<R> b
     post_union_cell<DIM, PM, R>(a, c);
 }
 
+template <int DIM, typename R>
+__global__ void __launch_bounds__(256) k_build_maps_batched(const BatchPost<R> b)
+{
+    const int inst = batch_post_domain(b, blockIdx.x);
+    if (!b.active[inst]) return;
+    const PostArgs<R> &a = b.args[inst];
+    if (!a.maps) return;
+    const int64_t c = (int64_t)(blockIdx.x - b.block_start[inst]) * blockDim.x + threadIdx.x;
+    if (c >= a.ncells) return;
+    build_maps_cell<DIM, R>(a, c);
+}
+
 template <typename R>
 static cudaError_t launch_post_batched(const BatchPost<R> &b, int dim, cudaStream_t s)
 {
@@ -247,6 +345,10 @@ static cudaError_t launch_post_batched(const BatchPost<R> &b, int dim, cudaStrea
     if (dim == 1) k_post_union_batched<1, CIPHER_PMAX, R><<<grid, block, 0, s>>>(b);
     else if (dim == 2) k_post_union_batched<2, CIPHER_PMAX, R><<<grid, block, 0, s>>>(b);
     else k_post_union_batched<3, CIPHER_PMAX, R><<<grid, block, 0, s>>>(b);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (dim == 1) k_build_maps_batched<1, R><<<grid, block, 0, s>>>(b);
+    else if (dim == 2) k_build_maps_batched<2, R><<<grid, block, 0, s>>>(b);
+    else k_build_maps_batched<3, R><<<grid, block, 0, s>>>(b);
     return cudaGetLastError();
 }
 
@@ -264,7 +366,8 @@ static cudaError_t launch_post(const PostArgs<R> &a, int dim, cudaStream_t s)
     if (dim == 1) k_post_union<1, CIPHER_PMAX, R><<<grid, block, 0, s>>>(a);
     else if (dim == 2) k_post_union<2, CIPHER_PMAX, R><<<grid, block, 0, s>>>(a);
     else k_post_union<3, CIPHER_PMAX, R><<<grid, block, 0, s>>>(a);
-    return cudaGetLastError();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return launch_maps(a, dim, s);
 }
 
 cudaError_t launch_poststep(const PostArgs<double> &a, int dim, cudaStream_t s) { return launch_post(a, dim, s); }

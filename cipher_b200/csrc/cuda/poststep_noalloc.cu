@@ -80,6 +80,8 @@ cipher::PostArgs<R> noalloc_args(const cipher_grid_desc *g, void *X, const Noall
     a.P = g->layout.pf_size;
     a.S = g->ex_per_phase;
     a.as = (uint16_t *)(x + g->layout.as_offset);
+    /* the face maps of the layout, when it has them, are rebuilt as well */
+    a.maps = g->layout.map_planes == 2 * g->dim ? (uint64_t *)(x + g->layout.map_offset) : nullptr;
     a.phi = (R *)(x + g->layout.pf_offset);
     a.ex = (double *)(x + g->layout.ex_offset);
     a.tm = (const R *)(x + g->layout.tm_offset);

@@ -40,7 +40,7 @@ template <int DIM, int PM>
 __device__ __forceinline__ void pf_mixed_single_cell(const PfArgs<float> &a, const CellIndex &ci,
                                                      const SlotColumns<float> &sc)
 {
-    const int n = load_and_gather<DIM, PM, float, false>(a, ci, sc);
+    const int n = load_and_gather<DIM, PM, float, false, false>(a, ci, sc);
     if (!ci.live) return;
     const int64_t S = a.stride, c = ci.c;
     uint32_t act = 0;
@@ -100,7 +100,7 @@ template <int DIM, int PM>
 __device__ __forceinline__ void pf_mixed_multi_cell(const PfArgs<float> &a, const CellIndex &ci,
                                                     const SlotColumns<float> &sc)
 {
-    const int n = load_and_gather<DIM, PM, float, false>(a, ci, sc);
+    const int n = load_and_gather<DIM, PM, float, false, true>(a, ci, sc);
     const double T = n == 0 ? 0.0 : (double)a.tm[ci.c];
     cell_rates_ordered<float, false>(a, sc, n, ci.c, ci.live, T);
     if (!ci.live) return;

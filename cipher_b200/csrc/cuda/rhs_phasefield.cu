@@ -31,7 +31,7 @@ template <int DIM, int PM, bool SINGLE>
 __device__ __forceinline__ void pf_fp64_cell(const PfArgs<double> &a, const CellIndex &ci,
                                              const SlotColumns<double> &sc)
 {
-    const int n = load_and_gather<DIM, PM, double, true>(a, ci, sc);
+    const int n = load_and_gather<DIM, PM, double, true, !SINGLE>(a, ci, sc);
     const double T = (SINGLE || n == 0) ? 0.0 : a.tm[ci.c];
     cell_rates_ordered<double, SINGLE>(a, sc, n, ci.c, ci.live, T);
     if (!ci.live) return;

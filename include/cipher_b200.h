@@ -120,14 +120,21 @@ enum { CIPHER_PREC_FP64 = 0,    /* plain FP64 drop-in */
 /*
  * Device state layout (structure of arrays, plane-major, one plane per slot):
  *   AS  uint16 [P+1][stride]   plane 0 = active count n, planes 1..P = sorted ids
+ *   MAP uint64 [2*dim][stride] per cell and face direction (2d: lower, 2d+1:
+ *                              upper neighbour along d): 4 bits per own slot,
+ *                              the neighbour's slot of the same phase or 15;
+ *                              all 15 where the reference's face gate is off.
+ *                              Derived from AS: rebuilt by cipher_poststep,
+ *                              cipher_state_from_aos and cipher_state_refresh
  *   PF  real   [P][stride]     phase fractions of the active phases
  *   DP  double [D][stride]     diffusion potentials mu
  *   EX  double [P*S][stride]   explicit site potentials, slot g*S+s*D+c
  *   TM  real   [stride]        temperature
  * real = double (FP64) or float (MIXED).  Offsets are bytes from the state
  * base pointer; every plane starts on a 256-byte boundary.  The RHS vector F
- * uses the same layout; its AS region is not written (the reference's F is
- * identically zero there).
+ * uses the same layout; its AS and MAP regions are not written (the
+ * reference's F is identically zero there).  AS and MAP together occupy
+ * [as_offset, pf_offset): copying that range copies a state's sets.
  */
 typedef struct cipher_state_layout {
     int64_t ncells;      /* owned cells */
@@ -135,6 +142,8 @@ typedef struct cipher_state_layout {
     int32_t pf_size, dp_size, ex_size, precision;
     int64_t as_offset, pf_offset, dp_offset, ex_offset, tm_offset;
     int64_t bytes;       /* total bytes of one state vector */
+    int64_t map_offset;  /* MAP region (between AS and PF) */
+    int32_t map_planes;  /* 2*dim */
 } cipher_state_layout;
 
 /* create a context on `device` for problem p over mesh m (owned cells only;
@@ -155,6 +164,10 @@ int cipher_poststep(cipher_ctx *c, void *X, void *stream);
 /* synchronise `stream`, then read and clear the error flags the kernels
  * raise instead of trapping (bad active counts, cap overflow) */
 int cipher_ctx_check(cipher_ctx *c, void *stream);
+
+/* rebuild the face maps of X from its active sets, for callers that write
+ * the AS planes themselves (the library's own producers keep them current) */
+int cipher_state_refresh(cipher_ctx *c, void *X, void *stream);
 
 /* chemistry of an initial state whose sets, phi and T are filled (device):
  * EX of every listed phase = SitepotentialExplicit(c0, T), mu = the summed
