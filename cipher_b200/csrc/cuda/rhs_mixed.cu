@@ -86,6 +86,159 @@ __device__ __forceinline__ void pf_mixed_single_cell(const PfArgs<float> &a, con
     a.ftm[c] = (float)tr;
 }
 
+/* ------------------------------------------------------------------ */
+/* single interface: (cell, slot) items spread over the block's threads  */
+/* ------------------------------------------------------------------ */
+/*
+ * One block is one tile of blockDim.x cells.  The face gather, the bulk of
+ * the work, runs over the tile's (cell, slot) items, so a thread never
+ * idles while a neighbour lane walks a larger set:
+ *   1. thread = cell: active count, the cell's face-map words and
+ *      neighbours into shared memory, a block scan of the counts;
+ *   2. thread = item: the slot's phase fraction and its Laplacian over the
+ *      cell's faces in the reference's face order;
+ *   3. thread = cell: the O(n) closed forms of the cell terms and all P
+ *      slots of F (coalesced plane by plane).
+ * Shared memory: tile_bytes(T, P) for T cells.
+ */
+__host__ __device__ constexpr size_t items_tile_bytes(int dim, int T, int P)
+{
+    return (size_t)T * (3 * dim * (8 + 4) + 4 * 4) + (size_t)T * P * (4 + 4 + 1) + 64;
+}
+
+template <int DIM>
+__device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const CellIndex &ci, unsigned char *smem)
+{
+    constexpr int NF = 3 * DIM;
+    const int T = blockDim.x, t = threadIdx.x, P = a.P;
+    const int64_t S = a.stride;
+    uint64_t *sw = (uint64_t *)smem;                              /* [NF][T] */
+    int *snb = (int *)(sw + (size_t)NF * T);                      /* [NF][T] */
+    int *scnt = snb + (size_t)NF * T;                             /* [T] */
+    int *soff = scnt + T;                                         /* [T] */
+    int *scell = soff + T;                                        /* [T] flat cell index */
+    int *swarp = scell + T;                                       /* [T/32] */
+    float *iphi = (float *)(swarp + T);                           /* [T*P] */
+    float *ilap = iphi + (size_t)T * P;                           /* [T*P] */
+    uint8_t *icell = (uint8_t *)(ilap + (size_t)T * P);           /* [T*P] */
+
+    __syncthreads();                 /* the previous tile's readers are done */
+    /* 1. cells */
+    int n = ci.live ? (int)__ldg(&a.as[ci.c]) : 0;
+    if (ci.live && (n < 1 || n > P)) {
+        atomicOr(a.err, ERR_BADSET);
+        n = 0;
+    }
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+        const int64_t nb = n > 0 ? face_nb<DIM, float>(a, ci, f) : -1;
+        sw[f * T + t] = nb >= 0 ? __ldg(&a.maps[(int64_t)face_dir<DIM>(f) * S + ci.c]) : ~0ull;
+        snb[f * T + t] = (int)nb;
+    }
+    scell[t] = (int)ci.c;
+    scnt[t] = n;
+    /* block exclusive scan of the counts */
+    const int lane = t & 31, warp = t >> 5, nwarps = T >> 5;
+    int v = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += y;
+    }
+    if (lane == 31) swarp[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        int u = lane < nwarps ? swarp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, u, o);
+            if (lane >= o) u += y;
+        }
+        if (lane < nwarps) swarp[lane] = u;
+    }
+    __syncthreads();
+    const int off = v - n + (warp > 0 ? swarp[warp - 1] : 0);
+    const int total = swarp[nwarps - 1];
+    soff[t] = off;
+    for (int k = 0; k < n; k++) icell[off + k] = (uint8_t)t;
+    __syncthreads();
+
+    /* 2. items: phase fraction and Laplacian of one slot */
+    const float coef = (float)a.face_coef;
+    for (int it = t; it < total; it += T) {
+        const int cell = icell[it];
+        const int i = it - soff[cell];
+        const float p = __ldg(&a.phi[(int64_t)i * S + scell[cell]]);
+        float l = 0.0f;
+#pragma unroll
+        for (int f = 0; f < NF; f++) {
+            const uint64_t w = sw[f * T + cell];
+            const int j = (int)((w >> (4 * i)) & 15u);
+            if (j < P) {
+                const float pn = __ldg(&a.phi[(int64_t)j * S + snb[f * T + cell]]);
+                if (f >= DIM && f < 2 * DIM) l += coef * (pn - p);
+                else l -= coef * (p - pn);
+            }
+        }
+        iphi[it] = p;
+        ilap[it] = l;
+    }
+    __syncthreads();
+
+    /* 3. cell terms */
+    if (!ci.live) return;
+    const int64_t c = ci.c;
+    uint32_t act = 0;
+    double nact = 0.0, Ca = 0.0;
+    const double mob = a.mob0;
+    if (n > 1) {
+        const float sig = (float)a.sig0, inv_w = (float)(1.0 / a.wid0);
+        const float w_pi2 = (float)(a.wid0 / (CIPHER_PI_D * CIPHER_PI_D));
+        const float tjh = (float)(0.5 * a.tj0);
+        float A = 0.0f, S1 = 0.0f, S2 = 0.0f;
+        for (int k = 0; k < n; k++) {
+            const float p = iphi[off + k];
+            A += p * inv_w + ilap[off + k] * w_pi2;
+            S1 += p;
+            S2 += p * p;
+        }
+        /* capillary force, stored over the consumed Laplacian */
+        double C = 0.0;
+        for (int k = 0; k < n; k++) {
+            const float p = iphi[off + k], l = ilap[off + k];
+            const float ak = p * inv_w + l * w_pi2;
+            const float o1 = S1 - p, o2 = S2 - p * p;
+            const float cap = 8.0f * (-sig * (A - ak) - tjh * (o1 * o1 - o2)) + l;
+            ilap[off + k] = cap;
+            C += (double)cap;
+        }
+        for (int k = 0; k < n; k++) {
+            const double cap = (double)ilap[off + k];
+            const double u = mob * ((double)n * cap - C);
+            const double p = (double)iphi[off + k];
+            const bool on = (p > CIPHER_TOL && p < 1.0 - CIPHER_TOL) || (p < CIPHER_TOL && u > 0.0) ||
+                            (p > 1.0 - CIPHER_TOL && u < 0.0);
+            if (on) { act |= 1u << k; nact += 1.0; Ca += cap; }
+        }
+    }
+    for (int m = 0; m < P; m++) {
+        float vv = 0.0f;
+        if (m < n && (act >> m & 1u)) vv = (float)(mob * (nact * (double)ilap[off + m] - Ca) / nact);
+        a.fphi[(int64_t)m * S + c] = vv;
+    }
+    double tr = 0.0;
+    if (a.has_temp_rate) tr += a.temp_rate;
+    a.ftm[c] = (float)tr;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_items(const PfArgs<float> a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const CellIndex ci = cell_index<kBX, kBY>(a.res);
+    mixed_items_tile<DIM>(a, ci, smem);
+}
+
 template <int DIM, int PM>
 __global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_single(const PfArgs<float> a)
 {
@@ -127,32 +280,10 @@ __global__ void __launch_bounds__(kBX * BY) k_rhs_pf_mixed_batched(const BatchTi
     for (int64_t t = blockIdx.x; t < b.total; t += gridDim.x) {
         int inst;
         const CellIndex ci = batch_cell_index<kBX, BY>(b, t, inst);
-        if (!b.active[inst]) continue;
-        if (SINGLE) pf_mixed_single_cell<DIM, PM>(b.args[inst], ci, sc);
+        if (!b.active[inst]) continue;          /* uniform across the block */
+        if (SINGLE) mixed_items_tile<DIM>(b.args[inst], ci, smem);
         else pf_mixed_multi_cell<DIM, PM>(b.args[inst], ci, sc);
     }
-}
-
-template <int DIM, int PM>
-static void launch_pm(const PfArgs<float> &a, cudaStream_t s)
-{
-    dim3 grid((unsigned)((a.res[0] + kBX - 1) / kBX), (unsigned)((a.res[1] + kBY - 1) / kBY), (unsigned)a.res[2]);
-    if (a.single) {
-        size_t sm = slot_columns_bytes(a.P, kMixedBlock, 4, false);
-        k_rhs_pf_mixed_single<DIM, PM><<<grid, kMixedBlock, sm, s>>>(a);
-    } else {
-        size_t sm = slot_columns_bytes(a.P, kMixedBlock, 4, true);
-        k_rhs_pf_mixed_multi<DIM, PM><<<grid, kMixedBlock, sm, s>>>(a);
-    }
-}
-
-template <int DIM>
-static void launch_dim(const PfArgs<float> &a, cudaStream_t s)
-{
-    if (a.P <= 4) launch_pm<DIM, 4>(a, s);
-    else if (a.P <= 8) launch_pm<DIM, 8>(a, s);
-    else if (a.P <= 12) launch_pm<DIM, 12>(a, s);
-    else launch_pm<DIM, 16>(a, s);
 }
 
 /* dynamic shared memory above the default 48 KB needs the kernel's opt-in;
@@ -172,10 +303,33 @@ static cudaError_t allow_smem(K kernel, size_t bytes)
     return e;
 }
 
+template <int DIM, int PM>
+static void launch_pm(const PfArgs<float> &a, cudaStream_t s)
+{
+    dim3 grid((unsigned)((a.res[0] + kBX - 1) / kBX), (unsigned)((a.res[1] + kBY - 1) / kBY), (unsigned)a.res[2]);
+    if (a.single) {
+        const size_t sm = items_tile_bytes(DIM, kMixedBlock, a.P);
+        if (allow_smem(k_rhs_pf_mixed_items<DIM>, sm) != cudaSuccess) return;
+        k_rhs_pf_mixed_items<DIM><<<grid, kMixedBlock, sm, s>>>(a);
+    } else {
+        size_t sm = slot_columns_bytes(a.P, kMixedBlock, 4, true);
+        k_rhs_pf_mixed_multi<DIM, PM><<<grid, kMixedBlock, sm, s>>>(a);
+    }
+}
+
+template <int DIM>
+static void launch_dim(const PfArgs<float> &a, cudaStream_t s)
+{
+    if (a.P <= 4) launch_pm<DIM, 4>(a, s);
+    else if (a.P <= 8) launch_pm<DIM, 8>(a, s);
+    else if (a.P <= 12) launch_pm<DIM, 12>(a, s);
+    else launch_pm<DIM, 16>(a, s);
+}
+
 template <int DIM, int PM, bool SINGLE>
 static cudaError_t launch_batched_by(const BatchTiles<float> &b, int by, int grid, cudaStream_t s)
 {
-    const size_t sm = slot_columns_bytes(b.pmax, kBX * by, 4, !SINGLE);
+    const size_t sm = SINGLE ? items_tile_bytes(DIM, kBX * by, b.pmax) : slot_columns_bytes(b.pmax, kBX * by, 4, true);
     cudaError_t e;
     if (by == 1) {
         if ((e = allow_smem(k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 1>, sm)) != cudaSuccess) return e;
