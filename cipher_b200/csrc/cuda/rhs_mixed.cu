@@ -34,58 +34,6 @@ namespace cipher {
 
 constexpr int kBX = CIPHER_MIXED_BX, kBY = CIPHER_MIXED_BY, kMixedBlock = kBX * kBY;
 
-/* one cell of the mixed RHS, single interface (shared by the single-domain
- * and the batched kernels) */
-template <int DIM, int PM>
-__device__ __forceinline__ void pf_mixed_single_cell(const PfArgs<float> &a, const CellIndex &ci,
-                                                     const SlotColumns<float> &sc)
-{
-    const int n = load_and_gather<DIM, PM, float, false, false>(a, ci, sc);
-    if (!ci.live) return;
-    const int64_t S = a.stride, c = ci.c;
-    uint32_t act = 0;
-    double nact = 0.0, Ca = 0.0;
-    const double mob = a.mob0;
-    if (n > 1) {
-        const float sig = (float)a.sig0, inv_w = (float)(1.0 / a.wid0);
-        const float w_pi2 = (float)(a.wid0 / (CIPHER_PI_D * CIPHER_PI_D));
-        const float tjh = (float)(0.5 * a.tj0);
-        float A = 0.0f, S1 = 0.0f, S2 = 0.0f;
-        for (int k = 0; k < n; k++) {
-            const float p = sc.PHI(k);
-            A += p * inv_w + sc.LAP(k) * w_pi2;
-            S1 += p;
-            S2 += p * p;
-        }
-        /* capillary force, stored over the consumed Laplacian */
-        double C = 0.0;
-        for (int k = 0; k < n; k++) {
-            const float p = sc.PHI(k), l = sc.LAP(k);
-            const float ak = p * inv_w + l * w_pi2;
-            const float o1 = S1 - p, o2 = S2 - p * p;
-            const float cap = 8.0f * (-sig * (A - ak) - tjh * (o1 * o1 - o2)) + l;
-            sc.LAP(k) = cap;
-            C += (double)cap;
-        }
-        for (int k = 0; k < n; k++) {
-            const double cap = (double)sc.LAP(k);
-            const double u = mob * ((double)n * cap - C);
-            const double p = (double)sc.PHI(k);
-            const bool on = (p > CIPHER_TOL && p < 1.0 - CIPHER_TOL) || (p < CIPHER_TOL && u > 0.0) ||
-                            (p > 1.0 - CIPHER_TOL && u < 0.0);
-            if (on) { act |= 1u << k; nact += 1.0; Ca += cap; }
-        }
-    }
-    for (int m = 0; m < a.P; m++) {
-        float v = 0.0f;
-        if (m < n && (act >> m & 1u)) v = (float)(mob * (nact * (double)sc.LAP(m) - Ca) / nact);
-        a.fphi[(int64_t)m * S + c] = v;
-    }
-    double tr = 0.0;
-    if (a.has_temp_rate) tr += a.temp_rate;
-    a.ftm[c] = (float)tr;
-}
-
 /* ------------------------------------------------------------------ */
 /* single interface: (cell, slot) items spread over the block's threads  */
 /* ------------------------------------------------------------------ */
@@ -103,23 +51,48 @@ __device__ __forceinline__ void pf_mixed_single_cell(const PfArgs<float> &a, con
  */
 __host__ __device__ constexpr size_t items_tile_bytes(int dim, int T, int P)
 {
-    return (size_t)T * (3 * dim * (8 + 4) + 4 * 4) + (size_t)T * P * (4 + 4 + 1) + 64;
+    return (size_t)T * (2 * dim * (8 + 4) + 3 * 4) + (size_t)T * P * (4 + 1) + 64;
+}
+
+/* Laplacian of slot i of a tile cell over its faces in the reference's face
+ * order (directions through face_dir; `mask` bit f = face position f has a
+ * neighbour) */
+template <int DIM>
+__device__ __forceinline__ float item_laplacian(const PfArgs<float> &a, const uint64_t *sw, const int *snb, int T,
+                                                int cell, int mask, int i, float p, float coef)
+{
+    const int64_t S = a.stride;
+    float pn[3 * DIM];
+    bool on[3 * DIM];
+#pragma unroll
+    for (int f = 0; f < 3 * DIM; f++) {
+        const int q = face_dir<DIM>(f);
+        const int j = (int)((sw[q * T + cell] >> (4 * i)) & 15u);
+        on[f] = ((mask >> f) & 1) && j < a.P;
+        pn[f] = on[f] ? __ldg(&a.phi[(int64_t)j * S + snb[q * T + cell]]) : 0.0f;
+    }
+    float l = 0.0f;
+#pragma unroll
+    for (int f = 0; f < 3 * DIM; f++) {
+        if (!on[f]) continue;
+        if (f >= DIM && f < 2 * DIM) l += coef * (pn[f] - p);
+        else l -= coef * (p - pn[f]);
+    }
+    return l;
 }
 
 template <int DIM>
 __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const CellIndex &ci, unsigned char *smem)
 {
-    constexpr int NF = 3 * DIM;
+    constexpr int ND = 2 * DIM;
     const int T = blockDim.x, t = threadIdx.x, P = a.P;
     const int64_t S = a.stride;
-    uint64_t *sw = (uint64_t *)smem;                              /* [NF][T] */
-    int *snb = (int *)(sw + (size_t)NF * T);                      /* [NF][T] */
-    int *scnt = snb + (size_t)NF * T;                             /* [T] */
-    int *soff = scnt + T;                                         /* [T] */
-    int *scell = soff + T;                                        /* [T] flat cell index */
-    int *swarp = scell + T;                                       /* [T/32] */
-    float *iphi = (float *)(swarp + T);                           /* [T*P] */
-    float *ilap = iphi + (size_t)T * P;                           /* [T*P] */
+    uint64_t *sw = (uint64_t *)smem;                              /* [ND][T] face-map words */
+    int *snb = (int *)(sw + (size_t)ND * T);                      /* [ND][T] neighbours */
+    int *soff = snb + (size_t)ND * T;                             /* [T] first item */
+    int *scm = soff + T;                                          /* [T] flat cell index */
+    int *sfm = scm + T;                                           /* [T] face mask, later the warp sums */
+    float *ilap = (float *)(sfm + T);                             /* [T*P] */
     uint8_t *icell = (uint8_t *)(ilap + (size_t)T * P);           /* [T*P] */
 
     __syncthreads();                 /* the previous tile's readers are done */
@@ -129,16 +102,21 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
         atomicOr(a.err, ERR_BADSET);
         n = 0;
     }
+    int mask = 0;
 #pragma unroll
-    for (int f = 0; f < NF; f++) {
+    for (int f = 0; f < 3 * DIM; f++) {
         const int64_t nb = n > 0 ? face_nb<DIM, float>(a, ci, f) : -1;
-        sw[f * T + t] = nb >= 0 ? __ldg(&a.maps[(int64_t)face_dir<DIM>(f) * S + ci.c]) : ~0ull;
-        snb[f * T + t] = (int)nb;
+        if (nb >= 0) {
+            const int q = face_dir<DIM>(f);
+            mask |= 1 << f;
+            sw[q * T + t] = __ldg(&a.maps[(int64_t)q * S + ci.c]);
+            snb[q * T + t] = (int)nb;
+        }
     }
-    scell[t] = (int)ci.c;
-    scnt[t] = n;
+    scm[t] = (int)ci.c;
     /* block exclusive scan of the counts */
     const int lane = t & 31, warp = t >> 5, nwarps = T >> 5;
+    __shared__ int swarp[32];
     int v = n;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -160,32 +138,27 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
     const int off = v - n + (warp > 0 ? swarp[warp - 1] : 0);
     const int total = swarp[nwarps - 1];
     soff[t] = off;
+    sfm[t] = mask;
     for (int k = 0; k < n; k++) icell[off + k] = (uint8_t)t;
     __syncthreads();
 
-    /* 2. items: phase fraction and Laplacian of one slot */
+    /* 2. items, two per pass so that both items' loads are in flight */
     const float coef = (float)a.face_coef;
-    for (int it = t; it < total; it += T) {
-        const int cell = icell[it];
-        const int i = it - soff[cell];
-        const float p = __ldg(&a.phi[(int64_t)i * S + scell[cell]]);
-        float l = 0.0f;
-#pragma unroll
-        for (int f = 0; f < NF; f++) {
-            const uint64_t w = sw[f * T + cell];
-            const int j = (int)((w >> (4 * i)) & 15u);
-            if (j < P) {
-                const float pn = __ldg(&a.phi[(int64_t)j * S + snb[f * T + cell]]);
-                if (f >= DIM && f < 2 * DIM) l += coef * (pn - p);
-                else l -= coef * (p - pn);
-            }
-        }
-        iphi[it] = p;
-        ilap[it] = l;
+    for (int it = t; it < total; it += 2 * T) {
+        const int it2 = it + T;
+        const int c1 = icell[it], i1 = it - soff[c1];
+        const bool two = it2 < total;
+        const int c2 = two ? icell[it2] : c1, i2 = two ? it2 - soff[c2] : i1;
+        const float p1 = __ldg(&a.phi[(int64_t)i1 * S + scm[c1]]);
+        const float p2 = __ldg(&a.phi[(int64_t)i2 * S + scm[c2]]);
+        const float l1 = item_laplacian<DIM>(a, sw, snb, T, c1, sfm[c1], i1, p1, coef);
+        const float l2 = item_laplacian<DIM>(a, sw, snb, T, c2, sfm[c2], i2, p2, coef);
+        ilap[it] = l1;
+        if (two) ilap[it2] = l2;
     }
     __syncthreads();
 
-    /* 3. cell terms */
+    /* 3. cell terms (phase fractions re-read: they are in L1) */
     if (!ci.live) return;
     const int64_t c = ci.c;
     uint32_t act = 0;
@@ -197,7 +170,7 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
         const float tjh = (float)(0.5 * a.tj0);
         float A = 0.0f, S1 = 0.0f, S2 = 0.0f;
         for (int k = 0; k < n; k++) {
-            const float p = iphi[off + k];
+            const float p = __ldg(&a.phi[(int64_t)k * S + c]);
             A += p * inv_w + ilap[off + k] * w_pi2;
             S1 += p;
             S2 += p * p;
@@ -205,7 +178,7 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
         /* capillary force, stored over the consumed Laplacian */
         double C = 0.0;
         for (int k = 0; k < n; k++) {
-            const float p = iphi[off + k], l = ilap[off + k];
+            const float p = __ldg(&a.phi[(int64_t)k * S + c]), l = ilap[off + k];
             const float ak = p * inv_w + l * w_pi2;
             const float o1 = S1 - p, o2 = S2 - p * p;
             const float cap = 8.0f * (-sig * (A - ak) - tjh * (o1 * o1 - o2)) + l;
@@ -215,7 +188,7 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
         for (int k = 0; k < n; k++) {
             const double cap = (double)ilap[off + k];
             const double u = mob * ((double)n * cap - C);
-            const double p = (double)iphi[off + k];
+            const double p = (double)__ldg(&a.phi[(int64_t)k * S + c]);
             const bool on = (p > CIPHER_TOL && p < 1.0 - CIPHER_TOL) || (p < CIPHER_TOL && u > 0.0) ||
                             (p > 1.0 - CIPHER_TOL && u < 0.0);
             if (on) { act |= 1u << k; nact += 1.0; Ca += cap; }
@@ -237,15 +210,6 @@ __global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_items(const PfArgs
     extern __shared__ __align__(16) unsigned char smem[];
     const CellIndex ci = cell_index<kBX, kBY>(a.res);
     mixed_items_tile<DIM>(a, ci, smem);
-}
-
-template <int DIM, int PM>
-__global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_single(const PfArgs<float> a)
-{
-    extern __shared__ __align__(16) unsigned char smem[];
-    const CellIndex ci = cell_index<kBX, kBY>(a.res);
-    const SlotColumns<float> sc = slot_columns<float>(smem, a.P, blockDim.x, threadIdx.x, false);
-    pf_mixed_single_cell<DIM, PM>(a, ci, sc);
 }
 
 /* one cell of the mixed RHS, several interfaces (reference-order cell terms in FP32) */
