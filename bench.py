@@ -419,19 +419,21 @@ def run_serving(dev: int, rate: float, duration: float):
         failed += r.status != L_BATCH_FINISHED()
         lat.append(r.t_finish - (mono0 + a) if r.t_finish > 0 else float("nan"))
     used, peak_b = srv.usage()
+    counters = srv.counters()
     srv.close()
     # the same trace one request at a time: each solved alone, FIFO from its arrival
     solve = []
     for a, kind, args, init, te in trace:
         P = W.trace_problem(kind, args)
-        M = cb.Mesh(P)
+        # the same work the server does per request: grid, context, the
+        # SetUpProblem state on the device, the solve, the result to host
+        t1 = time.perf_counter()
+        M = cb.Mesh(P, grid_only=True)
         ctx = cb.Context(P, M, "fp64", device=dev)
         X = ctx.alloc_state()
-        X0 = cb.initial_state_aos(P, M)
-        t1 = time.perf_counter()
-        ctx.from_aos(X0, X)
-        ctx.chem_init(X)
+        ctx.init_sharp(X)
         cb.TimeStepper(ctx, opts).solve(X, 0.0, te)
+        ctx.to_aos(X)
         solve.append(time.perf_counter() - t1)
     fin, lat1 = 0.0, []
     for (a, *_), sv in zip(trace, solve):
@@ -443,7 +445,7 @@ def run_serving(dev: int, rate: float, duration: float):
                         f"1/4 binary two-phase calphaddis 64^2-128^2 to t=0.02; RK 2a, rtol=atol=1e-4",
             "requests": len(trace), "failed": failed,
             "served": {"solves_per_s": len(trace) / wall, "p50_s": pct(lat, 50), "p99_s": pct(lat, 99),
-                       "peak_hbm_bytes": peak_b},
+                       "peak_hbm_bytes": peak_b, "host_counters": counters},
             "one_at_a_time": {"solves_per_s": len(trace) / fin, "p50_s": pct(lat1, 50), "p99_s": pct(lat1, 99),
                               "mean_solve_s": float(np.mean(solve))}}
 

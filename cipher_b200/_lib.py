@@ -146,6 +146,12 @@ class ServerResult(C.Structure):
                 ("ncells", C.c_int64), ("ndof", C.c_int32), ("footprint", C.c_int64)]
 
 
+class ServerCounters(C.Structure):
+    _fields_ = [("polls", C.c_int64), ("steps", C.c_int64), ("domain_steps", C.c_int64), ("rebuilds", C.c_int64),
+                ("graph_steps", C.c_int64), ("direct_steps", C.c_int64), ("t_admit", C.c_double),
+                ("t_step", C.c_double), ("t_retire", C.c_double)]
+
+
 INIT_SHARP, INIT_DIFFUSE = 0, 1
 TS_RK1FE, TS_RK2A, TS_RK3BS = 0, 1, 2
 BATCH_RUNNING, BATCH_FINISHED, BATCH_FAILED = 0, 1, 2
@@ -172,6 +178,7 @@ _SIGNATURES = [
     ("cipher_problem_alloy", C.c_int,
      [C.c_int, C.POINTER(C.c_int32), C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint, C.POINTER(PP)]),
     ("cipher_mesh_uniform", C.c_int, [PP, C.c_int, C.c_int, C.POINTER(MP)]),
+    ("cipher_mesh_grid", C.c_int, [PP, C.POINTER(MP)]),
     ("cipher_mesh_free", None, [MP]),
     ("cipher_initial_state_aos", C.c_int, [PP, MP, C.POINTER(C.c_double)]),
     ("cipher_initial_state_diffuse_aos", C.c_int, [PP, MP, C.c_double, C.POINTER(C.c_double)]),
@@ -184,6 +191,7 @@ _SIGNATURES = [
     ("cipher_ctx_check", C.c_int, [C.c_void_p, C.c_void_p]),
     ("cipher_chem_init", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_state_refresh", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("cipher_state_init_sharp", C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.c_void_p, C.c_void_p]),
     ("cipher_poststep_noalloc", C.c_int, [C.POINTER(GridDesc), C.c_void_p, C.c_void_p]),
     ("cipher_ts_default_opts", C.c_int, [PP, C.POINTER(TSOpts)]),
     ("cipher_ts_create", C.c_int, [C.c_void_p, C.POINTER(TSOpts), C.POINTER(C.c_void_p)]),
@@ -210,6 +218,9 @@ _SIGNATURES = [
     ("cipher_server_result", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(ServerResult), C.POINTER(C.c_double)]),
     ("cipher_server_release", C.c_int, [C.c_void_p, C.c_int64]),
     ("cipher_server_usage", C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    ("cipher_server_get_counters", C.c_int, [C.c_void_p, C.POINTER(ServerCounters)]),
+    ("cipher_batch_get_counters", C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                            C.POINTER(C.c_int64)]),
     ("cipher_state_from_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_state_to_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_rhs_aos_host", C.c_int,

@@ -80,12 +80,17 @@ class Problem:
 class Mesh:
     """Owns a ``cipher_mesh`` (uniform grid, whole domain or a slab + halo)."""
 
-    def __init__(self, problem: Problem, slab=None):
+    def __init__(self, problem: Problem, slab=None, grid_only: bool = False):
+        """grid_only: the face-list-free grid (cipher_mesh_grid), enough for
+        a device context but not for the host builders or the oracle"""
         self._lib = L.load()
         s = problem.s
-        lo, hi = (0, s.resolution[s.dim - 1]) if slab is None else slab
         out = L.MP()
-        L.check(self._lib.cipher_mesh_uniform(problem.ptr, lo, hi, C.byref(out)), "cipher_mesh_uniform")
+        if grid_only:
+            L.check(self._lib.cipher_mesh_grid(problem.ptr, C.byref(out)), "cipher_mesh_grid")
+        else:
+            lo, hi = (0, s.resolution[s.dim - 1]) if slab is None else slab
+            L.check(self._lib.cipher_mesh_uniform(problem.ptr, lo, hi, C.byref(out)), "cipher_mesh_uniform")
         self.ptr = out
         self.problem = problem
 
@@ -227,6 +232,14 @@ class Context:
 
     def check(self, stream=None):
         L.check(self._lib.cipher_ctx_check(self.ptr, _stream_handle(stream)), "cipher_ctx_check")
+
+    def init_sharp(self, X, stream=None):
+        """the SetUpProblem state built on the device from the problem's voxel map"""
+        vox = np.ascontiguousarray(self.problem.voxelphase(), dtype=np.int32)
+        L.check(self._lib.cipher_state_init_sharp(self.ptr, vox.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                  C.c_void_p(_ptr(X)), _stream_handle(stream)),
+                "cipher_state_init_sharp")
+        return X
 
     def chem_init(self, X, stream=None):
         """EX and mu of an initial state from the materials' c0 (SetUpProblem)."""
@@ -427,6 +440,11 @@ class Server:
 
     def release(self, rid: int):
         L.check(self._lib.cipher_server_release(self.ptr, int(rid)), "cipher_server_release")
+
+    def counters(self) -> dict:
+        c = L.ServerCounters()
+        L.check(self._lib.cipher_server_get_counters(self.ptr, C.byref(c)), "cipher_server_get_counters")
+        return {k: getattr(c, k) for k, _ in L.ServerCounters._fields_}
 
     def usage(self):
         u, p = C.c_int64(), C.c_int64()

@@ -93,6 +93,7 @@ struct cipher_ctx {
     int32_t *d_itflist;
     DevInterface *d_itfs;
     cipher_material *d_mat;
+    double *d_t0;                 /* [npf] temperature0 of each phase's material */
     cipher_material *d_mat_spec;  /* the materials specialised at one temperature */
     double *d_tspec;
     int32_t *d_pmm;
@@ -158,6 +159,7 @@ static void free_ctx(cipher_ctx *c)
     cudaFree(c->d_itflist);
     cudaFree(c->d_itfs);
     cudaFree(c->d_mat);
+    cudaFree(c->d_t0);
     cudaFree(c->d_mat_spec);
     cudaFree(c->d_tspec);
     cudaFree(c->d_pmm);
@@ -341,6 +343,15 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
             if ((e = cudaMalloc(&c->d_mob, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc mobility"); }
             if ((e = cudaMalloc(&c->d_tcond, (size_t)c->stride * sizeof(double))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc conductivity"); }
         }
+    }
+    {
+        double *t0 = (double *)malloc((size_t)p->npf * sizeof(double));
+        if (!t0) { free_ctx(c); return set_error(CIPHER_E_NOMEM, "host allocation"); }
+        for (int a = 0; a < p->npf; a++) t0[a] = p->material[p->phasematerialmapping[a]].temperature0;
+        e = cudaMalloc(&c->d_t0, (size_t)p->npf * sizeof(double));
+        if (e == cudaSuccess) e = cudaMemcpy(c->d_t0, t0, (size_t)p->npf * sizeof(double), cudaMemcpyHostToDevice);
+        free(t0);
+        if (e != cudaSuccess) { free_ctx(c); return cuda_fail(e, "temperature table"); }
     }
     if ((e = cudaMalloc(&c->d_pruned, (size_t)(c->P + 1) * c->stride * sizeof(uint16_t))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc pruned"); }
     if ((e = cudaMalloc(&c->d_err, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc err"); }
@@ -698,6 +709,35 @@ extern "C" int cipher_state_from_aos(cipher_ctx *c, const double *aos, void *X, 
     if (e != cudaSuccess) return cuda_fail(e, "aos->state launch");
     e = build_maps(c, X, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "face map launch");
+    return CIPHER_OK;
+}
+
+extern "C" int cipher_state_init_sharp(cipher_ctx *c, const int32_t *voxelphase, void *X, void *stream)
+{
+    if (!c || !voxelphase || !X) return set_error(CIPHER_E_ARG, "NULL argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    int32_t *d_vox = nullptr;
+    CUDA_TRY(cudaMalloc(&d_vox, (size_t)c->ncells * sizeof(int32_t)), "cudaMalloc voxel map");
+    cudaError_t e = cudaMemcpyAsync(d_vox, voxelphase, (size_t)c->ncells * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+    InitArgs a;
+    memset(&a, 0, sizeof(a));
+    a.L = layout_args(c, X);
+    for (int d = 0; d < 3; d++) { a.res[d] = c->res[d]; a.per[d] = c->per[d]; }
+    a.dim = c->dim;
+    a.npf = c->npf;
+    a.voxel = d_vox;
+    a.t0 = c->d_t0;
+    a.err = c->d_err;
+    if (e == cudaSuccess) e = launch_init_sharp(a, s);
+    if (e == cudaSuccess) e = build_maps(c, X, s);
+    if (e != cudaSuccess) { cudaFree(d_vox); return cuda_fail(e, "initial state"); }
+    int rc = cipher_chem_init(c, X, stream);
+    int flags = 0;
+    if (!rc) rc = read_flags(c, s, &flags);
+    cudaFree(d_vox);
+    if (rc) return rc;
+    if (flags & ERR_CAP) return set_error(CIPHER_E_CAP, "an initial active set exceeds the cap P=%d", c->P);
+    if (flags & ERR_BADSET) return set_error(CIPHER_E_ARG, "voxel map holds a phase outside 0..npf-1");
     return CIPHER_OK;
 }
 

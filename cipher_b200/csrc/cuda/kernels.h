@@ -154,6 +154,16 @@ struct LayoutArgs {
     void *tm;
 };
 cudaError_t launch_aos_to_soa(const LayoutArgs &a, const double *aos, cudaStream_t s);
+
+/* SetUpProblem state from a device voxel map (layout.cu) */
+struct InitArgs {
+    LayoutArgs L;
+    int res[3], per[3], dim, npf;
+    const int32_t *voxel;         /* [ncells] phase per cell */
+    const double *t0;             /* [npf] temperature0 of each phase's material */
+    int *err;
+};
+cudaError_t launch_init_sharp(const InitArgs &a, cudaStream_t s);
 cudaError_t launch_soa_to_aos(const LayoutArgs &a, double *aos, int include_as, cudaStream_t s);
 
 /* what the batch driver needs to know of a context (context.cu) */

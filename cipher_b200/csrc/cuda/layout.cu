@@ -10,6 +10,7 @@
  */
 #include <cstdint>
 #include <cuda_runtime.h>
+#include "device_common.cuh"
 #include "kernels.h"
 
 namespace cipher {
@@ -63,6 +64,68 @@ cudaError_t launch_soa_to_aos(const LayoutArgs &a, double *aos, int include_as, 
 {
     int64_t blocks = (a.ncells + 255) / 256;
     k_soa_to_aos<<<(unsigned)blocks, 256, 0, s>>>(a, aos, include_as);
+    return cudaGetLastError();
+}
+
+/* SetUpProblem state (src/init.c:1739-1827) from the voxel map: the own
+ * phase united with the face neighbours' phases (sorted), phi = 1 for the
+ * own phase, T = its material's temperature0, DP and EX zero (the
+ * chemistry is filled afterwards).  A set above P raises ERR_CAP and is
+ * written truncated. */
+__global__ void __launch_bounds__(256) k_init_sharp(const InitArgs a)
+{
+    const LayoutArgs &L = a.L;
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= L.ncells) return;
+    const int64_t S = L.stride;
+    const int64_t st[3] = {1, (int64_t)a.res[0], (int64_t)a.res[0] * a.res[1]};
+    int co[3];
+    co[0] = (int)(c % a.res[0]);
+    co[1] = (int)((c / a.res[0]) % a.res[1]);
+    co[2] = (int)(c / ((int64_t)a.res[0] * a.res[1]));
+    const int own = a.voxel[c];
+    if (own < 0 || own >= a.npf) {
+        atomicOr(a.err, ERR_BADSET);
+        return;
+    }
+    uint16_t set[CIPHER_PMAX + 1];
+    int n = 1;
+    set[0] = (uint16_t)own;
+    bool over = false;
+    for (int d = 0; d < a.dim; d++)
+        for (int side = 0; side < 2; side++) {
+            int64_t nb;
+            if (side == 0) nb = co[d] > 0 ? c - st[d] : (a.per[d] ? c + (int64_t)(a.res[d] - 1) * st[d] : -1);
+            else nb = co[d] < a.res[d] - 1 ? c + st[d] : (a.per[d] ? c - (int64_t)(a.res[d] - 1) * st[d] : -1);
+            if (nb < 0) continue;
+            const int v = a.voxel[nb];
+            if (v < 0 || v >= a.npf) continue;       /* that cell's own thread flags it */
+            int k = 0;
+            while (k < n && set[k] < v) k++;
+            if (k < n && set[k] == v) continue;
+            if (n == L.P) { over = true; continue; }
+            for (int m = n; m > k; m--) set[m] = set[m - 1];
+            set[k] = (uint16_t)v;
+            n++;
+        }
+    if (over) atomicOr(a.err, ERR_CAP);
+    L.as[c] = (uint16_t)n;
+    for (int k = 0; k < L.P; k++) {
+        L.as[(int64_t)(1 + k) * S + c] = k < n ? set[k] : (uint16_t)0;
+        const double v = (k < n && set[k] == own) ? 1.0 : 0.0;
+        if (L.real_bytes == 8) ((double *)L.phi)[(int64_t)k * S + c] = v;
+        else ((float *)L.phi)[(int64_t)k * S + c] = (float)v;
+    }
+    for (int d = 0; d < L.D; d++) L.dp[(int64_t)d * S + c] = 0.0;
+    for (int q = 0; q < L.E; q++) L.ex[(int64_t)q * S + c] = 0.0;
+    if (L.real_bytes == 8) ((double *)L.tm)[c] = a.t0[own];
+    else ((float *)L.tm)[c] = (float)a.t0[own];
+}
+
+cudaError_t launch_init_sharp(const InitArgs &a, cudaStream_t s)
+{
+    const int64_t blocks = (a.L.ncells + 255) / 256;
+    k_init_sharp<<<(unsigned)blocks, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

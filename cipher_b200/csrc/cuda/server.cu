@@ -61,6 +61,9 @@ struct cipher_server {
     std::vector<Request *> reqs;   /* by id */
     int64_t used, peak;
     int active;
+    cipher_server_counters cnt;
+    double *d_aos;                 /* reusable device buffer of results in AoS layout */
+    size_t aos_cap;
 };
 
 static void drop_device(Request *r)
@@ -98,6 +101,7 @@ extern "C" void cipher_server_destroy(cipher_server *s)
         delete r;
     }
     cipher_batch_destroy(s->batch);
+    cudaFree(s->d_aos);
     delete s;
 }
 
@@ -126,18 +130,26 @@ extern "C" int cipher_server_submit(cipher_server *s, cipher_problem *p, int kin
  * that error (a request that can never run does not block the queue) */
 static int admit(cipher_server *s, Request *r)
 {
-    int rc = cipher_mesh_uniform(r->p, 0, r->p->resolution[r->p->dim - 1], &r->m);
+    /* a sharp start is built on the device from the voxel map and needs only
+     * the grid; a diffuse start is built on the host over the full mesh */
+    const int sharp = r->kind == CIPHER_INIT_SHARP;
+    int rc = sharp ? cipher_mesh_grid(r->p, &r->m) : cipher_mesh_uniform(r->p, 0, r->p->resolution[r->p->dim - 1], &r->m);
     if (!rc) rc = cipher_ctx_create(r->p, r->m, s->o.precision, s->o.device, &r->ctx);
     cipher_state_layout L;
     if (!rc) rc = cipher_ctx_layout(r->ctx, &L);
     double *aos = nullptr, *d_aos = nullptr;
-    if (!rc) {
+    if (!rc && sharp) {
+        if (cudaMalloc(&r->X, (size_t)L.bytes) != cudaSuccess) rc = CIPHER_E_NOMEM;
+        if (!rc && cudaMemset(r->X, 0, (size_t)L.bytes) != cudaSuccess) rc = CIPHER_E_CUDA;
+        if (!rc) rc = cipher_state_init_sharp(r->ctx, r->p->voxelphase, r->X, NULL);
+        r->ncells = L.ncells;
+        r->ndof = cipher_problem_aos_layout(r->p).ndof;
+    } else if (!rc) {
         const cipher_aos_layout A = cipher_problem_aos_layout(r->p);
         const size_t nb = (size_t)r->m->ncells * A.ndof * sizeof(double);
         aos = (double *)malloc(nb);
         if (!aos) rc = CIPHER_E_NOMEM;
-        if (!rc) rc = r->kind == CIPHER_INIT_SHARP ? cipher_initial_state_aos(r->p, r->m, aos)
-                                                   : cipher_initial_state_diffuse_aos(r->p, r->m, r->width, aos);
+        if (!rc) rc = cipher_initial_state_diffuse_aos(r->p, r->m, r->width, aos);
         if (!rc && cudaMalloc(&r->X, (size_t)L.bytes) != cudaSuccess) rc = CIPHER_E_NOMEM;
         if (!rc && cudaMemset(r->X, 0, (size_t)L.bytes) != cudaSuccess) rc = CIPHER_E_CUDA;
         if (!rc && cudaMalloc(&d_aos, nb) != cudaSuccess) rc = CIPHER_E_NOMEM;
@@ -187,6 +199,8 @@ static int64_t footprint(const cipher_server *s, const cipher_problem *p)
 extern "C" int cipher_server_poll(cipher_server *s, int *queued, int *active, int *done)
 {
     if (!s) return cipher_set_error(CIPHER_E_ARG, "NULL argument");
+    s->cnt.polls++;
+    double t0 = now_s();
     /* 1. admission in arrival order */
     while (!s->queue.empty() && s->active < s->o.max_active) {
         Request *r = s->reqs[s->queue.front()];
@@ -210,12 +224,18 @@ extern "C" int cipher_server_poll(cipher_server *s, int *queued, int *active, in
             if (s->used > s->peak) s->peak = s->used;
         }
     }
+    double t1 = now_s();
+    s->cnt.t_admit += t1 - t0;
     /* 2. one step of every admitted domain */
     int running = 0;
     if (s->active > 0) {
         int rc = cipher_batch_step(s->batch, &running);
         if (rc) return rc;
+        s->cnt.steps++;
+        s->cnt.domain_steps += s->active;
     }
+    double t2 = now_s();
+    s->cnt.t_step += t2 - t1;
     /* 3. retirement */
     int ndone = 0;
     for (Request *r : s->reqs) {
@@ -228,13 +248,15 @@ extern "C" int cipher_server_poll(cipher_server *s, int *queued, int *active, in
             r->status = status;
             r->error = error ? error : rc;
             r->result.resize((size_t)r->ncells * r->ndof);
-            double *d_aos = nullptr;
             const size_t nb = r->result.size() * sizeof(double);
-            if (cudaMalloc(&d_aos, nb) == cudaSuccess) {
-                if (cipher_state_to_aos(r->ctx, r->X, d_aos, NULL) == CIPHER_OK)
-                    cudaMemcpy(r->result.data(), d_aos, nb, cudaMemcpyDeviceToHost);
-                cudaFree(d_aos);
+            if (nb > s->aos_cap) {
+                cudaFree(s->d_aos);
+                s->d_aos = nullptr;
+                s->aos_cap = 0;
+                if (cudaMalloc(&s->d_aos, nb + nb / 2) == cudaSuccess) s->aos_cap = nb + nb / 2;
             }
+            if (s->d_aos && cipher_state_to_aos(r->ctx, r->X, s->d_aos, NULL) == CIPHER_OK)
+                cudaMemcpy(r->result.data(), s->d_aos, nb, cudaMemcpyDeviceToHost);
             drop_device(r);
             r->state = 2;
             r->t_finish = now_s();
@@ -243,9 +265,18 @@ extern "C" int cipher_server_poll(cipher_server *s, int *queued, int *active, in
         }
         if (r->state == 2) ndone++;
     }
+    s->cnt.t_retire += now_s() - t2;
     if (queued) *queued = (int)s->queue.size();
     if (active) *active = s->active;
     if (done) *done = ndone;
+    return CIPHER_OK;
+}
+
+extern "C" int cipher_server_get_counters(const cipher_server *s, cipher_server_counters *c)
+{
+    if (!s || !c) return cipher_set_error(CIPHER_E_ARG, "NULL argument");
+    *c = s->cnt;
+    cipher_batch_get_counters(s->batch, &c->rebuilds, &c->graph_steps, &c->direct_steps);
     return CIPHER_OK;
 }
 

@@ -641,52 +641,106 @@ struct cipher_batch {
     char *d_out, *h_out;
     size_t out_bytes;
     cudaGraphExec_t graph;
+    int stable_steps;             /* steps since the last rebuild */
+    int64_t n_rebuilds, n_graph_steps, n_direct_steps;
     std::vector<TuneKey> tuned;
+    /* launch tables live in one device arena, filled by one copy */
+    char *d_arena;
+    size_t arena_cap, ctl_cap, out_cap;
+    std::vector<char> staging;
+    std::vector<std::pair<void **, size_t>> fixups;
 };
 
 
 static double *ctl_h(char *base) { return (double *)base; }
 
+/* append a table to the host staging area; its device pointer is set when
+ * the arena is committed */
 template <typename T_>
-static int upload(T_ **dptr, const std::vector<T_> &v)
+static void stage(cipher_batch *b, T_ **dptr, const std::vector<T_> &v)
 {
-    cudaFree(*dptr);
-    *dptr = nullptr;
-    if (v.empty()) return CIPHER_OK;
-    TS_CUDA(cudaMalloc(dptr, v.size() * sizeof(T_)), "batch table");
-    TS_CUDA(cudaMemcpy(*dptr, v.data(), v.size() * sizeof(T_), cudaMemcpyHostToDevice), "batch table");
+    size_t off = (b->staging.size() + 255) / 256 * 256;
+    b->staging.resize(off + v.size() * sizeof(T_));
+    if (!v.empty()) memcpy(b->staging.data() + off, v.data(), v.size() * sizeof(T_));
+    b->fixups.push_back({(void **)dptr, off});
+}
+
+static int commit_arena(cipher_batch *b)
+{
+    const size_t need = b->staging.size() + 256;
+    if (need > b->arena_cap) {
+        cudaFree(b->d_arena);
+        b->d_arena = nullptr;
+        b->arena_cap = 0;
+        const size_t cap = need + need / 2;
+        TS_CUDA(cudaMalloc(&b->d_arena, cap), "batch tables");
+        b->arena_cap = cap;
+    }
+    if (!b->staging.empty())
+        TS_CUDA(cudaMemcpy(b->d_arena, b->staging.data(), b->staging.size(), cudaMemcpyHostToDevice), "batch tables");
+    for (auto &f : b->fixups) *f.first = b->d_arena + f.second;
+    b->staging.clear();
+    b->fixups.clear();
     return CIPHER_OK;
 }
 
+/* grow-only device / pinned buffers of the control block and the outputs */
+static int ensure_io(cipher_batch *b, size_t ctl, size_t out)
+{
+    if (ctl > b->ctl_cap) {
+        cudaFree(b->d_ctl);
+        if (b->h_ctl) cudaFreeHost(b->h_ctl);
+        b->d_ctl = nullptr;
+        b->h_ctl = nullptr;
+        b->ctl_cap = 0;
+        const size_t cap = ctl + ctl / 2 + 256;
+        TS_CUDA(cudaMalloc(&b->d_ctl, cap), "batch control");
+        TS_CUDA(cudaMallocHost(&b->h_ctl, cap), "batch control");
+        b->ctl_cap = cap;
+    }
+    if (out > b->out_cap) {
+        cudaFree(b->d_out);
+        if (b->h_out) cudaFreeHost(b->h_out);
+        b->d_out = nullptr;
+        b->h_out = nullptr;
+        b->out_cap = 0;
+        const size_t cap = out + out / 2 + 256;
+        TS_CUDA(cudaMalloc(&b->d_out, cap), "batch outputs");
+        TS_CUDA(cudaMallocHost(&b->h_out, cap), "batch outputs");
+        b->out_cap = cap;
+    }
+    return CIPHER_OK;
+}
+
+/* forget the launch tables (their memory is reused by the next rebuild) */
 static void free_tables(cipher_batch *b)
 {
-    for (auto &g : b->groups) {
-        for (int j = 0; j < kMaxStages; j++) cudaFree(g.d_args[j]);
-        cudaFree(g.d_tile_start);
-    }
     b->groups.clear();
-    cudaFree(b->d_comb); b->d_comb = nullptr;
-    cudaFree(b->d_comb_start); b->d_comb_start = nullptr;
-    cudaFree(b->d_gx); b->d_gx = nullptr;
-    cudaFree(b->d_npartial); b->d_npartial = nullptr;
-    cudaFree((void *)b->d_cp_src); b->d_cp_src = nullptr;
-    cudaFree(b->d_cp_dst); b->d_cp_dst = nullptr;
-    cudaFree(b->d_cp_units); b->d_cp_units = nullptr;
-    cudaFree(b->d_cp_start); b->d_cp_start = nullptr;
-    cudaFree((void *)b->d_as_src); b->d_as_src = nullptr;
-    cudaFree(b->d_as_dst); b->d_as_dst = nullptr;
-    cudaFree(b->d_as_units); b->d_as_units = nullptr;
-    cudaFree(b->d_as_start); b->d_as_start = nullptr;
-    cudaFree(b->d_post); b->d_post = nullptr;
-    cudaFree(b->d_post_start); b->d_post_start = nullptr;
-    cudaFree(b->d_ctl); b->d_ctl = nullptr;
-    if (b->h_ctl) cudaFreeHost(b->h_ctl);
-    b->h_ctl = nullptr;
-    cudaFree(b->d_out); b->d_out = nullptr;
-    if (b->h_out) cudaFreeHost(b->h_out);
-    b->h_out = nullptr;
+    b->d_comb = nullptr;
+    b->d_comb_start = b->d_gx = b->d_npartial = nullptr;
+    b->d_cp_src = nullptr;
+    b->d_cp_dst = nullptr;
+    b->d_cp_units = b->d_cp_start = nullptr;
+    b->d_as_src = nullptr;
+    b->d_as_dst = nullptr;
+    b->d_as_units = b->d_as_start = nullptr;
+    b->d_post = nullptr;
+    b->d_post_start = nullptr;
     if (b->graph) cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
+    b->stable_steps = 0;
+}
+
+static void free_buffers(cipher_batch *b)
+{
+    free_tables(b);
+    cudaFree(b->d_arena);
+    cudaFree(b->d_ctl);
+    cudaFree(b->d_out);
+    if (b->h_ctl) cudaFreeHost(b->h_ctl);
+    if (b->h_out) cudaFreeHost(b->h_out);
+    b->d_arena = b->d_ctl = b->d_out = b->h_ctl = b->h_out = nullptr;
+    b->arena_cap = b->ctl_cap = b->out_cap = 0;
 }
 
 static void free_slot(BatchSlot &s)
@@ -730,7 +784,7 @@ extern "C" void cipher_batch_destroy(cipher_batch *b)
     if (!b) return;
     cudaSetDevice(b->device);
     cudaStreamSynchronize(b->stream);
-    free_tables(b);
+    free_buffers(b);
     for (auto &s : b->slots)
         if (s.used) free_slot(s);
     cudaStreamDestroy(b->stream);
@@ -949,6 +1003,7 @@ static int autotune_group(cipher_batch *b, RhsGroup &g)
 
 static int rebuild(cipher_batch *b)
 {
+    b->n_rebuilds++;
     free_tables(b);
     b->dense.clear();
     for (size_t i = 0; i < b->slots.size(); i++)
@@ -957,13 +1012,6 @@ static int rebuild(cipher_batch *b)
     b->dirty = 0;
     if (n == 0) return CIPHER_OK;
     const int ns = b->T.ns;
-    /* outputs first: the error words are referenced by the kernel arguments */
-    b->out_bytes = (size_t)n * (sizeof(double) + sizeof(int));
-    TS_CUDA(cudaMalloc(&b->d_out, b->out_bytes), "batch outputs");
-    TS_CUDA(cudaMemset(b->d_out, 0, b->out_bytes), "batch outputs");
-    TS_CUDA(cudaMallocHost(&b->h_out, b->out_bytes), "batch outputs");
-    int *d_err = (int *)(b->d_out + sizeof(double) * n);
-
     /* RHS groups: phase-field domains by (dim, interface kind); general ones alone */
     for (int i = 0; i < n; i++) {
         const BatchSlot &s = b->slots[b->dense[i]];
@@ -983,11 +1031,15 @@ static int rebuild(cipher_batch *b)
     }
     size_t gsum = 0;
     for (auto &g : b->groups) gsum += g.members.size();
+    /* control block and outputs first: kernel arguments point into them */
     b->ctl_bytes = (size_t)n * sizeof(double) + (size_t)(2 * n + gsum) * sizeof(int);
-    TS_CUDA(cudaMalloc(&b->d_ctl, b->ctl_bytes), "batch control");
+    b->out_bytes = (size_t)n * (sizeof(double) + sizeof(int));
+    int rc0 = ensure_io(b, b->ctl_bytes, b->out_bytes);
+    if (rc0) return rc0;
     TS_CUDA(cudaMemset(b->d_ctl, 0, b->ctl_bytes), "batch control");
-    TS_CUDA(cudaMallocHost(&b->h_ctl, b->ctl_bytes), "batch control");
     memset(b->h_ctl, 0, b->ctl_bytes);
+    TS_CUDA(cudaMemset(b->d_out, 0, b->out_bytes), "batch outputs");
+    int *d_err = (int *)(b->d_out + sizeof(double) * n);
     size_t goff = (size_t)n * sizeof(double) + (size_t)2 * n * sizeof(int);
     for (auto &g : b->groups) {
         g.goff = (int)goff;
@@ -999,19 +1051,17 @@ static int rebuild(cipher_batch *b)
                     BatchSlot &s = b->slots[b->dense[i]];
                     v.push_back(ctx_pf_args_d(s.ctx, stg == 0 ? s.X : s.Y, s.K[stg], d_err + i));
                 }
-                int rc = upload((PfArgs<double> **)&g.d_args[stg], v);
-                if (rc) return rc;
+                stage(b, (PfArgs<double> **)&g.d_args[stg], v);
             } else {
                 std::vector<PfArgs<float>> v;
                 for (int i : g.members) {
                     BatchSlot &s = b->slots[b->dense[i]];
                     v.push_back(ctx_pf_args_f(s.ctx, stg == 0 ? s.X : s.Y, s.K[stg], d_err + i));
                 }
-                int rc = upload((PfArgs<float> **)&g.d_args[stg], v);
-                if (rc) return rc;
+                stage(b, (PfArgs<float> **)&g.d_args[stg], v);
             }
         }
-        TS_CUDA(cudaMalloc(&g.d_tile_start, (g.members.size() + 1) * sizeof(int64_t)), "tiles");
+        stage(b, &g.d_tile_start, std::vector<int64_t>(g.members.size() + 1, 0));
     }
     /* combinations */
     {
@@ -1025,11 +1075,10 @@ static int rebuild(cipher_batch *b)
             np.push_back(s.npartial);
         }
         b->comb_total = st.back();
-        int rc = upload(&b->d_comb, v);
-        if (!rc) rc = upload(&b->d_comb_start, st);
-        if (!rc) rc = upload(&b->d_gx, gx);
-        if (!rc) rc = upload(&b->d_npartial, np);
-        if (rc) return rc;
+        stage(b, &b->d_comb, v);
+        stage(b, &b->d_comb_start, st);
+        stage(b, &b->d_gx, gx);
+        stage(b, &b->d_npartial, np);
     }
     /* copies */
     {
@@ -1050,38 +1099,39 @@ static int rebuild(cipher_batch *b)
         }
         b->cp_total = cst.back();
         b->as_total = ast.back();
-        int rc = upload(&b->d_cp_src, cs);
-        if (!rc) rc = upload(&b->d_cp_dst, cd);
-        if (!rc) rc = upload(&b->d_cp_units, cu);
-        if (!rc) rc = upload(&b->d_cp_start, cst);
-        if (!rc) rc = upload(&b->d_as_src, as);
-        if (!rc) rc = upload(&b->d_as_dst, ad);
-        if (!rc) rc = upload(&b->d_as_units, au);
-        if (!rc) rc = upload(&b->d_as_start, ast);
-        if (rc) return rc;
+        stage(b, (const uint4 ***)&b->d_cp_src, cs);
+        stage(b, &b->d_cp_dst, cd);
+        stage(b, &b->d_cp_units, cu);
+        stage(b, &b->d_cp_start, cst);
+        stage(b, (const uint4 ***)&b->d_as_src, as);
+        stage(b, &b->d_as_dst, ad);
+        stage(b, &b->d_as_units, au);
+        stage(b, &b->d_as_start, ast);
     }
     /* PostStep */
     {
         std::vector<int64_t> st(1, 0);
         for (int i = 0; i < n; i++) st.push_back(st.back() + (b->slots[b->dense[i]].lay.ncells + 255) / 256);
         b->post_total = st.back();
-        int rc = upload(&b->d_post_start, st);
-        if (rc) return rc;
+        stage(b, &b->d_post_start, st);
         if (b->precision == CIPHER_PREC_FP64) {
             std::vector<PostArgs<double>> v;
             for (int i = 0; i < n; i++) {
                 BatchSlot &s = b->slots[b->dense[i]];
                 v.push_back(ctx_post_args_d(s.ctx, s.X, s.pruned, d_err + i));
             }
-            rc = upload((PostArgs<double> **)&b->d_post, v);
+            stage(b, (PostArgs<double> **)&b->d_post, v);
         } else {
             std::vector<PostArgs<float>> v;
             for (int i = 0; i < n; i++) {
                 BatchSlot &s = b->slots[b->dense[i]];
                 v.push_back(ctx_post_args_f(s.ctx, s.X, s.pruned, d_err + i));
             }
-            rc = upload((PostArgs<float> **)&b->d_post, v);
+            stage(b, (PostArgs<float> **)&b->d_post, v);
         }
+    }
+    {
+        int rc = commit_arena(b);
         if (rc) return rc;
     }
     /* tile shapes: every group's domains run during tuning */
@@ -1208,7 +1258,11 @@ extern "C" int cipher_batch_step(cipher_batch *b, int *running)
         for (size_t k = 0; k < g.members.size(); k++) ga[k] = active[g.members[k]];
     }
     if (!any) return cipher_batch_flush(b);
-    if (b->use_graphs) {
+    /* while the membership changes from step to step (a request loop
+     * admitting and retiring), direct launches avoid re-instantiating a
+     * graph per step; a graph is captured once it has held for 3 steps */
+    b->stable_steps++;
+    if (b->use_graphs && b->stable_steps > 3) {
         if (!b->graph) {
             cudaGraph_t gr;
             TS_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
@@ -1221,9 +1275,11 @@ extern "C" int cipher_batch_step(cipher_batch *b, int *running)
             TS_CUDA(e, "graph instantiate");
         }
         TS_CUDA(cudaGraphLaunch(b->graph, b->stream), "graph launch");
+        b->n_graph_steps++;
     } else {
         int rc = launch_step(b);
         if (rc) return rc;
+        b->n_direct_steps++;
     }
     TS_CUDA(cudaStreamSynchronize(b->stream), "step sync");
     const double *norm = (const double *)b->h_out;
@@ -1249,5 +1305,15 @@ extern "C" int cipher_batch_step(cipher_batch *b, int *running)
         if (s.status == CIPHER_BATCH_RUNNING) nrun++;
     }
     if (running) *running = nrun;
+    return CIPHER_OK;
+}
+
+extern "C" int cipher_batch_get_counters(const cipher_batch *b, int64_t *rebuilds, int64_t *graph_steps,
+                                         int64_t *direct_steps)
+{
+    if (!b) return cipher_set_error(CIPHER_E_ARG, "NULL argument");
+    if (rebuilds) *rebuilds = b->n_rebuilds;
+    if (graph_steps) *graph_steps = b->n_graph_steps;
+    if (direct_steps) *direct_steps = b->n_direct_steps;
     return CIPHER_OK;
 }

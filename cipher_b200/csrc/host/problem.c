@@ -298,6 +298,42 @@ int cipher_problem_grain_growth(int dim, const int32_t *res, int ngrains, int ca
 /* uniform meshes                                                      */
 /* ------------------------------------------------------------------ */
 
+/*
+ * The whole-domain grid description a device context needs, without face
+ * lists: nfaces = nbfaces = 0, one cellgeom and cell_global entry.  Enough
+ * for cipher_ctx_create (the device derives faces from the grid); the host
+ * builders and the oracle need cipher_mesh_uniform instead.
+ */
+int cipher_mesh_grid(const cipher_problem *p, cipher_mesh **out)
+{
+    *out = NULL;
+    int dim = p->dim;
+    cipher_mesh *m = (cipher_mesh *)calloc(1, sizeof(cipher_mesh));
+    if (!m) return CIPHER_E_NOMEM;
+    m->dim = dim;
+    m->uniform = 1;
+    long cells = 1;
+    double vol = 1.0;
+    for (int d = 0; d < 3; d++) {
+        int r = d < dim ? p->resolution[d] : 1;
+        m->res[d] = r;
+        m->periodic[d] = d < dim ? (p->periodic[d] && r > 1) : 0;
+        cells *= r;
+        if (d < dim) vol *= p->size[d] / r;
+    }
+    if (cells > 2147483647L) { free(m); return CIPHER_E_ARG; }
+    m->ncells = m->nowned = (int32_t)cells;
+    m->slab_lo = 0;
+    m->slab_hi = m->res[dim - 1];
+    m->cellgeom = (double *)malloc(sizeof(double));
+    m->cell_global = (int32_t *)malloc(sizeof(int32_t));
+    if (!m->cellgeom || !m->cell_global) { cipher_mesh_free(m); return CIPHER_E_NOMEM; }
+    m->cellgeom[0] = pow(vol, 1.0 / dim);
+    m->cell_global[0] = 0;
+    *out = m;
+    return 0;
+}
+
 void cipher_mesh_free(cipher_mesh *m)
 {
     if (!m) return;

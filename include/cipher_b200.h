@@ -96,6 +96,9 @@ double cipher_rand_uniform(uint64_t *state);
 /* uniform leaf mesh; owned planes [slab_lo, slab_hi) of the slowest axis
  * plus a one-cell halo (pass 0, res[dim-1] for the whole domain) */
 int cipher_mesh_uniform(const cipher_problem *p, int slab_lo, int slab_hi, cipher_mesh **out);
+/* the whole-domain grid without face lists (O(1) memory): enough for a
+ * device context, not for the host builders or the oracle */
+int cipher_mesh_grid(const cipher_problem *p, cipher_mesh **out);
 void cipher_mesh_free(cipher_mesh *m);
 
 /* SetUpProblem active sets / phi / T in the reference AoS layout (host) */
@@ -164,6 +167,13 @@ int cipher_poststep(cipher_ctx *c, void *X, void *stream);
 /* synchronise `stream`, then read and clear the error flags the kernels
  * raise instead of trapping (bad active counts, cap overflow) */
 int cipher_ctx_check(cipher_ctx *c, void *stream);
+
+/* the SetUpProblem state (src/init.c:1721-1830) built on the device from
+ * the voxel map (host, x fastest, one phase per cell): sets = own phase and
+ * the face neighbours' phases, phi = 1 for the own phase, T = its
+ * material's temperature0, then the face maps and the chemistry of
+ * cipher_chem_init.  Returns CIPHER_E_CAP when a set exceeds P. */
+int cipher_state_init_sharp(cipher_ctx *c, const int32_t *voxelphase, void *X, void *stream);
 
 /* rebuild the face maps of X from its active sets, for callers that write
  * the AS planes themselves (the library's own producers keep them current) */
@@ -277,6 +287,8 @@ int cipher_batch_flush(cipher_batch *b);
 int cipher_batch_slot_stats(const cipher_batch *b, int slot, cipher_ts_stats *st, int *status, int *error);
 /* 1 (default): replay each step from a CUDA graph; 0: launch directly */
 int cipher_batch_set_graphs(cipher_batch *b, int on);
+/* launch-table rebuilds, and steps replayed from a graph or launched directly */
+int cipher_batch_get_counters(const cipher_batch *b, int64_t *rebuilds, int64_t *graph_steps, int64_t *direct_steps);
 
 /* ------------------------------------------------------------------ */
 /* serving: continuous batching of many simulations on one GPU          */
@@ -321,6 +333,14 @@ int cipher_server_result(const cipher_server *s, int64_t id, cipher_server_resul
 int cipher_server_release(cipher_server *s, int64_t id);
 /* device bytes held by admitted requests now and at most so far */
 int cipher_server_usage(const cipher_server *s, int64_t *used, int64_t *peak);
+
+/* where a server's host time goes */
+typedef struct cipher_server_counters {
+    int64_t polls, steps, domain_steps;      /* batch steps, and domains stepped in them */
+    int64_t rebuilds, graph_steps, direct_steps;
+    double t_admit, t_step, t_retire;        /* seconds in each phase of cipher_server_poll */
+} cipher_server_counters;
+int cipher_server_get_counters(const cipher_server *s, cipher_server_counters *c);
 
 /* reference AoS layout (ncells x ndof doubles, device) <-> device state */
 int cipher_state_from_aos(cipher_ctx *c, const double *aos, void *X, void *stream);

@@ -238,3 +238,30 @@ def test_unsupported_configurations_rejected():
     with pytest.raises(L.CipherError) as e:
         cb.Context(P, M, "fp64")
     assert e.value.code == L.E_UNSUPPORTED
+
+
+@pytest.mark.parametrize("kind", ["gg2d", "gg3d", "alloy"])
+def test_device_initial_state_matches_host(kind):
+    """cipher_state_init_sharp (device, from the voxel map) equals the host
+    SetUpProblem state converted to the device, chemistry included"""
+    if kind == "gg2d":
+        P = cb.Problem.grain_growth(2, [40, 32], 12, 8, 3)
+    elif kind == "gg3d":
+        P = cb.Problem.grain_growth(3, [12, 14, 10], 20, 12, 4)
+    else:
+        P = cb.Problem.alloy(2, [24, 20], "calphad2sl", 4, 6, 8, 7, 0xFF)
+    M = cb.Mesh(P)
+    ctx = cb.Context(P, M, "fp64")
+    Xh = ctx.alloc_state()
+    ctx.from_aos(cb.initial_state_aos(P, M), Xh)
+    ctx.chem_init(Xh)
+    Mg = cb.Mesh(P, grid_only=True)
+    ctxg = cb.Context(P, Mg, "fp64")
+    Xd = ctxg.alloc_state()
+    ctxg.init_sharp(Xd)
+    assert np.array_equal(ctx.to_aos(Xh), ctxg.to_aos(Xd))
+    # and the same RHS (face maps included)
+    Fh, Fd = ctx.alloc_state(), ctxg.alloc_state()
+    ctx.rhs(0.0, Xh, Fh)
+    ctxg.rhs(0.0, Xd, Fd)
+    assert np.array_equal(ctx.to_aos(Fh), ctxg.to_aos(Fd))
