@@ -5,7 +5,7 @@ the C ABI of ``include/cipher_b200.h``; this package is its Python face.
 """
 from ._lib import CipherError, load  # noqa: F401
 from .api import (Batch, Context, Mesh, Problem, Server, TimeStepper, TSView, diffuse_state_aos,  # noqa: F401
-                  initial_state_aos, ts_options)
+                  compute_output, initial_state_aos, ts_options, write_vtu)
 
 __all__ = ["Batch", "CipherError", "Context", "Mesh", "Problem", "Server", "TimeStepper", "TSView", "diffuse_state_aos",
-           "initial_state_aos", "load", "ts_options"]
+           "compute_output", "initial_state_aos", "load", "ts_options", "write_vtu"]

@@ -152,6 +152,11 @@ class ServerCounters(C.Structure):
                 ("t_step", C.c_double), ("t_retire", C.c_double)]
 
 
+class OutputField(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("index", C.c_int32), ("name", C.c_char * 48)]
+
+
+OUT_PHASEID, OUT_MATID, OUT_INTERFACEID, OUT_CHEMPOT, OUT_COMP, OUT_PHI, OUT_TEMPERATURE = range(7)
 INIT_SHARP, INIT_DIFFUSE = 0, 1
 TS_RK1FE, TS_RK2A, TS_RK3BS = 0, 1, 2
 BATCH_RUNNING, BATCH_FINISHED, BATCH_FAILED = 0, 1, 2
@@ -221,6 +226,8 @@ _SIGNATURES = [
     ("cipher_server_get_counters", C.c_int, [C.c_void_p, C.POINTER(ServerCounters)]),
     ("cipher_batch_get_counters", C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                             C.POINTER(C.c_int64)]),
+    ("cipher_output_fields", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    ("cipher_write_vtu", C.c_int, [C.c_char_p, PP, C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
     ("cipher_state_from_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_state_to_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_rhs_aos_host", C.c_int,

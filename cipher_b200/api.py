@@ -461,3 +461,37 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+OUTPUT_KINDS = {"phaseid": L.OUT_PHASEID, "matid": L.OUT_MATID, "interfaceid": L.OUT_INTERFACEID,
+                "chempot": L.OUT_CHEMPOT, "c": L.OUT_COMP, "phi": L.OUT_PHI, "temperature": L.OUT_TEMPERATURE}
+
+
+def output_fields(spec):
+    """[(name, kind, index)] -> ctypes array of cipher_output_field; kind is a
+    key of OUTPUT_KINDS (the reference's output names: phaseid, matid,
+    interfaceid, <comp>_chempot, <comp>_c, <phase>_phi, temperature)"""
+    arr = (L.OutputField * len(spec))()
+    for k, (name, kind, index) in enumerate(spec):
+        arr[k].kind = OUTPUT_KINDS[kind]
+        arr[k].index = int(index)
+        arr[k].name = name.encode()[:47]
+    return arr
+
+
+def compute_output(ctx: Context, X, spec, stream=None) -> np.ndarray:
+    """the derived fields of device state X: [nfields, ncells] (host)"""
+    import torch
+    fields = output_fields(spec)
+    out = torch.empty((len(spec), int(ctx.layout.ncells)), dtype=torch.float64, device=f"cuda:{ctx.device}")
+    L.check(ctx._lib.cipher_output_fields(ctx.ptr, C.c_void_p(_ptr(X)), C.cast(fields, C.c_void_p), len(spec),
+                                          C.c_void_p(_ptr(out)), _stream_handle(stream)), "cipher_output_fields")
+    return out.cpu().numpy()
+
+
+def write_vtu(path: str, problem: Problem, spec, values: np.ndarray):
+    """a .vtu file of the problem's grid with cell data values[nfields, ncells]"""
+    fields = output_fields(spec)
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    L.check(L.load().cipher_write_vtu(path.encode(), problem.ptr, C.cast(fields, C.c_void_p), len(spec),
+                                      v.ctypes.data_as(C.POINTER(C.c_double))), "cipher_write_vtu")

@@ -292,7 +292,7 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
         c->tj0 = t;
     }
     cudaError_t e;
-    if (!single || c->general) {
+    {   /* the pair table: the general kernels look pairs up; so does the output */
         for (int a = 0; a < p->npf; a++)
             for (int b = a + 1; b < p->npf; b++) {
                 int i = p->interfacelist[a * p->npf + b];
@@ -324,6 +324,11 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
         free(h);
         if (e != cudaSuccess) { free_ctx(c); return cuda_fail(e, "interface table"); }
     }
+    {
+        size_t nb = (size_t)p->npf * sizeof(int32_t);
+        if ((e = cudaMalloc(&c->d_pmm, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc phase map"); }
+        if ((e = cudaMemcpy(c->d_pmm, p->phasematerialmapping, nb, cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy phase map"); }
+    }
     if (c->general) {
         size_t nb = (size_t)p->nmat * sizeof(cipher_material);
         if ((e = cudaMalloc(&c->d_mat, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc materials"); }
@@ -334,9 +339,6 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
             const double nan = std::nan("");
             if ((e = cudaMemcpy(c->d_tspec, &nan, sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy"); }
         }
-        nb = (size_t)p->npf * sizeof(int32_t);
-        if ((e = cudaMalloc(&c->d_pmm, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc phase map"); }
-        if ((e = cudaMemcpy(c->d_pmm, p->phasematerialmapping, nb, cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy phase map"); }
         if (c->ndp) {
             nb = (size_t)c->ncp * c->stride * sizeof(double);
             if ((e = cudaMalloc(&c->d_comp, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc composition"); }
@@ -739,6 +741,35 @@ extern "C" int cipher_state_init_sharp(cipher_ctx *c, const int32_t *voxelphase,
     if (flags & ERR_CAP) return set_error(CIPHER_E_CAP, "an initial active set exceeds the cap P=%d", c->P);
     if (flags & ERR_BADSET) return set_error(CIPHER_E_ARG, "voxel map holds a phase outside 0..npf-1");
     return CIPHER_OK;
+}
+
+extern "C" int cipher_output_fields(cipher_ctx *c, const void *X, const cipher_output_field *fields, int nfields,
+                                    double *out, void *stream)
+{
+    if (!c || !X || !fields || !out || nfields < 1) return set_error(CIPHER_E_ARG, "bad argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    int32_t *h = (int32_t *)malloc((size_t)nfields * 2 * sizeof(int32_t));
+    if (!h) return set_error(CIPHER_E_NOMEM, "host allocation");
+    for (int k = 0; k < nfields; k++) {
+        if (fields[k].kind < CIPHER_OUT_PHASEID || fields[k].kind > CIPHER_OUT_TEMPERATURE) {
+            free(h);
+            return set_error(CIPHER_E_ARG, "output field %d: unknown kind %d", k, fields[k].kind);
+        }
+        h[k] = fields[k].kind;
+        h[nfields + k] = fields[k].index;
+    }
+    int32_t *d = nullptr;
+    cudaError_t e = cudaMalloc(&d, (size_t)nfields * 2 * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d, h, (size_t)nfields * 2 * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        if (c->precision == CIPHER_PREC_FP64) e = launch_output_fields(gen_args<double>(c, X, nullptr), d, d + nfields, nfields, out, s);
+        else e = launch_output_fields(gen_args<float>(c, X, nullptr), d, d + nfields, nfields, out, s);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d);
+    free(h);
+    if (e != cudaSuccess) return cuda_fail(e, "output fields");
+    return cipher_ctx_check(c, stream);
 }
 
 extern "C" int cipher_state_refresh(cipher_ctx *c, void *X, void *stream)

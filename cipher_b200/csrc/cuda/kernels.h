@@ -96,6 +96,12 @@ struct GenArgs {
     int *err;
 };
 
+/* output fields of a state (rhs_general.cu); fields are the public
+ * cipher_output_field descriptors in device memory */
+cudaError_t launch_output_fields(const GenArgs<double> &a, const int32_t *kinds, const int32_t *idx, int nf,
+                                 double *out, cudaStream_t s);
+cudaError_t launch_output_fields(const GenArgs<float> &a, const int32_t *kinds, const int32_t *idx, int nf,
+                                 double *out, cudaStream_t s);
 cudaError_t launch_rhs_general(const GenArgs<double> &a, int dim, cudaStream_t s);
 cudaError_t launch_rhs_general(const GenArgs<float> &a, int dim, cudaStream_t s);
 /* EX of every listed phase and mu of the majority phase from the materials'

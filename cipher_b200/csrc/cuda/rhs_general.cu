@@ -26,6 +26,7 @@
  */
 #include <cstdint>
 #include <cuda_runtime.h>
+#include "cipher_b200.h"
 #include "device_common.cuh"
 #include "kernels.h"
 #include "models.cuh"
@@ -555,6 +556,86 @@ __global__ void __launch_bounds__(kGenBlock) k_chem_init(const GenArgs<R> a, dou
         for (int d = 0; d < a.ndp; d++) mu[d] += sp[s * a.ndp + d];
     for (int d = 0; d < a.ndp; d++) dp[(int64_t)d * S + c] = mu[d];
 }
+
+/* ------------------------------------------------------------------ */
+/* output fields (src/cipher.c:976-1078)                                */
+/* ------------------------------------------------------------------ */
+
+template <int PM, typename R>
+__global__ void __launch_bounds__(kGenBlock) k_output_fields(const GenArgs<R> a, const int32_t *kinds,
+                                                             const int32_t *idx, int nf, double *out)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.ncells) return;
+    const int64_t S = a.stride;
+    uint16_t ids[PM];
+    double phi[PM], h[PM];
+    const int n = load_set<PM>(a, c, ids, phi);
+    const double T = n > 0 ? (double)a.tm[c] : 0.0;
+    if (n > 0) interpolant(a.interp, phi, n, h);
+    double comp[CIPHER_MAXCP];
+    bool have_comp = false;
+    for (int k = 0; k < nf; k++) {
+        double v = 0.0;
+        const int kind = kinds[k], ix = idx[k];
+        if (n == 0) {
+            v = 0.0;
+        } else if (kind == CIPHER_OUT_PHASEID || kind == CIPHER_OUT_MATID) {
+            double mx = -CIPHER_LARGE;
+            for (int g = 0; g < n; g++)
+                if (h[g] > mx) {
+                    mx = h[g];
+                    v = kind == CIPHER_OUT_PHASEID ? (double)ids[g] : (double)a.chem.pmm[ids[g]];
+                }
+        } else if (kind == CIPHER_OUT_INTERFACEID) {
+            v = -1.0;
+            for (int k2 = 0; k2 < n; k2++)
+                for (int j = k2 + 1; j < n; j++) v = (double)a.itflist[ids[k2] * a.npf + ids[j]];
+        } else if (kind == CIPHER_OUT_CHEMPOT) {
+            v = (ix >= 0 && ix < a.ndp) ? a.dp[(int64_t)ix * S + c] : 0.0;
+        } else if (kind == CIPHER_OUT_COMP) {
+            if (!have_comp) {
+                for (int d = 0; d < CIPHER_MAXCP; d++) comp[d] = 0.0;
+                if (a.ndp) {
+                    double mu[CIPHER_MAXCP], ci[CIPHER_MAXCP];
+                    for (int d = 0; d < a.ndp; d++) mu[d] = a.dp[(int64_t)d * S + c];
+                    segregation(a, ids, h, n, ci);
+                    for (int g = 0; g < n; g++) {
+                        const cipher_material &mat = material_of(a.chem, ids[g]);
+                        double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP];
+                        slot_potential(a, mat, mu, ci, c, g, pot);
+                        sitefrac(a.chem, ids[g], pot, T, y);
+                        for (int s2 = 0; s2 < mat.nsites; s2++)
+                            for (int d = 0; d < a.ncp; d++)
+                                comp[d] += h[g] * mat.stoichiometry[s2] * y[s2 * a.ncp + d];
+                    }
+                }
+                have_comp = true;
+            }
+            v = (ix >= 0 && ix < a.ncp) ? comp[ix] : 0.0;
+        } else if (kind == CIPHER_OUT_PHI) {
+            for (int g = 0; g < n; g++)
+                if ((int)ids[g] == ix) v = phi[g];
+        } else if (kind == CIPHER_OUT_TEMPERATURE) {
+            v = T;
+        }
+        out[(int64_t)k * a.ncells + c] = v;
+    }
+}
+
+template <typename R>
+static cudaError_t launch_out(const GenArgs<R> &a, const int32_t *kinds, const int32_t *idx, int nf, double *out,
+                              cudaStream_t s)
+{
+    const unsigned blocks = (unsigned)((a.ncells + kGenBlock - 1) / kGenBlock);
+    k_output_fields<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a, kinds, idx, nf, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_output_fields(const GenArgs<double> &a, const int32_t *kinds, const int32_t *idx, int nf,
+                                 double *out, cudaStream_t s) { return launch_out(a, kinds, idx, nf, out, s); }
+cudaError_t launch_output_fields(const GenArgs<float> &a, const int32_t *kinds, const int32_t *idx, int nf,
+                                 double *out, cudaStream_t s) { return launch_out(a, kinds, idx, nf, out, s); }
 
 /* ------------------------------------------------------------------ */
 /* materials specialised at one temperature                             */

@@ -342,6 +342,31 @@ typedef struct cipher_server_counters {
 } cipher_server_counters;
 int cipher_server_get_counters(const cipher_server *s, cipher_server_counters *c);
 
+/* ------------------------------------------------------------------ */
+/* output (the reference's output step in PostStep, src/cipher.c:976-1093) */
+/* ------------------------------------------------------------------ */
+
+enum { CIPHER_OUT_PHASEID = 0,      /* id of the phase with the largest interpolant */
+       CIPHER_OUT_MATID = 1,        /* its material */
+       CIPHER_OUT_INTERFACEID = 2,  /* interface of the cell's last phase pair, -1 for one phase */
+       CIPHER_OUT_CHEMPOT = 3,      /* mu of component `index` (0 for the last component) */
+       CIPHER_OUT_COMP = 4,         /* interpolated composition of component `index` */
+       CIPHER_OUT_PHI = 5,          /* phase fraction of phase `index` (0 where inactive) */
+       CIPHER_OUT_TEMPERATURE = 6 };
+
+typedef struct cipher_output_field {
+    int32_t kind, index;
+    char name[48];               /* array name in the output file */
+} cipher_output_field;
+
+/* derived fields of device state X into the device array out[nfields][ncells] */
+int cipher_output_fields(cipher_ctx *c, const void *X, const cipher_output_field *fields, int nfields, double *out,
+                         void *stream);
+/* a VTK XML unstructured-grid file (.vtu, raw appended data) of the uniform
+ * grid of p with cell-data arrays values[nfields][ncells] (host) */
+int cipher_write_vtu(const char *path, const cipher_problem *p, const cipher_output_field *fields, int nfields,
+                     const double *values);
+
 /* reference AoS layout (ncells x ndof doubles, device) <-> device state */
 int cipher_state_from_aos(cipher_ctx *c, const double *aos, void *X, void *stream);
 int cipher_state_to_aos(cipher_ctx *c, const void *X, double *aos, void *stream);

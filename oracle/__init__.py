@@ -55,6 +55,9 @@ def port():
         lib.oracle_poststep.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]
         lib.oracle_initial_state.restype = C.c_int
         lib.oracle_initial_state.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]
+        lib.oracle_output_fields.restype = C.c_int
+        lib.oracle_output_fields.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32),
+                                             C.POINTER(C.c_int32), C.c_int, C.POINTER(C.c_double)]
         lib.oracle_ts_create.restype = C.c_void_p
         lib.oracle_ts_create.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         lib.oracle_ts_destroy.restype = None
@@ -126,6 +129,19 @@ def port_initial_state(problem, mesh) -> np.ndarray:
     if rc:
         raise RuntimeError(f"oracle_initial_state failed ({rc})")
     return X
+
+
+def port_output_fields(problem, mesh, X: np.ndarray, kinds, idx) -> np.ndarray:
+    """the output step's derived fields of the owned cells: [nfields, nowned]"""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    k = np.ascontiguousarray(kinds, dtype=np.int32)
+    i = np.ascontiguousarray(idx, dtype=np.int32)
+    out = np.zeros((len(k), mesh.nowned), dtype=np.float64)
+    rc = port().oracle_output_fields(_addr(problem), _addr(mesh), _dp(X), k.ctypes.data_as(C.POINTER(C.c_int32)),
+                                     i.ctypes.data_as(C.POINTER(C.c_int32)), len(k), _dp(out))
+    if rc:
+        raise RuntimeError(f"oracle_output_fields failed ({rc})")
+    return out
 
 
 def simplex_projection(v: np.ndarray) -> np.ndarray:

@@ -36,5 +36,7 @@ int oracle_rhs(const cipher_problem *p, const cipher_mesh *m, double t,
                const double *Xlocal, double *F);
 int oracle_poststep(const cipher_problem *p, const cipher_mesh *m, double *X);
 int oracle_initial_state(const cipher_problem *p, const cipher_mesh *m, double *X);
+int oracle_output_fields(const cipher_problem *p, const cipher_mesh *m, const double *X, const int32_t *kinds,
+                         const int32_t *idx, int nf, double *out);
 
 #endif

@@ -570,3 +570,76 @@ int oracle_initial_state(const cipher_problem *p, const cipher_mesh *m, double *
     free(off); free(nbl);
     return rc;
 }
+
+/* derived output fields (cipher.c:990-1078) of the owned cells:
+ * out[k*nowned + c]; kinds/idx as the library's CIPHER_OUT_* descriptors */
+int oracle_output_fields(const cipher_problem *p, const cipher_mesh *m, const double *X, const int32_t *kinds,
+                         const int32_t *idx, int nf, double *out)
+{
+    cipher_aos_layout L = or_layout(p);
+    const int ndof = L.ndof, ncp = p->ncp, ndp = p->ndp, SP = L.sp_size, SF = L.sf_size;
+    uint16_t ids[CIPHER_MAXAP];
+    double h[CIPHER_MAXAP], pot[2 * CIPHER_MAXCP], y[CIPHER_MAXAP * 2 * CIPHER_MAXCP];
+    int n;
+    (void)SF;
+    for (int c = 0; c < m->nowned; c++) {
+        const double *cell = &X[(size_t)c * ndof];
+        decode_set(&cell[L.as_offset], ids, &n);
+        const double *phi = &cell[L.pf_offset];
+        const double *mu = &cell[L.dp_offset];
+        const double *ex = &cell[L.ex_offset];
+        double T = cell[L.tm_offset];
+        or_interpolant(p->interpolation, phi, n, h);
+        for (int k = 0; k < nf; k++) {
+            double v = 0.0, mx;
+            switch (kinds[k]) {
+            case 0: case 1:
+                mx = -CIPHER_LARGE;
+                for (int g = 0; g < n; g++)
+                    if (h[g] > mx) { mx = h[g]; v = kinds[k] == 0 ? (double)ids[g] : (double)p->phasematerialmapping[ids[g]]; }
+                break;
+            case 2:
+                v = -1.0;
+                for (int a = 0; a < n; a++)
+                    for (int b = a + 1; b < n; b++) v = (double)p->interfacelist[ids[a] * p->npf + ids[b]];
+                break;
+            case 3:
+                v = (idx[k] >= 0 && idx[k] < ndp) ? mu[idx[k]] : 0.0;
+                break;
+            case 4: {
+                double ci[CIPHER_MAXCP] = {0}, avg[CIPHER_MAXCP] = {0};
+                if (ndp) {
+                    for (int a = 0; a < n; a++)
+                        for (int b = a + 1; b < n; b++) {
+                            const cipher_interface *itf = pair_interface(p, ids[a], ids[b]);
+                            if (itf->has_potential)
+                                for (int d = 0; d < ndp; d++) ci[d] += h[a] * h[b] * itf->potential[d];
+                        }
+                    for (int g = 0; g < n; g++) {
+                        const cipher_material *mat = or_material(p, ids[g]);
+                        for (int s = 0; s < mat->nsites; s++)
+                            for (int d = 0; d < ndp; d++)
+                                pot[s * ndp + d] = mat->stoichiometry[s] * (mu[d] - ci[d]) - ex[g * SP + s * ndp + d];
+                        or_sitefrac(p, ids[g], pot, T, y);
+                        for (int s = 0; s < mat->nsites; s++)
+                            for (int d = 0; d < ncp; d++) avg[d] += h[g] * mat->stoichiometry[s] * y[s * ncp + d];
+                    }
+                }
+                v = (idx[k] >= 0 && idx[k] < ncp) ? avg[idx[k]] : 0.0;
+                break;
+            }
+            case 5:
+                for (int g = 0; g < n; g++)
+                    if ((int)ids[g] == idx[k]) v = phi[g];
+                break;
+            case 6:
+                v = T;
+                break;
+            default:
+                return 1;
+            }
+            out[(size_t)k * m->nowned + c] = v;
+        }
+    }
+    return 0;
+}
