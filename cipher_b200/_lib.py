@@ -152,6 +152,19 @@ class ServerCounters(C.Structure):
                 ("t_step", C.c_double), ("t_retire", C.c_double)]
 
 
+class Nucleus(C.Structure):
+    _fields_ = [("model", C.c_int32), ("nmatrix", C.c_int32), ("matrix", C.c_int32 * 16),
+                ("active_solutes", C.c_int8 * MAXCP), ("gamma", C.c_double), ("shapefactor", C.c_double),
+                ("minsize", C.c_double), ("atomicvolume", C.c_double), ("lengthscale", C.c_double),
+                ("incubationtimemin", C.c_double), ("liquidus", C.c_double), ("nucleation_rate", C.c_double),
+                ("solvus_temperature_0", C.c_double), ("enthalpy_fusion_0", C.c_double),
+                ("has_solvus_c", C.c_int32), ("has_enthalpy_c", C.c_int32),
+                ("solvus_temperature_c", C.c_double * MAXCP), ("enthalpy_fusion_c", C.c_double * MAXCP)]
+
+
+NUC_CNT, NUC_CONSTANT, NUC_THERMAL, NUC_NONE = 0, 1, 2, 3
+
+
 class OutputField(C.Structure):
     _fields_ = [("kind", C.c_int32), ("index", C.c_int32), ("name", C.c_char * 48)]
 
@@ -228,6 +241,15 @@ _SIGNATURES = [
                                             C.POINTER(C.c_int64)]),
     ("cipher_output_fields", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     ("cipher_write_vtu", C.c_int, [C.c_char_p, PP, C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
+    ("cipher_nucleation_create", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                           C.POINTER(C.c_int32), C.c_int, C.c_void_p, C.c_uint64,
+                                           C.POINTER(C.c_void_p)]),
+    ("cipher_nucleation_destroy", None, [C.c_void_p]),
+    ("cipher_nucleation_step", C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.POINTER(C.c_int),
+                                         C.c_void_p]),
+    ("cipher_nucleation_sites", C.c_int, [C.c_void_p, C.POINTER(C.c_int8), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    ("cipher_ts_set_nucleation", C.c_int, [C.c_void_p, C.c_void_p]),
     ("cipher_state_from_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_state_to_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_rhs_aos_host", C.c_int,

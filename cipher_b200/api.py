@@ -327,6 +327,11 @@ class TimeStepper:
     def set_dt(self, dt: float):
         L.check(self._lib.cipher_ts_set_dt(self.ptr, float(dt)), "cipher_ts_set_dt")
 
+    def set_nucleation(self, nu):
+        L.check(self._lib.cipher_ts_set_nucleation(self.ptr, nu.ptr if nu is not None else None),
+                "cipher_ts_set_nucleation")
+        self._nu = nu
+
     def close(self):
         if self.ptr:
             self._lib.cipher_ts_destroy(self.ptr)
@@ -495,3 +500,69 @@ def write_vtu(path: str, problem: Problem, spec, values: np.ndarray):
     v = np.ascontiguousarray(values, dtype=np.float64)
     L.check(L.load().cipher_write_vtu(path.encode(), problem.ptr, C.cast(fields, C.c_void_p), len(spec),
                                       v.ctypes.data_as(C.POINTER(C.c_double))), "cipher_write_vtu")
+
+
+def nuclei_array(specs) -> "C.Array":
+    """ctypes array of cipher_nucleus from dicts of its fields (matrix and
+    active_solutes as lists)"""
+    arr = (L.Nucleus * len(specs))()
+    for k, d in enumerate(specs):
+        for key, val in d.items():
+            if key == "matrix":
+                arr[k].nmatrix = len(val)
+                for j, v in enumerate(sorted(val)):
+                    arr[k].matrix[j] = int(v)
+            elif key in ("active_solutes", "solvus_temperature_c", "enthalpy_fusion_c"):
+                for j, v in enumerate(val):
+                    getattr(arr[k], key)[j] = v
+            else:
+                setattr(arr[k], key, val)
+    return arr
+
+
+class Nucleation:
+    """Nucleation sites of a context (cipher_nucleation_*)."""
+
+    def __init__(self, ctx: Context, voxelsite, sitephase, sitenucleus, nuclei, seed: int = 1):
+        self._lib = L.load()
+        self.ctx = ctx
+        self.voxelsite = np.ascontiguousarray(voxelsite, dtype=np.int32)
+        self.sitephase = np.ascontiguousarray(sitephase, dtype=np.int32)
+        self.sitenucleus = np.ascontiguousarray(sitenucleus, dtype=np.int32)
+        self.nuclei = nuclei if isinstance(nuclei, C.Array) else nuclei_array(nuclei)
+        self.nsites = len(self.sitephase)
+        out = C.c_void_p()
+        i32 = C.POINTER(C.c_int32)
+        L.check(self._lib.cipher_nucleation_create(ctx.ptr, self.nsites, self.voxelsite.ctypes.data_as(i32),
+                                                   self.sitephase.ctypes.data_as(i32),
+                                                   self.sitenucleus.ctypes.data_as(i32), len(self.nuclei),
+                                                   C.cast(self.nuclei, C.c_void_p), int(seed), C.byref(out)),
+                "cipher_nucleation_create")
+        self.ptr = out
+
+    def step(self, X, t: float, dt: float, stream=None) -> int:
+        nf = C.c_int()
+        L.check(self._lib.cipher_nucleation_step(self.ptr, C.c_void_p(_ptr(X)), float(t), float(dt), C.byref(nf),
+                                                 _stream_handle(stream)), "cipher_nucleation_step")
+        return nf.value
+
+    def sites(self) -> dict:
+        n = self.nsites
+        act = np.zeros(n, dtype=np.int8)
+        arrs = [np.zeros(n) for _ in range(4)]
+        d = C.POINTER(C.c_double)
+        L.check(self._lib.cipher_nucleation_sites(self.ptr, act.ctypes.data_as(C.POINTER(C.c_int8)),
+                                                  *[a.ctypes.data_as(d) for a in arrs]), "cipher_nucleation_sites")
+        return {"active": act, "barrier": arrs[0], "diffusivity": arrs[1], "temperature": arrs[2],
+                "volume": arrs[3]}
+
+    def close(self):
+        if self.ptr:
+            self._lib.cipher_nucleation_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -574,6 +574,10 @@ PostArgs<float> ctx_post_args_f(const cipher_ctx *c, void *X, uint16_t *pruned, 
     a.err = err;
     return a;
 }
+GenArgs<double> ctx_gen_args_d(const cipher_ctx *c, const void *X) { return gen_args<double>(c, X, nullptr); }
+GenArgs<float> ctx_gen_args_f(const cipher_ctx *c, const void *X) { return gen_args<float>(c, X, nullptr); }
+double ctx_cell_volume(const cipher_ctx *c) { return c->vol; }
+
 cudaError_t ctx_rhs_general(const cipher_ctx *c, const void *X, void *F, int *err, cudaStream_t s)
 {
     if (c->precision == CIPHER_PREC_FP64) {

@@ -5,6 +5,7 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include "cipher_b200.h"
 #include "device_common.cuh"
 
 namespace cipher {
@@ -95,6 +96,25 @@ struct GenArgs {
     R *ftm;
     int *err;
 };
+
+/* nucleation (rhs_general.cu): cells of site s are list[start[s] .. start[s+1]) */
+struct NucArgs {
+    int nsites, ncp_stride;               /* per-cell record: 3 + ncp doubles */
+    const int32_t *list;                  /* cells sorted by site */
+    const int64_t *start;                 /* [nsites+1] */
+    const int32_t *site_of;               /* [nlist] site of each listed cell */
+    const int32_t *sitephase, *sitenucleus;
+    const cipher_nucleus *nuclei;
+    const int8_t *active;                 /* [nsites] */
+    double *cellrec;                      /* [nlist][3 + ncp]: ok, barrier, T, diffusivity[ncp] */
+    double *siterec;                      /* [nsites][4 + ncp]: ok, volume, T*vol, barrier*vol, diff*vol[ncp] */
+    const int8_t *fired;                  /* [nsites] */
+    double vol;
+};
+cudaError_t launch_nucleation_sums(const GenArgs<double> &a, const NucArgs &n, int64_t nlist, cudaStream_t s);
+cudaError_t launch_nucleation_sums(const GenArgs<float> &a, const NucArgs &n, int64_t nlist, cudaStream_t s);
+cudaError_t launch_nucleation_reset(const GenArgs<double> &a, const NucArgs &n, int64_t nlist, cudaStream_t s);
+cudaError_t launch_nucleation_reset(const GenArgs<float> &a, const NucArgs &n, int64_t nlist, cudaStream_t s);
 
 /* output fields of a state (rhs_general.cu); fields are the public
  * cipher_output_field descriptors in device memory */
@@ -189,4 +209,7 @@ PfArgs<float> ctx_pf_args_f(const cipher_ctx *c, const void *X, void *F, int *er
 PostArgs<double> ctx_post_args_d(const cipher_ctx *c, void *X, uint16_t *pruned, int *err);
 PostArgs<float> ctx_post_args_f(const cipher_ctx *c, void *X, uint16_t *pruned, int *err);
 cudaError_t ctx_rhs_general(const cipher_ctx *c, const void *X, void *F, int *err, cudaStream_t s);
+GenArgs<double> ctx_gen_args_d(const cipher_ctx *c, const void *X);
+GenArgs<float> ctx_gen_args_f(const cipher_ctx *c, const void *X);
+double ctx_cell_volume(const cipher_ctx *c);
 }  // namespace cipher

@@ -558,6 +558,166 @@ __global__ void __launch_bounds__(kGenBlock) k_chem_init(const GenArgs<R> a, dou
 }
 
 /* ------------------------------------------------------------------ */
+/* nucleation (src/cipher.c:715-867, src/material.c:150-290)            */
+/* ------------------------------------------------------------------ */
+
+/* per listed cell of an active site: whether its phases are all matrix
+ * phases of the site's nucleus, the nucleation barrier, the temperature and
+ * the interpolated diffusivities of the nucleus model */
+template <int PM, typename R>
+__global__ void __launch_bounds__(kGenBlock) k_nuc_cells(const GenArgs<R> a, const NucArgs nu, int64_t nlist)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nlist) return;
+    const int site = nu.site_of[k];
+    double *rec = nu.cellrec + k * (3 + a.ncp);
+    for (int q = 0; q < 3 + a.ncp; q++) rec[q] = 0.0;
+    if (!nu.active[site]) return;
+    const int64_t c = nu.list[k], S = a.stride;
+    uint16_t ids[PM];
+    double phi[PM], h[PM];
+    const int n = load_set<PM>(a, c, ids, phi);
+    if (n == 0) return;
+    const cipher_nucleus &nz = nu.nuclei[nu.sitenucleus[site]];
+    /* active phases within the matrix list (SetIntersection size == n) */
+    int common = 0;
+    {
+        int i = 0, j = 0;
+        while (i < n && j < nz.nmatrix) {
+            if (ids[i] == nz.matrix[j]) { common++; i++; j++; }
+            else if (ids[i] < nz.matrix[j]) i++;
+            else j++;
+        }
+    }
+    if (common != n) return;                      /* rec[0] = 0: the site retires */
+    const double T = (double)a.tm[c];
+    const ChemTables ch = a.chem;
+    interpolant(a.interp, phi, n, h);
+    double barrier = 0.0, diff[CIPHER_MAXCP];
+    for (int d = 0; d < CIPHER_MAXCP; d++) diff[d] = 0.0;
+    if (nz.model == CIPHER_NUC_CNT || nz.model == CIPHER_NUC_THERMAL) {
+        double mu[CIPHER_MAXCP], ci[CIPHER_MAXCP];
+        for (int d = 0; d < a.ndp; d++) mu[d] = a.dp[(int64_t)d * S + c];
+        segregation(a, ids, h, n, ci);
+        double matrixenergy = 0.0, comp[CIPHER_MAXCP];
+        for (int d = 0; d < CIPHER_MAXCP; d++) comp[d] = 0.0;
+        for (int g = 0; g < n; g++) {
+            const cipher_material &mat = material_of(ch, ids[g]);
+            double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP], mob[CIPHER_MAXCP];
+            slot_potential(a, mat, mu, ci, c, g, pot);
+            sitefrac(ch, ids[g], pot, T, y);
+            if (nz.model == CIPHER_NUC_CNT) matrixenergy += h[g] * energy_raw(mat, y, T, a.ncp) / mat.molarvolume;
+            else
+                for (int d = 0; d < a.ncp; d++) {
+                    double avg = 0.0;
+                    for (int s2 = 0; s2 < mat.nsites; s2++) avg += mat.stoichiometry[s2] * y[s2 * a.ncp + d];
+                    comp[d] += h[g] * avg;
+                }
+            mobility_raw(mat, y, T, a.ncp, mob);
+            for (int d = 0; d < a.ncp; d++) diff[d] += h[g] * CIPHER_R_GAS * T * mob[d];
+        }
+        if (nz.model == CIPHER_NUC_CNT) {
+            const int sp = nu.sitephase[site];
+            const cipher_material &ms = material_of(ch, sp);
+            double ex[2 * CIPHER_MAXCP], pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP];
+            sitepot_explicit(ch, sp, ms.c0, T, ex);
+            for (int s2 = 0; s2 < ms.nsites; s2++)
+                for (int d = 0; d < a.ndp; d++)
+                    pot[s2 * a.ndp + d] = ms.stoichiometry[s2] * (mu[d] - ci[d]) - ex[s2 * a.ndp + d];
+            sitefrac(ch, sp, pot, T, y);
+            const double phaseenergy = energy_raw(ms, y, T, a.ncp) / ms.molarvolume;
+            barrier = matrixenergy - phaseenergy;
+        } else {
+            double solvus = nz.solvus_temperature_0, enthalpy = nz.enthalpy_fusion_0;
+            if (nz.has_solvus_c)
+                for (int d = 0; d < a.ncp; d++) solvus += comp[d] * nz.solvus_temperature_c[d];
+            if (nz.has_enthalpy_c)
+                for (int d = 0; d < a.ncp; d++) enthalpy += comp[d] * nz.enthalpy_fusion_c[d];
+            barrier = enthalpy * (1.0 - T / solvus);
+        }
+    }
+    rec[0] = 1.0;
+    rec[1] = barrier;
+    rec[2] = T;
+    for (int d = 0; d < a.ncp; d++) rec[3 + d] = diff[d];
+}
+
+/* one thread per site: the volume sums over its cells in list order */
+__global__ void __launch_bounds__(128) k_nuc_sites(const NucArgs nu, int ncp)
+{
+    const int site = blockIdx.x * blockDim.x + threadIdx.x;
+    if (site >= nu.nsites) return;
+    double *out = nu.siterec + (int64_t)site * (4 + ncp);
+    double ok = 1.0, vol = 0.0, tv = 0.0, gv = 0.0, dv[CIPHER_MAXCP];
+    for (int d = 0; d < CIPHER_MAXCP; d++) dv[d] = 0.0;
+    if (nu.active[site]) {
+        for (int64_t k = nu.start[site]; k < nu.start[site + 1]; k++) {
+            const double *rec = nu.cellrec + k * (3 + ncp);
+            if (rec[0] == 0.0) { ok = 0.0; break; }
+            vol += nu.vol;
+            tv += nu.vol * rec[2];
+            gv += nu.vol * rec[1];
+            for (int d = 0; d < ncp; d++) dv[d] += nu.vol * rec[3 + d];
+        }
+    } else {
+        ok = 0.0;
+    }
+    out[0] = ok;
+    out[1] = vol;
+    out[2] = tv;
+    out[3] = gv;
+    for (int d = 0; d < ncp; d++) out[4 + d] = dv[d];
+}
+
+/* cells of fired sites become their site's phase (src/cipher.c:831-851) */
+template <typename R>
+__global__ void __launch_bounds__(kGenBlock) k_nuc_reset(const GenArgs<R> a, const NucArgs nu, int64_t nlist)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nlist) return;
+    const int site = nu.site_of[k];
+    if (!nu.fired[site]) return;
+    const int64_t c = nu.list[k], S = a.stride;
+    const int sp = nu.sitephase[site];
+    uint16_t *as = (uint16_t *)a.as;
+    as[c] = 1;
+    as[S + c] = (uint16_t)sp;
+    ((R *)a.phi)[c] = (R)1.0;
+    if (a.ndp) {
+        const double T = (double)a.tm[c];
+        const cipher_material &ms = material_of(a.chem, sp);
+        double ex[2 * CIPHER_MAXCP];
+        sitepot_explicit(a.chem, sp, ms.c0, T, ex);
+        for (int q = 0; q < ms.nsites * a.ndp; q++) ((double *)a.ex)[(int64_t)q * S + c] = ex[q];
+    }
+}
+
+template <typename R>
+static cudaError_t launch_nsums(const GenArgs<R> &a, const NucArgs &n, int64_t nlist, cudaStream_t s)
+{
+    if (nlist > 0) {
+        k_nuc_cells<CIPHER_PMAX, R><<<(unsigned)((nlist + kGenBlock - 1) / kGenBlock), kGenBlock, 0, s>>>(a, n, nlist);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    k_nuc_sites<<<(n.nsites + 127) / 128, 128, 0, s>>>(n, a.ncp);
+    return cudaGetLastError();
+}
+
+template <typename R>
+static cudaError_t launch_nreset(const GenArgs<R> &a, const NucArgs &n, int64_t nlist, cudaStream_t s)
+{
+    if (nlist < 1) return cudaSuccess;
+    k_nuc_reset<R><<<(unsigned)((nlist + kGenBlock - 1) / kGenBlock), kGenBlock, 0, s>>>(a, n, nlist);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_nucleation_sums(const GenArgs<double> &a, const NucArgs &n, int64_t nlist, cudaStream_t s) { return launch_nsums(a, n, nlist, s); }
+cudaError_t launch_nucleation_sums(const GenArgs<float> &a, const NucArgs &n, int64_t nlist, cudaStream_t s) { return launch_nsums(a, n, nlist, s); }
+cudaError_t launch_nucleation_reset(const GenArgs<double> &a, const NucArgs &n, int64_t nlist, cudaStream_t s) { return launch_nreset(a, n, nlist, s); }
+cudaError_t launch_nucleation_reset(const GenArgs<float> &a, const NucArgs &n, int64_t nlist, cudaStream_t s) { return launch_nreset(a, n, nlist, s); }
+
+/* ------------------------------------------------------------------ */
 /* output fields (src/cipher.c:976-1078)                                */
 /* ------------------------------------------------------------------ */
 

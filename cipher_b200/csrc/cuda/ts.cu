@@ -411,6 +411,7 @@ struct cipher_ts {
     double *d_partial, *d_sum, *h_sum;
     int64_t npartial;
     Control ct;
+    cipher_nucleation *nu;         /* nucleation before the active-set update, or NULL */
 };
 
 static dim3 combine_grid(const cipher_state_layout &L)
@@ -535,11 +536,29 @@ extern "C" int cipher_ts_step(cipher_ts *ts, void *X, double t_end, int *accepte
         /* the candidate becomes the solution */
         TS_CUDA(cudaMemcpyAsync((char *)X + L.pf_offset, (const char *)ts->Y + L.pf_offset,
                                 (size_t)(L.bytes - L.pf_offset), cudaMemcpyDeviceToDevice, s), "accept");
+        if (ts->nu) {
+            int nfired = 0;
+            rc = cipher_nucleation_step(ts->nu, X, ts->ct.st.t, h, &nfired, stream);
+            if (rc) return rc;
+            /* a nucleus restarts the step size from the minimum (src/cipher.c:861) */
+            if (nfired) {
+                ts->ct.dt = ts->o.dtmin;
+                ts->ct.st.dt = ts->ct.dt;
+                ts->ct.have_prev = 0;
+            }
+        }
         if (ts->o.poststep) {
             rc = cipher_poststep(ts->ctx, X, stream);
             if (rc) return rc;
         }
     }
+    return CIPHER_OK;
+}
+
+extern "C" int cipher_ts_set_nucleation(cipher_ts *ts, struct cipher_nucleation *nu)
+{
+    if (!ts) return cipher_set_error(CIPHER_E_ARG, "NULL argument");
+    ts->nu = nu;
     return CIPHER_OK;
 }
 

@@ -253,6 +253,10 @@ int cipher_ts_solve(cipher_ts *ts, void *X, double t0, double t_end, cipher_ts_s
 int cipher_ts_get_stats(const cipher_ts *ts, cipher_ts_stats *st);
 /* next step size (clamped to the limits); resets the controller history */
 int cipher_ts_set_dt(cipher_ts *ts, double dt);
+/* run nucleation (before the active-set update) after every accepted step;
+ * a firing restarts the step size from dtmin as the reference does
+ * (src/cipher.c:861).  NULL detaches. */
+int cipher_ts_set_nucleation(cipher_ts *ts, struct cipher_nucleation *nu);
 
 /* ------------------------------------------------------------------ */
 /* many independent domains stepped together                           */
@@ -341,6 +345,49 @@ typedef struct cipher_server_counters {
     double t_admit, t_step, t_retire;        /* seconds in each phase of cipher_server_poll */
 } cipher_server_counters;
 int cipher_server_get_counters(const cipher_server *s, cipher_server_counters *c);
+
+/* ------------------------------------------------------------------ */
+/* nucleation (the first part of PostStep, src/cipher.c:715-867;        */
+/* models src/material.c:47-290)                                       */
+/* ------------------------------------------------------------------ */
+
+/* same numbering as nucleation_model_t (src/typedef.h:45-51) */
+enum { CIPHER_NUC_CNT = 0, CIPHER_NUC_CONSTANT = 1, CIPHER_NUC_THERMAL = 2, CIPHER_NUC_NONE = 3 };
+
+typedef struct cipher_nucleus {
+    int32_t model;
+    int32_t nmatrix;
+    int32_t matrix[16];                  /* sorted phase ids a site's cells may hold */
+    int8_t active_solutes[CIPHER_MAXCP];
+    double gamma, shapefactor, minsize, atomicvolume, lengthscale;   /* cnt and thermal */
+    double incubationtimemin, liquidus;
+    double nucleation_rate;                                          /* constant */
+    double solvus_temperature_0, enthalpy_fusion_0;                  /* thermal */
+    int32_t has_solvus_c, has_enthalpy_c;
+    double solvus_temperature_c[CIPHER_MAXCP], enthalpy_fusion_c[CIPHER_MAXCP];
+} cipher_nucleus;
+
+typedef struct cipher_nucleation cipher_nucleation;
+
+/* nucleation sites of context c: voxelsite[cell] = the cell's site or -1,
+ * sitephase/sitenucleus per site, the nuclei's parameters, and the seed of
+ * the event draws (the reference draws with rand(); here a splitmix64
+ * stream per object, so runs are reproducible) */
+int cipher_nucleation_create(cipher_ctx *c, int nsites, const int32_t *voxelsite, const int32_t *sitephase,
+                             const int32_t *sitenucleus, int nnuclei, const cipher_nucleus *nuclei, uint64_t seed,
+                             cipher_nucleation **out);
+void cipher_nucleation_destroy(cipher_nucleation *nu);
+/* one nucleation update of X at time t after a step of size dt: a site
+ * whose cells hold a phase outside its nucleus' matrix is retired; every
+ * other active site averages the barrier, diffusivity and temperature over
+ * its cells and draws its event; fired sites turn into their phase (set,
+ * phi, explicit potentials of c0) and are retired.  *nfired = sites fired
+ * (the reference then restarts the stepper from mintimestep).  Synchronises
+ * `stream`.  The active-set update (cipher_poststep) follows. */
+int cipher_nucleation_step(cipher_nucleation *nu, void *X, double t, double dt, int *nfired, void *stream);
+/* per site: 1 active, 0 retired; and the last averages (NaN when unset) */
+int cipher_nucleation_sites(const cipher_nucleation *nu, int8_t *active, double *barrier, double *diffusivity,
+                            double *temperature, double *volume);
 
 /* ------------------------------------------------------------------ */
 /* output (the reference's output step in PostStep, src/cipher.c:976-1093) */

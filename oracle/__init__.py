@@ -58,6 +58,11 @@ def port():
         lib.oracle_output_fields.restype = C.c_int
         lib.oracle_output_fields.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32),
                                              C.POINTER(C.c_int32), C.c_int, C.POINTER(C.c_double)]
+        lib.oracle_nucleation_step.restype = C.c_int
+        lib.oracle_nucleation_step.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_int,
+                                               C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                               C.c_void_p, C.c_double, C.c_double, C.POINTER(C.c_uint64),
+                                               C.POINTER(C.c_int8), C.POINTER(C.c_double)]
         lib.oracle_ts_create.restype = C.c_void_p
         lib.oracle_ts_create.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         lib.oracle_ts_destroy.restype = None
@@ -142,6 +147,36 @@ def port_output_fields(problem, mesh, X: np.ndarray, kinds, idx) -> np.ndarray:
     if rc:
         raise RuntimeError(f"oracle_output_fields failed ({rc})")
     return out
+
+
+class PortNucleation:
+    """CPU restatement of nucleation with the library's event stream."""
+
+    def __init__(self, problem, mesh, voxelsite, sitephase, sitenucleus, nuclei, seed: int = 1):
+        self.problem, self.mesh = problem, mesh
+        self.voxelsite = np.ascontiguousarray(voxelsite, dtype=np.int32)
+        self.sitephase = np.ascontiguousarray(sitephase, dtype=np.int32)
+        self.sitenucleus = np.ascontiguousarray(sitenucleus, dtype=np.int32)
+        self.nuclei = nuclei
+        self.nsites = len(self.sitephase)
+        self.rng = C.c_uint64(int(seed))
+        self.active = np.ones(self.nsites, dtype=np.int8)
+        self.last = np.full((self.nsites, 4), np.nan)
+
+    def step(self, X: np.ndarray, t: float, dt: float) -> int:
+        assert X.flags.c_contiguous and X.dtype == np.float64
+        out = np.full((self.nsites, 4), np.nan)
+        i32 = C.POINTER(C.c_int32)
+        nf = port().oracle_nucleation_step(_addr(self.problem), _addr(self.mesh), _dp(X), self.nsites,
+                                           self.voxelsite.ctypes.data_as(i32), self.sitephase.ctypes.data_as(i32),
+                                           self.sitenucleus.ctypes.data_as(i32), C.cast(self.nuclei, C.c_void_p),
+                                           t, dt, C.byref(self.rng), self.active.ctypes.data_as(C.POINTER(C.c_int8)),
+                                           _dp(out))
+        if nf < 0:
+            raise RuntimeError("oracle_nucleation_step failed")
+        ev = ~np.isnan(out[:, 0])
+        self.last[ev] = out[ev]
+        return nf
 
 
 def simplex_projection(v: np.ndarray) -> np.ndarray:

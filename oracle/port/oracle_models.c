@@ -597,3 +597,7 @@ void or_mobility(const cipher_problem *p, int phase, const double *y, double T, 
     mobility_raw(m, y, T, p->ncp, M);
     for (int c = 0; c < p->ncp; c++) M[c] *= m->molarvolume;
 }
+
+/* the raw model functions for the nucleation restatement */
+double or_energy_raw(const cipher_material *m, const double *y, double T, int ncp) { return energy_raw(m, y, T, ncp); }
+void or_mobility_raw(const cipher_material *m, const double *y, double T, int ncp, double *M) { mobility_raw(m, y, T, ncp, M); }
