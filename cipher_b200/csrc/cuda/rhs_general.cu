@@ -561,6 +561,50 @@ __global__ void __launch_bounds__(kGenBlock) k_chem_init(const GenArgs<R> a, dou
 /* nucleation (src/cipher.c:715-867, src/material.c:150-290)            */
 /* ------------------------------------------------------------------ */
 
+/* one matrix phase of a nucleation cell (src/material.c:150-290): its site
+ * fractions from the cell's implicit potentials stoichiometry*(mu - ci) - EX,
+ * then h * chemical energy density (cnt) or h * the phase's average
+ * composition (thermal), and h * R T M_raw into diff.  exslot points at the
+ * slot's first EX plane at this cell (planes S apart). */
+static __device__ __noinline__ void nuc_matrix_phase(const ChemTables ch, int phase, const double *exslot, int64_t S,
+                                                     const double *mu, const double *ci, double T, double hg,
+                                                     int cnt, double *matrixenergy, double *comp, double *diff)
+{
+    const cipher_material &mat = material_of(ch, phase);
+    const int ncp = ch.ncp, ndp = ch.ndp;
+    double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP], mob[CIPHER_MAXCP];
+    for (int s = 0; s < mat.nsites; s++)
+        for (int d = 0; d < ndp; d++)
+            pot[s * ndp + d] = mat.stoichiometry[s] * (mu[d] - ci[d]) - exslot[(int64_t)(s * ndp + d) * S];
+    sitefrac(ch, phase, pot, T, y);
+    if (cnt) {
+        *matrixenergy += hg * energy_raw(mat, y, T, ncp) / mat.molarvolume;
+    } else {
+        for (int d = 0; d < ncp; d++) {
+            double avg = 0.0;
+            for (int s = 0; s < mat.nsites; s++) avg += mat.stoichiometry[s] * y[s * ncp + d];
+            comp[d] += hg * avg;
+        }
+    }
+    mobility_raw(mat, y, T, ncp, mob);
+    for (int d = 0; d < ncp; d++) diff[d] += hg * CIPHER_R_GAS * T * mob[d];
+}
+
+/* chemical energy density of the nucleus phase at its c0 under the cell's
+ * potentials (NucleationBarrier_cnt) */
+static __device__ __noinline__ double nuc_phase_energy(const ChemTables ch, int phase, const double *mu,
+                                                       const double *ci, double T)
+{
+    const cipher_material &ms = material_of(ch, phase);
+    const int ndp = ch.ndp;
+    double ex[2 * CIPHER_MAXCP], pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP];
+    sitepot_explicit(ch, phase, ms.c0, T, ex);
+    for (int s = 0; s < ms.nsites; s++)
+        for (int d = 0; d < ndp; d++) pot[s * ndp + d] = ms.stoichiometry[s] * (mu[d] - ci[d]) - ex[s * ndp + d];
+    sitefrac(ch, phase, pot, T, y);
+    return energy_raw(ms, y, T, ch.ncp) / ms.molarvolume;
+}
+
 /* per listed cell of an active site: whether its phases are all matrix
  * phases of the site's nucleus, the nucleation barrier, the temperature and
  * the interpolated diffusivities of the nucleus model */
@@ -578,55 +622,33 @@ __global__ void __launch_bounds__(kGenBlock) k_nuc_cells(const GenArgs<R> a, con
     double phi[PM], h[PM];
     const int n = load_set<PM>(a, c, ids, phi);
     if (n == 0) return;
-    const cipher_nucleus &nz = nu.nuclei[nu.sitenucleus[site]];
+    const int model = nu.nuclei[nu.sitenucleus[site]].model;
+    const int nmatrix = nu.nuclei[nu.sitenucleus[site]].nmatrix;
+    const int32_t *matrix = nu.nuclei[nu.sitenucleus[site]].matrix;
     /* active phases within the matrix list (SetIntersection size == n) */
     int common = 0;
-    {
-        int i = 0, j = 0;
-        while (i < n && j < nz.nmatrix) {
-            if (ids[i] == nz.matrix[j]) { common++; i++; j++; }
-            else if (ids[i] < nz.matrix[j]) i++;
-            else j++;
-        }
+    for (int i = 0, j = 0; i < n && j < nmatrix;) {
+        if (ids[i] == matrix[j]) { common++; i++; j++; }
+        else if (ids[i] < matrix[j]) i++;
+        else j++;
     }
     if (common != n) return;                      /* rec[0] = 0: the site retires */
     const double T = (double)a.tm[c];
-    const ChemTables ch = a.chem;
     interpolant(a.interp, phi, n, h);
     double barrier = 0.0, diff[CIPHER_MAXCP];
     for (int d = 0; d < CIPHER_MAXCP; d++) diff[d] = 0.0;
-    if (nz.model == CIPHER_NUC_CNT || nz.model == CIPHER_NUC_THERMAL) {
-        double mu[CIPHER_MAXCP], ci[CIPHER_MAXCP];
+    if (model == CIPHER_NUC_CNT || model == CIPHER_NUC_THERMAL) {
+        const cipher_nucleus &nz = nu.nuclei[nu.sitenucleus[site]];
+        double mu[CIPHER_MAXCP], ci[CIPHER_MAXCP], comp[CIPHER_MAXCP], matrixenergy = 0.0;
+        for (int d = 0; d < CIPHER_MAXCP; d++) { mu[d] = 0.0; comp[d] = 0.0; }
         for (int d = 0; d < a.ndp; d++) mu[d] = a.dp[(int64_t)d * S + c];
         segregation(a, ids, h, n, ci);
-        double matrixenergy = 0.0, comp[CIPHER_MAXCP];
-        for (int d = 0; d < CIPHER_MAXCP; d++) comp[d] = 0.0;
-        for (int g = 0; g < n; g++) {
-            const cipher_material &mat = material_of(ch, ids[g]);
-            double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP], mob[CIPHER_MAXCP];
-            slot_potential(a, mat, mu, ci, c, g, pot);
-            sitefrac(ch, ids[g], pot, T, y);
-            if (nz.model == CIPHER_NUC_CNT) matrixenergy += h[g] * energy_raw(mat, y, T, a.ncp) / mat.molarvolume;
-            else
-                for (int d = 0; d < a.ncp; d++) {
-                    double avg = 0.0;
-                    for (int s2 = 0; s2 < mat.nsites; s2++) avg += mat.stoichiometry[s2] * y[s2 * a.ncp + d];
-                    comp[d] += h[g] * avg;
-                }
-            mobility_raw(mat, y, T, a.ncp, mob);
-            for (int d = 0; d < a.ncp; d++) diff[d] += h[g] * CIPHER_R_GAS * T * mob[d];
-        }
-        if (nz.model == CIPHER_NUC_CNT) {
-            const int sp = nu.sitephase[site];
-            const cipher_material &ms = material_of(ch, sp);
-            double ex[2 * CIPHER_MAXCP], pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP];
-            sitepot_explicit(ch, sp, ms.c0, T, ex);
-            for (int s2 = 0; s2 < ms.nsites; s2++)
-                for (int d = 0; d < a.ndp; d++)
-                    pot[s2 * a.ndp + d] = ms.stoichiometry[s2] * (mu[d] - ci[d]) - ex[s2 * a.ndp + d];
-            sitefrac(ch, sp, pot, T, y);
-            const double phaseenergy = energy_raw(ms, y, T, a.ncp) / ms.molarvolume;
-            barrier = matrixenergy - phaseenergy;
+        const int cnt = model == CIPHER_NUC_CNT;
+        for (int g = 0; g < n; g++)
+            nuc_matrix_phase(a.chem, ids[g], a.ex + (int64_t)g * a.SP * S + c, S, mu, ci, T, h[g], cnt,
+                             &matrixenergy, comp, diff);
+        if (cnt) {
+            barrier = matrixenergy - nuc_phase_energy(a.chem, nu.sitephase[site], mu, ci, T);
         } else {
             double solvus = nz.solvus_temperature_0, enthalpy = nz.enthalpy_fusion_0;
             if (nz.has_solvus_c)

@@ -236,6 +236,7 @@ typedef struct cipher_ts_stats {
 } cipher_ts_stats;
 
 typedef struct cipher_ts cipher_ts;
+struct cipher_nucleation;
 
 /* options from the problem: scheme 2a, PostStep on, dt0 = timestep0,
  * limits mintimestep/maxtimestep, tolerances reltol/abstol */
