@@ -51,6 +51,7 @@ struct BatchTiles {
     int n;
     int64_t total;                /* tile_start[n] */
     int pmax;                     /* largest P of the batch (shared-memory columns) */
+    int i32;                      /* every member's plane offsets fit 32-bit indices */
 };
 
 /* grid: persistent (a multiple of the SM count); by = tile rows (1, 2, 4) */

@@ -47,29 +47,38 @@ constexpr int kBX = CIPHER_MIXED_BX, kBY = CIPHER_MIXED_BY, kMixedBlock = kBX * 
  *      cell's faces in the reference's face order;
  *   3. thread = cell: the O(n) closed forms of the cell terms and all P
  *      slots of F (coalesced plane by plane).
- * Shared memory: tile_bytes(T, P) for T cells.
+ * IX is the index type of plane offsets: int when every offset of the
+ * domain fits (max(P, 2*dim) * stride < 2^31, all benchmark and batch
+ * sizes), int64_t otherwise.  Shared memory: items_tile_bytes(dim, T, P, ix).
  */
-__host__ __device__ constexpr size_t items_tile_bytes(int dim, int T, int P)
+__host__ __device__ constexpr size_t items_tile_bytes(int dim, int T, int P, int ix_bytes)
 {
-    return (size_t)T * (2 * dim * (8 + 4) + 3 * 4) + (size_t)T * P * (4 + 1) + 64;
+    return (size_t)T * (2 * dim * (8 + ix_bytes) + 8 + ix_bytes) + (size_t)T * P * (4 + 4 + 1) + 64;
+}
+
+/* whether a domain's plane offsets fit the 32-bit kernels */
+__host__ __device__ inline bool items_fit_i32(int64_t stride, int P, int dim)
+{
+    const int64_t planes = P > 2 * dim ? P : 2 * dim;
+    return planes * stride < ((int64_t)1 << 31) - 1;
 }
 
 /* Laplacian of slot i of a tile cell over its faces in the reference's face
  * order (directions through face_dir; `mask` bit f = face position f has a
  * neighbour) */
-template <int DIM>
-__device__ __forceinline__ float item_laplacian(const PfArgs<float> &a, const uint64_t *sw, const int *snb, int T,
-                                                int cell, int mask, int i, float p, float coef)
+template <int DIM, typename IX>
+__device__ __forceinline__ float item_laplacian(const float *phi, IX S, int P, const uint64_t *sw, const IX *snb,
+                                                int T, int cell, int mask, int i, float p, float coef)
 {
-    const int64_t S = a.stride;
     float pn[3 * DIM];
     bool on[3 * DIM];
+    const unsigned sh = 4u * (unsigned)i;
 #pragma unroll
     for (int f = 0; f < 3 * DIM; f++) {
         const int q = face_dir<DIM>(f);
-        const int j = (int)((sw[q * T + cell] >> (4 * i)) & 15u);
-        on[f] = ((mask >> f) & 1) && j < a.P;
-        pn[f] = on[f] ? __ldg(&a.phi[(int64_t)j * S + snb[q * T + cell]]) : 0.0f;
+        const int j = (int)((sw[q * T + cell] >> sh) & 15u);
+        on[f] = ((mask >> f) & 1) && j < P;
+        pn[f] = on[f] ? __ldg(&phi[(IX)j * S + snb[q * T + cell]]) : 0.0f;
     }
     float l = 0.0f;
 #pragma unroll
@@ -81,39 +90,57 @@ __device__ __forceinline__ float item_laplacian(const PfArgs<float> &a, const ui
     return l;
 }
 
-template <int DIM>
-__device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const CellIndex &ci, unsigned char *smem)
+template <int DIM, typename IX>
+__device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const CellIndex &cix, unsigned char *smem)
 {
     constexpr int ND = 2 * DIM;
     const int T = blockDim.x, t = threadIdx.x, P = a.P;
-    const int64_t S = a.stride;
+    const IX S = (IX)a.stride;
+    const float *phi = a.phi;
     uint64_t *sw = (uint64_t *)smem;                              /* [ND][T] face-map words */
-    int *snb = (int *)(sw + (size_t)ND * T);                      /* [ND][T] neighbours */
-    int *soff = snb + (size_t)ND * T;                             /* [T] first item */
-    int *scm = soff + T;                                          /* [T] flat cell index */
-    int *sfm = scm + T;                                           /* [T] face mask, later the warp sums */
-    float *ilap = (float *)(sfm + T);                             /* [T*P] */
-    uint8_t *icell = (uint8_t *)(ilap + (size_t)T * P);           /* [T*P] */
+    IX *snb = (IX *)(sw + (size_t)ND * T);                        /* [ND][T] neighbours */
+    IX *scm = snb + (size_t)ND * T;                               /* [T] flat cell index */
+    int *soff = (int *)(scm + T);                                 /* [T] first item */
+    int *sfm = soff + T;                                          /* [T] face mask */
+    float *ilap = (float *)(sfm + T);                             /* [T*P] Laplacian, later the capillary force */
+    float *iphi = ilap + (size_t)T * P;                           /* [T*P] phase fraction */
+    uint8_t *icell = (uint8_t *)(iphi + (size_t)T * P);           /* [T*P] */
 
     __syncthreads();                 /* the previous tile's readers are done */
     /* 1. cells */
-    int n = ci.live ? (int)__ldg(&a.as[ci.c]) : 0;
-    if (ci.live && (n < 1 || n > P)) {
+    const IX c = (IX)cix.c;
+    int n = cix.live ? (int)__ldg(&a.as[c]) : 0;
+    if (cix.live && (n < 1 || n > P)) {
         atomicOr(a.err, ERR_BADSET);
         n = 0;
     }
     int mask = 0;
+    if (n > 0) {
+        const int co[3] = {cix.x, cix.y, cix.z};
+        const IX st[3] = {1, (IX)a.res[0], (IX)a.res[0] * (IX)a.res[1]};
 #pragma unroll
-    for (int f = 0; f < 3 * DIM; f++) {
-        const int64_t nb = n > 0 ? face_nb<DIM, float>(a, ci, f) : -1;
-        if (nb >= 0) {
-            const int q = face_dir<DIM>(f);
-            mask |= 1 << f;
-            sw[q * T + t] = __ldg(&a.maps[(int64_t)q * S + ci.c]);
-            snb[q * T + t] = (int)nb;
+        for (int f = 0; f < 3 * DIM; f++) {
+            IX nb = -1;
+            if (f < DIM) {
+                const int e = DIM - 1 - f;
+                if (co[e] > 0) nb = c - st[e];
+            } else if (f < 2 * DIM) {
+                const int d = f - DIM;
+                if (co[d] < a.res[d] - 1) nb = c + st[d];
+                else if (a.per[d] && a.res[d] > 1) nb = c - (IX)(a.res[d] - 1) * st[d];
+            } else {
+                const int d = f - 2 * DIM;
+                if (co[d] == 0 && a.per[d] && a.res[d] > 1) nb = c + (IX)(a.res[d] - 1) * st[d];
+            }
+            if (nb >= 0) {
+                const int q = face_dir<DIM>(f);
+                mask |= 1 << f;
+                sw[q * T + t] = __ldg(&a.maps[(IX)q * S + c]);
+                snb[q * T + t] = nb;
+            }
         }
     }
-    scm[t] = (int)ci.c;
+    scm[t] = c;
     /* block exclusive scan of the counts */
     const int lane = t & 31, warp = t >> 5, nwarps = T >> 5;
     __shared__ int swarp[32];
@@ -149,67 +176,75 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
         const int c1 = icell[it], i1 = it - soff[c1];
         const bool two = it2 < total;
         const int c2 = two ? icell[it2] : c1, i2 = two ? it2 - soff[c2] : i1;
-        const float p1 = __ldg(&a.phi[(int64_t)i1 * S + scm[c1]]);
-        const float p2 = __ldg(&a.phi[(int64_t)i2 * S + scm[c2]]);
-        const float l1 = item_laplacian<DIM>(a, sw, snb, T, c1, sfm[c1], i1, p1, coef);
-        const float l2 = item_laplacian<DIM>(a, sw, snb, T, c2, sfm[c2], i2, p2, coef);
+        const float p1 = __ldg(&phi[(IX)i1 * S + scm[c1]]);
+        const float p2 = __ldg(&phi[(IX)i2 * S + scm[c2]]);
+        const float l1 = item_laplacian<DIM, IX>(phi, S, P, sw, snb, T, c1, sfm[c1], i1, p1, coef);
+        const float l2 = item_laplacian<DIM, IX>(phi, S, P, sw, snb, T, c2, sfm[c2], i2, p2, coef);
         ilap[it] = l1;
-        if (two) ilap[it2] = l2;
+        iphi[it] = p1;
+        if (two) {
+            ilap[it2] = l2;
+            iphi[it2] = p2;
+        }
     }
     __syncthreads();
 
-    /* 3. cell terms (phase fractions re-read: they are in L1) */
-    if (!ci.live) return;
-    const int64_t c = ci.c;
+    /* 3. cell terms */
+    if (!cix.live) return;
     uint32_t act = 0;
     double nact = 0.0, Ca = 0.0;
     const double mob = a.mob0;
+    const float *cp = iphi + off;
+    float *cl = ilap + off;
     if (n > 1) {
         const float sig = (float)a.sig0, inv_w = (float)(1.0 / a.wid0);
         const float w_pi2 = (float)(a.wid0 / (CIPHER_PI_D * CIPHER_PI_D));
         const float tjh = (float)(0.5 * a.tj0);
         float A = 0.0f, S1 = 0.0f, S2 = 0.0f;
         for (int k = 0; k < n; k++) {
-            const float p = __ldg(&a.phi[(int64_t)k * S + c]);
-            A += p * inv_w + ilap[off + k] * w_pi2;
+            const float p = cp[k];
+            A += p * inv_w + cl[k] * w_pi2;
             S1 += p;
             S2 += p * p;
         }
         /* capillary force, stored over the consumed Laplacian */
         double C = 0.0;
         for (int k = 0; k < n; k++) {
-            const float p = __ldg(&a.phi[(int64_t)k * S + c]), l = ilap[off + k];
+            const float p = cp[k], l = cl[k];
             const float ak = p * inv_w + l * w_pi2;
             const float o1 = S1 - p, o2 = S2 - p * p;
             const float cap = 8.0f * (-sig * (A - ak) - tjh * (o1 * o1 - o2)) + l;
-            ilap[off + k] = cap;
+            cl[k] = cap;
             C += (double)cap;
         }
         for (int k = 0; k < n; k++) {
-            const double cap = (double)ilap[off + k];
+            const double cap = (double)cl[k];
             const double u = mob * ((double)n * cap - C);
-            const double p = (double)__ldg(&a.phi[(int64_t)k * S + c]);
+            const double p = (double)cp[k];
             const bool on = (p > CIPHER_TOL && p < 1.0 - CIPHER_TOL) || (p < CIPHER_TOL && u > 0.0) ||
                             (p > 1.0 - CIPHER_TOL && u < 0.0);
             if (on) { act |= 1u << k; nact += 1.0; Ca += cap; }
         }
     }
+    const double scale = act ? mob / nact : 0.0;
+    float *fp = a.fphi + c;
     for (int m = 0; m < P; m++) {
         float vv = 0.0f;
-        if (m < n && (act >> m & 1u)) vv = (float)(mob * (nact * (double)ilap[off + m] - Ca) / nact);
-        a.fphi[(int64_t)m * S + c] = vv;
+        if (act >> m & 1u) vv = (float)(scale * (nact * (double)cl[m] - Ca));
+        *fp = vv;
+        fp += S;
     }
     double tr = 0.0;
     if (a.has_temp_rate) tr += a.temp_rate;
     a.ftm[c] = (float)tr;
 }
 
-template <int DIM>
+template <int DIM, typename IX>
 __global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_items(const PfArgs<float> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const CellIndex ci = cell_index<kBX, kBY>(a.res);
-    mixed_items_tile<DIM>(a, ci, smem);
+    mixed_items_tile<DIM, IX>(a, ci, smem);
 }
 
 /* one cell of the mixed RHS, several interfaces (reference-order cell terms in FP32) */
@@ -236,7 +271,7 @@ __global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_multi(const PfArgs
 }
 
 /* batched: a persistent grid walks the tiles of every domain of the batch */
-template <int DIM, int PM, bool SINGLE, int BY>
+template <int DIM, int PM, bool SINGLE, int BY, typename IX>
 __global__ void __launch_bounds__(kBX * BY) k_rhs_pf_mixed_batched(const BatchTiles<float> b)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -245,7 +280,7 @@ __global__ void __launch_bounds__(kBX * BY) k_rhs_pf_mixed_batched(const BatchTi
         int inst;
         const CellIndex ci = batch_cell_index<kBX, BY>(b, t, inst);
         if (!b.active[inst]) continue;          /* uniform across the block */
-        if (SINGLE) mixed_items_tile<DIM>(b.args[inst], ci, smem);
+        if (SINGLE) mixed_items_tile<DIM, IX>(b.args[inst], ci, smem);
         else pf_mixed_multi_cell<DIM, PM>(b.args[inst], ci, sc);
     }
 }
@@ -272,9 +307,15 @@ static void launch_pm(const PfArgs<float> &a, cudaStream_t s)
 {
     dim3 grid((unsigned)((a.res[0] + kBX - 1) / kBX), (unsigned)((a.res[1] + kBY - 1) / kBY), (unsigned)a.res[2]);
     if (a.single) {
-        const size_t sm = items_tile_bytes(DIM, kMixedBlock, a.P);
-        if (allow_smem(k_rhs_pf_mixed_items<DIM>, sm) != cudaSuccess) return;
-        k_rhs_pf_mixed_items<DIM><<<grid, kMixedBlock, sm, s>>>(a);
+        if (items_fit_i32(a.stride, a.P, DIM)) {
+            const size_t sm = items_tile_bytes(DIM, kMixedBlock, a.P, 4);
+            if (allow_smem(k_rhs_pf_mixed_items<DIM, int>, sm) != cudaSuccess) return;
+            k_rhs_pf_mixed_items<DIM, int><<<grid, kMixedBlock, sm, s>>>(a);
+        } else {
+            const size_t sm = items_tile_bytes(DIM, kMixedBlock, a.P, 8);
+            if (allow_smem(k_rhs_pf_mixed_items<DIM, int64_t>, sm) != cudaSuccess) return;
+            k_rhs_pf_mixed_items<DIM, int64_t><<<grid, kMixedBlock, sm, s>>>(a);
+        }
     } else {
         size_t sm = slot_columns_bytes(a.P, kMixedBlock, 4, true);
         k_rhs_pf_mixed_multi<DIM, PM><<<grid, kMixedBlock, sm, s>>>(a);
@@ -290,22 +331,32 @@ static void launch_dim(const PfArgs<float> &a, cudaStream_t s)
     else launch_pm<DIM, 16>(a, s);
 }
 
+template <int DIM, int PM, bool SINGLE, typename IX>
+static cudaError_t launch_batched_ix(const BatchTiles<float> &b, int by, int grid, cudaStream_t s)
+{
+    const size_t sm = SINGLE ? items_tile_bytes(DIM, kBX * by, b.pmax, (int)sizeof(IX))
+                             : slot_columns_bytes(b.pmax, kBX * by, 4, true);
+    cudaError_t e;
+    if (by == 1) {
+        if ((e = allow_smem(k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 1, IX>, sm)) != cudaSuccess) return e;
+        k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 1, IX><<<grid, kBX, sm, s>>>(b);
+    } else if (by == 2) {
+        if ((e = allow_smem(k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 2, IX>, sm)) != cudaSuccess) return e;
+        k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 2, IX><<<grid, kBX * 2, sm, s>>>(b);
+    } else {
+        if ((e = allow_smem(k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 4, IX>, sm)) != cudaSuccess) return e;
+        k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 4, IX><<<grid, kBX * 4, sm, s>>>(b);
+    }
+    return cudaGetLastError();
+}
+
+/* the several-interface form keeps 64-bit indices; single-interface groups
+ * take the 32-bit items kernel when every member fits */
 template <int DIM, int PM, bool SINGLE>
 static cudaError_t launch_batched_by(const BatchTiles<float> &b, int by, int grid, cudaStream_t s)
 {
-    const size_t sm = SINGLE ? items_tile_bytes(DIM, kBX * by, b.pmax) : slot_columns_bytes(b.pmax, kBX * by, 4, true);
-    cudaError_t e;
-    if (by == 1) {
-        if ((e = allow_smem(k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 1>, sm)) != cudaSuccess) return e;
-        k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 1><<<grid, kBX, sm, s>>>(b);
-    } else if (by == 2) {
-        if ((e = allow_smem(k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 2>, sm)) != cudaSuccess) return e;
-        k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 2><<<grid, kBX * 2, sm, s>>>(b);
-    } else {
-        if ((e = allow_smem(k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 4>, sm)) != cudaSuccess) return e;
-        k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 4><<<grid, kBX * 4, sm, s>>>(b);
-    }
-    return cudaGetLastError();
+    if (SINGLE && b.i32) return launch_batched_ix<DIM, PM, SINGLE, int>(b, by, grid, s);
+    return launch_batched_ix<DIM, PM, SINGLE, int64_t>(b, by, grid, s);
 }
 
 template <int DIM>

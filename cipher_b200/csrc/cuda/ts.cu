@@ -621,6 +621,7 @@ struct BatchSlot {
 
 struct RhsGroup {
     int dim = 0, single = 0, pmax = 0, by = 2, grid = 0;
+    int64_t maxstride = 0;
     std::vector<int> members;      /* dense indices */
     void *d_args[kMaxStages] = {}; /* PfArgs<R>[m] per stage */
     int64_t *d_tile_start = nullptr;
@@ -951,6 +952,10 @@ static BatchTiles<R> group_batch(const cipher_batch *b, const RhsGroup &g, int s
     t.n = (int)g.members.size();
     t.total = g.total;
     t.pmax = g.pmax;
+    {
+        const int64_t planes = g.pmax > 2 * g.dim ? g.pmax : 2 * g.dim;
+        t.i32 = planes * g.maxstride < ((int64_t)1 << 31) - 1;
+    }
     return t;
 }
 
@@ -1047,6 +1052,7 @@ static int rebuild(cipher_batch *b)
         }
         g->members.push_back(i);
         if (s.info.P > g->pmax) g->pmax = s.info.P;
+        if (s.lay.stride > g->maxstride) g->maxstride = s.lay.stride;
     }
     size_t gsum = 0;
     for (auto &g : b->groups) gsum += g.members.size();
