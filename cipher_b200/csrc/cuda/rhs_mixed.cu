@@ -35,25 +35,33 @@ namespace cipher {
 constexpr int kBX = CIPHER_MIXED_BX, kBY = CIPHER_MIXED_BY, kMixedBlock = kBX * kBY;
 
 /* ------------------------------------------------------------------ */
-/* single interface: (cell, slot) items spread over the block's threads  */
+/* single interface: (cell, slot) items spread over a warp's lanes       */
 /* ------------------------------------------------------------------ */
 /*
- * One block is one tile of blockDim.x cells.  The face gather, the bulk of
- * the work, runs over the tile's (cell, slot) items, so a thread never
- * idles while a neighbour lane walks a larger set:
- *   1. thread = cell: active count, the cell's face-map words and
- *      neighbours into shared memory, a block scan of the counts;
- *   2. thread = item: the slot's phase fraction and its Laplacian over the
- *      cell's faces in the reference's face order;
- *   3. thread = cell: the O(n) closed forms of the cell terms and all P
+ * Each warp owns one row of 32 cells and its own slice of shared memory, so
+ * warps never wait for one another.  The face gather, the bulk of the work,
+ * runs over the row's (cell, slot) items, so a lane never idles while a
+ * neighbour lane walks a larger set:
+ *   1. lane = cell: active count, the cell's face-map words and neighbours
+ *      into shared memory, a warp scan of the counts;
+ *   2. lane = item: the slot's phase fraction and its Laplacian over the
+ *      cell's 2*dim faces (absent or gated faces map every slot to 15);
+ *   3. lane = cell: the O(n) closed forms of the cell terms and all P
  *      slots of F (coalesced plane by plane).
+ * The mixed path sums a Laplacian in direction order, not in the
+ * reference's face order: the difference is FP32 rounding.
  * IX is the index type of plane offsets: int when every offset of the
  * domain fits (max(P, 2*dim) * stride < 2^31, all benchmark and batch
- * sizes), int64_t otherwise.  Shared memory: items_tile_bytes(dim, T, P, ix).
+ * sizes), int64_t otherwise.
  */
+__host__ __device__ constexpr size_t items_warp_bytes(int dim, int P, int ix_bytes)
+{
+    return ((size_t)32 * (2 * dim * (8 + ix_bytes) + ix_bytes + 4) + (size_t)32 * P * (4 + 4 + 1) + 15) / 16 * 16;
+}
+
 __host__ __device__ constexpr size_t items_tile_bytes(int dim, int T, int P, int ix_bytes)
 {
-    return (size_t)T * (2 * dim * (8 + ix_bytes) + 8 + ix_bytes) + (size_t)T * P * (4 + 4 + 1) + 64;
+    return (size_t)(T / 32) * items_warp_bytes(dim, P, ix_bytes);
 }
 
 /* whether a domain's plane offsets fit the 32-bit kernels */
@@ -63,50 +71,44 @@ __host__ __device__ inline bool items_fit_i32(int64_t stride, int P, int dim)
     return planes * stride < ((int64_t)1 << 31) - 1;
 }
 
-/* Laplacian of slot i of a tile cell over its faces in the reference's face
- * order (directions through face_dir; `mask` bit f = face position f has a
- * neighbour) */
+/* Laplacian of slot i of row cell `cell`: sum over the faces whose map
+ * gives slot i a neighbour slot j < P of (phi_nb[j] - phi) */
 template <int DIM, typename IX>
 __device__ __forceinline__ float item_laplacian(const float *phi, IX S, int P, const uint64_t *sw, const IX *snb,
-                                                int T, int cell, int mask, int i, float p, float coef)
+                                                int cell, int i, float p, float coef)
 {
-    float pn[3 * DIM];
-    bool on[3 * DIM];
     const unsigned sh = 4u * (unsigned)i;
+    float pn[2 * DIM];
+    bool on[2 * DIM];
 #pragma unroll
-    for (int f = 0; f < 3 * DIM; f++) {
-        const int q = face_dir<DIM>(f);
-        const int j = (int)((sw[q * T + cell] >> sh) & 15u);
-        on[f] = ((mask >> f) & 1) && j < P;
-        pn[f] = on[f] ? __ldg(&phi[(IX)j * S + snb[q * T + cell]]) : 0.0f;
+    for (int q = 0; q < 2 * DIM; q++) {
+        const int j = (int)((sw[q * 32 + cell] >> sh) & 15u);
+        on[q] = j < P;
+        pn[q] = on[q] ? __ldg(&phi[(IX)j * S + snb[q * 32 + cell]]) : p;
     }
     float l = 0.0f;
 #pragma unroll
-    for (int f = 0; f < 3 * DIM; f++) {
-        if (!on[f]) continue;
-        if (f >= DIM && f < 2 * DIM) l += coef * (pn[f] - p);
-        else l -= coef * (p - pn[f]);
-    }
-    return l;
+    for (int q = 0; q < 2 * DIM; q++) l += pn[q] - p;
+    return coef * l;
 }
 
 template <int DIM, typename IX>
 __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const CellIndex &cix, unsigned char *smem)
 {
     constexpr int ND = 2 * DIM;
-    const int T = blockDim.x, t = threadIdx.x, P = a.P;
+    const int lane = threadIdx.x & 31, P = a.P;
     const IX S = (IX)a.stride;
     const float *phi = a.phi;
-    uint64_t *sw = (uint64_t *)smem;                              /* [ND][T] face-map words */
-    IX *snb = (IX *)(sw + (size_t)ND * T);                        /* [ND][T] neighbours */
-    IX *scm = snb + (size_t)ND * T;                               /* [T] flat cell index */
-    int *soff = (int *)(scm + T);                                 /* [T] first item */
-    int *sfm = soff + T;                                          /* [T] face mask */
-    float *ilap = (float *)(sfm + T);                             /* [T*P] Laplacian, later the capillary force */
-    float *iphi = ilap + (size_t)T * P;                           /* [T*P] phase fraction */
-    uint8_t *icell = (uint8_t *)(iphi + (size_t)T * P);           /* [T*P] */
+    unsigned char *ws = smem + (size_t)(threadIdx.x >> 5) * items_warp_bytes(DIM, P, (int)sizeof(IX));
+    uint64_t *sw = (uint64_t *)ws;                                /* [ND][32] face-map words */
+    IX *snb = (IX *)(sw + ND * 32);                               /* [ND][32] neighbours */
+    IX *scm = snb + ND * 32;                                      /* [32] flat cell index */
+    int *soff = (int *)(scm + 32);                                /* [32] first item */
+    float *ilap = (float *)(soff + 32);                           /* [32*P] Laplacian, later the capillary force */
+    float *iphi = ilap + 32 * P;                                  /* [32*P] phase fraction */
+    uint8_t *icell = (uint8_t *)(iphi + 32 * P);                  /* [32*P] */
 
-    __syncthreads();                 /* the previous tile's readers are done */
+    __syncwarp();                    /* the previous row's readers are done */
     /* 1. cells */
     const IX c = (IX)cix.c;
     int n = cix.live ? (int)__ldg(&a.as[c]) : 0;
@@ -114,72 +116,47 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
         atomicOr(a.err, ERR_BADSET);
         n = 0;
     }
-    int mask = 0;
     if (n > 0) {
         const int co[3] = {cix.x, cix.y, cix.z};
         const IX st[3] = {1, (IX)a.res[0], (IX)a.res[0] * (IX)a.res[1]};
 #pragma unroll
-        for (int f = 0; f < 3 * DIM; f++) {
-            IX nb = -1;
-            if (f < DIM) {
-                const int e = DIM - 1 - f;
-                if (co[e] > 0) nb = c - st[e];
-            } else if (f < 2 * DIM) {
-                const int d = f - DIM;
-                if (co[d] < a.res[d] - 1) nb = c + st[d];
-                else if (a.per[d] && a.res[d] > 1) nb = c - (IX)(a.res[d] - 1) * st[d];
-            } else {
-                const int d = f - 2 * DIM;
-                if (co[d] == 0 && a.per[d] && a.res[d] > 1) nb = c + (IX)(a.res[d] - 1) * st[d];
-            }
-            if (nb >= 0) {
-                const int q = face_dir<DIM>(f);
-                mask |= 1 << f;
-                sw[q * T + t] = __ldg(&a.maps[(IX)q * S + c]);
-                snb[q * T + t] = nb;
-            }
+        for (int d = 0; d < DIM; d++) {
+            const bool wrap = a.per[d] && a.res[d] > 1;
+            const IX span = (IX)(a.res[d] - 1) * st[d];
+            const bool lo = co[d] > 0 || wrap, hi = co[d] < a.res[d] - 1 || wrap;
+            const IX nlo = co[d] > 0 ? c - st[d] : c + span;
+            const IX nhi = co[d] < a.res[d] - 1 ? c + st[d] : c - span;
+            sw[(2 * d) * 32 + lane] = lo ? __ldg(&a.maps[(IX)(2 * d) * S + c]) : ~0ull;
+            sw[(2 * d + 1) * 32 + lane] = hi ? __ldg(&a.maps[(IX)(2 * d + 1) * S + c]) : ~0ull;
+            snb[(2 * d) * 32 + lane] = lo ? nlo : c;
+            snb[(2 * d + 1) * 32 + lane] = hi ? nhi : c;
         }
     }
-    scm[t] = c;
-    /* block exclusive scan of the counts */
-    const int lane = t & 31, warp = t >> 5, nwarps = T >> 5;
-    __shared__ int swarp[32];
+    scm[lane] = c;
+    /* warp exclusive scan of the counts */
     int v = n;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const int y = __shfl_up_sync(0xffffffffu, v, o);
         if (lane >= o) v += y;
     }
-    if (lane == 31) swarp[warp] = v;
-    __syncthreads();
-    if (warp == 0) {
-        int u = lane < nwarps ? swarp[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, u, o);
-            if (lane >= o) u += y;
-        }
-        if (lane < nwarps) swarp[lane] = u;
-    }
-    __syncthreads();
-    const int off = v - n + (warp > 0 ? swarp[warp - 1] : 0);
-    const int total = swarp[nwarps - 1];
-    soff[t] = off;
-    sfm[t] = mask;
-    for (int k = 0; k < n; k++) icell[off + k] = (uint8_t)t;
-    __syncthreads();
+    const int off = v - n;
+    const int total = __shfl_sync(0xffffffffu, v, 31);
+    soff[lane] = off;
+    for (int k = 0; k < n; k++) icell[off + k] = (uint8_t)lane;
+    __syncwarp();
 
     /* 2. items, two per pass so that both items' loads are in flight */
     const float coef = (float)a.face_coef;
-    for (int it = t; it < total; it += 2 * T) {
-        const int it2 = it + T;
+    for (int it = lane; it < total; it += 64) {
+        const int it2 = it + 32;
         const int c1 = icell[it], i1 = it - soff[c1];
         const bool two = it2 < total;
         const int c2 = two ? icell[it2] : c1, i2 = two ? it2 - soff[c2] : i1;
         const float p1 = __ldg(&phi[(IX)i1 * S + scm[c1]]);
         const float p2 = __ldg(&phi[(IX)i2 * S + scm[c2]]);
-        const float l1 = item_laplacian<DIM, IX>(phi, S, P, sw, snb, T, c1, sfm[c1], i1, p1, coef);
-        const float l2 = item_laplacian<DIM, IX>(phi, S, P, sw, snb, T, c2, sfm[c2], i2, p2, coef);
+        const float l1 = item_laplacian<DIM, IX>(phi, S, P, sw, snb, c1, i1, p1, coef);
+        const float l2 = item_laplacian<DIM, IX>(phi, S, P, sw, snb, c2, i2, p2, coef);
         ilap[it] = l1;
         iphi[it] = p1;
         if (two) {
@@ -187,7 +164,7 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
             iphi[it2] = p2;
         }
     }
-    __syncthreads();
+    __syncwarp();
 
     /* 3. cell terms */
     if (!cix.live) return;
