@@ -38,30 +38,35 @@ constexpr int kBX = CIPHER_MIXED_BX, kBY = CIPHER_MIXED_BY, kMixedBlock = kBX * 
 /* single interface: (cell, slot) items spread over a warp's lanes       */
 /* ------------------------------------------------------------------ */
 /*
- * Each warp owns one row of 32 cells and its own slice of shared memory, so
- * warps never wait for one another.  The face gather, the bulk of the work,
- * runs over the row's (cell, slot) items, so a lane never idles while a
- * neighbour lane walks a larger set:
- *   1. lane = cell: active count, the cell's face-map words and neighbours
- *      into shared memory, a warp scan of the counts;
+ * Each warp owns one row of 32 consecutive cells (same y and z) and its own
+ * slice of shared memory, so warps never wait for one another.  The face
+ * gather, the bulk of the work, runs over the row's (cell, slot) items, so a
+ * lane never idles while a neighbour lane walks a larger set:
+ *   1. lane = cell: active count and the cell's face-map words into shared
+ *      memory, a warp scan of the counts, one 16-bit tag (cell lane, slot)
+ *      per item;
  *   2. lane = item: the slot's phase fraction and its Laplacian over the
  *      cell's 2*dim faces (absent or gated faces map every slot to 15);
+ *      neighbour cells follow from the row's position (y and z offsets are
+ *      the same for the whole row);
  *   3. lane = cell: the O(n) closed forms of the cell terms and all P
  *      slots of F (coalesced plane by plane).
+ * (phi, Laplacian) pairs pass from phase 2 to phase 3 in a slot-major table
+ * with row pitch 33, so that phase 3's lanes read distinct banks.
  * The mixed path sums a Laplacian in direction order, not in the
  * reference's face order: the difference is FP32 rounding.
  * IX is the index type of plane offsets: int when every offset of the
  * domain fits (max(P, 2*dim) * stride < 2^31, all benchmark and batch
  * sizes), int64_t otherwise.
  */
-__host__ __device__ constexpr size_t items_warp_bytes(int dim, int P, int ix_bytes)
+__host__ __device__ constexpr size_t items_warp_bytes(int dim, int P)
 {
-    return ((size_t)32 * (2 * dim * (8 + ix_bytes) + ix_bytes + 4) + (size_t)32 * P * (4 + 4 + 1) + 15) / 16 * 16;
+    return ((size_t)32 * 2 * dim * 8 + (size_t)33 * P * 8 + (size_t)32 * P * 2 + 15) / 16 * 16;
 }
 
 __host__ __device__ constexpr size_t items_tile_bytes(int dim, int T, int P, int ix_bytes)
 {
-    return (size_t)(T / 32) * items_warp_bytes(dim, P, ix_bytes);
+    return (void)ix_bytes, (size_t)(T / 32) * items_warp_bytes(dim, P);
 }
 
 /* whether a domain's plane offsets fit the 32-bit kernels */
@@ -71,27 +76,6 @@ __host__ __device__ inline bool items_fit_i32(int64_t stride, int P, int dim)
     return planes * stride < ((int64_t)1 << 31) - 1;
 }
 
-/* Laplacian of slot i of row cell `cell`: sum over the faces whose map
- * gives slot i a neighbour slot j < P of (phi_nb[j] - phi) */
-template <int DIM, typename IX>
-__device__ __forceinline__ float item_laplacian(const float *phi, IX S, int P, const uint64_t *sw, const IX *snb,
-                                                int cell, int i, float p, float coef)
-{
-    const unsigned sh = 4u * (unsigned)i;
-    float pn[2 * DIM];
-    bool on[2 * DIM];
-#pragma unroll
-    for (int q = 0; q < 2 * DIM; q++) {
-        const int j = (int)((sw[q * 32 + cell] >> sh) & 15u);
-        on[q] = j < P;
-        pn[q] = on[q] ? __ldg(&phi[(IX)j * S + snb[q * 32 + cell]]) : p;
-    }
-    float l = 0.0f;
-#pragma unroll
-    for (int q = 0; q < 2 * DIM; q++) l += pn[q] - p;
-    return coef * l;
-}
-
 template <int DIM, typename IX>
 __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const CellIndex &cix, unsigned char *smem)
 {
@@ -99,40 +83,44 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
     const int lane = threadIdx.x & 31, P = a.P;
     const IX S = (IX)a.stride;
     const float *phi = a.phi;
-    unsigned char *ws = smem + (size_t)(threadIdx.x >> 5) * items_warp_bytes(DIM, P, (int)sizeof(IX));
+    unsigned char *ws = smem + (size_t)(threadIdx.x >> 5) * items_warp_bytes(DIM, P);
     uint64_t *sw = (uint64_t *)ws;                                /* [ND][32] face-map words */
-    IX *snb = (IX *)(sw + ND * 32);                               /* [ND][32] neighbours */
-    IX *scm = snb + ND * 32;                                      /* [32] flat cell index */
-    int *soff = (int *)(scm + 32);                                /* [32] first item */
-    float *ilap = (float *)(soff + 32);                           /* [32*P] Laplacian, later the capillary force */
-    float *iphi = ilap + 32 * P;                                  /* [32*P] phase fraction */
-    uint8_t *icell = (uint8_t *)(iphi + 32 * P);                  /* [32*P] */
+    float2 *spl = (float2 *)(sw + ND * 32);                       /* [P][33] (phi, Laplacian / capillary force) */
+    uint16_t *itag = (uint16_t *)(spl + 33 * P);                  /* [32*P] cell lane | slot << 5 */
 
     __syncwarp();                    /* the previous row's readers are done */
     /* 1. cells */
     const IX c = (IX)cix.c;
+    const IX crow = c - (IX)lane;    /* cell of lane 0: the row is contiguous */
+    const int xrow = cix.x - lane;
     int n = cix.live ? (int)__ldg(&a.as[c]) : 0;
     if (cix.live && (n < 1 || n > P)) {
         atomicOr(a.err, ERR_BADSET);
         n = 0;
     }
+    /* neighbour offsets along y and z (the same for the row) */
+    IX dlo[3] = {0, 0, 0}, dhi[3] = {0, 0, 0};
+    {
+        const int co[3] = {cix.x, cix.y, cix.z};
+        IX st = 1;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            const IX span = (IX)(a.res[d] - 1) * st;
+            dlo[d] = co[d] > 0 ? -st : span;
+            dhi[d] = co[d] < a.res[d] - 1 ? st : -span;
+            st *= (IX)a.res[d];
+        }
+    }
     if (n > 0) {
         const int co[3] = {cix.x, cix.y, cix.z};
-        const IX st[3] = {1, (IX)a.res[0], (IX)a.res[0] * (IX)a.res[1]};
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
             const bool wrap = a.per[d] && a.res[d] > 1;
-            const IX span = (IX)(a.res[d] - 1) * st[d];
             const bool lo = co[d] > 0 || wrap, hi = co[d] < a.res[d] - 1 || wrap;
-            const IX nlo = co[d] > 0 ? c - st[d] : c + span;
-            const IX nhi = co[d] < a.res[d] - 1 ? c + st[d] : c - span;
             sw[(2 * d) * 32 + lane] = lo ? __ldg(&a.maps[(IX)(2 * d) * S + c]) : ~0ull;
             sw[(2 * d + 1) * 32 + lane] = hi ? __ldg(&a.maps[(IX)(2 * d + 1) * S + c]) : ~0ull;
-            snb[(2 * d) * 32 + lane] = lo ? nlo : c;
-            snb[(2 * d + 1) * 32 + lane] = hi ? nhi : c;
         }
     }
-    scm[lane] = c;
     /* warp exclusive scan of the counts */
     int v = n;
 #pragma unroll
@@ -140,29 +128,45 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
         const int y = __shfl_up_sync(0xffffffffu, v, o);
         if (lane >= o) v += y;
     }
-    const int off = v - n;
     const int total = __shfl_sync(0xffffffffu, v, 31);
-    soff[lane] = off;
-    for (int k = 0; k < n; k++) icell[off + k] = (uint8_t)lane;
+    {
+        const int off = v - n;
+        for (int k = 0; k < n; k++) itag[off + k] = (uint16_t)(lane | k << 5);
+    }
     __syncwarp();
 
     /* 2. items, two per pass so that both items' loads are in flight */
     const float coef = (float)a.face_coef;
+    const IX xlo_wrap = (IX)(a.res[0] - 1), xhi_wrap = -(IX)(a.res[0] - 1);
     for (int it = lane; it < total; it += 64) {
         const int it2 = it + 32;
-        const int c1 = icell[it], i1 = it - soff[c1];
         const bool two = it2 < total;
-        const int c2 = two ? icell[it2] : c1, i2 = two ? it2 - soff[c2] : i1;
-        const float p1 = __ldg(&phi[(IX)i1 * S + scm[c1]]);
-        const float p2 = __ldg(&phi[(IX)i2 * S + scm[c2]]);
-        const float l1 = item_laplacian<DIM, IX>(phi, S, P, sw, snb, c1, i1, p1, coef);
-        const float l2 = item_laplacian<DIM, IX>(phi, S, P, sw, snb, c2, i2, p2, coef);
-        ilap[it] = l1;
-        iphi[it] = p1;
-        if (two) {
-            ilap[it2] = l2;
-            iphi[it2] = p2;
+        const int tg1 = itag[it], tg2 = two ? itag[it2] : tg1;
+        int cl[2] = {tg1 & 31, tg2 & 31}, sl[2] = {tg1 >> 5, tg2 >> 5};
+        float p[2], l[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const IX cc = crow + (IX)cl[u];
+            const int x = xrow + cl[u];
+            p[u] = __ldg(&phi[(IX)sl[u] * S + cc]);
+            const unsigned sh = 4u * (unsigned)sl[u];
+            float pn[ND];
+#pragma unroll
+            for (int q = 0; q < ND; q++) {
+                const int j = (int)((sw[q * 32 + cl[u]] >> sh) & 15u);
+                IX dq;
+                if (q == 0) dq = x > 0 ? (IX)-1 : xlo_wrap;
+                else if (q == 1) dq = x < a.res[0] - 1 ? (IX)1 : xhi_wrap;
+                else dq = (q & 1) ? dhi[q >> 1] : dlo[q >> 1];
+                pn[q] = j < P ? __ldg(&phi[(IX)j * S + cc + dq]) : p[u];
+            }
+            float acc = 0.0f;
+#pragma unroll
+            for (int q = 0; q < ND; q++) acc += pn[q] - p[u];
+            l[u] = coef * acc;
         }
+        spl[sl[0] * 33 + cl[0]] = make_float2(p[0], l[0]);
+        if (two) spl[sl[1] * 33 + cl[1]] = make_float2(p[1], l[1]);
     }
     __syncwarp();
 
@@ -171,35 +175,36 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
     uint32_t act = 0;
     double nact = 0.0, Ca = 0.0;
     const double mob = a.mob0;
-    const float *cp = iphi + off;
-    float *cl = ilap + off;
+    float2 *cpl = spl + lane;        /* slot k at cpl[33 * k] */
     if (n > 1) {
         const float sig = (float)a.sig0, inv_w = (float)(1.0 / a.wid0);
         const float w_pi2 = (float)(a.wid0 / (CIPHER_PI_D * CIPHER_PI_D));
         const float tjh = (float)(0.5 * a.tj0);
         float A = 0.0f, S1 = 0.0f, S2 = 0.0f;
         for (int k = 0; k < n; k++) {
-            const float p = cp[k];
-            A += p * inv_w + cl[k] * w_pi2;
-            S1 += p;
-            S2 += p * p;
+            const float2 e = cpl[33 * k];
+            A += e.x * inv_w + e.y * w_pi2;
+            S1 += e.x;
+            S2 += e.x * e.x;
         }
         /* capillary force, stored over the consumed Laplacian */
         double C = 0.0;
         for (int k = 0; k < n; k++) {
-            const float p = cp[k], l = cl[k];
-            const float ak = p * inv_w + l * w_pi2;
-            const float o1 = S1 - p, o2 = S2 - p * p;
-            const float cap = 8.0f * (-sig * (A - ak) - tjh * (o1 * o1 - o2)) + l;
-            cl[k] = cap;
+            const float2 e = cpl[33 * k];
+            const float pk = e.x, lk = e.y;
+            const float ak = pk * inv_w + lk * w_pi2;
+            const float o1 = S1 - pk, o2 = S2 - pk * pk;
+            const float cap = 8.0f * (-sig * (A - ak) - tjh * (o1 * o1 - o2)) + lk;
+            cpl[33 * k].y = cap;
             C += (double)cap;
         }
         for (int k = 0; k < n; k++) {
-            const double cap = (double)cl[k];
+            const float2 e = cpl[33 * k];
+            const double cap = (double)e.y;
             const double u = mob * ((double)n * cap - C);
-            const double p = (double)cp[k];
-            const bool on = (p > CIPHER_TOL && p < 1.0 - CIPHER_TOL) || (p < CIPHER_TOL && u > 0.0) ||
-                            (p > 1.0 - CIPHER_TOL && u < 0.0);
+            const double pk = (double)e.x;
+            const bool on = (pk > CIPHER_TOL && pk < 1.0 - CIPHER_TOL) || (pk < CIPHER_TOL && u > 0.0) ||
+                            (pk > 1.0 - CIPHER_TOL && u < 0.0);
             if (on) { act |= 1u << k; nact += 1.0; Ca += cap; }
         }
     }
@@ -207,7 +212,7 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
     float *fp = a.fphi + c;
     for (int m = 0; m < P; m++) {
         float vv = 0.0f;
-        if (act >> m & 1u) vv = (float)(scale * (nact * (double)cl[m] - Ca));
+        if (act >> m & 1u) vv = (float)(scale * (nact * (double)cpl[33 * m].y - Ca));
         *fp = vv;
         fp += S;
     }
