@@ -43,8 +43,8 @@ constexpr int kBX = CIPHER_MIXED_BX, kBY = CIPHER_MIXED_BY, kMixedBlock = kBX * 
  * gather, the bulk of the work, runs over the row's (cell, slot) items, so a
  * lane never idles while a neighbour lane walks a larger set:
  *   1. lane = cell: active count and the cell's face-map words into shared
- *      memory, a warp scan of the counts, one 16-bit tag (cell lane, slot)
- *      per item;
+ *      memory, one 16-bit tag (cell lane, slot) per item in slot-major
+ *      order;
  *   2. lane = item: the slot's phase fraction and its Laplacian over the
  *      cell's 2*dim faces (absent or gated faces map every slot to 15);
  *      neighbour cells follow from the row's position (y and z offsets are
@@ -121,17 +121,16 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
             sw[(2 * d + 1) * 32 + lane] = hi ? __ldg(&a.maps[(IX)(2 * d + 1) * S + c]) : ~0ull;
         }
     }
-    /* warp exclusive scan of the counts */
-    int v = n;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += y;
-    }
-    const int total = __shfl_sync(0xffffffffu, v, 31);
-    {
-        const int off = v - n;
-        for (int k = 0; k < n; k++) itag[off + k] = (uint16_t)(lane | k << 5);
+    /* items in slot-major order (slot 0 of every cell, then slot 1 of the
+     * cells that have one, ...): consecutive lanes then gather neighbouring
+     * cells of the same planes, which share sectors */
+    const int maxn = __reduce_max_sync(0xffffffffu, n);
+    const unsigned below = (1u << lane) - 1u;
+    int total = 0;
+    for (int k = 0; k < maxn; k++) {
+        const unsigned m = __ballot_sync(0xffffffffu, n > k);
+        if (n > k) itag[total + __popc(m & below)] = (uint16_t)(lane | k << 5);
+        total += __popc(m);
     }
     __syncwarp();
 
