@@ -382,6 +382,34 @@ extern "C" int cipher_ctx_layout(const cipher_ctx *c, cipher_state_layout *out)
 /* RHS and PostStep                                                     */
 /* ------------------------------------------------------------------ */
 
+/* largest float whose double value is <= x, smallest whose value is >= x */
+static float float_at_most(double x)
+{
+    float f = (float)x;
+    return (double)f > x ? nextafterf(f, -INFINITY) : f;
+}
+static float float_at_least(double x)
+{
+    float f = (float)x;
+    return (double)f < x ? nextafterf(f, INFINITY) : f;
+}
+
+template <typename R>
+static void mixed_consts(PfArgs<R> &a)
+{
+    const double pi2 = CIPHER_PI_D * CIPHER_PI_D;
+    a.sig_f = (float)a.sig0;
+    a.inv_w_f = (float)(1.0 / a.wid0);
+    a.w_pi2_f = (float)(a.wid0 / pi2);
+    a.tjh_f = (float)(0.5 * a.tj0);
+    a.mob_f = (float)a.mob0;
+    a.coef_f = (float)a.face_coef;
+    a.tol_gt = float_at_most(CIPHER_TOL);
+    a.tol1_lt = float_at_least(1.0 - CIPHER_TOL);
+    a.tol_lt = float_at_least(CIPHER_TOL);
+    a.tol1_gt = float_at_most(1.0 - CIPHER_TOL);
+}
+
 template <typename R>
 static PfArgs<R> pf_args(const cipher_ctx *c, const void *X, void *F)
 {
@@ -413,6 +441,7 @@ static PfArgs<R> pf_args(const cipher_ctx *c, const void *X, void *F)
     a.mob0 = c->mob0;
     a.wid0 = c->wid0;
     a.tj0 = c->tj0;
+    mixed_consts(a);
     a.itflist = c->d_itflist;
     a.itfs = c->d_itfs;
     a.as = (const uint16_t *)(x + c->lay.as_offset);

@@ -26,6 +26,12 @@ struct PfArgs {
     double temp_rate;
     int single;                   /* every pair uses one T-independent interface */
     double sig0, mob0, wid0, tj0; /* its sigma, m, w and triple-junction weight */
+    /* FP32 forms for the mixed single-interface kernel: sigma, 1/w, w/pi^2,
+     * tj/2, m and ffactor/vol; thresholds such that for a float p the float
+     * tests p > tol_gt, p < tol1_lt, p < tol_lt, p > tol1_gt equal the double
+     * tests p > TOL, p < 1-TOL, p < TOL, p > 1-TOL */
+    float sig_f, inv_w_f, w_pi2_f, tjh_f, mob_f, coef_f;
+    float tol_gt, tol1_lt, tol_lt, tol1_gt;
     const int32_t *itflist;
     const DevInterface *itfs;
     const uint16_t *as;

@@ -42,8 +42,8 @@ constexpr int kBX = CIPHER_MIXED_BX, kBY = CIPHER_MIXED_BY, kMixedBlock = kBX * 
  * slice of shared memory, so warps never wait for one another.  The face
  * gather, the bulk of the work, runs over the row's (cell, slot) items, so a
  * lane never idles while a neighbour lane walks a larger set:
- *   1. lane = cell: active count and the cell's face-map words into shared
- *      memory, one 16-bit tag (cell lane, slot) per item in slot-major
+ *   1. lane = cell: active count and the cell's face-map words (as 32-bit
+ *      halves, slots 0-7 and 8-15) into shared memory, one 16-bit tag (cell lane, slot) per item in slot-major
  *      order;
  *   2. lane = item: the slot's phase fraction and its Laplacian over the
  *      cell's 2*dim faces (absent or gated faces map every slot to 15);
@@ -84,8 +84,8 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
     const IX S = (IX)a.stride;
     const float *phi = a.phi;
     unsigned char *ws = smem + (size_t)(threadIdx.x >> 5) * items_warp_bytes(DIM, P);
-    uint64_t *sw = (uint64_t *)ws;                                /* [ND][32] face-map words */
-    float2 *spl = (float2 *)(sw + ND * 32);                       /* [P][33] (phi, Laplacian / capillary force) */
+    uint32_t *sw = (uint32_t *)ws;                                /* [ND][2][32] face-map word halves */
+    float2 *spl = (float2 *)(sw + ND * 64);                       /* [P][33] (phi, Laplacian / capillary force) */
     uint16_t *itag = (uint16_t *)(spl + 33 * P);                  /* [32*P] cell lane | slot << 5 */
 
     __syncwarp();                    /* the previous row's readers are done */
@@ -117,8 +117,12 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
         for (int d = 0; d < DIM; d++) {
             const bool wrap = a.per[d] && a.res[d] > 1;
             const bool lo = co[d] > 0 || wrap, hi = co[d] < a.res[d] - 1 || wrap;
-            sw[(2 * d) * 32 + lane] = lo ? __ldg(&a.maps[(IX)(2 * d) * S + c]) : ~0ull;
-            sw[(2 * d + 1) * 32 + lane] = hi ? __ldg(&a.maps[(IX)(2 * d + 1) * S + c]) : ~0ull;
+            const uint64_t wl = lo ? __ldg(&a.maps[(IX)(2 * d) * S + c]) : ~0ull;
+            const uint64_t wh = hi ? __ldg(&a.maps[(IX)(2 * d + 1) * S + c]) : ~0ull;
+            sw[(4 * d + 0) * 32 + lane] = (uint32_t)wl;
+            sw[(4 * d + 1) * 32 + lane] = (uint32_t)(wl >> 32);
+            sw[(4 * d + 2) * 32 + lane] = (uint32_t)wh;
+            sw[(4 * d + 3) * 32 + lane] = (uint32_t)(wh >> 32);
         }
     }
     /* items in slot-major order (slot 0 of every cell, then slot 1 of the
@@ -135,7 +139,7 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
     __syncwarp();
 
     /* 2. items, two per pass so that both items' loads are in flight */
-    const float coef = (float)a.face_coef;
+    const float coef = a.coef_f;
     const IX xlo_wrap = (IX)(a.res[0] - 1), xhi_wrap = -(IX)(a.res[0] - 1);
     for (int it = lane; it < total; it += 64) {
         const int it2 = it + 32;
@@ -148,11 +152,12 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
             const IX cc = crow + (IX)cl[u];
             const int x = xrow + cl[u];
             p[u] = __ldg(&phi[(IX)sl[u] * S + cc]);
-            const unsigned sh = 4u * (unsigned)sl[u];
+            const unsigned sh = 4u * (unsigned)(sl[u] & 7);
+            const uint32_t *swh = sw + (sl[u] >> 3) * 32 + cl[u];   /* the word half holding slot sl */
             float pn[ND];
 #pragma unroll
             for (int q = 0; q < ND; q++) {
-                const int j = (int)((sw[q * 32 + cl[u]] >> sh) & 15u);
+                const int j = (int)((swh[q * 64] >> sh) & 15u);
                 IX dq;
                 if (q == 0) dq = x > 0 ? (IX)-1 : xlo_wrap;
                 else if (q == 1) dq = x < a.res[0] - 1 ? (IX)1 : xhi_wrap;
@@ -169,16 +174,15 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
     }
     __syncwarp();
 
-    /* 3. cell terms */
+    /* 3. cell terms: FP32 closed forms; the active-set decision sums in
+     * FP64 (interior slots need no sum) */
     if (!cix.live) return;
     uint32_t act = 0;
-    double nact = 0.0, Ca = 0.0;
-    const double mob = a.mob0;
+    int nact = 0;
+    double Ca = 0.0;
     float2 *cpl = spl + lane;        /* slot k at cpl[33 * k] */
     if (n > 1) {
-        const float sig = (float)a.sig0, inv_w = (float)(1.0 / a.wid0);
-        const float w_pi2 = (float)(a.wid0 / (CIPHER_PI_D * CIPHER_PI_D));
-        const float tjh = (float)(0.5 * a.tj0);
+        const float inv_w = a.inv_w_f, w_pi2 = a.w_pi2_f, sig = a.sig_f, tjh = a.tjh_f;
         float A = 0.0f, S1 = 0.0f, S2 = 0.0f;
         for (int k = 0; k < n; k++) {
             const float2 e = cpl[33 * k];
@@ -197,21 +201,24 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
             cpl[33 * k].y = cap;
             C += (double)cap;
         }
+        const double nd = (double)n, mob = a.mob0;
         for (int k = 0; k < n; k++) {
             const float2 e = cpl[33 * k];
-            const double cap = (double)e.y;
-            const double u = mob * ((double)n * cap - C);
-            const double pk = (double)e.x;
-            const bool on = (pk > CIPHER_TOL && pk < 1.0 - CIPHER_TOL) || (pk < CIPHER_TOL && u > 0.0) ||
-                            (pk > 1.0 - CIPHER_TOL && u < 0.0);
-            if (on) { act |= 1u << k; nact += 1.0; Ca += cap; }
+            bool on = e.x > a.tol_gt && e.x < a.tol1_lt;
+            if (!on) {
+                const double u = mob * (nd * (double)e.y - C);
+                on = (e.x < a.tol_lt && u > 0.0) || (e.x > a.tol1_gt && u < 0.0);
+            }
+            if (on) { act |= 1u << k; nact++; Ca += (double)e.y; }
         }
     }
-    const double scale = act ? mob / nact : 0.0;
+    /* F = m (nact cap - Ca) / nact on the active slots, 0 elsewhere */
+    const float nf = (float)nact, Caf = (float)Ca;
+    const float scale = nact ? a.mob_f * __frcp_rn(nf) : 0.0f;
     float *fp = a.fphi + c;
     for (int m = 0; m < P; m++) {
         float vv = 0.0f;
-        if (act >> m & 1u) vv = (float)(scale * (nact * (double)cpl[33 * m].y - Ca));
+        if (act >> m & 1u) vv = scale * fmaf(nf, cpl[33 * m].y, -Caf);
         *fp = vv;
         fp += S;
     }
