@@ -51,8 +51,9 @@ constexpr int kBX = CIPHER_MIXED_BX, kBY = CIPHER_MIXED_BY, kMixedBlock = kBX * 
  *      the same for the whole row);
  *   3. lane = cell: the O(n) closed forms of the cell terms and all P
  *      slots of F (coalesced plane by plane).
- * (phi, Laplacian) pairs pass from phase 2 to phase 3 in a slot-major table
- * with row pitch 33, so that phase 3's lanes read distinct banks.
+ * Laplacians pass from phase 2 to phase 3 in a slot-major table with row
+ * pitch 33, so that phase 3's lanes read distinct banks; phase 3 re-reads
+ * the cell's phase fractions (coalesced, cached since phase 2).
  * The mixed path sums a Laplacian in direction order, not in the
  * reference's face order: the difference is FP32 rounding.
  * IX is the index type of plane offsets: int when every offset of the
@@ -61,7 +62,7 @@ constexpr int kBX = CIPHER_MIXED_BX, kBY = CIPHER_MIXED_BY, kMixedBlock = kBX * 
  */
 __host__ __device__ constexpr size_t items_warp_bytes(int dim, int P)
 {
-    return ((size_t)32 * 2 * dim * 8 + (size_t)33 * P * 8 + (size_t)32 * P * 2 + 15) / 16 * 16;
+    return ((size_t)32 * 2 * dim * 8 + (size_t)33 * P * 4 + (size_t)32 * P * 2 + 15) / 16 * 16;
 }
 
 __host__ __device__ constexpr size_t items_tile_bytes(int dim, int T, int P, int ix_bytes)
@@ -85,8 +86,8 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
     const float *phi = a.phi;
     unsigned char *ws = smem + (size_t)(threadIdx.x >> 5) * items_warp_bytes(DIM, P);
     uint32_t *sw = (uint32_t *)ws;                                /* [ND][2][32] face-map word halves */
-    float2 *spl = (float2 *)(sw + ND * 64);                       /* [P][33] (phi, Laplacian / capillary force) */
-    uint16_t *itag = (uint16_t *)(spl + 33 * P);                  /* [32*P] cell lane | slot << 5 */
+    float *slap = (float *)(sw + ND * 64);                        /* [P][33] Laplacian, later the capillary force */
+    uint16_t *itag = (uint16_t *)(slap + 33 * P);                 /* [32*P] cell lane | slot << 5 */
 
     __syncwarp();                    /* the previous row's readers are done */
     /* 1. cells */
@@ -169,8 +170,8 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
             for (int q = 0; q < ND; q++) acc += pn[q] - p[u];
             l[u] = coef * acc;
         }
-        spl[sl[0] * 33 + cl[0]] = make_float2(p[0], l[0]);
-        if (two) spl[sl[1] * 33 + cl[1]] = make_float2(p[1], l[1]);
+        slap[sl[0] * 33 + cl[0]] = l[0];
+        if (two) slap[sl[1] * 33 + cl[1]] = l[1];
     }
     __syncwarp();
 
@@ -180,36 +181,36 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
     uint32_t act = 0;
     int nact = 0;
     double Ca = 0.0;
-    float2 *cpl = spl + lane;        /* slot k at cpl[33 * k] */
+    float *cl3 = slap + lane;        /* slot k at cl3[33 * k] */
+    const float *cp3 = phi + c;      /* slot k at cp3[k * S] (cached since phase 2) */
     if (n > 1) {
         const float inv_w = a.inv_w_f, w_pi2 = a.w_pi2_f, sig = a.sig_f, tjh = a.tjh_f;
         float A = 0.0f, S1 = 0.0f, S2 = 0.0f;
         for (int k = 0; k < n; k++) {
-            const float2 e = cpl[33 * k];
-            A += e.x * inv_w + e.y * w_pi2;
-            S1 += e.x;
-            S2 += e.x * e.x;
+            const float pk = __ldg(&cp3[(IX)k * S]), lk = cl3[33 * k];
+            A += pk * inv_w + lk * w_pi2;
+            S1 += pk;
+            S2 += pk * pk;
         }
         /* capillary force, stored over the consumed Laplacian */
         double C = 0.0;
         for (int k = 0; k < n; k++) {
-            const float2 e = cpl[33 * k];
-            const float pk = e.x, lk = e.y;
+            const float pk = __ldg(&cp3[(IX)k * S]), lk = cl3[33 * k];
             const float ak = pk * inv_w + lk * w_pi2;
             const float o1 = S1 - pk, o2 = S2 - pk * pk;
             const float cap = 8.0f * (-sig * (A - ak) - tjh * (o1 * o1 - o2)) + lk;
-            cpl[33 * k].y = cap;
+            cl3[33 * k] = cap;
             C += (double)cap;
         }
         const double nd = (double)n, mob = a.mob0;
         for (int k = 0; k < n; k++) {
-            const float2 e = cpl[33 * k];
-            bool on = e.x > a.tol_gt && e.x < a.tol1_lt;
+            const float pk = __ldg(&cp3[(IX)k * S]), capk = cl3[33 * k];
+            bool on = pk > a.tol_gt && pk < a.tol1_lt;
             if (!on) {
-                const double u = mob * (nd * (double)e.y - C);
-                on = (e.x < a.tol_lt && u > 0.0) || (e.x > a.tol1_gt && u < 0.0);
+                const double u = mob * (nd * (double)capk - C);
+                on = (pk < a.tol_lt && u > 0.0) || (pk > a.tol1_gt && u < 0.0);
             }
-            if (on) { act |= 1u << k; nact++; Ca += (double)e.y; }
+            if (on) { act |= 1u << k; nact++; Ca += (double)capk; }
         }
     }
     /* F = m (nact cap - Ca) / nact on the active slots, 0 elsewhere */
@@ -218,7 +219,7 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
     float *fp = a.fphi + c;
     for (int m = 0; m < P; m++) {
         float vv = 0.0f;
-        if (act >> m & 1u) vv = scale * fmaf(nf, cpl[33 * m].y, -Caf);
+        if (act >> m & 1u) vv = scale * fmaf(nf, cl3[33 * m], -Caf);
         *fp = vv;
         fp += S;
     }
