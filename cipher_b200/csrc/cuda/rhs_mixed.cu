@@ -4,9 +4,11 @@
  * rhs_phasefield.cu; the equations are src/cipher.c:235-317 and 391-555).
  *
  * Phase fractions, the stencil and the interface terms are FP32 (storage and
- * arithmetic); the pair-rate reductions that decide the active set and the
- * constrained rate are accumulated in FP64.  For a single interface the
- * pair and triple sums of the reference collapse to per-cell sums:
+ * arithmetic).  The single-interface kernel keeps every cell term in FP32;
+ * the several-interface form accumulates the pair-rate reductions that
+ * decide the active set and the constrained rate in FP64.  For a single
+ * interface the pair and triple sums of the reference collapse to per-cell
+ * sums:
  *   sum_{j != k} sigma*a_j              = sigma*(A - a_k)
  *   sum_{j<i; j,i != k} phi_j*phi_i    = ((S1-phi_k)^2 - (S2-phi_k^2))/2
  *   sum_{j != k} m*(cap_k - cap_j)     = m*(n*cap_k - C)
@@ -33,6 +35,10 @@
 namespace cipher {
 
 constexpr int kBX = CIPHER_MIXED_BX, kBY = CIPHER_MIXED_BY, kMixedBlock = kBX * kBY;
+#ifndef CIPHER_MIXED_IPP
+#define CIPHER_MIXED_IPP 2
+#endif
+constexpr int kIPP = CIPHER_MIXED_IPP;   /* items per lane and pass in the items kernel */
 
 /* ------------------------------------------------------------------ */
 /* single interface: (cell, slot) items spread over a warp's lanes       */
@@ -139,20 +145,25 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
     }
     __syncwarp();
 
-    /* 2. items, two per pass so that both items' loads are in flight */
+    /* 2. items, kIPP per pass so that their loads are in flight together */
     const float coef = a.coef_f;
     const IX xlo_wrap = (IX)(a.res[0] - 1), xhi_wrap = -(IX)(a.res[0] - 1);
-    for (int it = lane; it < total; it += 64) {
-        const int it2 = it + 32;
-        const bool two = it2 < total;
-        const int tg1 = itag[it], tg2 = two ? itag[it2] : tg1;
-        int cl[2] = {tg1 & 31, tg2 & 31}, sl[2] = {tg1 >> 5, tg2 >> 5};
-        float p[2], l[2];
+    for (int it = lane; it < total; it += 32 * kIPP) {
+        int cl[kIPP], sl[kIPP];
+        bool ok[kIPP];
+        float l[kIPP];
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
+        for (int u = 0; u < kIPP; u++) {
+            ok[u] = it + 32 * u < total;
+            const int tg = itag[ok[u] ? it + 32 * u : it];
+            cl[u] = tg & 31;
+            sl[u] = tg >> 5;
+        }
+#pragma unroll
+        for (int u = 0; u < kIPP; u++) {
             const IX cc = crow + (IX)cl[u];
             const int x = xrow + cl[u];
-            p[u] = __ldg(&phi[(IX)sl[u] * S + cc]);
+            const float p = __ldg(&phi[(IX)sl[u] * S + cc]);
             const unsigned sh = 4u * (unsigned)(sl[u] & 7);
             const uint32_t *swh = sw + (sl[u] >> 3) * 32 + cl[u];   /* the word half holding slot sl */
             float pn[ND];
@@ -163,64 +174,67 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
                 if (q == 0) dq = x > 0 ? (IX)-1 : xlo_wrap;
                 else if (q == 1) dq = x < a.res[0] - 1 ? (IX)1 : xhi_wrap;
                 else dq = (q & 1) ? dhi[q >> 1] : dlo[q >> 1];
-                pn[q] = j < P ? __ldg(&phi[(IX)j * S + cc + dq]) : p[u];
+                pn[q] = j < P ? __ldg(&phi[(IX)j * S + cc + dq]) : p;
             }
             float acc = 0.0f;
 #pragma unroll
-            for (int q = 0; q < ND; q++) acc += pn[q] - p[u];
+            for (int q = 0; q < ND; q++) acc += pn[q] - p;
             l[u] = coef * acc;
         }
-        slap[sl[0] * 33 + cl[0]] = l[0];
-        if (two) slap[sl[1] * 33 + cl[1]] = l[1];
+#pragma unroll
+        for (int u = 0; u < kIPP; u++)
+            if (ok[u]) slap[sl[u] * 33 + cl[u]] = l[u];
     }
     __syncwarp();
 
-    /* 3. cell terms: FP32 closed forms; the active-set decision sums in
-     * FP64 (interior slots need no sum) */
+    /* 3. cell terms in FP32.  The sum of the capillary forces over the
+     * cell's slots has a closed form in the slot sums:
+     *   C = 8 (-sigma (n-1) A - tj/2 (n-2)(S1^2 - S2)) + L,   L = sum of Laplacians,
+     * so one pass gives the sums and a second the forces and the active set */
     if (!cix.live) return;
     uint32_t act = 0;
-    int nact = 0;
-    double Ca = 0.0;
+    float nf = 0.0f, Caf = 0.0f;
     float *cl3 = slap + lane;        /* slot k at cl3[33 * k] */
     const float *cp3 = phi + c;      /* slot k at cp3[k * S] (cached since phase 2) */
     if (n > 1) {
-        const float inv_w = a.inv_w_f, w_pi2 = a.w_pi2_f, sig = a.sig_f, tjh = a.tjh_f;
-        float A = 0.0f, S1 = 0.0f, S2 = 0.0f;
+        const float inv_w = a.inv_w_f, w_pi2 = a.w_pi2_f, sig = a.sig_f, tjh = a.tjh_f, mob = a.mob_f;
+        float A = 0.0f, S1 = 0.0f, S2 = 0.0f, L = 0.0f;
         for (int k = 0; k < n; k++) {
             const float pk = __ldg(&cp3[(IX)k * S]), lk = cl3[33 * k];
             A += pk * inv_w + lk * w_pi2;
             S1 += pk;
             S2 += pk * pk;
+            L += lk;
         }
-        /* capillary force, stored over the consumed Laplacian */
-        double C = 0.0;
+        const float fn = (float)n;
+        const float C = 8.0f * (-sig * (fn - 1.0f) * A - tjh * (fn - 2.0f) * (S1 * S1 - S2)) + L;
         for (int k = 0; k < n; k++) {
             const float pk = __ldg(&cp3[(IX)k * S]), lk = cl3[33 * k];
             const float ak = pk * inv_w + lk * w_pi2;
             const float o1 = S1 - pk, o2 = S2 - pk * pk;
             const float cap = 8.0f * (-sig * (A - ak) - tjh * (o1 * o1 - o2)) + lk;
             cl3[33 * k] = cap;
-            C += (double)cap;
-        }
-        const double nd = (double)n, mob = a.mob0;
-        for (int k = 0; k < n; k++) {
-            const float pk = __ldg(&cp3[(IX)k * S]), capk = cl3[33 * k];
             bool on = pk > a.tol_gt && pk < a.tol1_lt;
             if (!on) {
-                const double u = mob * (nd * (double)capk - C);
-                on = (pk < a.tol_lt && u > 0.0) || (pk > a.tol1_gt && u < 0.0);
+                const float u = mob * (fn * cap - C);
+                on = (pk < a.tol_lt && u > 0.0f) || (pk > a.tol1_gt && u < 0.0f);
             }
-            if (on) { act |= 1u << k; nact++; Ca += (double)capk; }
+            if (on) { act |= 1u << k; nf += 1.0f; Caf += cap; }
         }
     }
-    /* F = m (nact cap - Ca) / nact on the active slots, 0 elsewhere */
-    const float nf = (float)nact, Caf = (float)Ca;
-    const float scale = nact ? a.mob_f * __frcp_rn(nf) : 0.0f;
+    /* F = m (nact cap - Ca) / nact on the active slots, 0 elsewhere; slots
+     * at or above the row's largest count are 0 for every lane */
+    const float scale = act ? a.mob_f * __frcp_rn(nf) : 0.0f;
     float *fp = a.fphi + c;
-    for (int m = 0; m < P; m++) {
+    int m = 0;
+    for (; m < maxn; m++) {
         float vv = 0.0f;
         if (act >> m & 1u) vv = scale * fmaf(nf, cl3[33 * m], -Caf);
         *fp = vv;
+        fp += S;
+    }
+    for (; m < P; m++) {
+        *fp = 0.0f;
         fp += S;
     }
     double tr = 0.0;
