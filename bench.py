@@ -598,7 +598,7 @@ def run_cipher(args, rank, world, local_rank):
                      "traffic": tr32, "peak_source": peak_src, "algorithmic_bytes_per_launch": b32,
                      "bytes_per_cell_update": b32 // ncells, "fp64_format_frac": b64 / avg32 / 1e9 / peak,
                      "state_exact_bytes_per_launch": e32, "state_exact_frac": e32 / avg32 / 1e9 / peak,
-                     "kernel": "k_rhs_pf_mixed_items<3>"},
+                     "kernel": "k_rhs_pf_mixed_items<3,int>"},
         "cpu_baseline": cpu,
         "e2e": {"value": ncells * e2e_steps * world / (tot_e2e / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": aos_bytes, "d2h_bytes_per_step": aos_bytes,
