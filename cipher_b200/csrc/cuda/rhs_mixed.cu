@@ -199,27 +199,33 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
     if (n > 1) {
         const float inv_w = a.inv_w_f, w_pi2 = a.w_pi2_f, sig = a.sig_f, tjh = a.tjh_f, mob = a.mob_f;
         float A = 0.0f, S1 = 0.0f, S2 = 0.0f, L = 0.0f;
-        for (int k = 0; k < n; k++) {
-            const float pk = __ldg(&cp3[(IX)k * S]), lk = cl3[33 * k];
-            A += pk * inv_w + lk * w_pi2;
-            S1 += pk;
-            S2 += pk * pk;
-            L += lk;
+        {
+            const float *pp = cp3;
+#pragma unroll 2
+            for (int k = 0; k < n; k++, pp += S) {
+                const float pk = __ldg(pp), lk = cl3[33 * k];
+                A += pk * inv_w + lk * w_pi2;
+                S1 += pk;
+                S2 += pk * pk;
+                L += lk;
+            }
         }
         const float fn = (float)n;
         const float C = 8.0f * (-sig * (fn - 1.0f) * A - tjh * (fn - 2.0f) * (S1 * S1 - S2)) + L;
-        for (int k = 0; k < n; k++) {
-            const float pk = __ldg(&cp3[(IX)k * S]), lk = cl3[33 * k];
+        const float *pp = cp3;
+#pragma unroll 2
+        for (int k = 0; k < n; k++, pp += S) {
+            const float pk = __ldg(pp), lk = cl3[33 * k];
             const float ak = pk * inv_w + lk * w_pi2;
             const float o1 = S1 - pk, o2 = S2 - pk * pk;
             const float cap = 8.0f * (-sig * (A - ak) - tjh * (o1 * o1 - o2)) + lk;
             cl3[33 * k] = cap;
-            bool on = pk > a.tol_gt && pk < a.tol1_lt;
-            if (!on) {
-                const float u = mob * (fn * cap - C);
-                on = (pk < a.tol_lt && u > 0.0f) || (pk > a.tol1_gt && u < 0.0f);
-            }
-            if (on) { act |= 1u << k; nf += 1.0f; Caf += cap; }
+            const float u = mob * (fn * cap - C);
+            const bool on = (pk > a.tol_gt && pk < a.tol1_lt) || (pk < a.tol_lt && u > 0.0f) ||
+                            (pk > a.tol1_gt && u < 0.0f);
+            act |= (uint32_t)on << k;
+            nf += on ? 1.0f : 0.0f;
+            Caf += on ? cap : 0.0f;
         }
     }
     /* F = m (nact cap - Ca) / nact on the active slots, 0 elsewhere; slots
