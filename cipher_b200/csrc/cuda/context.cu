@@ -105,7 +105,14 @@ struct cipher_ctx {
     /* buffers of the host-AoS entry point, allocated on first use */
     double *d_aos_x, *d_aos_f;
     void *d_X, *d_F;
+    /* its slab pipeline: copy-in, compute and copy-out streams and their
+     * events, created on first use */
+    int pipe_ready;
+    cudaStream_t s_up, s_cp, s_dn;
+    cudaEvent_t ev_start, ev_end, ev_up[32], ev_done[32];
 };
+
+static constexpr int kAosSlabs = 32;
 
 static int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 
@@ -174,6 +181,17 @@ static void free_ctx(cipher_ctx *c)
     cudaFree(c->d_aos_f);
     cudaFree(c->d_X);
     cudaFree(c->d_F);
+    if (c->pipe_ready) {
+        cudaStreamDestroy(c->s_up);
+        cudaStreamDestroy(c->s_cp);
+        cudaStreamDestroy(c->s_dn);
+        cudaEventDestroy(c->ev_start);
+        cudaEventDestroy(c->ev_end);
+        for (int i = 0; i < kAosSlabs; i++) {
+            cudaEventDestroy(c->ev_up[i]);
+            cudaEventDestroy(c->ev_done[i]);
+        }
+    }
     free(c);
 }
 
@@ -821,6 +839,82 @@ extern "C" int cipher_state_to_aos(cipher_ctx *c, const void *X, double *aos, vo
     return CIPHER_OK;
 }
 
+static int make_pipeline(cipher_ctx *c)
+{
+    if (c->pipe_ready) return CIPHER_OK;
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->s_up, cudaStreamNonBlocking), "stream");
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->s_cp, cudaStreamNonBlocking), "stream");
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->s_dn, cudaStreamNonBlocking), "stream");
+    CUDA_TRY(cudaEventCreateWithFlags(&c->ev_start, cudaEventDisableTiming), "event");
+    CUDA_TRY(cudaEventCreateWithFlags(&c->ev_end, cudaEventDisableTiming), "event");
+    for (int i = 0; i < kAosSlabs; i++) {
+        CUDA_TRY(cudaEventCreateWithFlags(&c->ev_up[i], cudaEventDisableTiming), "event");
+        CUDA_TRY(cudaEventCreateWithFlags(&c->ev_done[i], cudaEventDisableTiming), "event");
+    }
+    c->pipe_ready = 1;
+    return CIPHER_OK;
+}
+
+/* phase-field RHS of 3D grids in z-slabs: slab i is copied in and converted
+ * on s_up; once its own and both neighbouring slabs are in, its face maps,
+ * RHS and F conversion run on s_cp and its F rows are copied out on s_dn,
+ * so that copies out of finished slabs overlap copies into later ones.
+ * With periodic z the last slab is copied in second, so that the slabs can
+ * run in order with each waiting for one more copy. */
+template <typename R>
+static int aos_host_slabs(cipher_ctx *c, const double *X_host, double *F_host, cudaStream_t s)
+{
+    int rc = make_pipeline(c);
+    if (rc) return rc;
+    const int Rz = c->res[2];
+    const int K = Rz < kAosSlabs ? Rz : kAosSlabs;
+    const int64_t plane = (int64_t)c->res[0] * c->res[1];
+    const int64_t ndof = c->aos.ndof;
+    int zs[kAosSlabs + 1];
+    for (int i = 0; i <= K; i++) zs[i] = (int)((int64_t)Rz * i / K);
+    const bool wrap = c->per[2] && Rz > 1;
+    CUDA_TRY(cudaEventRecord(c->ev_start, s), "event");
+    CUDA_TRY(cudaStreamWaitEvent(c->s_up, c->ev_start, 0), "wait");
+    CUDA_TRY(cudaStreamWaitEvent(c->s_cp, c->ev_start, 0), "wait");
+    CUDA_TRY(cudaStreamWaitEvent(c->s_dn, c->ev_start, 0), "wait");
+    const LayoutArgs lx = layout_args(c, c->d_X), lf = layout_args(c, c->d_F);
+    cudaError_t e;
+    for (int u = 0; u < K; u++) {
+        const int i = !wrap || u == 0 ? u : u == 1 ? K - 1 : u - 1;   /* periodic: 0, K-1, 1, 2, ... */
+        const int64_t c0 = zs[i] * plane, c1 = zs[i + 1] * plane;
+        CUDA_TRY(cudaMemcpyAsync(c->d_aos_x + c0 * ndof, X_host + c0 * ndof, (size_t)((c1 - c0) * ndof) * sizeof(double),
+                                 cudaMemcpyHostToDevice, c->s_up), "copy X slab to device");
+        if ((e = launch_aos_to_soa_range(lx, c->d_aos_x, c0, c1, c->s_up)) != cudaSuccess) return cuda_fail(e, "aos->state launch");
+        CUDA_TRY(cudaEventRecord(c->ev_up[i], c->s_up), "event");
+    }
+    for (int i = 0; i < K; i++) {
+        for (int d = -1; d <= 1; d++) {
+            int j = i + d;
+            if (j < 0 || j >= K) {
+                if (!wrap) continue;
+                j = (j + K) % K;
+            }
+            CUDA_TRY(cudaStreamWaitEvent(c->s_cp, c->ev_up[j], 0), "wait");
+        }
+        const int64_t c0 = zs[i] * plane, c1 = zs[i + 1] * plane;
+        if ((e = launch_build_maps_range(post_args<R>(c, c->d_X), 3, c0, c1, c->s_cp)) != cudaSuccess)
+            return cuda_fail(e, "face map launch");
+        PfArgs<R> a = pf_args<R>(c, c->d_X, c->d_F);
+        a.zbase = zs[i];
+        a.zcount = zs[i + 1] - zs[i];
+        if ((e = launch_rhs_phasefield(a, 3, c->s_cp)) != cudaSuccess) return cuda_fail(e, "rhs launch");
+        if ((e = launch_soa_to_aos_range(lf, c->d_aos_f, 0, c0, c1, c->s_cp)) != cudaSuccess)
+            return cuda_fail(e, "state->aos launch");
+        CUDA_TRY(cudaEventRecord(c->ev_done[i], c->s_cp), "event");
+        CUDA_TRY(cudaStreamWaitEvent(c->s_dn, c->ev_done[i], 0), "wait");
+        CUDA_TRY(cudaMemcpyAsync(F_host + c0 * ndof, c->d_aos_f + c0 * ndof, (size_t)((c1 - c0) * ndof) * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c->s_dn), "copy F slab to host");
+    }
+    CUDA_TRY(cudaEventRecord(c->ev_end, c->s_dn), "event");
+    CUDA_TRY(cudaStreamWaitEvent(s, c->ev_end, 0), "wait");
+    return CIPHER_OK;
+}
+
 extern "C" int cipher_rhs_aos_host(cipher_ctx *c, double t, const double *X_host, double *F_host, void *stream)
 {
     if (!c || !X_host || !F_host) return set_error(CIPHER_E_ARG, "NULL argument");
@@ -831,18 +925,25 @@ extern "C" int cipher_rhs_aos_host(cipher_ctx *c, double t, const double *X_host
         CUDA_TRY(cudaMalloc(&c->d_aos_f, nb), "cudaMalloc aos f");
         CUDA_TRY(cudaMalloc(&c->d_X, (size_t)c->lay.bytes), "cudaMalloc X");
         CUDA_TRY(cudaMalloc(&c->d_F, (size_t)c->lay.bytes), "cudaMalloc F");
-        CUDA_TRY(cudaMemset(c->d_F, 0, (size_t)c->lay.bytes), "cudaMemset F");
+        CUDA_TRY(cudaMemsetAsync(c->d_F, 0, (size_t)c->lay.bytes, s), "cudaMemset F");
     }
-    CUDA_TRY(cudaMemcpyAsync(c->d_aos_x, X_host, nb, cudaMemcpyHostToDevice, s), "copy X to device");
-    cudaError_t e = launch_aos_to_soa(layout_args(c, c->d_X), c->d_aos_x, s);
-    if (e != cudaSuccess) return cuda_fail(e, "aos->state launch");
-    e = build_maps(c, c->d_X, s);
-    if (e != cudaSuccess) return cuda_fail(e, "face map launch");
-    int rc = cipher_rhs(c, t, c->d_X, c->d_F, stream);
-    if (rc) return rc;
-    e = launch_soa_to_aos(layout_args(c, c->d_F), c->d_aos_f, 0, s);
-    if (e != cudaSuccess) return cuda_fail(e, "state->aos launch");
-    CUDA_TRY(cudaMemcpyAsync(F_host, c->d_aos_f, nb, cudaMemcpyDeviceToHost, s), "copy F to host");
+    if (!c->general && c->dim == 3 && c->res[2] >= 4) {
+        /* 3D phase field: z-slab pipeline */
+        const int rc = c->precision == CIPHER_PREC_FP64 ? aos_host_slabs<double>(c, X_host, F_host, s)
+                                                        : aos_host_slabs<float>(c, X_host, F_host, s);
+        if (rc) return rc;
+    } else {
+        CUDA_TRY(cudaMemcpyAsync(c->d_aos_x, X_host, nb, cudaMemcpyHostToDevice, s), "copy X to device");
+        cudaError_t e = launch_aos_to_soa(layout_args(c, c->d_X), c->d_aos_x, s);
+        if (e != cudaSuccess) return cuda_fail(e, "aos->state launch");
+        e = build_maps(c, c->d_X, s);
+        if (e != cudaSuccess) return cuda_fail(e, "face map launch");
+        int rc = cipher_rhs(c, t, c->d_X, c->d_F, stream);
+        if (rc) return rc;
+        e = launch_soa_to_aos(layout_args(c, c->d_F), c->d_aos_f, 0, s);
+        if (e != cudaSuccess) return cuda_fail(e, "state->aos launch");
+        CUDA_TRY(cudaMemcpyAsync(F_host, c->d_aos_f, nb, cudaMemcpyDeviceToHost, s), "copy F to host");
+    }
     CUDA_TRY(cudaStreamSynchronize(s), "stream sync");
     return cipher_ctx_check(c, stream);
 }

@@ -25,6 +25,7 @@ struct PfArgs {
     int has_temp_rate;
     double temp_rate;
     int single;                   /* every pair uses one T-independent interface */
+    int zbase, zcount;            /* planes [zbase, zbase+zcount) of a 3D grid; zcount 0 = all */
     double sig0, mob0, wid0, tj0; /* its sigma, m, w and triple-junction weight */
     /* FP32 forms for the mixed single-interface kernel: sigma, 1/w, w/pi^2,
      * tj/2, m and ffactor/vol; thresholds such that for a float p the float
@@ -160,6 +161,9 @@ cudaError_t launch_poststep(const PostArgs<float> &a, int dim, cudaStream_t s);
 /* the face maps of a state from its sets (also part of launch_poststep) */
 cudaError_t launch_build_maps(const PostArgs<double> &a, int dim, cudaStream_t s);
 cudaError_t launch_build_maps(const PostArgs<float> &a, int dim, cudaStream_t s);
+/* cells [c0, c1) only */
+cudaError_t launch_build_maps_range(const PostArgs<double> &a, int dim, int64_t c0, int64_t c1, cudaStream_t s);
+cudaError_t launch_build_maps_range(const PostArgs<float> &a, int dim, int64_t c0, int64_t c1, cudaStream_t s);
 
 /* batched PostStep: domain i owns blocks [block_start[i], block_start[i+1])
  * of 256 cells; domains whose `active` entry is 0 are skipped */
@@ -187,6 +191,8 @@ struct LayoutArgs {
     void *tm;
 };
 cudaError_t launch_aos_to_soa(const LayoutArgs &a, const double *aos, cudaStream_t s);
+/* cells [c0, c1) of the domain (aos is the whole domain's array) */
+cudaError_t launch_aos_to_soa_range(const LayoutArgs &a, const double *aos, int64_t c0, int64_t c1, cudaStream_t s);
 
 /* SetUpProblem state from a device voxel map (layout.cu) */
 struct InitArgs {
@@ -198,6 +204,8 @@ struct InitArgs {
 };
 cudaError_t launch_init_sharp(const InitArgs &a, cudaStream_t s);
 cudaError_t launch_soa_to_aos(const LayoutArgs &a, double *aos, int include_as, cudaStream_t s);
+cudaError_t launch_soa_to_aos_range(const LayoutArgs &a, double *aos, int include_as, int64_t c0, int64_t c1,
+                                    cudaStream_t s);
 
 /* what the batch driver needs to know of a context (context.cu) */
 struct CtxInfo {

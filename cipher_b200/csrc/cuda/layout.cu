@@ -15,10 +15,11 @@
 
 namespace cipher {
 
-__global__ void __launch_bounds__(256) k_aos_to_soa(const LayoutArgs a, const double *__restrict__ aos)
+__global__ void __launch_bounds__(256) k_aos_to_soa(const LayoutArgs a, const double *__restrict__ aos, int64_t c0,
+                                                    int64_t c1)
 {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.ncells) return;
+    const int64_t c = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= c1) return;
     const int64_t S = a.stride;
     const double *row = aos + c * a.ndof;
     for (int k = 0; k <= a.P; k++) {
@@ -38,10 +39,11 @@ __global__ void __launch_bounds__(256) k_aos_to_soa(const LayoutArgs a, const do
     else ((float *)a.tm)[c] = (float)t;
 }
 
-__global__ void __launch_bounds__(256) k_soa_to_aos(const LayoutArgs a, double *__restrict__ aos, int include_as)
+__global__ void __launch_bounds__(256) k_soa_to_aos(const LayoutArgs a, double *__restrict__ aos, int include_as,
+                                                    int64_t c0, int64_t c1)
 {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.ncells) return;
+    const int64_t c = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= c1) return;
     const int64_t S = a.stride;
     double *row = aos + c * a.ndof;
     for (int k = 0; k <= a.P; k++) row[a.as_off + k] = include_as ? (double)a.as[(int64_t)k * S + c] : 0.0;
@@ -53,18 +55,32 @@ __global__ void __launch_bounds__(256) k_soa_to_aos(const LayoutArgs a, double *
     row[a.tm_off] = a.real_bytes == 8 ? ((const double *)a.tm)[c] : (double)((const float *)a.tm)[c];
 }
 
+/* cells [c0, c1) of the domain; aos is the whole domain's AoS array */
+cudaError_t launch_aos_to_soa_range(const LayoutArgs &a, const double *aos, int64_t c0, int64_t c1, cudaStream_t s)
+{
+    if (c1 <= c0) return cudaSuccess;
+    const int64_t blocks = (c1 - c0 + 255) / 256;
+    k_aos_to_soa<<<(unsigned)blocks, 256, 0, s>>>(a, aos, c0, c1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_soa_to_aos_range(const LayoutArgs &a, double *aos, int include_as, int64_t c0, int64_t c1,
+                                    cudaStream_t s)
+{
+    if (c1 <= c0) return cudaSuccess;
+    const int64_t blocks = (c1 - c0 + 255) / 256;
+    k_soa_to_aos<<<(unsigned)blocks, 256, 0, s>>>(a, aos, include_as, c0, c1);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_aos_to_soa(const LayoutArgs &a, const double *aos, cudaStream_t s)
 {
-    int64_t blocks = (a.ncells + 255) / 256;
-    k_aos_to_soa<<<(unsigned)blocks, 256, 0, s>>>(a, aos);
-    return cudaGetLastError();
+    return launch_aos_to_soa_range(a, aos, 0, a.ncells, s);
 }
 
 cudaError_t launch_soa_to_aos(const LayoutArgs &a, double *aos, int include_as, cudaStream_t s)
 {
-    int64_t blocks = (a.ncells + 255) / 256;
-    k_soa_to_aos<<<(unsigned)blocks, 256, 0, s>>>(a, aos, include_as);
-    return cudaGetLastError();
+    return launch_soa_to_aos_range(a, aos, include_as, 0, a.ncells, s);
 }
 
 /* SetUpProblem state (src/init.c:1739-1827) from the voxel map: the own

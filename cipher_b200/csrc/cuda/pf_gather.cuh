@@ -93,14 +93,15 @@ struct CellIndex {
     bool live;
 };
 
-/* blocks of BX x BY cells in (x, y); grid (ceil(res0/BX), ceil(res1/BY), res2) */
+/* blocks of BX x BY cells in (x, y); grid (ceil(res0/BX), ceil(res1/BY),
+ * planes), plane zbase + blockIdx.z */
 template <int BX, int BY>
-__device__ __forceinline__ CellIndex cell_index(const int *res)
+__device__ __forceinline__ CellIndex cell_index(const int *res, int zbase = 0)
 {
     CellIndex ci;
     ci.x = blockIdx.x * BX + (int)threadIdx.x % BX;
     ci.y = blockIdx.y * BY + (int)threadIdx.x / BX;
-    ci.z = blockIdx.z;
+    ci.z = zbase + (int)blockIdx.z;
     ci.live = ci.x < res[0] && ci.y < res[1];
     ci.c = (int64_t)ci.x + (int64_t)res[0] * ((int64_t)ci.y + (int64_t)res[1] * ci.z);
     return ci;

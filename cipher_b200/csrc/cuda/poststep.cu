@@ -266,26 +266,34 @@ __device__ __forceinline__ void build_maps_cell(const PostArgs<R> &a, int64_t c)
 }
 
 template <int DIM, typename R>
-__global__ void __launch_bounds__(256) k_build_maps(const PostArgs<R> a)
+__global__ void __launch_bounds__(256) k_build_maps(const PostArgs<R> a, int64_t c0, int64_t c1)
 {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.ncells) return;
+    const int64_t c = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= c1) return;
     build_maps_cell<DIM, R>(a, c);
 }
 
 template <typename R>
-static cudaError_t launch_maps(const PostArgs<R> &a, int dim, cudaStream_t s)
+static cudaError_t launch_maps(const PostArgs<R> &a, int dim, int64_t c0, int64_t c1, cudaStream_t s)
 {
-    if (!a.maps) return cudaSuccess;
-    const int64_t blocks = (a.ncells + 255) / 256;
-    if (dim == 1) k_build_maps<1, R><<<(unsigned)blocks, 256, 0, s>>>(a);
-    else if (dim == 2) k_build_maps<2, R><<<(unsigned)blocks, 256, 0, s>>>(a);
-    else k_build_maps<3, R><<<(unsigned)blocks, 256, 0, s>>>(a);
+    if (!a.maps || c1 <= c0) return cudaSuccess;
+    const int64_t blocks = (c1 - c0 + 255) / 256;
+    if (dim == 1) k_build_maps<1, R><<<(unsigned)blocks, 256, 0, s>>>(a, c0, c1);
+    else if (dim == 2) k_build_maps<2, R><<<(unsigned)blocks, 256, 0, s>>>(a, c0, c1);
+    else k_build_maps<3, R><<<(unsigned)blocks, 256, 0, s>>>(a, c0, c1);
     return cudaGetLastError();
 }
 
-cudaError_t launch_build_maps(const PostArgs<double> &a, int dim, cudaStream_t s) { return launch_maps(a, dim, s); }
-cudaError_t launch_build_maps(const PostArgs<float> &a, int dim, cudaStream_t s) { return launch_maps(a, dim, s); }
+cudaError_t launch_build_maps(const PostArgs<double> &a, int dim, cudaStream_t s) { return launch_maps(a, dim, 0, a.ncells, s); }
+cudaError_t launch_build_maps(const PostArgs<float> &a, int dim, cudaStream_t s) { return launch_maps(a, dim, 0, a.ncells, s); }
+cudaError_t launch_build_maps_range(const PostArgs<double> &a, int dim, int64_t c0, int64_t c1, cudaStream_t s)
+{
+    return launch_maps(a, dim, c0, c1, s);
+}
+cudaError_t launch_build_maps_range(const PostArgs<float> &a, int dim, int64_t c0, int64_t c1, cudaStream_t s)
+{
+    return launch_maps(a, dim, c0, c1, s);
+}
 
 /* batched: block k of the list belongs to the domain whose range holds k */
 template <typename R>
@@ -367,7 +375,7 @@ static cudaError_t launch_post(const PostArgs<R> &a, int dim, cudaStream_t s)
     else if (dim == 2) k_post_union<2, CIPHER_PMAX, R><<<grid, block, 0, s>>>(a);
     else k_post_union<3, CIPHER_PMAX, R><<<grid, block, 0, s>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    return launch_maps(a, dim, s);
+    return launch_maps(a, dim, 0, a.ncells, s);
 }
 
 cudaError_t launch_poststep(const PostArgs<double> &a, int dim, cudaStream_t s) { return launch_post(a, dim, s); }

@@ -252,7 +252,7 @@ template <int DIM, typename IX>
 __global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_items(const PfArgs<float> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const CellIndex ci = cell_index<kBX, kBY>(a.res);
+    const CellIndex ci = cell_index<kBX, kBY>(a.res, a.zbase);
     mixed_items_tile<DIM, IX>(a, ci, smem);
 }
 
@@ -274,7 +274,7 @@ template <int DIM, int PM>
 __global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_multi(const PfArgs<float> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const CellIndex ci = cell_index<kBX, kBY>(a.res);
+    const CellIndex ci = cell_index<kBX, kBY>(a.res, a.zbase);
     const SlotColumns<float> sc = slot_columns<float>(smem, a.P, blockDim.x, threadIdx.x, true);
     pf_mixed_multi_cell<DIM, PM>(a, ci, sc);
 }
@@ -314,7 +314,8 @@ static cudaError_t allow_smem(K kernel, size_t bytes)
 template <int DIM, int PM>
 static void launch_pm(const PfArgs<float> &a, cudaStream_t s)
 {
-    dim3 grid((unsigned)((a.res[0] + kBX - 1) / kBX), (unsigned)((a.res[1] + kBY - 1) / kBY), (unsigned)a.res[2]);
+    dim3 grid((unsigned)((a.res[0] + kBX - 1) / kBX), (unsigned)((a.res[1] + kBY - 1) / kBY),
+              (unsigned)(a.zcount > 0 ? a.zcount : a.res[2]));
     if (a.single) {
         if (items_fit_i32(a.stride, a.P, DIM)) {
             const size_t sm = items_tile_bytes(DIM, kMixedBlock, a.P, 4);

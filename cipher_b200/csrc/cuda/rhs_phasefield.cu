@@ -45,7 +45,7 @@ template <int DIM, int PM, bool SINGLE>
 __global__ void __launch_bounds__(kFp64Block) k_rhs_pf_fp64(const PfArgs<double> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const CellIndex ci = cell_index<kBX, kBY>(a.res);
+    const CellIndex ci = cell_index<kBX, kBY>(a.res, a.zbase);
     const SlotColumns<double> sc = slot_columns<double>(smem, a.P, blockDim.x, threadIdx.x, true);
     pf_fp64_cell<DIM, PM, SINGLE>(a, ci, sc);
 }
@@ -67,7 +67,8 @@ __global__ void __launch_bounds__(kBX * BY) k_rhs_pf_fp64_batched(const BatchTil
 template <int DIM, int PM>
 static void launch_pm(const PfArgs<double> &a, cudaStream_t s)
 {
-    dim3 grid((unsigned)((a.res[0] + kBX - 1) / kBX), (unsigned)((a.res[1] + kBY - 1) / kBY), (unsigned)a.res[2]);
+    dim3 grid((unsigned)((a.res[0] + kBX - 1) / kBX), (unsigned)((a.res[1] + kBY - 1) / kBY),
+              (unsigned)(a.zcount > 0 ? a.zcount : a.res[2]));
     size_t sm = slot_columns_bytes(a.P, kFp64Block, 8, true);
     if (a.single) k_rhs_pf_fp64<DIM, PM, true><<<grid, kFp64Block, sm, s>>>(a);
     else k_rhs_pf_fp64<DIM, PM, false><<<grid, kFp64Block, sm, s>>>(a);

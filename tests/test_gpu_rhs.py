@@ -126,12 +126,25 @@ def test_rhs_mixed_within_1e6(case):
     assert err <= 1e-6, err
 
 
-def test_rhs_host_aos_entry_point_matches_device_path():
-    P, M, X = _build(3, [12, 12, 12], 20, 12, 8, "diffuse")
-    ctx = cb.Context(P, M, "fp64")
-    F1 = ctx.rhs_aos_host(0.0, X)
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("res,periodic_z", [([12, 12, 12], 1), ([12, 12, 12], 0), ([16, 8, 5], 1), ([10, 6, 3], 1)])
+def test_rhs_host_aos_entry_point_matches_device_path(precision, res, periodic_z):
+    """the host-buffer call (3D grids of 4 or more planes run as a z-slab
+    pipeline; fewer planes take one pass) equals the device-buffer call bit
+    for bit, on repeated calls"""
+    P = cb.Problem.grain_growth(3, res, 20, 12, 8)
+    P.s.periodic[2] = periodic_z
+    M = cb.Mesh(P)
+    X = cb.diffuse_state_aos(P, M, 4.0)
+    if precision == "mixed":
+        L = P.aos
+        X[:, L.pf_offset:L.pf_offset + P.s.pf_size] = X[:, L.pf_offset:L.pf_offset + P.s.pf_size].astype(np.float32)
+        X[:, L.tm_offset] = X[:, L.tm_offset].astype(np.float32)
+    ctx = cb.Context(P, M, precision)
     F2 = _device_rhs(ctx, X)
-    assert np.array_equal(F1, F2)
+    for _ in range(2):
+        F1 = ctx.rhs_aos_host(0.0, X)
+        assert np.array_equal(F1, F2)
 
 
 def test_bad_active_count_is_reported_not_trapped():
