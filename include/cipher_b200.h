@@ -420,7 +420,10 @@ int cipher_state_from_aos(cipher_ctx *c, const double *aos, void *X, void *strea
 int cipher_state_to_aos(cipher_ctx *c, const void *X, double *aos, void *stream);
 
 /* drop-in call with HOST buffers in the reference AoS layout: copies X to the
- * device, evaluates the RHS and copies F back (synchronous on `stream`) */
+ * device, evaluates the RHS and copies F back (synchronous on `stream`;
+ * RHSFunction, src/cipher.c:27).  3D phase-field grids of four or more
+ * planes go through in z-slabs on the context's own streams, so that copies
+ * out overlap copies in; pinned host buffers give full copy speed. */
 int cipher_rhs_aos_host(cipher_ctx *c, double t, const double *X_host, double *F_host, void *stream);
 
 #ifdef __cplusplus
