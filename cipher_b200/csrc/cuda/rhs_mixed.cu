@@ -233,12 +233,14 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
     const float scale = act ? a.mob_f * __frcp_rn(nf) : 0.0f;
     float *fp = a.fphi + c;
     int m = 0;
+#pragma unroll 2
     for (; m < maxn; m++) {
         float vv = 0.0f;
         if (act >> m & 1u) vv = scale * fmaf(nf, cl3[33 * m], -Caf);
         *fp = vv;
         fp += S;
     }
+#pragma unroll 2
     for (; m < P; m++) {
         *fp = 0.0f;
         fp += S;
