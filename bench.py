@@ -319,24 +319,23 @@ def run_chemistry(dev: int, steps: int, peak: float):
     return out
 
 
-def run_batched(dev: int, n_domains: int, t_end: float, n_alone: int):
-    """config 3: independent 2D grain-growth domains of uneven size stepped
-    together to t_end (one graph launch per step) vs a sample solved one at
-    a time with the single stepper"""
+def _batched_leg(dev: int, precision: str, specs, t_end: float, n_alone: int):
+    """one precision of the batched configuration: every domain attached to
+    one batch and stepped together (one graph launch per step), then a
+    sample solved one at a time with the single stepper"""
     import cipher_b200 as cb
     from cipher_b200 import workloads as W
-    specs = W.batch_domains(n_domains)
-    probe = W.batch_problem(specs[0])
-    opts = cb.ts_options(probe, "2a")
+    n_domains = len(specs)
+    opts = cb.ts_options(W.batch_problem(specs[0]), "2a")
     doms = []
     for sp in specs:
         P = W.batch_problem(sp)
         M = cb.Mesh(P)
-        ctx = cb.Context(P, M, "fp64", device=dev)
+        ctx = cb.Context(P, M, precision, device=dev)
         X = ctx.alloc_state()
         ctx.from_aos(cb.initial_state_aos(P, M), X)
         doms.append((P, M, ctx, X))
-    b = cb.Batch(opts, "fp64", device=dev)
+    b = cb.Batch(opts, precision, device=dev)
     slots = [b.attach(ctx, X, 0.0, t_end) for _, _, ctx, X in doms]
     b.step()                      # builds the tables, tunes the tile shapes, captures the graph
     t0 = time.perf_counter()
@@ -345,19 +344,19 @@ def run_batched(dev: int, n_domains: int, t_end: float, n_alone: int):
         nsteps += 1
     b.flush()
     t_batch = time.perf_counter() - t0
-    cells = sum(M.ncells for _, M, _, _ in doms)
     upd, failed = 0, 0
     for (P, M, _, _), sl in zip(doms, slots):
         st, status, _ = b.stats(sl)
         upd += M.ncells * st.rhs_calls
         failed += status != L_BATCH_FINISHED()
+    b.close()
     # one at a time: every (n/n_alone)-th domain, solved alone from t = 0
     stride = max(1, n_domains // n_alone)
     t_alone, alone_upd, n_al = 0.0, 0, 0
     for k in range(0, n_domains, stride):
         P = W.batch_problem(specs[k])
         M = cb.Mesh(P)
-        ctx = cb.Context(P, M, "fp64", device=dev)
+        ctx = cb.Context(P, M, precision, device=dev)
         X = ctx.alloc_state()
         ctx.from_aos(cb.initial_state_aos(P, M), X)
         ts = cb.TimeStepper(ctx, opts)
@@ -366,15 +365,30 @@ def run_batched(dev: int, n_domains: int, t_end: float, n_alone: int):
         t_alone += time.perf_counter() - t1
         alone_upd += M.ncells * st.rhs_calls
         n_al += 1
-    b.close()
-    return {"workload": f"{n_domains} 2D grain-growth domains, side 2^U[5,8] (32..256), 8-128 grains, P=8, "
-                        f"SetUpProblem start, RK 2a at rtol=atol=1e-4 to t={t_end}",
-            "domains": n_domains, "cells": cells, "batched_steps": nsteps, "failed": failed,
+    return {"batched_steps": nsteps, "failed": failed,
             "batched": {"solves_per_s": n_domains / t_batch, "seconds": t_batch,
                         "cell_updates_per_s": upd / t_batch},
             "one_at_a_time": {"solves_per_s": n_al / t_alone, "seconds_per_solve": t_alone / n_al,
                               "cell_updates_per_s": alone_upd / t_alone, "sample": n_al},
             "speedup_solves_per_s": (n_domains / t_batch) / (n_al / t_alone)}
+
+
+def run_batched(dev: int, n_domains: int, t_end: float, n_alone: int):
+    """config 3: independent 2D grain-growth domains of uneven size stepped
+    together to t_end, FP32-mixed and FP64, each against a sample solved one
+    at a time in the same precision"""
+    import cipher_b200 as cb
+    from cipher_b200 import workloads as W
+    specs = W.batch_domains(n_domains)
+    cells = sum(cb.Mesh(W.batch_problem(sp)).ncells for sp in specs)
+    out = {"workload": f"{n_domains} 2D grain-growth domains, side 2^U[5,8] (32..256), 8-128 grains, P=8, "
+                       f"SetUpProblem start, RK 2a at rtol=atol=1e-4 to t={t_end}",
+           "domains": n_domains, "cells": cells}
+    for precision in ("fp64", "mixed"):
+        out[precision] = _batched_leg(dev, precision, specs, t_end, n_alone)
+    out["mixed_vs_fp64_batched_solves_per_s"] = (out["mixed"]["batched"]["solves_per_s"] /
+                                                 out["fp64"]["batched"]["solves_per_s"])
+    return out
 
 
 def L_BATCH_FINISHED():
