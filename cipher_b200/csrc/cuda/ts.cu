@@ -78,12 +78,49 @@ __device__ __forceinline__ void store_real(char *base, int esize, int64_t i, dou
     else ((float *)base)[i] = (float)v;
 }
 
+/* the cells [c0, c1) of one plane (byte offset `off`) in element type E:
+ * y = x + sum_j w_j k_j, and with NORM the thread's share of the weighted
+ * error sum.  Stages are unrolled to kMaxStages (registers, no local
+ * arrays); the operations and their order are those of the FP64 path. */
+template <bool NORM, typename E>
+__device__ __forceinline__ double combine_cells(const CombineArgs &a, int nk, const double *w, const double *we,
+                                                int64_t off, int64_t c0, int64_t c1)
+{
+    const E *x = (const E *)(a.x + off);
+    E *y = (E *)(a.y + off);
+    const E *kp[kMaxStages];
+#pragma unroll
+    for (int j = 0; j < kMaxStages; j++) kp[j] = j < nk ? (const E *)(a.k[j] + off) : x;
+    double sum = 0.0;
+    for (int64_t c = c0 + threadIdx.x; c < c1; c += kTsThreads) {
+        const double xv = (double)x[c];
+        double acc = 0.0, acce = 0.0;
+#pragma unroll
+        for (int j = 0; j < kMaxStages; j++) {
+            if (j < nk) {
+                const double kv = (double)kp[j][c];
+                acc += w[j] * kv;
+                if (NORM) acce += we[j] * kv;
+            }
+        }
+        const double xn = xv + acc;
+        y[c] = (E)xn;
+        if (NORM) {
+            const double xe = xv + acce;
+            const double tol = a.atol + a.rtol * fmax(fabs(xn), fabs(xe));
+            const double e = (xn - xe) / tol;
+            sum += e * e;
+        }
+    }
+    return sum;
+}
+
 /* one block of a combination: cells [bx*2048, +2048) of state plane
  * `plane`; with NORM also the block's share of the weighted error sum,
  * written to *partial (the caller passes &partials[plane*gx + bx]) */
 template <bool NORM>
-__device__ __forceinline__ void rk_combine_block(const CombineArgs &a, const double *w, const double *we, int plane,
-                                                 int64_t bx, double *partial)
+__device__ __forceinline__ void rk_combine_block(const CombineArgs &a, int nk, const double *w, const double *we,
+                                                 int plane, int64_t bx, double *partial)
 {
     int gi = 0;
     while (gi < a.ngroups && plane >= a.groups[gi].nplanes) plane -= a.groups[gi++].nplanes;
@@ -93,23 +130,8 @@ __device__ __forceinline__ void rk_combine_block(const CombineArgs &a, const dou
         const int64_t off = g.offset + (int64_t)plane * a.stride * g.esize;
         const int64_t c0 = bx * kTsCellsPerBlock;
         const int64_t c1 = c0 + kTsCellsPerBlock < a.ncells ? c0 + kTsCellsPerBlock : a.ncells;
-        for (int64_t c = c0 + threadIdx.x; c < c1; c += kTsThreads) {
-            const double x = load_real(a.x + off, g.esize, c);
-            double acc = 0.0, acce = 0.0;
-            for (int j = 0; j < a.nk; j++) {
-                const double kv = load_real(a.k[j] + off, g.esize, c);
-                acc += w[j] * kv;
-                if (NORM) acce += we[j] * kv;
-            }
-            const double xn = x + acc;
-            store_real(a.y + off, g.esize, c, xn);
-            if (NORM) {
-                const double xe = x + acce;
-                const double tol = a.atol + a.rtol * fmax(fabs(xn), fabs(xe));
-                const double e = (xn - xe) / tol;
-                sum += e * e;
-            }
-        }
+        sum = g.esize == 8 ? combine_cells<NORM, double>(a, nk, w, we, off, c0, c1)
+                           : combine_cells<NORM, float>(a, nk, w, we, off, c0, c1);
     }
     if (NORM) {
         /* fixed-order block reduction: shuffle tree per warp, then the warps in order */
@@ -129,7 +151,7 @@ __device__ __forceinline__ void rk_combine_block(const CombineArgs &a, const dou
 template <bool NORM>
 __global__ void __launch_bounds__(kTsThreads) k_rk_combine(const CombineArgs a)
 {
-    rk_combine_block<NORM>(a, a.w, a.we, blockIdx.y, blockIdx.x,
+    rk_combine_block<NORM>(a, a.nk, a.w, a.we, blockIdx.y, blockIdx.x,
                            a.partial + (int64_t)blockIdx.y * gridDim.x + blockIdx.x);
 }
 
@@ -186,10 +208,9 @@ __global__ void __launch_bounds__(kTsThreads) k_rk_combine_batched(const BatchCo
     const int64_t bx = local % gx;
     const double h = b.h[lo];
     double w[kMaxStages], we[kMaxStages];
-    for (int j = 0; j < b.nk; j++) { w[j] = h * b.coef[j]; we[j] = h * b.coefe[j]; }
-    CombineArgs ac = a;
-    ac.nk = b.nk;
-    rk_combine_block<NORM>(ac, w, we, plane, bx, a.partial + (int64_t)plane * gx + bx);
+#pragma unroll
+    for (int j = 0; j < kMaxStages; j++) { w[j] = h * b.coef[j]; we[j] = h * b.coefe[j]; }
+    rk_combine_block<NORM>(a, b.nk, w, we, plane, bx, a.partial + (int64_t)plane * gx + bx);
 }
 
 /* one block per domain: its partials reduced as the single form does */
