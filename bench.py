@@ -373,7 +373,7 @@ def _batched_leg(dev: int, precision: str, specs, t_end: float, n_alone: int):
             "speedup_solves_per_s": (n_domains / t_batch) / (n_al / t_alone)}
 
 
-def run_batched(dev: int, n_domains: int, t_end: float, n_alone: int):
+def run_batched(dev: int, n_domains: int, t_end: float, n_alone: int, precisions=("fp64", "mixed")):
     """config 3: independent 2D grain-growth domains of uneven size stepped
     together to t_end, FP32-mixed and FP64, each against a sample solved one
     at a time in the same precision"""
@@ -384,10 +384,11 @@ def run_batched(dev: int, n_domains: int, t_end: float, n_alone: int):
     out = {"workload": f"{n_domains} 2D grain-growth domains, side 2^U[5,8] (32..256), 8-128 grains, P=8, "
                        f"SetUpProblem start, RK 2a at rtol=atol=1e-4 to t={t_end}",
            "domains": n_domains, "cells": cells}
-    for precision in ("fp64", "mixed"):
+    for precision in precisions:
         out[precision] = _batched_leg(dev, precision, specs, t_end, n_alone)
-    out["mixed_vs_fp64_batched_solves_per_s"] = (out["mixed"]["batched"]["solves_per_s"] /
-                                                 out["fp64"]["batched"]["solves_per_s"])
+    if "fp64" in out and "mixed" in out:
+        out["mixed_vs_fp64_batched_solves_per_s"] = (out["mixed"]["batched"]["solves_per_s"] /
+                                                     out["fp64"]["batched"]["solves_per_s"])
     return out
 
 
@@ -647,6 +648,9 @@ def main():
                     help="skip the chemistry, batched and serving legs reported beside the headline")
     ap.add_argument("--only", choices=["chemistry", "batched", "serving"],
                     help="run one of the legs beside the headline alone (for profiling) and print its object")
+    ap.add_argument("--batch-domains", type=int, default=256, help="--only batched: number of domains")
+    ap.add_argument("--batch-t-end", type=float, default=50.0, help="--only batched: end time of every domain")
+    ap.add_argument("--batch-precisions", default="fp64,mixed", help="--only batched: precisions to run")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -659,7 +663,8 @@ def main():
         torch.cuda.set_device(local_rank)
         peak, _ = hbm_peak()
         fn = {"chemistry": lambda: run_chemistry(local_rank, args.steps, peak),
-              "batched": lambda: run_batched(local_rank, 256, 50.0, 16),
+              "batched": lambda: run_batched(local_rank, args.batch_domains, args.batch_t_end, 16,
+                                             tuple(args.batch_precisions.split(","))),
               "serving": lambda: run_serving(local_rank, 50.0, 4.0)}[args.only]
         print(json.dumps({args.only: fn()}), flush=True)
     elif args.impl == "reference":
