@@ -241,6 +241,18 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def reduce_max(v: float, dist=None, device: str = "cpu") -> float:
+    """the largest of every rank's v (the timing rule: a multi-GPU time is
+    the slowest rank's); v itself without a process group.  `device` is
+    where the backend reduces: cuda:<rank> for NCCL, cpu for gloo."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def time_launches(fn, steps, stream):
     """Run fn() `steps` times on `stream`, one CUDA-event pair per launch."""
     import torch
@@ -484,11 +496,7 @@ def run_cipher(args, rank, world, local_rank):
         torch.cuda.synchronize()
 
     def max_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(v, dist, f"cuda:{dev}")
 
     t_setup = time.time()
     P = build_problem()
