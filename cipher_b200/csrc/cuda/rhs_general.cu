@@ -203,7 +203,7 @@ __device__ __forceinline__ double face_div(const GenArgs<R> &a, double x)
 }
 
 template <int PM, typename R>
-__global__ void __launch_bounds__(kGenBlock) k_rhs_general(const GenArgs<R> a, const int DIM)
+__global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> a, const int DIM)
 {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= a.ncells) return;
