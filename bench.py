@@ -409,15 +409,12 @@ def L_BATCH_FINISHED():
     return L.BATCH_FINISHED
 
 
-def run_serving(dev: int, rate: float, duration: float):
-    """config 4: Poisson arrivals served with continuous batching vs the same
-    trace served one request at a time (each solved alone, FIFO)"""
+def _serve_trace(dev: int, precision: str, trace, opts):
+    """the trace served with continuous batching in `precision`: wall time,
+    per-request latency from arrival, failures, peak HBM, host counters"""
     import cipher_b200 as cb
     from cipher_b200 import workloads as W
-    trace = W.serving_trace(rate, duration)
-    opts = cb.ts_options(W.trace_problem(trace[0][1], trace[0][2]), "2a", dt0=1e-6, dtmin=1e-12, dtmax=1.0,
-                         reltol=1e-4, abstol=1e-4)
-    srv = cb.Server(opts, "fp64", device=dev, hbm_budget=16 << 30, max_active=512)
+    srv = cb.Server(opts, precision, device=dev, hbm_budget=16 << 30, max_active=512)
     # warm the kernels and the tile tuner on one request of each kind
     for kind in ("gg", "alloy"):
         ex = next(t for t in trace if t[1] == kind)
@@ -448,6 +445,26 @@ def run_serving(dev: int, rate: float, duration: float):
     used, peak_b = srv.usage()
     counters = srv.counters()
     srv.close()
+    return wall, lat, failed, peak_b, counters
+
+
+def run_serving(dev: int, rate: float, duration: float):
+    """config 4: Poisson arrivals served with continuous batching (FP64, and
+    FP32-mixed) vs the same trace served one request at a time with the
+    plain FP64 path (each solved alone, FIFO)"""
+    import cipher_b200 as cb
+    from cipher_b200 import workloads as W
+    trace = W.serving_trace(rate, duration)
+    opts = cb.ts_options(W.trace_problem(trace[0][1], trace[0][2]), "2a", dt0=1e-6, dtmin=1e-12, dtmax=1.0,
+                         reltol=1e-4, abstol=1e-4)
+    pct = lambda v, q: float(np.percentile(np.asarray(v), q))
+    served = {}
+    failed = 0
+    for precision in ("fp64", "mixed"):
+        wall, lat, nf, peak_b, counters = _serve_trace(dev, precision, trace, opts)
+        failed += nf
+        served[precision] = {"solves_per_s": len(trace) / wall, "p50_s": pct(lat, 50), "p99_s": pct(lat, 99),
+                             "peak_hbm_bytes": peak_b, "host_counters": counters}
     # the same trace one request at a time: each solved alone, FIFO from its arrival
     solve = []
     for a, kind, args, init, te in trace:
@@ -467,14 +484,12 @@ def run_serving(dev: int, rate: float, duration: float):
         start = max(a, fin)
         fin = start + sv
         lat1.append(fin - a)
-    pct = lambda v, q: float(np.percentile(np.asarray(v), q))
     return {"workload": f"Poisson({rate}/s) arrivals for {duration} s: 3/4 grain growth 64^2-256^2 to t=5, "
                         f"1/4 binary two-phase calphaddis 64^2-128^2 to t=0.02; RK 2a, rtol=atol=1e-4",
             "requests": len(trace), "failed": failed,
-            "served": {"solves_per_s": len(trace) / wall, "p50_s": pct(lat, 50), "p99_s": pct(lat, 99),
-                       "peak_hbm_bytes": peak_b, "host_counters": counters},
+            "served": served["fp64"], "served_mixed": served["mixed"],
             "one_at_a_time": {"solves_per_s": len(trace) / fin, "p50_s": pct(lat1, 50), "p99_s": pct(lat1, 99),
-                              "mean_solve_s": float(np.mean(solve))}}
+                              "mean_solve_s": float(np.mean(solve)), "precision": "fp64"}}
 
 
 def run_cipher(args, rank, world, local_rank):
