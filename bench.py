@@ -39,7 +39,9 @@ METRIC = "cell-updates/s mixed vs FP64 at 1e-6 rel err"
 UNIT = "cell-updates/s"
 WORKLOAD = dict(dim=3, res=(128, 128, 128), ngrains=2000, cap=12, seed=12345, width=4.0)
 WORKLOAD_NAME = "3D grain growth 128^3, 2000 Voronoi grains, P=12, diffuse state (width 4)"
-HBM_PEAK_MEASURED = 6423.4   # GB/s, MEASURED_PEAKS.json hbm_gbs on this pool
+# GB/s used only when MEASURED_PEAKS.json is absent: an earlier STREAM-style
+# copy measurement on B200, reported with peak_source "fallback"
+HBM_PEAK_FALLBACK = 6650.0
 
 
 def log(*a):
@@ -87,7 +89,7 @@ def hbm_peak():
         with open(path) as f:
             return float(json.load(f)["hbm_gbs"]), "measured"
     except Exception:
-        return HBM_PEAK_MEASURED, "measured (pool value recorded with this build)"
+        return HBM_PEAK_FALLBACK, "fallback"
 
 
 def traffic_per_launch(kind: str):
@@ -204,6 +206,13 @@ def reference_rate(X_aos: np.ndarray, procs: int, reps: int, warm: int):
     return ncells / statistics.mean(per_step), per_step
 
 
+def workload_config(ncells: int, pcap: int, mean_n: float, world: int) -> dict:
+    """the `config` object of both arms' lines (the same workload, the same keys)"""
+    return {"workload": WORKLOAD_NAME, "cells": int(ncells), "max_phases": int(pcap),
+            "mean_active_phases": float(mean_n), "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (no flush)"}
+
+
 def host_cores() -> int:
     try:
         return len(os.sched_getaffinity(0))
@@ -233,7 +242,8 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, "parallelism": f"{cores} host processes (slab + halo)"},
+            "config": workload_config(M.nowned, P.s.pf_size, float(X[:M.nowned, 0].mean()), world),
+            "host_parallelism": f"{cores} host processes (slab + halo)",
             "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
                              "sample": f"each step one RHSFunction over all {int(np.prod(WORKLOAD['res']))} "
                                        f"cells split in {cores} slabs"},
@@ -624,9 +634,7 @@ def run_cipher(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": tot32 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_NAME, "cells": ncells, "max_phases": Pcap,
-                   "mean_active_phases": nsum / ncells, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (no flush)"},
+        "config": workload_config(ncells, Pcap, nsum / ncells, world),
         "fp64": {"value": value64, "unit": UNIT, "ms_per_step": tot64 / args.steps,
                  "roofline_frac": ach64 / peak, "algorithmic_bytes_per_launch": b64,
                  "state_exact_roofline_frac": e64 / avg64 / 1e9 / peak},

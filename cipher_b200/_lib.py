@@ -122,7 +122,8 @@ class StateLayout(C.Structure):
 
 class GridDesc(C.Structure):
     _fields_ = [("dim", C.c_int32), ("res", C.c_int32 * 3), ("periodic", C.c_int32 * 3),
-                ("ex_per_phase", C.c_int32), ("layout", StateLayout), ("ex_init", C.c_void_p)]
+                ("ex_per_phase", C.c_int32), ("layout", StateLayout), ("npf", C.c_int32), ("ncp", C.c_int32),
+                ("nmat", C.c_int32), ("materials", C.c_void_p), ("phasematerialmapping", C.c_void_p)]
 
 
 class TSOpts(C.Structure):

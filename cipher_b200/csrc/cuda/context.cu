@@ -99,7 +99,6 @@ struct cipher_ctx {
     int32_t *d_pmm;
     double *d_comp, *d_mob, *d_tcond;
     uint16_t *d_pruned;
-    double *d_ex_init;
     int *d_err;
     int *h_err;
     /* buffers of the host-AoS entry point, allocated on first use */
@@ -174,7 +173,6 @@ static void free_ctx(cipher_ctx *c)
     cudaFree(c->d_mob);
     cudaFree(c->d_tcond);
     cudaFree(c->d_pruned);
-    cudaFree(c->d_ex_init);
     cudaFree(c->d_err);
     if (c->h_err) cudaFreeHost(c->h_err);
     cudaFree(c->d_aos_x);
@@ -567,7 +565,6 @@ static PostArgs<R> post_args(const cipher_ctx *c, void *X)
     a.ex = (double *)(x + c->lay.ex_offset);
     a.tm = (const R *)(x + c->lay.tm_offset);
     a.pruned = c->d_pruned;
-    a.ex_init = c->d_ex_init;
     a.chem.mat = c->d_mat;
     a.chem.pmm = c->d_pmm;
     a.chem.ncp = c->ncp;

@@ -151,7 +151,6 @@ struct PostArgs {
     uint16_t *pruned;             /* scratch: pruned sets, [P+1][stride] */
     uint64_t *maps;               /* face maps rebuilt after the union, or NULL */
     int npf;
-    const double *ex_init;        /* [npf*S] explicit potential of c0 at T0 per phase, or NULL */
     ChemTables chem;              /* with chem.mat set, new phases get SitepotentialExplicit(c0, T) */
     int *err;
 };

@@ -181,8 +181,7 @@ __device__ __forceinline__ void post_union_cell(const PostArgs<R> &a, int64_t c)
                 for (int q = 0; q < a.S; q++) exss[g * a.S + q] = 0.0;
                 sitepot_explicit(a.chem, sup[g], mat.c0, T, &exss[g * a.S]);
             } else {
-                for (int q = 0; q < a.S; q++)
-                    exss[g * a.S + q] = a.ex_init ? a.ex_init[(int64_t)sup[g] * a.S + q] : 0.0;
+                for (int q = 0; q < a.S; q++) exss[g * a.S + q] = 0.0;
             }
         }
         for (int g = 0; g < ns; g++)

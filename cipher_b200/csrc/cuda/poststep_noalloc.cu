@@ -23,6 +23,10 @@
  *     on the GPU (other streams, other host threads) race.  The error word is
  *     cleared at the start of each call; the pruned sets are fully rewritten.
  *   - no cudaMalloc, cudaFree or allocating library call is made.
+ *   - with chemistry (S > 0) the caller passes device copies of the
+ *     problem's material table and phase-material mapping, so that a phase
+ *     that joins a cell starts at SitepotentialExplicit(c0, T of the cell),
+ *     the same branch cipher_poststep takes (src/cipher.c:953-964).
  */
 #include <cstdint>
 #include <cstring>
@@ -79,6 +83,7 @@ cipher::PostArgs<R> noalloc_args(const cipher_grid_desc *g, void *X, const Noall
     }
     a.P = g->layout.pf_size;
     a.S = g->ex_per_phase;
+    a.npf = g->npf;
     a.as = (uint16_t *)(x + g->layout.as_offset);
     /* the face maps of the layout, when it has them, are rebuilt as well */
     a.maps = g->layout.map_planes == 2 * g->dim ? (uint64_t *)(x + g->layout.map_offset) : nullptr;
@@ -86,7 +91,13 @@ cipher::PostArgs<R> noalloc_args(const cipher_grid_desc *g, void *X, const Noall
     a.ex = (double *)(x + g->layout.ex_offset);
     a.tm = (const R *)(x + g->layout.tm_offset);
     a.pruned = sy.pruned;
-    a.ex_init = g->ex_init;
+    if (g->ex_per_phase > 0) {
+        a.chem.mat = g->materials;
+        a.chem.pmm = g->phasematerialmapping;
+        a.chem.ncp = g->ncp;
+        a.chem.ndp = g->ncp - 1;
+        a.chem.nmat = g->nmat;
+    }
     a.err = sy.flags;
     return a;
 }
@@ -105,7 +116,17 @@ extern "C" int cipher_poststep_noalloc(const cipher_grid_desc *g, void *X, void 
         cells *= g->res[d];
     }
     if (cells != g->layout.ncells) return CIPHER_E_ARG;
-    if (g->ex_per_phase > 0 && !g->ex_init) return CIPHER_E_ARG;
+    if (g->npf < 1 || g->npf > 65535) return CIPHER_E_ARG;
+    /* the face maps are rebuilt when the layout has them; any other plane count is a foreign layout */
+    if (g->layout.map_planes != 0 && g->layout.map_planes != 2 * g->dim) return CIPHER_E_ARG;
+    /* explicit site potentials: S per phase, at most two sublattices of ncp-1 potentials */
+    const int S = g->ex_per_phase;
+    if (S < 0 || S > 2 * CIPHER_MAXCP) return CIPHER_E_ARG;
+    if (g->layout.ex_size != P * S) return CIPHER_E_ARG;
+    if (S > 0) {
+        if (!g->materials || !g->phasematerialmapping) return CIPHER_E_ARG;
+        if (g->ncp < 2 || g->ncp > CIPHER_MAXCP || g->nmat < 1 || S > 2 * (g->ncp - 1)) return CIPHER_E_ARG;
+    }
     if (g->layout.precision != CIPHER_PREC_FP64 && g->layout.precision != CIPHER_PREC_MIXED) return CIPHER_E_ARG;
     /* the static scratch holds (P+1) planes of `stride` pruned-set entries */
     if ((uint64_t)(P + 1) * (uint64_t)g->layout.stride > CIPHER_NOALLOC_MAX_PRUNED) return CIPHER_E_ARG;
@@ -113,9 +134,15 @@ extern "C" int cipher_poststep_noalloc(const cipher_grid_desc *g, void *X, void 
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= CIPHER_NOALLOC_MAX_DEVICES)
         return CIPHER_E_CUDA;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (s) {
+        /* the scratch looked up below is the current device's */
+        int sdev = -1;
+        if (cudaStreamGetDevice(s, &sdev) != cudaSuccess) return CIPHER_E_CUDA;
+        if (sdev != device) return CIPHER_E_ARG;
+    }
     NoallocSymbols sy;
     if (noalloc_symbols(device, sy) != cudaSuccess) return CIPHER_E_CUDA;
-    cudaStream_t s = (cudaStream_t)stream;
     if (cudaMemsetAsync(sy.flags, 0, sizeof(int), s) != cudaSuccess) return CIPHER_E_CUDA;
     cudaError_t e;
     if (g->layout.precision == CIPHER_PREC_FP64)

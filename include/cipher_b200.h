@@ -191,9 +191,17 @@ typedef struct cipher_grid_desc {
     int32_t dim;
     int32_t res[3];
     int32_t periodic[3];
-    int32_t ex_per_phase;        /* S: explicit site potentials per phase */
-    cipher_state_layout layout;  /* offsets of the state planes (see above) */
-    const double *ex_init;       /* device [npf*S] potentials of new phases, or NULL when S == 0 */
+    int32_t ex_per_phase;        /* S: explicit site potentials per phase, 0..2*CIPHER_MAXCP;
+                                    layout.ex_size must be pf_size*S */
+    cipher_state_layout layout;  /* offsets of the state planes (see above); map_planes 0 or 2*dim */
+    int32_t npf;                 /* phases of the problem: a set holding an id >= npf is a bad set */
+    int32_t ncp, nmat;           /* components and materials (read when S > 0) */
+    /* device copies of the problem's material[nmat] and phasematerialmapping[npf]
+     * (in memory the caller owns); required when S > 0, NULL otherwise.  A phase
+     * that joins a cell gets SitepotentialExplicit(c0, T of the cell) from them,
+     * exactly as cipher_poststep does. */
+    const cipher_material *materials;
+    const int32_t *phasematerialmapping;
 } cipher_grid_desc;
 
 /* The per-step active-set update of cipher_poststep for callers that cannot
@@ -203,9 +211,11 @@ typedef struct cipher_grid_desc {
  * allocates its work vectors through PETSc.  Needs no context and calls no
  * allocator; its scratch is a fixed 8 MiB device array inside the library,
  * so grids with (P+1)*stride above 4 Mi entries are rejected (CIPHER_E_ARG).
- * The first call on a device looks the array up and must precede any stream
- * capture; calls that overlap on the GPU share the array and race.
- * Synchronises `stream`; returns CIPHER_E_CAP when a superset exceeds P. */
+ * The first call on a device looks the array up with that device current;
+ * make that first call before any stream capture.  `stream` must belong to
+ * the current device (CIPHER_E_ARG otherwise).  Calls that overlap on the GPU
+ * share the array and race.  Synchronises `stream`; returns CIPHER_E_CAP when
+ * a superset exceeds P and CIPHER_E_ARG for a bad set in X. */
 int cipher_poststep_noalloc(const cipher_grid_desc *g, void *X, void *stream);
 
 /* Y = X + a*F on the PF, DP, EX and TM planes; AS is copied from X

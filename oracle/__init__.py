@@ -23,7 +23,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_LIB = os.path.join(HERE, "liboracle_port.so")
 REF_LIB = os.path.join(HERE, "_ref", "libcipher_ref.so")
-REF_SRC = "/root/reference/src"
+# the reference's src/ directory: CIPHER_REF_SRC, else the location the
+# build recipe (oracle/Makefile) assumes
+REF_SRC = os.environ.get("CIPHER_REF_SRC") or "/root/reference/src"
 
 _port = None
 _ref = None
@@ -34,7 +36,7 @@ def build(ref: bool = True) -> None:
     targets = ["port"]
     if ref and os.path.isdir(REF_SRC):
         targets.append("ref")
-    r = subprocess.run(["make", "-s", "-C", HERE] + targets, capture_output=True, text=True)
+    r = subprocess.run(["make", "-s", "-C", HERE, f"REF_SRC={REF_SRC}"] + targets, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
 
