@@ -341,6 +341,50 @@ def run_chemistry(dev: int, steps: int, peak: float):
     return out
 
 
+def run_config1_steps(dev: int, P, M, X, steps: int = 200):
+    """configuration 1 as specified: the 128^3 diffuse state stepped for
+    `steps` accepted adaptive RK 2a steps through cipher_ts_solve (stage
+    combinations, error norm, PostStep with its face maps, every step), in
+    both precisions; cell-updates/s counts every RHS call of the solve and
+    divides by the whole solve's device time"""
+    import torch
+    import cipher_b200 as cb
+    A = P.aos
+    out = {"workload": f"{WORKLOAD_NAME}, {steps} accepted RK 2a steps through cipher_ts_solve (PostStep each step)"}
+    stream = torch.cuda.current_stream()
+    for name in ("fp64", "mixed"):
+        Xin = X
+        if name == "mixed":
+            Xin = X.copy()
+            Xin[:, A.pf_offset:A.pf_offset + A.pf_size] = Xin[:, A.pf_offset:A.pf_offset + A.pf_size].astype(np.float32)
+            Xin[:, A.tm_offset] = Xin[:, A.tm_offset].astype(np.float32)
+        ctx = cb.Context(P, M, name, device=dev)
+        dX = ctx.alloc_state()
+        ctx.from_aos(Xin, dX)
+        ts = cb.TimeStepper(ctx, cb.ts_options(P, "2a", max_steps=steps))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = ts.solve(dX, 0.0, 1.0e30)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[name] = {"value": M.ncells * st.rhs_calls / (ms / 1e3), "unit": UNIT, "ms_total": ms,
+                     "steps": int(st.steps), "rejected": int(st.rejected), "rhs_calls": int(st.rhs_calls),
+                     "t_reached": float(st.t), "ms_per_rhs_call": ms / max(int(st.rhs_calls), 1),
+                     "mean_active_phases_end": float(ctx.planes(dX)[0][0, :M.ncells].float().mean().item())}
+        del ts, ctx, dX
+    out["mixed_speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
+
+
+def _config1_only(dev: int, steps: int):
+    import cipher_b200 as cb
+    P = build_problem()
+    M = cb.Mesh(P)
+    return run_config1_steps(dev, P, M, build_state(P, M), steps)
+
+
 def _batched_leg(dev: int, precision: str, specs, t_end: float, n_alone: int):
     """one precision of the batched configuration: every domain attached to
     one batch and stepped together (one graph launch per step), then a
@@ -654,7 +698,8 @@ def run_cipher(args, rank, world, local_rank):
         "gpu_launches": args.steps,
     }
     if not args.no_extra and world == 1:
-        for key, fn in (("chemistry", lambda: run_chemistry(dev, 20, peak)),
+        for key, fn in (("config1_steps", lambda: run_config1_steps(dev, P, M, X, 200)),
+                        ("chemistry", lambda: run_chemistry(dev, 20, peak)),
                         ("batched", lambda: run_batched(dev, 256, 50.0, 16)),
                         ("serving", lambda: run_serving(dev, 50.0, 4.0))):
             t1 = time.time()
@@ -677,7 +722,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the chemistry, batched and serving legs reported beside the headline")
-    ap.add_argument("--only", choices=["chemistry", "batched", "serving"],
+    ap.add_argument("--only", choices=["chemistry", "batched", "serving", "config1_steps"],
                     help="run one of the legs beside the headline alone (for profiling) and print its object")
     ap.add_argument("--batch-domains", type=int, default=256, help="--only batched: number of domains")
     ap.add_argument("--batch-t-end", type=float, default=50.0, help="--only batched: end time of every domain")
@@ -696,7 +741,8 @@ def main():
         fn = {"chemistry": lambda: run_chemistry(local_rank, args.steps, peak),
               "batched": lambda: run_batched(local_rank, args.batch_domains, args.batch_t_end, 16,
                                              tuple(args.batch_precisions.split(","))),
-              "serving": lambda: run_serving(local_rank, 50.0, 4.0)}[args.only]
+              "serving": lambda: run_serving(local_rank, 50.0, 4.0),
+              "config1_steps": lambda: _config1_only(local_rank, args.steps)}[args.only]
         print(json.dumps({args.only: fn()}), flush=True)
     elif args.impl == "reference":
         run_reference(args, rank, world)

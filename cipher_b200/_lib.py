@@ -33,6 +33,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 ALLOY_SEGREGATION, ALLOY_ITF_MOBILITY, ALLOY_ACTIVATION, ALLOY_THERMAL = 0x01, 0x02, 0x04, 0x08
 ALLOY_SOURCES, ALLOY_WALLS, ALLOY_TEMP_RATE, ALLOY_MIXED_MODELS = 0x10, 0x20, 0x40, 0x80
 ALLOY_ALL = 0x7F
+GG_ACTIVATION, GG_WIDTHS = 0x01, 0x02
 
 OK = 0
 E_ARG, E_NOMEM, E_CAP, E_NONFINITE, E_CUDA, E_TIMEOUT, E_UNSUPPORTED, E_STEP = range(1, 9)
@@ -183,6 +184,7 @@ _SIGNATURES = [
     ("cipher_strerror", C.c_char_p, [C.c_int]),
     ("cipher_last_error", C.c_char_p, []),
     ("cipher_abi_sizes", C.c_int, [C.POINTER(C.c_int64), C.c_int]),
+    ("cipher_pool_trim", C.c_int, [C.c_int]),
     ("cipher_problem_new", PP, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     ("cipher_problem_free", None, [PP]),
     ("cipher_problem_finalize", C.c_int, [PP]),
@@ -191,6 +193,8 @@ _SIGNATURES = [
     ("cipher_problem_grain_growth", C.c_int,
      [C.c_int, C.POINTER(C.c_int32), C.c_int, C.c_int, C.c_uint64, C.c_double, C.c_double, C.c_double,
       C.c_double, C.c_double, C.POINTER(PP)]),
+    ("cipher_problem_grain_growth_multi", C.c_int,
+     [C.c_int, C.POINTER(C.c_int32), C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_uint, C.POINTER(PP)]),
     ("cipher_voronoi", C.c_int, [C.c_int, C.POINTER(C.c_int32), C.c_int, C.c_uint64, C.POINTER(C.c_int32),
                                  C.POINTER(C.c_double)]),
     ("cipher_rand_uniform", C.c_double, [C.POINTER(C.c_uint64)]),

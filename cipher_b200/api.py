@@ -36,6 +36,19 @@ class Problem:
         return cls(out)
 
     @classmethod
+    def grain_growth_multi(cls, dim: int, res, ngrains: int, cap: int, seed: int, ninterfaces: int = 4,
+                           activation: bool = False, widths: bool = False) -> "Problem":
+        """Grain growth with several seeded interfaces (per-pair energy and
+        mobility; optionally T-dependent, optionally of different widths)."""
+        lib = L.load()
+        r = (C.c_int32 * 3)(*(list(res) + [1] * (3 - len(res))))
+        feats = (L.GG_ACTIVATION if activation else 0) | (L.GG_WIDTHS if widths else 0)
+        out = L.PP()
+        L.check(lib.cipher_problem_grain_growth_multi(dim, r, ngrains, cap, seed, ninterfaces, feats,
+                                                      C.byref(out)), "cipher_problem_grain_growth_multi")
+        return cls(out)
+
+    @classmethod
     def alloy(cls, dim: int, res, model: str = "calphad2sl", ncp: int = 4, nprecip: int = 20, cap: int = 15,
               seed: int = 1, features: int = 0) -> "Problem":
         """Seeded alloy problem (cipher_problem_alloy): two matrix grains with

@@ -162,23 +162,25 @@ static int phasefield_only(const cipher_problem *p)
 static void free_ctx(cipher_ctx *c)
 {
     if (!c) return;
-    cudaFree(c->d_itflist);
-    cudaFree(c->d_itfs);
-    cudaFree(c->d_mat);
-    cudaFree(c->d_t0);
-    cudaFree(c->d_mat_spec);
-    cudaFree(c->d_tspec);
-    cudaFree(c->d_pmm);
-    cudaFree(c->d_comp);
-    cudaFree(c->d_mob);
-    cudaFree(c->d_tcond);
-    cudaFree(c->d_pruned);
-    cudaFree(c->d_err);
-    if (c->h_err) cudaFreeHost(c->h_err);
-    cudaFree(c->d_aos_x);
-    cudaFree(c->d_aos_f);
-    cudaFree(c->d_X);
-    cudaFree(c->d_F);
+    /* pool frees do not wait: finish every queued use of the buffers first */
+    cudaDeviceSynchronize();
+    dev_free(c->d_itflist);
+    dev_free(c->d_itfs);
+    dev_free(c->d_mat);
+    dev_free(c->d_t0);
+    dev_free(c->d_mat_spec);
+    dev_free(c->d_tspec);
+    dev_free(c->d_pmm);
+    dev_free(c->d_comp);
+    dev_free(c->d_mob);
+    dev_free(c->d_tcond);
+    dev_free(c->d_pruned);
+    dev_free(c->d_err);
+    pinned_word_free(c->h_err);
+    dev_free(c->d_aos_x);
+    dev_free(c->d_aos_f);
+    dev_free(c->d_X);
+    dev_free(c->d_F);
     if (c->pipe_ready) {
         cudaStreamDestroy(c->s_up);
         cudaStreamDestroy(c->s_cp);
@@ -315,7 +317,7 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
                 if (i < 0 || i >= p->nf) { free_ctx(c); return set_error(CIPHER_E_ARG, "interface index out of range"); }
             }
         size_t nb = (size_t)p->npf * p->npf * sizeof(int32_t);
-        if ((e = cudaMalloc(&c->d_itflist, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc itflist"); }
+        if ((e = dev_alloc(&c->d_itflist, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc itflist"); }
         if ((e = cudaMemcpy(c->d_itflist, p->interfacelist, nb, cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy itflist"); }
     }
     {
@@ -335,46 +337,46 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
             h[i].nsources = s->nsources;
             memcpy(h[i].sources, s->sources, sizeof(h[i].sources));
         }
-        e = cudaMalloc(&c->d_itfs, (size_t)p->nf * sizeof(DevInterface));
+        e = dev_alloc(&c->d_itfs, (size_t)p->nf * sizeof(DevInterface));
         if (e == cudaSuccess) e = cudaMemcpy(c->d_itfs, h, (size_t)p->nf * sizeof(DevInterface), cudaMemcpyHostToDevice);
         free(h);
         if (e != cudaSuccess) { free_ctx(c); return cuda_fail(e, "interface table"); }
     }
     {
         size_t nb = (size_t)p->npf * sizeof(int32_t);
-        if ((e = cudaMalloc(&c->d_pmm, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc phase map"); }
+        if ((e = dev_alloc(&c->d_pmm, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc phase map"); }
         if ((e = cudaMemcpy(c->d_pmm, p->phasematerialmapping, nb, cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy phase map"); }
     }
     if (c->general) {
         size_t nb = (size_t)p->nmat * sizeof(cipher_material);
-        if ((e = cudaMalloc(&c->d_mat, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc materials"); }
+        if ((e = dev_alloc(&c->d_mat, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc materials"); }
         if ((e = cudaMemcpy(c->d_mat, p->material, nb, cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy materials"); }
-        if ((e = cudaMalloc(&c->d_mat_spec, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc materials"); }
-        if ((e = cudaMalloc(&c->d_tspec, sizeof(double))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc materials"); }
+        if ((e = dev_alloc(&c->d_mat_spec, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc materials"); }
+        if ((e = dev_alloc(&c->d_tspec, sizeof(double))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc materials"); }
         {
             const double nan = std::nan("");
             if ((e = cudaMemcpy(c->d_tspec, &nan, sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy"); }
         }
         if (c->ndp) {
             nb = (size_t)c->ncp * c->stride * sizeof(double);
-            if ((e = cudaMalloc(&c->d_comp, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc composition"); }
-            if ((e = cudaMalloc(&c->d_mob, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc mobility"); }
-            if ((e = cudaMalloc(&c->d_tcond, (size_t)c->stride * sizeof(double))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc conductivity"); }
+            if ((e = dev_alloc(&c->d_comp, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc composition"); }
+            if ((e = dev_alloc(&c->d_mob, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc mobility"); }
+            if ((e = dev_alloc(&c->d_tcond, (size_t)c->stride * sizeof(double))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc conductivity"); }
         }
     }
     {
         double *t0 = (double *)malloc((size_t)p->npf * sizeof(double));
         if (!t0) { free_ctx(c); return set_error(CIPHER_E_NOMEM, "host allocation"); }
         for (int a = 0; a < p->npf; a++) t0[a] = p->material[p->phasematerialmapping[a]].temperature0;
-        e = cudaMalloc(&c->d_t0, (size_t)p->npf * sizeof(double));
+        e = dev_alloc(&c->d_t0, (size_t)p->npf * sizeof(double));
         if (e == cudaSuccess) e = cudaMemcpy(c->d_t0, t0, (size_t)p->npf * sizeof(double), cudaMemcpyHostToDevice);
         free(t0);
         if (e != cudaSuccess) { free_ctx(c); return cuda_fail(e, "temperature table"); }
     }
-    if ((e = cudaMalloc(&c->d_pruned, (size_t)(c->P + 1) * c->stride * sizeof(uint16_t))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc pruned"); }
-    if ((e = cudaMalloc(&c->d_err, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc err"); }
+    if ((e = dev_alloc(&c->d_pruned, (size_t)(c->P + 1) * c->stride * sizeof(uint16_t))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc pruned"); }
+    if ((e = dev_alloc(&c->d_err, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc err"); }
     if ((e = cudaMemset(c->d_err, 0, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMemset err"); }
-    if ((e = cudaMallocHost(&c->h_err, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMallocHost err"); }
+    if ((e = pinned_word_alloc(&c->h_err)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "pinned error word"); }
     *c->h_err = 0;
     *out = c;
     return CIPHER_OK;
@@ -767,7 +769,7 @@ extern "C" int cipher_state_init_sharp(cipher_ctx *c, const int32_t *voxelphase,
     if (!c || !voxelphase || !X) return set_error(CIPHER_E_ARG, "NULL argument");
     cudaStream_t s = (cudaStream_t)stream;
     int32_t *d_vox = nullptr;
-    CUDA_TRY(cudaMalloc(&d_vox, (size_t)c->ncells * sizeof(int32_t)), "cudaMalloc voxel map");
+    CUDA_TRY(dev_alloc(&d_vox, (size_t)c->ncells * sizeof(int32_t)), "voxel map");
     cudaError_t e = cudaMemcpyAsync(d_vox, voxelphase, (size_t)c->ncells * sizeof(int32_t), cudaMemcpyHostToDevice, s);
     InitArgs a;
     memset(&a, 0, sizeof(a));
@@ -780,11 +782,13 @@ extern "C" int cipher_state_init_sharp(cipher_ctx *c, const int32_t *voxelphase,
     a.err = c->d_err;
     if (e == cudaSuccess) e = launch_init_sharp(a, s);
     if (e == cudaSuccess) e = build_maps(c, X, s);
-    if (e != cudaSuccess) { cudaFree(d_vox); return cuda_fail(e, "initial state"); }
+    if (e != cudaSuccess) { cudaStreamSynchronize(s); dev_free(d_vox); return cuda_fail(e, "initial state"); }
     int rc = cipher_chem_init(c, X, stream);
     int flags = 0;
     if (!rc) rc = read_flags(c, s, &flags);
-    cudaFree(d_vox);
+    /* the map's readers are done once the stream is (read_flags synchronises it) */
+    cudaStreamSynchronize(s);
+    dev_free(d_vox);
     if (rc) return rc;
     if (flags & ERR_CAP) return set_error(CIPHER_E_CAP, "an initial active set exceeds the cap P=%d", c->P);
     if (flags & ERR_BADSET) return set_error(CIPHER_E_ARG, "voxel map holds a phase outside 0..npf-1");
@@ -918,10 +922,10 @@ extern "C" int cipher_rhs_aos_host(cipher_ctx *c, double t, const double *X_host
     cudaStream_t s = (cudaStream_t)stream;
     size_t nb = (size_t)c->ncells * c->aos.ndof * sizeof(double);
     if (!c->d_aos_x) {
-        CUDA_TRY(cudaMalloc(&c->d_aos_x, nb), "cudaMalloc aos x");
-        CUDA_TRY(cudaMalloc(&c->d_aos_f, nb), "cudaMalloc aos f");
-        CUDA_TRY(cudaMalloc(&c->d_X, (size_t)c->lay.bytes), "cudaMalloc X");
-        CUDA_TRY(cudaMalloc(&c->d_F, (size_t)c->lay.bytes), "cudaMalloc F");
+        CUDA_TRY(dev_alloc(&c->d_aos_x, nb), "cudaMalloc aos x");
+        CUDA_TRY(dev_alloc(&c->d_aos_f, nb), "cudaMalloc aos f");
+        CUDA_TRY(dev_alloc(&c->d_X, (size_t)c->lay.bytes), "cudaMalloc X");
+        CUDA_TRY(dev_alloc(&c->d_F, (size_t)c->lay.bytes), "cudaMalloc F");
         CUDA_TRY(cudaMemsetAsync(c->d_F, 0, (size_t)c->lay.bytes, s), "cudaMemset F");
     }
     if (!c->general && c->dim == 3 && c->res[2] >= 4) {

@@ -10,6 +10,19 @@
 
 namespace cipher {
 
+/* long-lived device buffers from a per-device stream-ordered pool
+ * (devmem.cu): dev_alloc's memory is usable on any stream when it returns;
+ * dev_free does not wait, so no queued work may still use the block */
+cudaError_t dev_alloc(void **ptr, size_t bytes);
+void dev_free(void *ptr);
+template <typename T>
+inline cudaError_t dev_alloc(T **ptr, size_t bytes) { return dev_alloc((void **)ptr, bytes); }
+/* a pinned host slot of up to 64 bytes (zeroed), for small device-to-host results */
+cudaError_t pinned_word_alloc(void **ptr);
+void pinned_word_free(void *ptr);
+template <typename T>
+inline cudaError_t pinned_word_alloc(T **ptr) { return pinned_word_alloc((void **)ptr); }
+
 /* arguments of the phase-field-only RHS on a uniform grid */
 template <typename R>
 struct PfArgs {

@@ -25,6 +25,10 @@
 #include <vector>
 #include <cuda_runtime.h>
 #include "cipher_b200.h"
+#include "kernels.h"
+
+using cipher::dev_alloc;
+using cipher::dev_free;
 
 int cipher_set_error(int code, const char *fmt, ...);
 
@@ -68,7 +72,9 @@ struct cipher_server {
 
 static void drop_device(Request *r)
 {
-    cudaFree(r->X);
+    /* pool frees do not wait: the request's work must be finished */
+    cudaDeviceSynchronize();
+    dev_free(r->X);
     r->X = nullptr;
     if (r->ctx) cipher_ctx_destroy(r->ctx);
     r->ctx = nullptr;
@@ -101,7 +107,8 @@ extern "C" void cipher_server_destroy(cipher_server *s)
         delete r;
     }
     cipher_batch_destroy(s->batch);
-    cudaFree(s->d_aos);
+    cudaDeviceSynchronize();
+    dev_free(s->d_aos);
     delete s;
 }
 
@@ -139,7 +146,7 @@ static int admit(cipher_server *s, Request *r)
     if (!rc) rc = cipher_ctx_layout(r->ctx, &L);
     double *aos = nullptr, *d_aos = nullptr;
     if (!rc && sharp) {
-        if (cudaMalloc(&r->X, (size_t)L.bytes) != cudaSuccess) rc = CIPHER_E_NOMEM;
+        if (dev_alloc(&r->X, (size_t)L.bytes) != cudaSuccess) rc = CIPHER_E_NOMEM;
         if (!rc && cudaMemset(r->X, 0, (size_t)L.bytes) != cudaSuccess) rc = CIPHER_E_CUDA;
         if (!rc) rc = cipher_state_init_sharp(r->ctx, r->p->voxelphase, r->X, NULL);
         r->ncells = L.ncells;
@@ -150,14 +157,14 @@ static int admit(cipher_server *s, Request *r)
         aos = (double *)malloc(nb);
         if (!aos) rc = CIPHER_E_NOMEM;
         if (!rc) rc = cipher_initial_state_diffuse_aos(r->p, r->m, r->width, aos);
-        if (!rc && cudaMalloc(&r->X, (size_t)L.bytes) != cudaSuccess) rc = CIPHER_E_NOMEM;
+        if (!rc && dev_alloc(&r->X, (size_t)L.bytes) != cudaSuccess) rc = CIPHER_E_NOMEM;
         if (!rc && cudaMemset(r->X, 0, (size_t)L.bytes) != cudaSuccess) rc = CIPHER_E_CUDA;
-        if (!rc && cudaMalloc(&d_aos, nb) != cudaSuccess) rc = CIPHER_E_NOMEM;
+        if (!rc && dev_alloc(&d_aos, nb) != cudaSuccess) rc = CIPHER_E_NOMEM;
         if (!rc && cudaMemcpy(d_aos, aos, nb, cudaMemcpyHostToDevice) != cudaSuccess) rc = CIPHER_E_CUDA;
         if (!rc) rc = cipher_state_from_aos(r->ctx, d_aos, r->X, NULL);
         if (!rc) rc = cipher_chem_init(r->ctx, r->X, NULL);
-        if (!rc && cudaDeviceSynchronize() != cudaSuccess) rc = CIPHER_E_CUDA;
-        cudaFree(d_aos);
+        if (cudaDeviceSynchronize() != cudaSuccess && !rc) rc = CIPHER_E_CUDA;
+        dev_free(d_aos);
         free(aos);
         r->ncells = r->m->ncells;
         r->ndof = A.ndof;
@@ -250,10 +257,11 @@ extern "C" int cipher_server_poll(cipher_server *s, int *queued, int *active, in
             r->result.resize((size_t)r->ncells * r->ndof);
             const size_t nb = r->result.size() * sizeof(double);
             if (nb > s->aos_cap) {
-                cudaFree(s->d_aos);
+                cudaDeviceSynchronize();
+                dev_free(s->d_aos);
                 s->d_aos = nullptr;
                 s->aos_cap = 0;
-                if (cudaMalloc(&s->d_aos, nb + nb / 2) == cudaSuccess) s->aos_cap = nb + nb / 2;
+                if (dev_alloc(&s->d_aos, nb + nb / 2) == cudaSuccess) s->aos_cap = nb + nb / 2;
             }
             if (s->d_aos && cipher_state_to_aos(r->ctx, r->X, s->d_aos, NULL) == CIPHER_OK)
                 cudaMemcpy(r->result.data(), s->d_aos, nb, cudaMemcpyDeviceToHost);

@@ -443,11 +443,13 @@ static dim3 combine_grid(const cipher_state_layout &L)
 static void free_ts(cipher_ts *ts)
 {
     if (!ts) return;
-    for (int j = 0; j < kMaxStages; j++) cudaFree(ts->K[j]);
-    cudaFree(ts->Y);
-    cudaFree(ts->d_partial);
-    cudaFree(ts->d_sum);
-    if (ts->h_sum) cudaFreeHost(ts->h_sum);
+    /* pool frees do not wait: finish every queued use of the buffers first */
+    cudaDeviceSynchronize();
+    for (int j = 0; j < kMaxStages; j++) dev_free(ts->K[j]);
+    dev_free(ts->Y);
+    dev_free(ts->d_partial);
+    dev_free(ts->d_sum);
+    pinned_word_free(ts->h_sum);
     free(ts);
 }
 
@@ -466,14 +468,14 @@ extern "C" int cipher_ts_create(cipher_ctx *c, const cipher_ts_opts *o, cipher_t
     rc = cipher_ctx_layout(c, &ts->lay);
     if (rc) { free(ts); return rc; }
     cudaError_t e = cudaSuccess;
-    for (int j = 0; j < tab.ns && e == cudaSuccess; j++) e = cudaMalloc(&ts->K[j], (size_t)ts->lay.bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&ts->Y, (size_t)ts->lay.bytes);
+    for (int j = 0; j < tab.ns && e == cudaSuccess; j++) e = dev_alloc(&ts->K[j], (size_t)ts->lay.bytes);
+    if (e == cudaSuccess) e = dev_alloc(&ts->Y, (size_t)ts->lay.bytes);
     if (e == cudaSuccess) e = cudaMemset(ts->Y, 0, (size_t)ts->lay.bytes);
     dim3 g = combine_grid(ts->lay);
     ts->npartial = (int64_t)g.x * g.y;
-    if (e == cudaSuccess) e = cudaMalloc(&ts->d_partial, (size_t)ts->npartial * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&ts->d_sum, sizeof(double));
-    if (e == cudaSuccess) e = cudaMallocHost(&ts->h_sum, sizeof(double));
+    if (e == cudaSuccess) e = dev_alloc(&ts->d_partial, (size_t)ts->npartial * sizeof(double));
+    if (e == cudaSuccess) e = dev_alloc(&ts->d_sum, sizeof(double));
+    if (e == cudaSuccess) e = pinned_word_alloc(&ts->h_sum);
     if (e != cudaSuccess) {
         free_ts(ts);
         return cipher_set_error(CIPHER_E_NOMEM, "stepper buffers: %s", cudaGetErrorString(e));
@@ -710,11 +712,12 @@ static int commit_arena(cipher_batch *b)
 {
     const size_t need = b->staging.size() + 256;
     if (need > b->arena_cap) {
-        cudaFree(b->d_arena);
+        cudaDeviceSynchronize();
+        dev_free(b->d_arena);
         b->d_arena = nullptr;
         b->arena_cap = 0;
         const size_t cap = need + need / 2;
-        TS_CUDA(cudaMalloc(&b->d_arena, cap), "batch tables");
+        TS_CUDA(dev_alloc(&b->d_arena, cap), "batch tables");
         b->arena_cap = cap;
     }
     if (!b->staging.empty())
@@ -729,24 +732,26 @@ static int commit_arena(cipher_batch *b)
 static int ensure_io(cipher_batch *b, size_t ctl, size_t out)
 {
     if (ctl > b->ctl_cap) {
-        cudaFree(b->d_ctl);
+        cudaDeviceSynchronize();
+        dev_free(b->d_ctl);
         if (b->h_ctl) cudaFreeHost(b->h_ctl);
         b->d_ctl = nullptr;
         b->h_ctl = nullptr;
         b->ctl_cap = 0;
         const size_t cap = ctl + ctl / 2 + 256;
-        TS_CUDA(cudaMalloc(&b->d_ctl, cap), "batch control");
+        TS_CUDA(dev_alloc(&b->d_ctl, cap), "batch control");
         TS_CUDA(cudaMallocHost(&b->h_ctl, cap), "batch control");
         b->ctl_cap = cap;
     }
     if (out > b->out_cap) {
-        cudaFree(b->d_out);
+        cudaDeviceSynchronize();
+        dev_free(b->d_out);
         if (b->h_out) cudaFreeHost(b->h_out);
         b->d_out = nullptr;
         b->h_out = nullptr;
         b->out_cap = 0;
         const size_t cap = out + out / 2 + 256;
-        TS_CUDA(cudaMalloc(&b->d_out, cap), "batch outputs");
+        TS_CUDA(dev_alloc(&b->d_out, cap), "batch outputs");
         TS_CUDA(cudaMallocHost(&b->h_out, cap), "batch outputs");
         b->out_cap = cap;
     }
@@ -775,9 +780,10 @@ static void free_tables(cipher_batch *b)
 static void free_buffers(cipher_batch *b)
 {
     free_tables(b);
-    cudaFree(b->d_arena);
-    cudaFree(b->d_ctl);
-    cudaFree(b->d_out);
+    cudaDeviceSynchronize();
+    dev_free(b->d_arena);
+    dev_free(b->d_ctl);
+    dev_free(b->d_out);
     if (b->h_ctl) cudaFreeHost(b->h_ctl);
     if (b->h_out) cudaFreeHost(b->h_out);
     b->d_arena = b->d_ctl = b->d_out = b->h_ctl = b->h_out = nullptr;
@@ -786,10 +792,11 @@ static void free_buffers(cipher_batch *b)
 
 static void free_slot(BatchSlot &s)
 {
-    for (int j = 0; j < kMaxStages; j++) cudaFree(s.K[j]);
-    cudaFree(s.Y);
-    cudaFree(s.pruned);
-    cudaFree(s.partial);
+    cudaDeviceSynchronize();
+    for (int j = 0; j < kMaxStages; j++) dev_free(s.K[j]);
+    dev_free(s.Y);
+    dev_free(s.pruned);
+    dev_free(s.partial);
     memset(&s, 0, sizeof(s));
 }
 
@@ -868,11 +875,11 @@ extern "C" int cipher_batch_attach(cipher_batch *b, cipher_ctx *c, void *X, doub
     s.gx = (s.lay.ncells + kTsCellsPerBlock - 1) / kTsCellsPerBlock;
     s.npartial = s.gx * nplanes_of(s.lay);
     cudaError_t e = cudaSuccess;
-    for (int j = 0; j < b->T.ns && e == cudaSuccess; j++) e = cudaMalloc(&s.K[j], (size_t)s.lay.bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&s.Y, (size_t)s.lay.bytes);
+    for (int j = 0; j < b->T.ns && e == cudaSuccess; j++) e = dev_alloc(&s.K[j], (size_t)s.lay.bytes);
+    if (e == cudaSuccess) e = dev_alloc(&s.Y, (size_t)s.lay.bytes);
     if (e == cudaSuccess) e = cudaMemset(s.Y, 0, (size_t)s.lay.bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&s.pruned, (size_t)(s.lay.pf_size + 1) * s.lay.stride * sizeof(uint16_t));
-    if (e == cudaSuccess) e = cudaMalloc(&s.partial, (size_t)s.npartial * sizeof(double));
+    if (e == cudaSuccess) e = dev_alloc(&s.pruned, (size_t)(s.lay.pf_size + 1) * s.lay.stride * sizeof(uint16_t));
+    if (e == cudaSuccess) e = dev_alloc(&s.partial, (size_t)s.npartial * sizeof(double));
     if (e != cudaSuccess) {
         free_slot(s);
         cudaGetLastError();

@@ -294,6 +294,46 @@ int cipher_problem_grain_growth(int dim, const int32_t *res, int ngrains, int ca
     return 0;
 }
 
+int cipher_problem_grain_growth_multi(int dim, const int32_t *res, int ngrains, int cap, uint64_t seed,
+                                      int ninterfaces, unsigned features, cipher_problem **out)
+{
+    *out = NULL;
+    if (ninterfaces < 1 || ninterfaces > 4096) return CIPHER_E_ARG;
+    cipher_problem *base = NULL;
+    int rc = cipher_problem_grain_growth(dim, res, ngrains, cap, seed, 1.0, 1.0, 4.0, 1.0e-5, 500.0, &base);
+    if (rc) return rc;
+    /* the same grid, voxel map and material with an interface table of its own */
+    cipher_interface *itf = (cipher_interface *)calloc((size_t)ninterfaces, sizeof(cipher_interface));
+    if (!itf) { cipher_problem_free(base); return CIPHER_E_NOMEM; }
+    free(base->interface);
+    base->interface = itf;
+    base->nf = ninterfaces;
+    uint64_t st = seed ^ 0x5bd1e995c0ffee11ull;
+    for (int i = 0; i < ninterfaces; i++) {
+        itf[i].width = (features & CIPHER_GG_WIDTHS) ? 3.0 + 2.0 * cipher_rand_uniform(&st) : 4.0;
+        itf[i].energy_m0 = 0.5 + cipher_rand_uniform(&st);
+        itf[i].mobility_m0 = 0.5 + cipher_rand_uniform(&st);
+        if ((features & CIPHER_GG_ACTIVATION) && (i % 2 == 1)) {
+            /* exp(Q/(R T)) factors (src/cipher.c:462-466) with Q in [-3000, 3000] J/mol */
+            itf[i].energy_activation.n = 1;
+            itf[i].energy_activation.exp[0] = 0;
+            itf[i].energy_activation.coeff[0] = -3000.0 + 6000.0 * cipher_rand_uniform(&st);
+            itf[i].mobility_activation.n = 1;
+            itf[i].mobility_activation.exp[0] = 0;
+            itf[i].mobility_activation.coeff[0] = -3000.0 + 6000.0 * cipher_rand_uniform(&st);
+        }
+    }
+    /* the upper triangle, as the reference's parser fills it (src/init.c:1501) */
+    const int npf = base->npf;
+    for (int a = 0; a < npf; a++)
+        for (int b = a + 1; b < npf; b++) {
+            int i = (int)(cipher_rand_uniform(&st) * ninterfaces);
+            base->interfacelist[a * npf + b] = i < ninterfaces ? i : ninterfaces - 1;
+        }
+    *out = base;
+    return 0;
+}
+
 /* ------------------------------------------------------------------ */
 /* uniform meshes                                                      */
 /* ------------------------------------------------------------------ */

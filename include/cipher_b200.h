@@ -42,6 +42,11 @@ extern "C" {
 const char *cipher_strerror(int code);
 const char *cipher_last_error(void);
 
+/* Contexts, steppers, batches and served requests take their device
+ * buffers from a stream-ordered pool per device that keeps freed blocks for
+ * reuse; this hands the pooled blocks of `device` back to the driver. */
+int cipher_pool_trim(int device);
+
 /* sizeof of the public structs, for binding generators to check their
  * mirrors: out[0..8] = tseries, rk, mobility, source, material, interface,
  * bc, problem, mesh; returns how many were written (at most n) */
@@ -69,6 +74,20 @@ int cipher_problem_grain_growth(int dim, const int32_t *res, int ngrains, int ca
                                 double energy, double mobility, double width,
                                 double molarvolume, double temperature0,
                                 cipher_problem **out);
+/* feature bits of cipher_problem_grain_growth_multi */
+#define CIPHER_GG_ACTIVATION  0x01u  /* T-dependent energy and mobility on every other interface */
+#define CIPHER_GG_WIDTHS      0x02u  /* interface widths uniform in [3, 5] cells instead of 4 */
+
+/* grain growth with several interfaces: the problem of
+ * cipher_problem_grain_growth (energy 1, mobility 1, width 4, Vm 1e-5,
+ * T0 500) with `ninterfaces` seeded interfaces (energy and mobility
+ * prefactors uniform in [0.5, 1.5], plus the CIPHER_GG_* features), and every
+ * grain pair a<b assigned a seeded interface in the upper triangle of
+ * interfacelist, as the reference's parser fills it (src/init.c:1501).
+ * Misorientation-dependent boundaries in the reference are such tables. */
+int cipher_problem_grain_growth_multi(int dim, const int32_t *res, int ngrains, int cap, uint64_t seed,
+                                      int ninterfaces, unsigned features, cipher_problem **out);
+
 /* feature bits of cipher_problem_alloy */
 #define CIPHER_ALLOY_SEGREGATION   0x01u  /* segregation potentials on grain and phase boundaries */
 #define CIPHER_ALLOY_ITF_MOBILITY  0x02u  /* interface factors on the solute mobilities */

@@ -9,7 +9,7 @@ through the PETSc shim into oracle/_ref/libcipher_ref.so) produce the outputs:
   Xpost  PostStep(X) (projection, pruning, neighbour union, reorder)
 
 Run from the repository root where the reference sources exist:
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture names...]
 """
 import os
 import sys
@@ -44,6 +44,20 @@ ALLOY_CASES = [
 ]
 MODEL_ID = {"quadratic": 0, "calphaddis": 1, "calphad2sl": 2}
 
+# grain growth with several interfaces (cipher_problem_grain_growth_multi):
+# (name, dim, res, ngrains, cap, seed, ninterfaces, features), diffuse state
+MULTI_CASES = [
+    ("ggmulti2d_act_widths", 2, [24, 24], 12, 8, 11, 5, 0x3),
+    ("ggmulti3d_act_cap15", 3, [10, 10, 10], 30, 15, 3, 6, 0x1),
+]
+
+# alloy cases with another interpolant: an ALLOY_CASES entry plus the
+# interpolation (0 linear, 1 quadratic; the other fixtures are cubic)
+ALLOY_INTERP_CASES = [
+    ("alloy2sl_linear_2d", 2, [16, 12], "calphad2sl", 4, 4, 8, 21, 0, 3, 0),
+    ("alloydis_quadinterp_2d", 2, [16, 12], "calphaddis", 3, 4, 8, 22, 0xFF, 2, 1),
+]
+
 
 def build_alloy(dim, res, model, ncp, nprecip, cap, seed, features):
     P = cb.Problem.alloy(dim, res, model, ncp, nprecip, cap, seed, features)
@@ -73,9 +87,49 @@ def build_case(dim, res, ngrains, cap, seed, kind):
     return P, M, X
 
 
-def main():
+def build_multi(dim, res, ng, cap, seed, nitf, feats):
+    P = cb.Problem.grain_growth_multi(dim, res, ng, cap, seed, nitf, activation=bool(feats & 1),
+                                      widths=bool(feats & 2))
+    M = cb.Mesh(P)
+    return P, M, cb.diffuse_state_aos(P, M, 4.0)
+
+
+def main(only=None):
+    """regenerate every fixture, or only the named ones"""
     oracle.build(ref=True)
+
+    def wanted(name):
+        return not only or name in only
+
+    for name, dim, res, ng, nitf_cap, seed, nitf, feats in MULTI_CASES:
+        if not wanted(name):
+            continue
+        P, M, X = build_multi(dim, res, ng, nitf_cap, seed, nitf, feats)
+        with oracle.RefOracle(P, M) as R:
+            F = R.rhs(X)
+            Xp = X.copy()
+            assert R.poststep(Xp) == 0
+        meta = [dim] + list(res) + [0] * (3 - len(res)) + [ng, nitf_cap, seed, nitf, feats]
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), X=X, F=F, Xpost=Xp, meta=np.array(meta))
+        print(name, X.shape, "max|F|", np.abs(F).max(), "mean n", X[:, 0].mean())
+    for name, dim, res, model, ncp, npr, cap, seed, feats, steps, interp in ALLOY_INTERP_CASES:
+        if not wanted(name):
+            continue
+        P, M = build_alloy(dim, res, model, ncp, npr, cap, seed, feats)
+        P.s.interpolation = interp
+        X0 = oracle.port_initial_state(P, M)
+        with oracle.RefOracle(P, M) as R:
+            X = evolve_with_reference(P, M, R, X0, steps)
+            F = R.rhs(X)
+            Xp = X.copy()
+            assert R.poststep(Xp) == 0
+        meta = [dim] + list(res) + [0] * (3 - len(res)) + [MODEL_ID[model], ncp, npr, cap, seed, feats, steps,
+                                                            interp]
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), X=X, F=F, Xpost=Xp, meta=np.array(meta))
+        print(name, X.shape, "max|F|", np.abs(F).max(), "mean n", X[:, 0].mean())
     for name, dim, res, ng, cap, seed, kind in CASES:
+        if not wanted(name):
+            continue
         P, M, X = build_case(dim, res, ng, cap, seed, kind)
         with oracle.RefOracle(P, M) as R:
             F = R.rhs(X)
@@ -87,6 +141,8 @@ def main():
                                                                                         int(kind == "sharp")]))
         print(name, X.shape, "max|F|", np.abs(F).max())
     for name, dim, res, model, ncp, npr, cap, seed, feats, steps in ALLOY_CASES:
+        if not wanted(name):
+            continue
         P, M = build_alloy(dim, res, model, ncp, npr, cap, seed, feats)
         X0 = oracle.port_initial_state(P, M)
         with oracle.RefOracle(P, M) as R:
@@ -100,4 +156,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -37,6 +37,8 @@ def _fixture(path):
     res = meta[1:1 + dim]
     model, ncp, npr, cap, seed, feats = meta[4:10]
     P = cb.Problem.alloy(dim, res, MODELS[model], ncp, npr, cap, seed, feats)
+    if len(meta) == 12:             # fixtures of the linear / quadratic interpolants
+        P.s.interpolation = meta[11]
     return P, cb.Mesh(P), g
 
 

@@ -22,8 +22,10 @@ MODELS = {0: "quadratic", 1: "calphaddis", 2: "calphad2sl"}
 
 
 def _case(meta, X_fixture=None):
-    """Rebuild a fixture's problem and mesh; grain-growth fixtures (8 meta
-    entries) also rebuild their state, alloy fixtures (11) carry theirs."""
+    """Rebuild a fixture's problem and mesh.  Grain-growth fixtures (8 meta
+    entries) and several-interface grain growth (9: + ninterfaces, features)
+    also rebuild their state; alloy fixtures (11, or 12 with the
+    interpolation) carry theirs."""
     dim = int(meta[0])
     res = [int(v) for v in meta[1:1 + dim]]
     if len(meta) == 8:
@@ -32,15 +34,24 @@ def _case(meta, X_fixture=None):
         M = cb.Mesh(P)
         X = cb.initial_state_aos(P, M) if sharp else cb.diffuse_state_aos(P, M, 4.0)
         return P, M, X
+    if len(meta) == 9:
+        ng, cap, seed, nitf, feats = (int(v) for v in meta[4:9])
+        P = cb.Problem.grain_growth_multi(dim, res, ng, cap, seed, nitf, activation=bool(feats & 1),
+                                          widths=bool(feats & 2))
+        M = cb.Mesh(P)
+        return P, M, cb.diffuse_state_aos(P, M, 4.0)
     model, ncp, npr, cap, seed, feats = (int(v) for v in meta[4:10])
     P = cb.Problem.alloy(dim, res, MODELS[model], ncp, npr, cap, seed, feats)
+    if len(meta) == 12:
+        P.s.interpolation = int(meta[11])
     M = cb.Mesh(P)
     return P, M, X_fixture
 
 
 def test_golden_fixtures_exist():
-    assert len(GOLDEN) >= 7
-    assert sum(1 for p in GOLDEN if os.path.basename(p).startswith("alloy")) >= 3
+    assert len(GOLDEN) >= 11
+    assert sum(1 for p in GOLDEN if os.path.basename(p).startswith("alloy")) >= 5
+    assert sum(1 for p in GOLDEN if os.path.basename(p).startswith("ggmulti")) >= 2
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
