@@ -185,6 +185,19 @@ _SIGNATURES = [
     ("cipher_last_error", C.c_char_p, []),
     ("cipher_abi_sizes", C.c_int, [C.POINTER(C.c_int64), C.c_int]),
     ("cipher_pool_trim", C.c_int, [C.c_int]),
+    ("cipher_forest_create", C.c_int, [C.c_int, C.POINTER(C.c_int32), C.c_int, C.c_int, C.c_int,
+                                       C.POINTER(C.c_int32), C.POINTER(C.c_double), C.POINTER(C.c_void_p)]),
+    ("cipher_forest_destroy", None, [C.c_void_p]),
+    ("cipher_forest_nleaves", C.c_int64, [C.c_void_p]),
+    ("cipher_forest_leaves", C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    ("cipher_forest_resolution", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    ("cipher_forest_mark_active", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_int8)]),
+    ("cipher_forest_adapt", C.c_int, [C.c_void_p, C.POINTER(C.c_int8), C.POINTER(C.c_double), C.c_int, C.c_int]),
+    ("cipher_forest_transfer_plan", C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+    ("cipher_forest_transfer_aos", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double)]),
+    ("cipher_forest_mesh", C.c_int, [C.c_void_p, C.POINTER(MP)]),
+    ("cipher_state_transfer", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int64),
+                                        C.POINTER(C.c_int32), C.c_void_p]),
     ("cipher_problem_new", PP, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     ("cipher_problem_free", None, [PP]),
     ("cipher_problem_finalize", C.c_int, [PP]),

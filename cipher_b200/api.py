@@ -107,6 +107,15 @@ class Mesh:
         self.ptr = out
         self.problem = problem
 
+    @classmethod
+    def adopt(cls, problem: Problem, ptr) -> "Mesh":
+        """take ownership of a cipher_mesh built elsewhere (e.g. by a forest)"""
+        m = cls.__new__(cls)
+        m._lib = L.load()
+        m.ptr = ptr
+        m.problem = problem
+        return m
+
     @property
     def s(self) -> L.MeshStruct:
         return self.ptr.contents
@@ -125,6 +134,92 @@ class Mesh:
     def close(self):
         if self.ptr:
             self._lib.cipher_mesh_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Forest:
+    """An adaptive quadtree / octree mesh (cipher_forest_*): the role the
+    reference's p4est forest plays.  Leaves are the cells of `mesh()`."""
+
+    def __init__(self, dim: int, nblocks, lmin: int, lmax: int, linit: int = None, periodic=(1, 1, 1), size=None):
+        self._lib = L.load()
+        nb = (C.c_int32 * 3)(*(list(nblocks) + [1] * (3 - len(nblocks))))
+        per = (C.c_int32 * 3)(*(list(periodic) + [0] * (3 - len(periodic))))
+        sz = None if size is None else (C.c_double * 3)(*(list(size) + [1.0] * (3 - len(size))))
+        out = C.c_void_p()
+        L.check(self._lib.cipher_forest_create(dim, nb, lmin, lmax, lmax if linit is None else linit, per, sz,
+                                               C.byref(out)), "cipher_forest_create")
+        self.ptr = out
+        self.dim = dim
+
+    @property
+    def nleaves(self) -> int:
+        return int(self._lib.cipher_forest_nleaves(self.ptr))
+
+    def leaves(self):
+        """(level[n], corner[n, 3]) on the finest grid"""
+        n = self.nleaves
+        lev = np.zeros(n, dtype=np.int32)
+        cor = np.zeros((n, 3), dtype=np.int32)
+        L.check(self._lib.cipher_forest_leaves(self.ptr, lev.ctypes.data_as(C.POINTER(C.c_int32)),
+                                               cor.ctypes.data_as(C.POINTER(C.c_int32))), "cipher_forest_leaves")
+        return lev, cor
+
+    def resolution(self):
+        r = (C.c_int32 * 3)()
+        L.check(self._lib.cipher_forest_resolution(self.ptr, r), "cipher_forest_resolution")
+        return list(r)
+
+    def mark_active(self, X: np.ndarray) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        mark = np.zeros(self.nleaves, dtype=np.int8)
+        L.check(self._lib.cipher_forest_mark_active(self.ptr, X.ctypes.data_as(C.POINTER(C.c_double)), X.shape[1],
+                                                    mark.ctypes.data_as(C.POINTER(C.c_int8))),
+                "cipher_forest_mark_active")
+        return mark
+
+    def adapt(self, mark, X: np.ndarray = None, as_size: int = 0):
+        """refine / coarsen by marks (+1 / -1 / 0) and balance; with X the
+        families whose active sets (first as_size dofs) differ are kept"""
+        mark = np.ascontiguousarray(mark, dtype=np.int8)
+        xp, nd = None, 0
+        if X is not None:
+            X = np.ascontiguousarray(X, dtype=np.float64)
+            xp, nd = X.ctypes.data_as(C.POINTER(C.c_double)), X.shape[1]
+        L.check(self._lib.cipher_forest_adapt(self.ptr, mark.ctypes.data_as(C.POINTER(C.c_int8)), xp, nd, as_size),
+                "cipher_forest_adapt")
+
+    def transfer_plan(self):
+        n = self.nleaves
+        s0 = np.zeros(n, dtype=np.int64)
+        ns = np.zeros(n, dtype=np.int32)
+        L.check(self._lib.cipher_forest_transfer_plan(self.ptr, s0.ctypes.data_as(C.POINTER(C.c_int64)),
+                                                      ns.ctypes.data_as(C.POINTER(C.c_int32))),
+                "cipher_forest_transfer_plan")
+        return s0, ns
+
+    def transfer_aos(self, Xold: np.ndarray) -> np.ndarray:
+        Xold = np.ascontiguousarray(Xold, dtype=np.float64)
+        Xnew = np.zeros((self.nleaves, Xold.shape[1]), dtype=np.float64)
+        L.check(self._lib.cipher_forest_transfer_aos(self.ptr, Xold.ctypes.data_as(C.POINTER(C.c_double)),
+                                                     Xold.shape[1], Xnew.ctypes.data_as(C.POINTER(C.c_double))),
+                "cipher_forest_transfer_aos")
+        return Xnew
+
+    def mesh(self, problem: "Problem") -> "Mesh":
+        out = L.MP()
+        L.check(self._lib.cipher_forest_mesh(self.ptr, C.byref(out)), "cipher_forest_mesh")
+        return Mesh.adopt(problem, out)
+
+    def close(self):
+        if self.ptr:
+            self._lib.cipher_forest_destroy(self.ptr)
             self.ptr = None
 
     def __del__(self):
@@ -258,6 +353,16 @@ class Context:
         """EX and mu of an initial state from the materials' c0 (SetUpProblem)."""
         L.check(self._lib.cipher_chem_init(self.ptr, C.c_void_p(_ptr(X)), _stream_handle(stream)),
                 "cipher_chem_init")
+
+    def transfer_from(self, X, src: "Context", Xsrc, forest: "Forest", stream=None):
+        """X (this context's adapted mesh) <- Xsrc (src's mesh before the
+        forest's last adaptation), by the forest's transfer plan"""
+        s0, ns = forest.transfer_plan()
+        L.check(self._lib.cipher_state_transfer(self.ptr, C.c_void_p(_ptr(X)), src.ptr, C.c_void_p(_ptr(Xsrc)),
+                                                s0.ctypes.data_as(C.POINTER(C.c_int64)),
+                                                ns.ctypes.data_as(C.POINTER(C.c_int32)), _stream_handle(stream)),
+                "cipher_state_transfer")
+        return X
 
     def RHSFunction(self, ts: TSView, ftime: float, X, F) -> int:
         """Reference-shaped callback: F = RHS(ftime, X); returns 0 like PetscErrorCode."""

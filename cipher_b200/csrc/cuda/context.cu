@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <cmath>
+#include <vector>
 #include <cuda_runtime.h>
 #include "cipher_b200.h"
 #include "device_common.cuh"
@@ -90,6 +91,11 @@ struct cipher_ctx {
     double temp_rate;
     int interp, nbcs;
     DevBC bcs[CIPHER_MAXBC];
+    /* an adapted (non-uniform) mesh: per-cell face lists, face factors and
+     * cell volumes on the device (FaceLists); 0 on uniform grids */
+    int listed;
+    int32_t *d_fl_start, *d_fl_nbr, *d_fl_face, *d_fl_bstart, *d_fl_blabel;
+    double *d_fl_ff, *d_fl_vol, *d_fl_delta;
     int32_t *d_itflist;
     DevInterface *d_itfs;
     cipher_material *d_mat;
@@ -164,6 +170,14 @@ static void free_ctx(cipher_ctx *c)
     if (!c) return;
     /* pool frees do not wait: finish every queued use of the buffers first */
     cudaDeviceSynchronize();
+    dev_free(c->d_fl_start);
+    dev_free(c->d_fl_nbr);
+    dev_free(c->d_fl_face);
+    dev_free(c->d_fl_bstart);
+    dev_free(c->d_fl_blabel);
+    dev_free(c->d_fl_ff);
+    dev_free(c->d_fl_vol);
+    dev_free(c->d_fl_delta);
     dev_free(c->d_itflist);
     dev_free(c->d_itfs);
     dev_free(c->d_mat);
@@ -195,6 +209,89 @@ static void free_ctx(cipher_ctx *c)
     free(c);
 }
 
+/* per-cell face lists of an adapted mesh (FaceLists): every face in the
+ * mesh's face order is appended to its L and R cells' lists, so each list is
+ * in the reference's face order; face factors and volumes exactly as the
+ * reference forms them (src/cipher.c:273-275, FastPow src/utility.c:112-124) */
+static double fast_pow(double base, unsigned e)
+{
+    double r = 1.0;
+    while (e) {
+        if (e & 1u) r *= base;
+        e >>= 1;
+        base *= base;
+    }
+    return r;
+}
+
+static int upload_face_lists(cipher_ctx *c, const cipher_mesh *m, int dim)
+{
+    const int64_t n = m->ncells, nf = m->nfaces, nbf = m->nbfaces;
+    std::vector<int32_t> start(n + 1, 0), nbr(2 * nf), face(2 * nf), bstart(n + 1, 0), blabel(nbf > 0 ? nbf : 1);
+    std::vector<double> ff(nf > 0 ? nf : 1), vol(n), delta(n);
+    for (int64_t i = 0; i < n; i++) {
+        delta[i] = m->cellgeom[i];
+        vol[i] = fast_pow(m->cellgeom[i], (unsigned)dim);
+    }
+    for (int64_t f = 0; f < nf; f++) {
+        const int32_t L = m->face_cells[2 * f], R = m->face_cells[2 * f + 1];
+        if (L < 0 || L >= n || R < 0 || R >= n || L == R) return set_error(CIPHER_E_ARG, "face %lld has bad cells", (long long)f);
+        start[L + 1]++;
+        start[R + 1]++;
+        const double dl = delta[L], dr = delta[R];
+        ff[f] = 2.0 * (dl < dr ? vol[L] / dl : vol[R] / dr) / (dl + dr);
+    }
+    for (int64_t i = 0; i < n; i++) start[i + 1] += start[i];
+    std::vector<int32_t> fill(start.begin(), start.end() - 1);
+    for (int64_t f = 0; f < nf; f++) {
+        const int32_t L = m->face_cells[2 * f], R = m->face_cells[2 * f + 1];
+        nbr[fill[L]] = R | FACE_SELF_L;
+        face[fill[L]++] = (int32_t)f;
+        nbr[fill[R]] = L;
+        face[fill[R]++] = (int32_t)f;
+    }
+    for (int64_t b = 0; b < nbf; b++) {
+        const int32_t cell = m->bface_cell[b];
+        if (cell < 0 || cell >= n) return set_error(CIPHER_E_ARG, "boundary face %lld has a bad cell", (long long)b);
+        bstart[cell + 1]++;
+    }
+    for (int64_t i = 0; i < n; i++) bstart[i + 1] += bstart[i];
+    std::vector<int32_t> bfill(bstart.begin(), bstart.end() - 1);
+    for (int64_t b = 0; b < nbf; b++) blabel[bfill[m->bface_cell[b]]++] = m->bface_label[b];
+    cudaError_t e = cudaSuccess;
+    auto up = [&](auto **dst, const auto &v) {
+        const size_t bytes = v.size() * sizeof(v[0]);
+        if (e == cudaSuccess) e = dev_alloc(dst, bytes);
+        if (e == cudaSuccess) e = cudaMemcpy(*dst, v.data(), bytes, cudaMemcpyHostToDevice);
+    };
+    up(&c->d_fl_start, start);
+    up(&c->d_fl_nbr, nbr.size() ? nbr : std::vector<int32_t>(1, 0));
+    up(&c->d_fl_face, face.size() ? face : std::vector<int32_t>(1, 0));
+    up(&c->d_fl_bstart, bstart);
+    up(&c->d_fl_blabel, blabel);
+    up(&c->d_fl_ff, ff);
+    up(&c->d_fl_vol, vol);
+    up(&c->d_fl_delta, delta);
+    if (e != cudaSuccess) return cuda_fail(e, "face lists");
+    return CIPHER_OK;
+}
+
+static FaceLists face_lists(const cipher_ctx *c)
+{
+    FaceLists f;
+    memset(&f, 0, sizeof(f));
+    if (!c->listed) return f;
+    f.start = c->d_fl_start;
+    f.nbr = c->d_fl_nbr;
+    f.face = c->d_fl_face;
+    f.ff = c->d_fl_ff;
+    f.vol = c->d_fl_vol;
+    f.delta = c->d_fl_delta;
+    f.bstart = c->d_fl_bstart;
+    f.blabel = c->d_fl_blabel;
+    return f;
+}
+
 extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, int precision, int device,
                                  cipher_ctx **out)
 {
@@ -203,8 +300,10 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
     if (!p || !m) return set_error(CIPHER_E_ARG, "problem or mesh is NULL");
     if (precision != CIPHER_PREC_FP64 && precision != CIPHER_PREC_MIXED)
         return set_error(CIPHER_E_ARG, "unknown precision %d", precision);
-    if (!m->uniform || m->ncells != m->nowned)
-        return set_error(CIPHER_E_UNSUPPORTED, "device path needs a whole-domain uniform mesh");
+    if (m->ncells != m->nowned)
+        return set_error(CIPHER_E_UNSUPPORTED, "device path needs a whole-domain mesh (no ghost cells)");
+    if (!m->uniform && (!m->face_cells && m->nfaces > 0))
+        return set_error(CIPHER_E_ARG, "an adapted mesh needs its face list");
     if (p->pf_size < 1 || p->pf_size > CIPHER_MAXAP) return set_error(CIPHER_E_ARG, "bad phase cap %d", p->pf_size);
     /* kernels launch one block row per (y, z) grid line */
     if ((p->dim > 1 && m->res[1] > 65535) || (p->dim > 2 && m->res[2] > 65535))
@@ -237,7 +336,10 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
     c->S = p->maxsites * p->ndp;
     c->nmat = p->nmat;
     c->junctionpenalty = p->junctionpenalty;
-    c->general = !phasefield_only(p);
+    c->listed = !m->uniform;
+    /* the phase-field kernels walk uniform grids; adapted meshes take the
+     * general kernels over their face lists */
+    c->general = c->listed || !phasefield_only(p);
     c->interp = p->interpolation;
     c->delta = m->cellgeom[0];
     c->nbcs = p->nbcs;
@@ -276,7 +378,8 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
     L.precision = precision;
     int64_t off = 0;
     L.as_offset = off; off = align_up(off + (int64_t)(c->P + 1) * c->stride * 2, 256);
-    L.map_offset = off; L.map_planes = 2 * c->dim; off = align_up(off + (int64_t)L.map_planes * c->stride * 8, 256);
+    L.map_offset = off; L.map_planes = c->listed ? 0 : 2 * c->dim;
+    off = align_up(off + (int64_t)L.map_planes * c->stride * 8, 256);
     L.pf_offset = off; off = align_up(off + (int64_t)c->P * c->stride * rb, 256);
     L.dp_offset = off; off = align_up(off + (int64_t)c->ndp * c->stride * 8, 256);
     L.ex_offset = off; off = align_up(off + (int64_t)L.ex_size * c->stride * 8, 256);
@@ -377,6 +480,10 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
     if ((e = dev_alloc(&c->d_err, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc err"); }
     if ((e = cudaMemset(c->d_err, 0, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMemset err"); }
     if ((e = pinned_word_alloc(&c->h_err)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "pinned error word"); }
+    if (c->listed) {
+        int rc = upload_face_lists(c, m, p->dim);
+        if (rc) { free_ctx(c); return rc; }
+    }
     *c->h_err = 0;
     *out = c;
     return CIPHER_OK;
@@ -518,6 +625,7 @@ static GenArgs<R> gen_args(const cipher_ctx *c, const void *X, void *F)
     a.dp = (const double *)(x + c->lay.dp_offset);
     a.ex = (const double *)(x + c->lay.ex_offset);
     a.tm = (const R *)(x + c->lay.tm_offset);
+    a.fl = face_lists(c);
     a.comp = c->d_comp;
     a.mob = c->d_mob;
     a.tcond = c->d_tcond;
@@ -561,7 +669,9 @@ static PostArgs<R> post_args(const cipher_ctx *c, void *X)
     a.P = c->P;
     a.S = c->S;
     a.as = (uint16_t *)(x + c->lay.as_offset);
-    a.maps = (uint64_t *)(x + c->lay.map_offset);
+    /* adapted meshes have no face maps (their general kernels merge sets) */
+    a.maps = c->lay.map_planes ? (uint64_t *)(x + c->lay.map_offset) : nullptr;
+    a.fl = face_lists(c);
     a.npf = c->npf;
     a.phi = (R *)(x + c->lay.pf_offset);
     a.ex = (double *)(x + c->lay.ex_offset);
@@ -589,6 +699,7 @@ CtxInfo ctx_info(const cipher_ctx *c)
     i.dim = c->dim;
     i.general = c->general;
     i.single = c->single;
+    i.listed = c->listed;
     i.P = c->P;
     i.ncells = c->ncells;
     i.res[0] = c->res[0]; i.res[1] = c->res[1]; i.res[2] = c->res[2];
@@ -767,6 +878,9 @@ extern "C" int cipher_state_from_aos(cipher_ctx *c, const double *aos, void *X, 
 extern "C" int cipher_state_init_sharp(cipher_ctx *c, const int32_t *voxelphase, void *X, void *stream)
 {
     if (!c || !voxelphase || !X) return set_error(CIPHER_E_ARG, "NULL argument");
+    if (c->listed)
+        return set_error(CIPHER_E_UNSUPPORTED, "the device initial state needs a uniform grid; build an adapted "
+                                               "mesh's state on the host (cipher_initial_state_aos)");
     cudaStream_t s = (cudaStream_t)stream;
     int32_t *d_vox = nullptr;
     CUDA_TRY(dev_alloc(&d_vox, (size_t)c->ncells * sizeof(int32_t)), "voxel map");
@@ -822,6 +936,33 @@ extern "C" int cipher_output_fields(cipher_ctx *c, const void *X, const cipher_o
     free(h);
     if (e != cudaSuccess) return cuda_fail(e, "output fields");
     return cipher_ctx_check(c, stream);
+}
+
+extern "C" int cipher_state_transfer(cipher_ctx *dst, void *Xdst, const cipher_ctx *src, const void *Xsrc,
+                                     const int64_t *src0, const int32_t *nsrc, void *stream)
+{
+    if (!dst || !Xdst || !src || !Xsrc || !src0 || !nsrc) return set_error(CIPHER_E_ARG, "NULL argument");
+    if (dst->device != src->device || dst->precision != src->precision || dst->P != src->P || dst->ndp != src->ndp ||
+        dst->S != src->S)
+        return set_error(CIPHER_E_ARG, "the two contexts differ in device, precision or state layout");
+    for (int64_t i = 0; i < dst->ncells; i++)
+        if (nsrc[i] < 1 || src0[i] < 0 || src0[i] + nsrc[i] > src->ncells)
+            return set_error(CIPHER_E_ARG, "transfer plan entry %lld is out of range", (long long)i);
+    cudaStream_t s = (cudaStream_t)stream;
+    int64_t *d_s0 = nullptr;
+    int32_t *d_ns = nullptr;
+    cudaError_t e = dev_alloc(&d_s0, (size_t)dst->ncells * sizeof(int64_t));
+    if (e == cudaSuccess) e = dev_alloc(&d_ns, (size_t)dst->ncells * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_s0, src0, (size_t)dst->ncells * sizeof(int64_t), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_ns, nsrc, (size_t)dst->ncells * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = launch_transfer(layout_args(dst, Xdst), layout_args(src, (void *)Xsrc), d_s0, d_ns, s);
+    if (e == cudaSuccess) e = build_maps(dst, Xdst, s);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    dev_free(d_s0);
+    dev_free(d_ns);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return cuda_fail(e, "state transfer");
+    return CIPHER_OK;
 }
 
 extern "C" int cipher_state_refresh(cipher_ctx *c, void *X, void *stream)

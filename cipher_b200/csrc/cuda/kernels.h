@@ -23,6 +23,21 @@ void pinned_word_free(void *ptr);
 template <typename T>
 inline cudaError_t pinned_word_alloc(T **ptr) { return pinned_word_alloc((void **)ptr); }
 
+/* the faces of a non-uniform (adapted) mesh, per cell: entries
+ * [start[c], start[c+1]) list cell c's faces in the reference's face order
+ * (the order of the mesh's face list).  start == NULL: a uniform grid whose
+ * faces follow from res/per. */
+struct FaceLists {
+    const int32_t *start;        /* [ncells+1] */
+    const int32_t *nbr;          /* [nnz] the other cell of the face; bit 31 set when c is the face's L cell */
+    const int32_t *face;         /* [nnz] face index */
+    const double *ff;            /* [nfaces] 2*(vol/delta of the smaller cell)/(delta_L+delta_R) (src/cipher.c:273-275) */
+    const double *vol, *delta;   /* [ncells] delta^dim and cellgeom */
+    const int32_t *bstart;       /* [ncells+1] boundary faces of each cell */
+    const int32_t *blabel;       /* their labels 1..2*dim */
+};
+constexpr int32_t FACE_SELF_L = (int32_t)0x80000000u;
+
 /* arguments of the phase-field-only RHS on a uniform grid */
 template <typename R>
 struct PfArgs {
@@ -112,6 +127,7 @@ struct GenArgs {
     const double *ex;
     const R *tm;
     double *comp, *mob, *tcond;   /* per-cell scratch: [ncp][stride], [ncp][stride], [stride] */
+    FaceLists fl;                 /* face lists of an adapted mesh (fl.start == NULL: uniform grid) */
     R *fphi;
     double *fdp, *fex;
     R *ftm;
@@ -165,6 +181,7 @@ struct PostArgs {
     uint64_t *maps;               /* face maps rebuilt after the union, or NULL */
     int npf;
     ChemTables chem;              /* with chem.mat set, new phases get SitepotentialExplicit(c0, T) */
+    FaceLists fl;                 /* neighbours of an adapted mesh (fl.start == NULL: uniform grid) */
     int *err;
 };
 
@@ -203,6 +220,9 @@ struct LayoutArgs {
     void *tm;
 };
 cudaError_t launch_aos_to_soa(const LayoutArgs &a, const double *aos, cudaStream_t s);
+/* state of an adapted mesh from the old mesh's state (src0/nsrc: device transfer plan) */
+cudaError_t launch_transfer(const LayoutArgs &dst, const LayoutArgs &src, const int64_t *src0, const int32_t *nsrc,
+                            cudaStream_t s);
 /* cells [c0, c1) of the domain (aos is the whole domain's array) */
 cudaError_t launch_aos_to_soa_range(const LayoutArgs &a, const double *aos, int64_t c0, int64_t c1, cudaStream_t s);
 
@@ -222,6 +242,7 @@ cudaError_t launch_soa_to_aos_range(const LayoutArgs &a, double *aos, int includ
 /* what the batch driver needs to know of a context (context.cu) */
 struct CtxInfo {
     int device, precision, dim, general, single, P;
+    int listed;                   /* an adapted mesh (face lists) */
     int64_t ncells;
     int res[3];
 };

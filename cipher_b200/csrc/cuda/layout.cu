@@ -145,4 +145,50 @@ cudaError_t launch_init_sharp(const InitArgs &a, cudaStream_t s)
     return cudaGetLastError();
 }
 
+/* ------------------------------------------------------------------ */
+/* state transfer after a mesh adaptation                               */
+/* ------------------------------------------------------------------ */
+
+/* new cell i takes the mean of old cells [src0[i], src0[i] + nsrc[i]): the
+ * finite-volume transfer of the forest (children copy their parent, a
+ * coarsened family averages into the parent; sums in cell order, then one
+ * division, as the host transfer forms them).  The sets are copied from the
+ * first old cell (a coarsened family shares its set). */
+template <typename R>
+__global__ void __launch_bounds__(256) k_transfer(const LayoutArgs dst, const LayoutArgs src, const int64_t *src0,
+                                                  const int32_t *nsrc)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= dst.ncells) return;
+    const int64_t s0 = src0[i];
+    const int k = nsrc[i];
+    for (int q = 0; q <= dst.P; q++) dst.as[q * dst.stride + i] = src.as[q * src.stride + s0];
+    auto mean = [&](auto get) {
+        if (k == 1) return get(s0);
+        double acc = 0.0;
+        for (int j = 0; j < k; j++) acc += get(s0 + j);
+        return acc / (double)k;
+    };
+    const R *sp = (const R *)src.phi;
+    R *dp_ = (R *)dst.phi;
+    for (int g = 0; g < dst.P; g++)
+        dp_[g * dst.stride + i] = (R)mean([&](int64_t c) { return (double)sp[g * src.stride + c]; });
+    for (int d = 0; d < dst.D; d++)
+        dst.dp[d * dst.stride + i] = mean([&](int64_t c) { return src.dp[d * src.stride + c]; });
+    for (int e = 0; e < dst.E; e++)
+        dst.ex[e * dst.stride + i] = mean([&](int64_t c) { return src.ex[e * src.stride + c]; });
+    const R *st = (const R *)src.tm;
+    ((R *)dst.tm)[i] = (R)mean([&](int64_t c) { return (double)st[c]; });
+}
+
+cudaError_t launch_transfer(const LayoutArgs &dst, const LayoutArgs &src, const int64_t *src0, const int32_t *nsrc,
+                            cudaStream_t s)
+{
+    if (dst.ncells < 1) return cudaSuccess;
+    const unsigned blocks = (unsigned)((dst.ncells + 255) / 256);
+    if (dst.real_bytes == 8) k_transfer<double><<<blocks, 256, 0, s>>>(dst, src, src0, nsrc);
+    else k_transfer<float><<<blocks, 256, 0, s>>>(dst, src, src0, nsrc);
+    return cudaGetLastError();
+}
+
 }  // namespace cipher

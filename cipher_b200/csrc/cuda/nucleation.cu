@@ -104,6 +104,9 @@ extern "C" int cipher_nucleation_create(cipher_ctx *c, int nsites, const int32_t
         return cipher_set_error(CIPHER_E_ARG, "bad nucleation arguments");
     *out = NULL;
     CtxInfo info = ctx_info(c);
+    if (info.listed)
+        return cipher_set_error(CIPHER_E_UNSUPPORTED, "nucleation sites average over uniform cells; the context's "
+                                                      "mesh is adapted");
     for (int i = 0; i < nsites; i++)
         if (sitenucleus[i] < 0 || sitenucleus[i] >= nnuclei || sitephase[i] < 0)
             return cipher_set_error(CIPHER_E_ARG, "site %d: bad nucleus or phase", i);

@@ -118,36 +118,47 @@ __device__ __forceinline__ void post_union_cell(const PostArgs<R> &a, int64_t c)
     uint16_t sup[PM], tmp[PM];
     for (int k = 0; k < ns; k++) sup[k] = a.pruned[(int64_t)(1 + k) * S + c];
 
-    const int res[3] = {a.res[0], a.res[1], a.res[2]};
-    const int64_t st[3] = {1, (int64_t)res[0], (int64_t)res[0] * res[1]};
-    int co[3];
-    co[0] = (int)(c % res[0]);
-    co[1] = DIM > 1 ? (int)((c / res[0]) % res[1]) : 0;
-    co[2] = DIM > 2 ? (int)(c / ((int64_t)res[0] * res[1])) : 0;
+    /* union with the neighbours' pruned sets: over the faces of the cell
+     * (src/cipher.c:930-945); the union does not depend on their order */
+    auto unite = [&](int64_t nb) -> bool {
+        if (nb == c) return true;
+        int nbn = a.pruned[nb];
+        if (nbn > a.P) nbn = a.P;
+        int m = merge_union<PM>(sup, ns, a.pruned, S, nb, nbn, tmp, a.P);
+        if (m > a.P) {
+            atomicOr(a.err, ERR_CAP);
+            return false;
+        }
+        for (int k = 0; k < m; k++) sup[k] = tmp[k];
+        ns = m;
+        return true;
+    };
+    if (a.fl.start) {
+        for (int32_t e = a.fl.start[c]; e < a.fl.start[c + 1]; e++)
+            if (!unite(a.fl.nbr[e] & 0x7fffffff)) return;
+    } else {
+        const int res[3] = {a.res[0], a.res[1], a.res[2]};
+        const int64_t st[3] = {1, (int64_t)res[0], (int64_t)res[0] * res[1]};
+        int co[3];
+        co[0] = (int)(c % res[0]);
+        co[1] = DIM > 1 ? (int)((c / res[0]) % res[1]) : 0;
+        co[2] = DIM > 2 ? (int)(c / ((int64_t)res[0] * res[1])) : 0;
 #pragma unroll
-    for (int d = 0; d < DIM; d++) {
+        for (int d = 0; d < DIM; d++) {
 #pragma unroll
-        for (int side = 0; side < 2; side++) {
-            int64_t nb;
-            if (side == 0) {
-                if (co[d] > 0) nb = c - st[d];
-                else if (a.per[d] && res[d] > 1) nb = c + (int64_t)(res[d] - 1) * st[d];
-                else continue;
-            } else {
-                if (co[d] < res[d] - 1) nb = c + st[d];
-                else if (a.per[d] && res[d] > 1) nb = c - (int64_t)(res[d] - 1) * st[d];
-                else continue;
+            for (int side = 0; side < 2; side++) {
+                int64_t nb;
+                if (side == 0) {
+                    if (co[d] > 0) nb = c - st[d];
+                    else if (a.per[d] && res[d] > 1) nb = c + (int64_t)(res[d] - 1) * st[d];
+                    else continue;
+                } else {
+                    if (co[d] < res[d] - 1) nb = c + st[d];
+                    else if (a.per[d] && res[d] > 1) nb = c - (int64_t)(res[d] - 1) * st[d];
+                    else continue;
+                }
+                if (!unite(nb)) return;
             }
-            if (nb == c) continue;
-            int nbn = a.pruned[nb];
-            if (nbn > a.P) nbn = a.P;
-            int m = merge_union<PM>(sup, ns, a.pruned, S, nb, nbn, tmp, a.P);
-            if (m > a.P) {
-                atomicOr(a.err, ERR_CAP);
-                return;
-            }
-            for (int k = 0; k < m; k++) sup[k] = tmp[k];
-            ns = m;
         }
     }
 

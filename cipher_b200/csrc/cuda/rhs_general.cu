@@ -210,10 +210,13 @@ __global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> 
     const int64_t S = a.stride;
     const int ncp = a.ncp, ndp = a.ndp, SP = a.SP;
     const double PI = CIPHER_PI_D;
-    int co[3];
-    co[0] = (int)(c % a.res[0]);
-    co[1] = DIM > 1 ? (int)((c / a.res[0]) % a.res[1]) : 0;
-    co[2] = DIM > 2 ? (int)(c / ((int64_t)a.res[0] * a.res[1])) : 0;
+    const bool listed = a.fl.start != nullptr;   /* an adapted mesh: faces from the lists */
+    int co[3] = {0, 0, 0};
+    if (!listed) {
+        co[0] = (int)(c % a.res[0]);
+        co[1] = DIM > 1 ? (int)((c / a.res[0]) % a.res[1]) : 0;
+        co[2] = DIM > 2 ? (int)(c / ((int64_t)a.res[0] * a.res[1])) : 0;
+    }
 
     uint16_t ids[PM];
     double phi[PM], h[PM], lap[PM], pf[PM];
@@ -227,11 +230,25 @@ __global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> 
     for (int g = 0; g < n; g++) lap[g] = 0.0;
 
     /* ---- faces in the reference's face order (src/cipher.c:235-317) ---- */
+    const int f0 = listed ? a.fl.start[c] : 0, f1 = listed ? a.fl.start[c + 1] : 3 * DIM;
+    const double vol_c = listed ? a.fl.vol[c] : 0.0;
 #pragma unroll 1
-    for (int f = 0; f < 3 * DIM; f++) {
-        const int64_t nb = gen_face_nb(a.res, a.per, c, co, f, DIM);
-        if (nb < 0) continue;
-        const bool self_L = f >= DIM && f < 2 * DIM;
+    for (int f = f0; f < f1; f++) {
+        int64_t nb;
+        bool self_L;
+        double ffv = 0.0;
+        if (listed) {
+            const int32_t v = a.fl.nbr[f];
+            nb = v & 0x7fffffff;
+            self_L = (v & FACE_SELF_L) != 0;
+            ffv = a.fl.ff[a.fl.face[f]];
+        } else {
+            nb = gen_face_nb(a.res, a.per, c, co, f, DIM);
+            if (nb < 0) continue;
+            self_L = f >= DIM && f < 2 * DIM;
+        }
+        /* ff*x/vol of this cell, as the reference forms it (src/cipher.c:281-282) */
+        auto fdiv = [&](double x) { return listed ? (ffv * x) / vol_c : face_div(a, x); };
         const int64_t cl = self_L ? c : nb, cr = self_L ? nb : c;
         const int nn = a.as[nb];
         if (nn < 1 || nn > a.P) continue;          /* that cell's own thread raises the flag */
@@ -243,8 +260,8 @@ __global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> 
                 const uint16_t b = a.as[(int64_t)(1 + j) * S + nb];
                 if (ids[i] == b) {
                     const double pn = (double)a.phi[(int64_t)j * S + nb];
-                    if (self_L) lap[i] += face_div(a, pn - phi[i]);
-                    else lap[i] -= face_div(a, phi[i] - pn);
+                    if (self_L) lap[i] += fdiv(pn - phi[i]);
+                    else lap[i] -= fdiv(phi[i] - pn);
                     i++;
                     j++;
                 } else if (ids[i] < b) {
@@ -275,8 +292,8 @@ __global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> 
             for (int d = 0; d < ndp; d++) dmu[d] = a.dp[(int64_t)d * S + cr] - a.dp[(int64_t)d * S + cl];
             matvec(fl, MB, dmu, ndp);
             for (int d = 0; d < ndp; d++) {
-                if (self_L) ldp[d] += face_div(a, fl[d]);
-                else ldp[d] -= face_div(a, fl[d]);
+                if (self_L) ldp[d] += fdiv(fl[d]);
+                else ldp[d] -= fdiv(fl[d]);
             }
         }
         /* heat flux */
@@ -284,25 +301,30 @@ __global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> 
             const double tl = a.tcond[cl], tr = a.tcond[cr];
             if (fabs(tl) > 1e-32 && fabs(tr) > 1e-32) {
                 const double ft = 2.0 * tl * tr / (tl + tr) * ((double)a.tm[cr] - (double)a.tm[cl]);
-                if (self_L) ltm += face_div(a, ft);
-                else ltm -= face_div(a, ft);
+                if (self_L) ltm += fdiv(ft);
+                else ltm -= fdiv(ft);
             }
         }
     }
 
     /* ---- boundary faces (src/cipher.c:319-389) ---- */
     if (a.nbcs) {
-        const double dc = a.delta;
+        const double dc = listed ? a.fl.delta[c] : a.delta;
         const double cf = 1.0 / ipow(dc, 2);
         const double tcc = a.tcond ? a.tcond[c] : 0.0;
+        const int q0 = listed ? a.fl.bstart[c] : 0, q1 = listed ? a.fl.bstart[c + 1] : 2 * DIM;
         for (int b = 0; b < a.nbcs; b++) {
             const DevBC &bc = a.bcs[b];
 #pragma unroll 1
-            for (int q = 0; q < 2 * DIM; q++) {
-                const int d = q >> 1;
-                if (a.per[d]) continue;
-                const bool on = (q & 1) ? co[d] == a.res[d] - 1 : co[d] == 0;
-                if (!on || bc.label != 2 * d + 1 + (q & 1)) continue;
+            for (int q = q0; q < q1; q++) {
+                if (listed) {
+                    if (bc.label != a.fl.blabel[q]) continue;
+                } else {
+                    const int d = q >> 1;
+                    if (a.per[d]) continue;
+                    const bool on = (q & 1) ? co[d] == a.res[d] - 1 : co[d] == 0;
+                    if (!on || bc.label != 2 * d + 1 + (q & 1)) continue;
+                }
                 double fd[CIPHER_MAXCP];
                 for (int k = 0; k < CIPHER_MAXCP; k++) fd[k] = 0.0;
                 if (bc.chem_type != CIPHER_BC_NONE) {

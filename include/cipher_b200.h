@@ -120,6 +120,46 @@ int cipher_mesh_uniform(const cipher_problem *p, int slab_lo, int slab_hi, ciphe
 int cipher_mesh_grid(const cipher_problem *p, cipher_mesh **out);
 void cipher_mesh_free(cipher_mesh *m);
 
+/* ------------------------------------------------------------------ */
+/* adaptive meshes: a quadtree / octree forest over a brick of blocks  */
+/* (the reference's p4est forest, src/cipher.c:1149-1159; its adaptation */
+/*  src/cipher.c:1365-1586 and 1607-1829)                              */
+/* ------------------------------------------------------------------ */
+
+typedef struct cipher_forest cipher_forest;
+
+/* nblocks[d] blocks per direction; leaves between levels lmin and lmax (a
+ * level-l leaf spans 2^(lmax-l) finest cells, so the finest grid, which is
+ * the grid of voxel maps and of cell_global, has nblocks[d]*2^lmax cells);
+ * uniform at level linit to start with.  size = physical extent (NULL: one
+ * unit per finest cell). */
+int cipher_forest_create(int dim, const int32_t *nblocks, int lmin, int lmax, int linit, const int32_t *periodic,
+                         const double *size, cipher_forest **out);
+void cipher_forest_destroy(cipher_forest *f);
+int64_t cipher_forest_nleaves(const cipher_forest *f);
+/* per leaf: level and lower corner on the finest grid (corner[3*i+d]); either may be NULL */
+int cipher_forest_leaves(const cipher_forest *f, int32_t *level, int32_t *corner);
+int cipher_forest_resolution(const cipher_forest *f, int32_t *res);
+/* the reference's marks (src/cipher.c:1380-1386): +1 (refine) where a leaf's
+ * active set holds more than one phase, -1 (coarsen) elsewhere; X is the
+ * reference AoS state of the leaves */
+int cipher_forest_mark_active(const cipher_forest *f, const double *X, int ndof, int8_t *mark);
+/* adapt by marks (+1 refine once, -1 coarsen a whole family of siblings, 0
+ * keep) within [lmin, lmax], then 2:1 face balance; with Xold (AoS, ndof
+ * doubles per leaf) a family whose first as_size dofs (the active set)
+ * differ is kept.  The transfer plan is kept for the two calls below. */
+int cipher_forest_adapt(cipher_forest *f, const int8_t *mark, const double *Xold, int ndof, int as_size);
+/* new leaf i takes the mean of old leaves [src0[i], src0[i] + nsrc[i]) */
+int cipher_forest_transfer_plan(const cipher_forest *f, int64_t *src0, int32_t *nsrc);
+/* the finite-volume transfer of an AoS state (DMForestTransferVec): children
+ * copy their parent, a coarsened family's mean goes to the parent */
+int cipher_forest_transfer_aos(const cipher_forest *f, const double *Xold, int ndof, double *Xnew);
+/* the mesh of the leaves: cells in leaf order with cellgeom = vol^(1/dim),
+ * every interior face once (conforming faces, and the hanging faces between
+ * a coarse leaf and each finer neighbour), boundary faces of non-periodic
+ * sides labelled 2d+1 (low) / 2d+2 (high) */
+int cipher_forest_mesh(const cipher_forest *f, cipher_mesh **out);
+
 /* SetUpProblem active sets / phi / T in the reference AoS layout (host) */
 int cipher_initial_state_aos(const cipher_problem *p, const cipher_mesh *m, double *X);
 
@@ -193,6 +233,15 @@ int cipher_ctx_check(cipher_ctx *c, void *stream);
  * material's temperature0, then the face maps and the chemistry of
  * cipher_chem_init.  Returns CIPHER_E_CAP when a set exceeds P. */
 int cipher_state_init_sharp(cipher_ctx *c, const int32_t *voxelphase, void *X, void *stream);
+
+/* after a forest adaptation: Xdst (context dst, the new mesh) from Xsrc
+ * (context src, the old mesh) by the forest's transfer plan (host arrays,
+ * cipher_forest_transfer_plan): children copy their parent, a coarsened
+ * family's mean goes to the parent (DMForestTransferVec,
+ * src/cipher.c:1433).  Equal to cipher_forest_transfer_aos in FP64.
+ * Synchronises `stream`. */
+int cipher_state_transfer(cipher_ctx *dst, void *Xdst, const cipher_ctx *src, const void *Xsrc,
+                          const int64_t *src0, const int32_t *nsrc, void *stream);
 
 /* rebuild the face maps of X from its active sets, for callers that write
  * the AS planes themselves (the library's own producers keep them current) */

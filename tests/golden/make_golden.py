@@ -59,6 +59,43 @@ ALLOY_INTERP_CASES = [
 ]
 
 
+# adapted meshes: (name, kind, dim, res, a, ncp, nprecip, cap, seed, features,
+# lmin, lmax, adapt iterations, diffuse start, reference steps).  kind 0:
+# grain growth with a = ngrains; kind 1: alloy with a = model id.  The forest
+# starts at the finest level (res), the state is adapted `iterations` times
+# by the reference's marks (the initcoarsen loop of src/cipher.c:1365), then
+# evolved by `steps` explicit reference steps on the adapted mesh.
+AMR_CASES = [
+    ("amr2d_gg_diffuse", 0, 2, [32, 32], 6, 1, 0, 8, 3, 0, 2, 5, 3, 1, 0),
+    ("amr3d_gg_sharp", 0, 3, [16, 16, 16], 4, 1, 0, 12, 4, 0, 1, 4, 2, 0, 0),
+    ("amr2d_alloy2sl_walls", 1, 2, [32, 32], 2, 3, 3, 8, 4, 0x28, 2, 5, 2, 0, 2),
+]
+
+
+def build_amr(kind, dim, r0, r1, r2, a, ncp, npr, cap, seed, feats, lmin, lmax, iters, diffuse, steps=0):
+    """the problem, forest and mesh of an adapted-mesh case (the forest is
+    rebuilt deterministically from the problem's initial state)"""
+    res = [r0, r1, r2][:dim]
+    if kind == 0:
+        P = cb.Problem.grain_growth(dim, res, a, cap, seed)
+    else:
+        P = cb.Problem.alloy(dim, res, {0: "quadratic", 1: "calphaddis", 2: "calphad2sl"}[a], ncp, npr, cap, seed,
+                             feats)
+    nb = [r // (1 << lmax) for r in res]
+    F = cb.Forest(dim, nb, lmin, lmax, periodic=tuple(P.s.periodic[d] for d in range(3)))
+    M = F.mesh(P)
+    if kind == 0:
+        X = cb.diffuse_state_aos(P, M, 4.0) if diffuse else cb.initial_state_aos(P, M)
+    else:
+        X = oracle.port_initial_state(P, M)
+    for _ in range(iters):
+        F.adapt(F.mark_active(X), X, P.aos.pf_offset)
+        X = F.transfer_aos(X)
+        M = F.mesh(P)
+    build_amr.state = X
+    return P, F, M
+
+
 def build_alloy(dim, res, model, ncp, nprecip, cap, seed, features):
     P = cb.Problem.alloy(dim, res, model, ncp, nprecip, cap, seed, features)
     M = cb.Mesh(P)
@@ -101,6 +138,23 @@ def main(only=None):
     def wanted(name):
         return not only or name in only
 
+    for name, kind, dim, res, a, ncp, npr, cap, seed, feats, lmin, lmax, iters, diffuse, steps in AMR_CASES:
+        if not wanted(name):
+            continue
+        r = list(res) + [1] * (3 - len(res))
+        meta = [kind, dim] + r + [a, ncp, npr, cap, seed, feats, lmin, lmax, iters, diffuse]
+        P, F, M = build_amr(*meta)
+        X = build_amr.state
+        with oracle.RefOracle(P, M) as R:
+            if steps:
+                X = evolve_with_reference(P, M, R, X, steps)
+            F_ = R.rhs(X)
+            Xp = X.copy()
+            assert R.poststep(Xp) == 0
+        lev, _ = F.leaves()
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), X=X, F=F_, Xpost=Xp, meta=np.array(meta),
+                            levels=lev)
+        print(name, X.shape, "levels", np.bincount(lev), "max|F|", np.abs(F_).max(), "mean n", X[:, 0].mean())
     for name, dim, res, ng, nitf_cap, seed, nitf, feats in MULTI_CASES:
         if not wanted(name):
             continue
