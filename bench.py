@@ -596,6 +596,16 @@ def run_cipher(args, rank, world, local_rank):
     sl = slice(Lay.pf_offset, Lay.pf_offset + Pcap)
     rel_err = float(np.abs(Fb[:, sl] - Fa[:, sl]).max() / np.abs(Fa[:, sl]).max())
     del Xc, Fc, Fa, Fb
+    # the FP64 closed form against the FP64 reference-order kernel on the FP64 state
+    Fref, Fcf = c64.alloc_state(), c64.alloc_state()
+    c64.rhs(0.0, X64d, Fref)
+    c64.set_rhs_form("closed")
+    c64.rhs(0.0, X64d, Fcf)
+    c64.set_rhs_form("reference")
+    c64.check()
+    Fa, Fb = c64.to_aos(Fref), c64.to_aos(Fcf)
+    rel_err_cf = float(np.abs(Fb[:, sl] - Fa[:, sl]).max() / np.abs(Fa[:, sl]).max())
+    del Fref, Fcf, Fa, Fb
 
     for _ in range(args.warmup):
         c64.rhs(0.0, X64d, F64d)
@@ -612,11 +622,20 @@ def run_cipher(args, rank, world, local_rank):
     barrier()
     tot32, per32 = time_launches(lambda: c32.rhs(0.0, X32d, F32d), args.steps, stream)
     barrier()
+    # FP64 closed form (the mixed kernel's algebra on the FP64 state)
+    c64.set_rhs_form("closed")
+    for _ in range(args.warmup):
+        c64.rhs(0.0, X64d, F64d)
+    barrier()
+    totcf, percf = time_launches(lambda: c64.rhs(0.0, X64d, F64d), args.steps, stream)
+    barrier()
+    c64.set_rhs_form("reference")
     clk.stop()
     c64.check()
     c32.check()
     tot64 = max_over_ranks(tot64)
     tot32 = max_over_ranks(tot32)
+    totcf = max_over_ranks(totcf)
 
     # end to end through the host-buffer entry point (reference AoS layout,
     # pinned host memory, copies inside the timed region)
@@ -643,6 +662,8 @@ def run_cipher(args, rank, world, local_rank):
     peak, peak_src = hbm_peak()
     avg32 = statistics.mean(per32) / 1e3
     avg64 = statistics.mean(per64) / 1e3
+    valuecf = ncells * args.steps * world / (totcf / 1e3)
+    avgcf = statistics.mean(percf) / 1e3
     b32 = survey_bytes_per_cell(Pcap, 0, 0, 4) * ncells
     b64 = survey_bytes_per_cell(Pcap, 0, 0, 8) * ncells
     e32 = state_exact_bytes(nsum, ncells, Pcap, 4)
@@ -678,13 +699,17 @@ def run_cipher(args, rank, world, local_rank):
         "fp64": {"value": value64, "unit": UNIT, "ms_per_step": tot64 / args.steps,
                  "roofline_frac": ach64 / peak, "algorithmic_bytes_per_launch": b64,
                  "state_exact_roofline_frac": e64 / avg64 / 1e9 / peak},
+        "fp64_closed_form": {"value": valuecf, "unit": UNIT, "ms_per_step": totcf / args.steps,
+                             "roofline_frac": b64 / avgcf / 1e9 / peak, "rel_err_vs_reference_order": rel_err_cf,
+                             "kernel": "k_rhs_pf_items<3,int,double>"},
         "mixed_speedup_vs_fp64": value / value64,
+        "mixed_speedup_vs_fp64_closed_form": value / valuecf,
         "mixed_rel_err_vs_fp64": rel_err,
         "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak,
                      "traffic": tr32, "peak_source": peak_src, "algorithmic_bytes_per_launch": b32,
                      "bytes_per_cell_update": b32 // ncells, "fp64_format_frac": b64 / avg32 / 1e9 / peak,
                      "state_exact_bytes_per_launch": e32, "state_exact_frac": e32 / avg32 / 1e9 / peak,
-                     "kernel": "k_rhs_pf_mixed_items<3,int>"},
+                     "kernel": "k_rhs_pf_items<3,int,float>"},
         "cpu_baseline": cpu,
         "e2e": {"value": ncells * e2e_steps * world / (tot_e2e / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": aos_bytes, "d2h_bytes_per_step": aos_bytes,

@@ -34,6 +34,7 @@ ALLOY_SEGREGATION, ALLOY_ITF_MOBILITY, ALLOY_ACTIVATION, ALLOY_THERMAL = 0x01, 0
 ALLOY_SOURCES, ALLOY_WALLS, ALLOY_TEMP_RATE, ALLOY_MIXED_MODELS = 0x10, 0x20, 0x40, 0x80
 ALLOY_ALL = 0x7F
 GG_ACTIVATION, GG_WIDTHS = 0x01, 0x02
+RHS_REFERENCE_ORDER, RHS_CLOSED_FORM = 0, 1
 
 OK = 0
 E_ARG, E_NOMEM, E_CAP, E_NONFINITE, E_CUDA, E_TIMEOUT, E_UNSUPPORTED, E_STEP = range(1, 9)
@@ -185,6 +186,7 @@ _SIGNATURES = [
     ("cipher_last_error", C.c_char_p, []),
     ("cipher_abi_sizes", C.c_int, [C.POINTER(C.c_int64), C.c_int]),
     ("cipher_pool_trim", C.c_int, [C.c_int]),
+    ("cipher_ctx_set_rhs_form", C.c_int, [C.c_void_p, C.c_int]),
     ("cipher_forest_create", C.c_int, [C.c_int, C.POINTER(C.c_int32), C.c_int, C.c_int, C.c_int,
                                        C.POINTER(C.c_int32), C.POINTER(C.c_double), C.POINTER(C.c_void_p)]),
     ("cipher_forest_destroy", None, [C.c_void_p]),

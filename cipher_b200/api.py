@@ -338,6 +338,12 @@ class Context:
         L.check(self._lib.cipher_waxpy(self.ptr, C.c_void_p(_ptr(Y)), C.c_void_p(_ptr(X)), float(a),
                                        C.c_void_p(_ptr(F)), _stream_handle(stream)), "cipher_waxpy")
 
+    def set_rhs_form(self, form: str):
+        """FP64 single-interface kernel: "reference" (bit-identical to the
+        reference, the default) or "closed" (the closed form in FP64)"""
+        f = {"reference": L.RHS_REFERENCE_ORDER, "closed": L.RHS_CLOSED_FORM}[form]
+        L.check(self._lib.cipher_ctx_set_rhs_form(self.ptr, f), "cipher_ctx_set_rhs_form")
+
     def check(self, stream=None):
         L.check(self._lib.cipher_ctx_check(self.ptr, _stream_handle(stream)), "cipher_ctx_check")
 

@@ -94,6 +94,7 @@ struct cipher_ctx {
     /* an adapted (non-uniform) mesh: per-cell face lists, face factors and
      * cell volumes on the device (FaceLists); 0 on uniform grids */
     int listed;
+    int rhs_form;                 /* CIPHER_RHS_*: FP64 single-interface kernel choice */
     int32_t *d_fl_start, *d_fl_nbr, *d_fl_face, *d_fl_bstart, *d_fl_blabel;
     double *d_fl_ff, *d_fl_vol, *d_fl_delta;
     int32_t *d_itflist;
@@ -378,8 +379,9 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
     L.precision = precision;
     int64_t off = 0;
     L.as_offset = off; off = align_up(off + (int64_t)(c->P + 1) * c->stride * 2, 256);
-    L.map_offset = off; L.map_planes = c->listed ? 0 : 2 * c->dim;
-    off = align_up(off + (int64_t)L.map_planes * c->stride * 8, 256);
+    /* face maps: one 32-bit word per slot (uniform grids only) */
+    L.map_offset = off; L.map_planes = c->listed ? 0 : c->P;
+    off = align_up(off + (int64_t)L.map_planes * c->stride * 4, 256);
     L.pf_offset = off; off = align_up(off + (int64_t)c->P * c->stride * rb, 256);
     L.dp_offset = off; off = align_up(off + (int64_t)c->ndp * c->stride * 8, 256);
     L.ex_offset = off; off = align_up(off + (int64_t)L.ex_size * c->stride * 8, 256);
@@ -570,7 +572,7 @@ static PfArgs<R> pf_args(const cipher_ctx *c, const void *X, void *F)
     a.itflist = c->d_itflist;
     a.itfs = c->d_itfs;
     a.as = (const uint16_t *)(x + c->lay.as_offset);
-    a.maps = (const uint64_t *)(x + c->lay.map_offset);
+    a.maps = (const uint32_t *)(x + c->lay.map_offset);
     a.phi = (const R *)(x + c->lay.pf_offset);
     a.tm = (const R *)(x + c->lay.tm_offset);
     a.fphi = (R *)(f + c->lay.pf_offset);
@@ -649,11 +651,24 @@ extern "C" int cipher_rhs(cipher_ctx *c, double t, const void *X, void *F, void 
     if (c->general) {
         if (c->precision == CIPHER_PREC_FP64) e = launch_rhs_general(gen_args<double>(c, X, F), c->dim, s);
         else e = launch_rhs_general(gen_args<float>(c, X, F), c->dim, s);
+    } else if (c->precision == CIPHER_PREC_FP64) {
+        if (c->rhs_form == CIPHER_RHS_CLOSED_FORM && c->single)
+            e = launch_rhs_items_fp64(pf_args<double>(c, X, F), c->dim, s);
+        else
+            e = launch_rhs_phasefield(pf_args<double>(c, X, F), c->dim, s);
     } else {
-        if (c->precision == CIPHER_PREC_FP64) e = launch_rhs_phasefield(pf_args<double>(c, X, F), c->dim, s);
-        else e = launch_rhs_phasefield(pf_args<float>(c, X, F), c->dim, s);
+        e = launch_rhs_phasefield(pf_args<float>(c, X, F), c->dim, s);
     }
     if (e != cudaSuccess) return cuda_fail(e, "rhs launch");
+    return CIPHER_OK;
+}
+
+extern "C" int cipher_ctx_set_rhs_form(cipher_ctx *c, int form)
+{
+    if (!c) return set_error(CIPHER_E_ARG, "NULL context");
+    if (form != CIPHER_RHS_REFERENCE_ORDER && form != CIPHER_RHS_CLOSED_FORM)
+        return set_error(CIPHER_E_ARG, "unknown RHS form %d", form);
+    c->rhs_form = form;
     return CIPHER_OK;
 }
 
@@ -670,7 +685,7 @@ static PostArgs<R> post_args(const cipher_ctx *c, void *X)
     a.S = c->S;
     a.as = (uint16_t *)(x + c->lay.as_offset);
     /* adapted meshes have no face maps (their general kernels merge sets) */
-    a.maps = c->lay.map_planes ? (uint64_t *)(x + c->lay.map_offset) : nullptr;
+    a.maps = c->lay.map_planes ? (uint32_t *)(x + c->lay.map_offset) : nullptr;
     a.fl = face_lists(c);
     a.npf = c->npf;
     a.phi = (R *)(x + c->lay.pf_offset);

@@ -64,7 +64,7 @@ struct PfArgs {
     const int32_t *itflist;
     const DevInterface *itfs;
     const uint16_t *as;
-    const uint64_t *maps;         /* [2*dim][stride] face maps (cipher_b200.h) */
+    const uint32_t *maps;         /* [P][stride] face maps: one word per slot (cipher_b200.h) */
     const R *phi;
     const R *tm;
     R *fphi;
@@ -73,6 +73,8 @@ struct PfArgs {
 };
 
 cudaError_t launch_rhs_phasefield(const PfArgs<double> &a, int dim, cudaStream_t s);
+/* the closed-form single-interface kernel in FP64 (rhs_mixed.cu) */
+cudaError_t launch_rhs_items_fp64(const PfArgs<double> &a, int dim, cudaStream_t s);
 cudaError_t launch_rhs_phasefield(const PfArgs<float> &a, int dim, cudaStream_t s);
 
 /* many independent domains in one launch: domain i owns tiles
@@ -178,7 +180,7 @@ struct PostArgs {
     double *ex;
     const R *tm;
     uint16_t *pruned;             /* scratch: pruned sets, [P+1][stride] */
-    uint64_t *maps;               /* face maps rebuilt after the union, or NULL */
+    uint32_t *maps;               /* face maps rebuilt after the union, or NULL */
     int npf;
     ChemTables chem;              /* with chem.mat set, new phases get SitepotentialExplicit(c0, T) */
     FaceLists fl;                 /* neighbours of an adapted mesh (fl.start == NULL: uniform grid) */
@@ -199,11 +201,16 @@ cudaError_t launch_build_maps_range(const PostArgs<float> &a, int dim, int64_t c
 template <typename R>
 struct BatchPost {
     const PostArgs<R> *args;      /* [n] device */
-    const int64_t *block_start;   /* [n+1] device */
+    const int64_t *block_start;   /* [n+1] device: blocks of 256 cells (pruning) */
     const int *active;            /* [n] device */
     int n;
     int64_t total;
+    const int64_t *row_start;     /* [n+1] device: row blocks (4 rows of 32 cells; union and face maps) */
+    int64_t row_total;
+    int pmax;                     /* largest P of the batch (shared-memory staging) */
 };
+/* row blocks of a uniform grid (union and face-map kernels) */
+int64_t post_row_blocks(const int *res);
 cudaError_t launch_poststep_batched(const BatchPost<double> &b, int dim, cudaStream_t s);
 cudaError_t launch_poststep_batched(const BatchPost<float> &b, int dim, cudaStream_t s);
 

@@ -9,7 +9,7 @@
  * memory, one column per thread (SlotColumns).  Which neighbour slot holds
  * each own phase (SetIntersection, src/utility.c:168-190, with the gate of
  * src/cipher.c:277) is read from the state's face maps, built from the sets
- * when they change (poststep.cu: build_maps_cell), so the RHS does no set
+ * when they change (poststep.cu: build_maps_row), so the RHS does no set
  * merging at all.
  *
  * Launch geometry: blocks of BX x BY cells in (x, y), grid
@@ -182,13 +182,9 @@ __device__ __forceinline__ int load_and_gather(const PfArgs<R> &a, const CellInd
         return 0;
     }
     if (n == 0) return 0;
-    /* the face maps first: independent loads, one per face */
-    uint64_t w[3 * DIM];
+    int64_t nbs[3 * DIM];
 #pragma unroll
-    for (int f = 0; f < 3 * DIM; f++) {
-        const int64_t nb = face_nb<DIM, R>(a, ci, f);
-        w[f] = nb >= 0 ? __ldg(&a.maps[(int64_t)face_dir<DIM>(f) * S + c]) : ~0ull;
-    }
+    for (int f = 0; f < 3 * DIM; f++) nbs[f] = face_nb<DIM, R>(a, ci, f);
     for (int g0 = 0; g0 < n; g0 += 4) {
         R tp[4];
         uint16_t ti[4];
@@ -208,23 +204,29 @@ __device__ __forceinline__ int load_and_gather(const PfArgs<R> &a, const CellInd
             }
         }
     }
+    /* four slots at a time: their face-map words, then for each face in the
+     * reference's order the matched neighbour slots (loads issue together).
+     * Each slot still receives its faces' contributions in face order. */
+    for (int i0 = 0; i0 < n; i0 += 4) {
+        uint32_t w[4];
 #pragma unroll
-    for (int f = 0; f < 3 * DIM; f++) {
-        if (w[f] == ~0ull) continue;
-        const int64_t nb = face_nb<DIM, R>(a, ci, f);
-        const bool cell_is_L = f >= DIM && f < 2 * DIM;
-        /* the matched neighbour slots four at a time: loads issue together */
-        for (int i0 = 0; i0 < n; i0 += 4) {
+        for (int k = 0; k < 4; k++) w[k] = i0 + k < n ? __ldg(&a.maps[(int64_t)(i0 + k) * S + c]) : ~0u;
+#pragma unroll
+        for (int f = 0; f < 3 * DIM; f++) {
+            const int64_t nb = nbs[f];
+            if (nb < 0) continue;
+            const bool cell_is_L = f >= DIM && f < 2 * DIM;
+            const unsigned sh = 4u * (unsigned)face_dir<DIM>(f);
             R pn[4];
 #pragma unroll
             for (int k = 0; k < 4; k++) {
-                const int j = (int)((w[f] >> (4 * (i0 + k))) & 15u);
+                const int j = (int)((w[k] >> sh) & 15u);
                 pn[k] = (i0 + k < n && j < a.P) ? __ldg(&a.phi[(int64_t)j * S + nb]) : (R)0;
             }
 #pragma unroll
             for (int k = 0; k < 4; k++) {
                 const int i = i0 + k;
-                const int j = (int)((w[f] >> (4 * i)) & 15u);
+                const int j = (int)((w[k] >> sh) & 15u);
                 if (i < n && j < a.P) {
                     if (cell_is_L) sc.LAP(i) += face_term<R, EXACT>(a, pn[k] - sc.PHI(i));
                     else sc.LAP(i) -= face_term<R, EXACT>(a, sc.PHI(i) - pn[k]);

@@ -108,60 +108,13 @@ __device__ __forceinline__ int merge_union(const uint16_t *sa, int na, const uin
     return n;
 }
 
-template <int DIM, int PM, typename R>
-__device__ __forceinline__ void post_union_cell(const PostArgs<R> &a, int64_t c)
+/* write cell c's superset sup[0..ns): phi and EX of surviving phases move
+ * to their new slots, new phases start at phi = 0 and EX =
+ * SitepotentialExplicit(c0, T of the cell) (src/cipher.c:947-973) */
+template <int PM, typename R>
+__device__ __forceinline__ void post_write_cell(const PostArgs<R> &a, int64_t c, int n, int ns, const uint16_t *sup)
 {
     const int64_t S = a.stride;
-    int n = a.as[c];
-    int ns = a.pruned[c];
-    if (n < 1 || n > a.P || ns < 1 || ns > a.P) return;   /* flagged by k_post_prune */
-    uint16_t sup[PM], tmp[PM];
-    for (int k = 0; k < ns; k++) sup[k] = a.pruned[(int64_t)(1 + k) * S + c];
-
-    /* union with the neighbours' pruned sets: over the faces of the cell
-     * (src/cipher.c:930-945); the union does not depend on their order */
-    auto unite = [&](int64_t nb) -> bool {
-        if (nb == c) return true;
-        int nbn = a.pruned[nb];
-        if (nbn > a.P) nbn = a.P;
-        int m = merge_union<PM>(sup, ns, a.pruned, S, nb, nbn, tmp, a.P);
-        if (m > a.P) {
-            atomicOr(a.err, ERR_CAP);
-            return false;
-        }
-        for (int k = 0; k < m; k++) sup[k] = tmp[k];
-        ns = m;
-        return true;
-    };
-    if (a.fl.start) {
-        for (int32_t e = a.fl.start[c]; e < a.fl.start[c + 1]; e++)
-            if (!unite(a.fl.nbr[e] & 0x7fffffff)) return;
-    } else {
-        const int res[3] = {a.res[0], a.res[1], a.res[2]};
-        const int64_t st[3] = {1, (int64_t)res[0], (int64_t)res[0] * res[1]};
-        int co[3];
-        co[0] = (int)(c % res[0]);
-        co[1] = DIM > 1 ? (int)((c / res[0]) % res[1]) : 0;
-        co[2] = DIM > 2 ? (int)(c / ((int64_t)res[0] * res[1])) : 0;
-#pragma unroll
-        for (int d = 0; d < DIM; d++) {
-#pragma unroll
-            for (int side = 0; side < 2; side++) {
-                int64_t nb;
-                if (side == 0) {
-                    if (co[d] > 0) nb = c - st[d];
-                    else if (a.per[d] && res[d] > 1) nb = c + (int64_t)(res[d] - 1) * st[d];
-                    else continue;
-                } else {
-                    if (co[d] < res[d] - 1) nb = c + st[d];
-                    else if (a.per[d] && res[d] > 1) nb = c - (int64_t)(res[d] - 1) * st[d];
-                    else continue;
-                }
-                if (!unite(nb)) return;
-            }
-        }
-    }
-
     /* old (unpruned) set of this cell: phi survives for phases in the superset */
     uint16_t old[PM];
     for (int k = 0; k < n; k++) old[k] = a.as[(int64_t)(1 + k) * S + c];
@@ -178,8 +131,6 @@ __device__ __forceinline__ void post_union_cell(const PostArgs<R> &a, int64_t c)
     }
     for (int g = 0; g < ns; g++)
         if (from[g] >= 0) phiss[g] = a.phi[(int64_t)from[g] * S + c];
-    /* explicit site potentials: survivors keep theirs, new phases start at
-     * SitepotentialExplicit(c0) (src/cipher.c:953-964) */
     if (a.S > 0) {
         double exss[PM * 2 * CIPHER_MAXCP];
         const double T = (double)a.tm[c];
@@ -203,116 +154,365 @@ __device__ __forceinline__ void post_union_cell(const PostArgs<R> &a, int64_t c)
     for (int g = 0; g < ns; g++) a.as[(int64_t)(1 + g) * S + c] = sup[g];
 }
 
-template <int DIM, int PM, typename R>
-__global__ void __launch_bounds__(256) k_post_union(const PostArgs<R> a)
+/* union of an adapted mesh's cell with its listed neighbours' pruned sets
+ * (src/cipher.c:930-945; the union does not depend on their order) */
+template <int PM, typename R>
+__device__ __forceinline__ void post_union_listed(const PostArgs<R> &a, int64_t c)
+{
+    const int64_t S = a.stride;
+    const int n = a.as[c];
+    int ns = a.pruned[c];
+    if (n < 1 || n > a.P || ns < 1 || ns > a.P) return;   /* flagged by k_post_prune */
+    uint16_t sup[PM], tmp[PM];
+    for (int k = 0; k < ns; k++) sup[k] = a.pruned[(int64_t)(1 + k) * S + c];
+    for (int32_t e = a.fl.start[c]; e < a.fl.start[c + 1]; e++) {
+        const int64_t nb = a.fl.nbr[e] & 0x7fffffff;
+        if (nb == c) continue;
+        int nbn = a.pruned[nb];
+        if (nbn > a.P) nbn = a.P;
+        const int m = merge_union<PM>(sup, ns, a.pruned, S, nb, nbn, tmp, a.P);
+        if (m > a.P) {
+            atomicOr(a.err, ERR_CAP);
+            return;
+        }
+        for (int k = 0; k < m; k++) sup[k] = tmp[k];
+        ns = m;
+    }
+    post_write_cell<PM, R>(a, c, n, ns, sup);
+}
+
+template <int PM, typename R>
+__global__ void __launch_bounds__(256) k_post_union_listed(const PostArgs<R> a)
 {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= a.ncells) return;
-    post_union_cell<DIM, PM, R>(a, c);
+    post_union_listed<PM, R>(a, c);
 }
 
-/* face maps of cell c (cipher_b200.h, MAP): for each direction q = 2d+side
- * the neighbour's slot of every own phase, 15 where the neighbour lacks it
- * or where the face's L cell fails the phase-flux gate of src/cipher.c:277
- * (the L cell is the lower one of the face, as the reference enumerates
- * faces (c, c+e_d)).  Invalid sets raise ERR_BADSET. */
-template <int DIM, typename R>
-__device__ __forceinline__ void build_maps_cell(const PostArgs<R> &a, int64_t c)
+/* ------------------------------------------------------------------ */
+/* uniform grids: one warp per row of 32 cells, sets staged in shared   */
+/* memory                                                               */
+/* ------------------------------------------------------------------ */
+/*
+ * The union and the face maps of a cell need the sets of its 2*dim face
+ * neighbours.  A warp owns a row of 32 consecutive x cells of grid line
+ * (y, z) and stages, plane by plane with coalesced loads, the sets (count,
+ * then ids) of its own row and of the rows at y-1, y+1, z-1, z+1 in shared
+ * memory, plus the two cells just outside the row along x.  Every merge then
+ * reads shared memory instead of chaining dependent global loads.  Blocks are
+ * 4 warps on 4 consecutive y rows.
+ */
+constexpr int kPostRowWarps = 4;
+
+/* staged rows: 0 own, 1 y-1, 2 y+1, 3 z-1, 4 z+1; entries [row][k][32], k = 0
+ * count, 1..P ids; then two halo cells [2][P+1] */
+__host__ __device__ constexpr size_t post_stage_elems(int P) { return (size_t)5 * (P + 1) * 32 + 2 * (P + 1); }
+
+__host__ __device__ constexpr size_t post_row_warp_bytes(int P)
 {
-    const int64_t S = a.stride;
-    const int res[3] = {a.res[0], a.res[1], a.res[2]};
-    const int64_t st[3] = {1, (int64_t)res[0], (int64_t)res[0] * res[1]};
-    int co[3];
-    co[0] = (int)(c % res[0]);
-    co[1] = DIM > 1 ? (int)((c / res[0]) % res[1]) : 0;
-    co[2] = DIM > 2 ? (int)(c / ((int64_t)res[0] * res[1])) : 0;
-    const int n = a.as[c];
-    bool ok = n >= 1 && n <= a.P;
-    uint16_t own[CIPHER_PMAX];
-    if (ok)
-        for (int k = 0; k < n; k++) {
-            own[k] = a.as[(int64_t)(1 + k) * S + c];
-            if (a.npf > 0 && own[k] >= a.npf) ok = false;
+    /* staged sets, then the per-lane work columns: two uint16 superset
+     * columns [P][32] each (union) or one uint32 map-word column [P][32]
+     * (maps) */
+    return (post_stage_elems(P) * 2 + (size_t)P * 32 * 4 + 15) / 16 * 16;
+}
+
+struct RowCells {
+    int x0, y, z;          /* row origin */
+    int x;                 /* this lane's x */
+    bool live;
+    int64_t c;             /* this lane's cell */
+    int nlive;             /* live lanes of the row */
+};
+
+template <int DIM>
+__device__ __forceinline__ bool row_of(const int *res, int64_t rb, int wib, RowCells &r)
+{
+    const int nxs = (res[0] + 31) >> 5;
+    const int nyb = (res[1] + kPostRowWarps - 1) / kPostRowWarps;
+    const int xs = (int)(rb % nxs);
+    const int64_t rest = rb / nxs;
+    r.y = (int)(rest % nyb) * kPostRowWarps + wib;
+    r.z = (int)(rest / nyb);
+    if (r.y >= res[1] || r.z >= res[2]) return false;
+    r.x0 = xs * 32;
+    r.x = r.x0 + (int)(threadIdx.x & 31);
+    r.live = r.x < res[0];
+    r.nlive = res[0] - r.x0 < 32 ? res[0] - r.x0 : 32;
+    r.c = (int64_t)r.x + (int64_t)res[0] * ((int64_t)r.y + (int64_t)res[1] * r.z);
+    return true;
+}
+
+/* cell offset of the neighbour row along d (1: y, 2: z) on `side`, or
+ * INT64_MIN when that row is absent (non-periodic boundary, or a
+ * dimension of one cell) */
+__device__ __forceinline__ int64_t row_offset(const int *res, const int *per, const RowCells &r, int d, int side)
+{
+    const int co = d == 1 ? r.y : r.z;
+    const int64_t st = d == 1 ? (int64_t)res[0] : (int64_t)res[0] * res[1];
+    if (side == 0) {
+        if (co > 0) return -st;
+        if (per[d] && res[d] > 1) return (int64_t)(res[d] - 1) * st;
+    } else {
+        if (co < res[d] - 1) return st;
+        if (per[d] && res[d] > 1) return -(int64_t)(res[d] - 1) * st;
+    }
+    return INT64_MIN;
+}
+
+/* x of the lower / upper x neighbour of x, or -1 */
+__device__ __forceinline__ int x_nb(const int *res, const int *per, int x, int side)
+{
+    if (side == 0) return x > 0 ? x - 1 : (per[0] && res[0] > 1 ? res[0] - 1 : -1);
+    return x < res[0] - 1 ? x + 1 : (per[0] && res[0] > 1 ? 0 : -1);
+}
+
+/* stage the sets held in planes (count plane, then P id planes, stride S) of
+ * the row, its neighbour rows and its two outer x neighbours */
+template <int DIM>
+__device__ __forceinline__ void stage_row_sets(const uint16_t *planes, int64_t S, int P, const int *res, const int *per,
+                                               const RowCells &r, uint16_t *st, bool *row_present)
+{
+    const int lane = threadIdx.x & 31;
+    const int P1 = P + 1;
+    for (int row = 0; row < 5; row++) {
+        int64_t off = 0;
+        bool present = row == 0;
+        if (row > 0) {
+            const int d = (row + 1) >> 1;           /* 1,2 -> y ; 3,4 -> z */
+            if (d < DIM) {
+                off = row_offset(res, per, r, d, (row + 1) & 1);
+                present = off != INT64_MIN;
+            }
         }
-    if (!ok) atomicOr(a.err, ERR_BADSET);
-#pragma unroll
-    for (int d = 0; d < DIM; d++) {
-#pragma unroll
-        for (int side = 0; side < 2; side++) {
-            int64_t nb = -1;
-            if (side == 0) {
-                if (co[d] > 0) nb = c - st[d];
-                else if (a.per[d] && res[d] > 1) nb = c + (int64_t)(res[d] - 1) * st[d];
-            } else {
-                if (co[d] < res[d] - 1) nb = c + st[d];
-                else if (a.per[d] && res[d] > 1) nb = c - (int64_t)(res[d] - 1) * st[d];
-            }
-            uint64_t w = ~0ull;
-            if (ok && nb >= 0) {
-                const int nn = a.as[nb];
-                if (nn >= 1 && nn <= a.P) {
-                    const bool gate = side == 1 ? (n > 1 || own[0] > 1) : (nn > 1 || a.as[S + nb] > 1);
-                    if (gate) {
-                        int i = 0, j = 0;
-                        while (i < n && j < nn) {
-                            const uint16_t b = a.as[(int64_t)(1 + j) * S + nb];
-                            if (own[i] == b) {
-                                w &= ~(0xFull << (4 * i));
-                                w |= (uint64_t)j << (4 * i);
-                                i++;
-                                j++;
-                            } else if (own[i] < b) {
-                                i++;
-                            } else {
-                                j++;
-                            }
-                        }
-                    }
-                }
-            }
-            a.maps[(int64_t)(2 * d + side) * S + c] = w;
+        row_present[row] = present;
+        if (!present) continue;
+        uint16_t *rs = st + (size_t)row * P1 * 32;
+        const int64_t cc = r.c + off;
+        int n = r.live ? (int)planes[cc] : 0;
+        if (n > P) n = P;
+        rs[lane] = (uint16_t)n;
+        const int maxn = __reduce_max_sync(0xffffffffu, n);
+        for (int k = 0; k < maxn; k++)
+            if (k < n) rs[(1 + k) * 32 + lane] = planes[(int64_t)(1 + k) * S + cc];
+    }
+    /* the lower x neighbour of the first lane and the upper one of the last
+     * live lane, when they lie outside the row */
+    uint16_t *halo = st + (size_t)5 * P1 * 32;
+    if (lane < 2) {
+        const int xl = lane == 0 ? r.x0 : r.x0 + r.nlive - 1;
+        const int xn = x_nb(res, per, xl, lane);
+        uint16_t *h = halo + lane * P1;
+        h[0] = 0;
+        if (xn >= 0 && (xn < r.x0 || xn >= r.x0 + r.nlive)) {
+            const int64_t cc = r.c - (r.x - xn);
+            int n = planes[cc];
+            if (n > P) n = P;
+            h[0] = (uint16_t)n;
+            for (int k = 0; k < n; k++) h[1 + k] = planes[(int64_t)(1 + k) * S + cc];
         }
     }
+    __syncwarp();
+}
+
+/* the staged set of face neighbour q (2d + side) of this lane: its count
+ * (0 when absent), the address of its first id and the id stride; `self`
+ * tells that the neighbour is the cell itself (a periodic dimension of one
+ * cell along x) */
+template <int DIM>
+__device__ __forceinline__ int staged_nb(const uint16_t *st, int P, const int *res, const int *per, const RowCells &r,
+                                         const bool *row_present, int q, const uint16_t *&ids, int &stride)
+{
+    const int lane = threadIdx.x & 31;
+    const int P1 = P + 1;
+    const int d = q >> 1, side = q & 1;
+    if (d == 0) {
+        const int xn = x_nb(res, per, r.x, side);
+        if (xn < 0 || xn == r.x) return 0;
+        if (xn >= r.x0 && xn < r.x0 + r.nlive) {
+            const uint16_t *rs = st + (xn - r.x0);
+            ids = rs + 32;
+            stride = 32;
+            return rs[0];
+        }
+        const uint16_t *h = st + (size_t)5 * P1 * 32 + side * P1;   /* only the first / last lane gets here */
+        ids = h + 1;
+        stride = 1;
+        return h[0];
+    }
+    const int row = 2 * d - 1 + side;
+    if (!row_present[row]) return 0;
+    const uint16_t *rs = st + (size_t)row * P1 * 32 + lane;
+    ids = rs + 32;
+    stride = 32;
+    return rs[0];
+}
+
+/* union of this lane's pruned set with its face neighbours' (all staged) */
+template <int DIM, int PM, typename R>
+__device__ __forceinline__ void post_union_row(const PostArgs<R> &a, int64_t rb, unsigned char *wsm)
+{
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    RowCells r;
+    if (!row_of<DIM>(a.res, rb, wib, r)) return;           /* whole warp */
+    const int P = a.P;
+    uint16_t *st = (uint16_t *)wsm;
+    uint16_t *supA = st + post_stage_elems(P), *supB = supA + P * 32;
+    bool present[5];
+    stage_row_sets<DIM>(a.pruned, a.stride, P, a.res, a.per, r, st, present);
+    if (!r.live) return;
+    const int n = a.as[r.c];
+    int ns = st[lane];
+    if (n < 1 || n > P || ns < 1 || ns > P) return;       /* flagged by k_post_prune */
+    for (int k = 0; k < ns; k++) supA[k * 32 + lane] = st[(1 + k) * 32 + lane];
+    uint16_t *cur = supA + lane, *nxt = supB + lane;
+    for (int q = 0; q < 2 * DIM; q++) {
+        const uint16_t *ids;
+        int stride;
+        const int nbn = staged_nb<DIM>(st, P, a.res, a.per, r, present, q, ids, stride);
+        if (nbn == 0) continue;
+        /* sorted merge cur U nb -> nxt */
+        int i = 0, j = 0, m = 0;
+        bool over = false;
+        while (i < ns || j < nbn) {
+            const uint16_t u = i < ns ? cur[i * 32] : 0xffff, v = j < nbn ? ids[j * stride] : 0xffff;
+            uint16_t w;
+            if (j >= nbn || (i < ns && u < v)) { w = u; i++; }
+            else if (i >= ns || v < u) { w = v; j++; }
+            else { w = u; i++; j++; }
+            if (m >= P) { over = true; break; }
+            nxt[m++ * 32] = w;
+        }
+        if (over) {
+            atomicOr(a.err, ERR_CAP);
+            return;
+        }
+        uint16_t *t = cur;
+        cur = nxt;
+        nxt = t;
+        ns = m;
+    }
+    uint16_t sup[PM];
+    for (int k = 0; k < ns; k++) sup[k] = cur[k * 32];
+    post_write_cell<PM, R>(a, r.c, n, ns, sup);
+}
+
+template <int DIM, int PM, typename R>
+__global__ void __launch_bounds__(32 * kPostRowWarps) k_post_union_rows(const PostArgs<R> a, int64_t rb0)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned char *wsm = smem + (size_t)(threadIdx.x >> 5) * post_row_warp_bytes(a.P);
+    post_union_row<DIM, PM, R>(a, rb0 + blockIdx.x, wsm);
+}
+
+/*
+ * Face maps (cipher_b200.h, MAP) of this lane's cell: one 32-bit word per
+ * active slot, nibble q = 2d + side holding the slot of the same phase in
+ * the neighbour across face q, or 15 where the neighbour lacks it or the
+ * face's L cell (the lower one, as the reference enumerates faces (c, c+e_d))
+ * fails the phase-flux gate of src/cipher.c:277.  Bad sets raise
+ * ERR_BADSET.
+ */
+template <int DIM, typename R>
+__device__ __forceinline__ void build_maps_row(const PostArgs<R> &a, int64_t rb, unsigned char *wsm)
+{
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    RowCells r;
+    if (!row_of<DIM>(a.res, rb, wib, r)) return;
+    const int P = a.P;
+    const int64_t S = a.stride;
+    uint16_t *st = (uint16_t *)wsm;
+    uint32_t *mw = (uint32_t *)(st + post_stage_elems(P));   /* 4-byte aligned: 324 (P+1) bytes of staging */
+    bool present[5];
+    stage_row_sets<DIM>(a.as, S, P, a.res, a.per, r, st, present);
+    if (!r.live) return;
+    const int n = a.as[r.c];
+    bool ok = n >= 1 && n <= P;
+    const uint16_t *own = st + 32 + lane;
+    if (ok && a.npf > 0)
+        for (int k = 0; k < n; k++)
+            if (own[k * 32] >= a.npf) ok = false;
+    if (!ok) {
+        atomicOr(a.err, ERR_BADSET);
+        return;
+    }
+    uint32_t *w = mw + lane;
+    for (int k = 0; k < n; k++) w[k * 32] = 0xffffffffu;
+    const bool gate_self = n > 1 || own[0] > 1;
+    for (int q = 0; q < 2 * DIM; q++) {
+        const uint16_t *ids;
+        int stride;
+        const int nn = staged_nb<DIM>(st, P, a.res, a.per, r, present, q, ids, stride);
+        if (nn < 1) continue;
+        const bool gate = (q & 1) ? gate_self : (nn > 1 || ids[0] > 1);
+        if (!gate) continue;
+        const unsigned sh = 4u * (unsigned)q;
+        int i = 0, j = 0;
+        while (i < n && j < nn) {
+            const uint16_t u = own[i * 32], v = ids[j * stride];
+            if (u == v) {
+                w[i * 32] = (w[i * 32] & ~(15u << sh)) | ((uint32_t)j << sh);
+                i++;
+                j++;
+            } else if (u < v) {
+                i++;
+            } else {
+                j++;
+            }
+        }
+    }
+    for (int k = 0; k < n; k++) a.maps[(int64_t)k * S + r.c] = w[k * 32];
 }
 
 template <int DIM, typename R>
-__global__ void __launch_bounds__(256) k_build_maps(const PostArgs<R> a, int64_t c0, int64_t c1)
+__global__ void __launch_bounds__(32 * kPostRowWarps) k_build_maps_rows(const PostArgs<R> a, int64_t rb0)
 {
-    const int64_t c = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= c1) return;
-    build_maps_cell<DIM, R>(a, c);
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned char *wsm = smem + (size_t)(threadIdx.x >> 5) * post_row_warp_bytes(a.P);
+    build_maps_row<DIM, R>(a, rb0 + blockIdx.x, wsm);
 }
 
-template <typename R>
-static cudaError_t launch_maps(const PostArgs<R> &a, int dim, int64_t c0, int64_t c1, cudaStream_t s)
+/* row blocks of a grid (4 rows of 32 cells each) and of its z-planes [z0, z1) */
+__host__ __device__ inline int64_t row_blocks_per_plane(const int *res)
 {
-    if (!a.maps || c1 <= c0) return cudaSuccess;
-    const int64_t blocks = (c1 - c0 + 255) / 256;
-    if (dim == 1) k_build_maps<1, R><<<(unsigned)blocks, 256, 0, s>>>(a, c0, c1);
-    else if (dim == 2) k_build_maps<2, R><<<(unsigned)blocks, 256, 0, s>>>(a, c0, c1);
-    else k_build_maps<3, R><<<(unsigned)blocks, 256, 0, s>>>(a, c0, c1);
+    return (int64_t)((res[0] + 31) >> 5) * ((res[1] + kPostRowWarps - 1) / kPostRowWarps);
+}
+__host__ __device__ inline int64_t row_blocks(const int *res) { return row_blocks_per_plane(res) * res[2]; }
+int64_t post_row_blocks(const int *res) { return row_blocks(res); }
+
+template <typename R>
+static cudaError_t launch_maps(const PostArgs<R> &a, int dim, int64_t z0, int64_t z1, cudaStream_t s)
+{
+    if (!a.maps || z1 <= z0) return cudaSuccess;
+    const int64_t per = row_blocks_per_plane(a.res);
+    const unsigned blocks = (unsigned)((z1 - z0) * per);
+    const size_t sm = kPostRowWarps * post_row_warp_bytes(a.P);
+    if (dim == 1) k_build_maps_rows<1, R><<<blocks, 32 * kPostRowWarps, sm, s>>>(a, z0 * per);
+    else if (dim == 2) k_build_maps_rows<2, R><<<blocks, 32 * kPostRowWarps, sm, s>>>(a, z0 * per);
+    else k_build_maps_rows<3, R><<<blocks, 32 * kPostRowWarps, sm, s>>>(a, z0 * per);
     return cudaGetLastError();
 }
 
-cudaError_t launch_build_maps(const PostArgs<double> &a, int dim, cudaStream_t s) { return launch_maps(a, dim, 0, a.ncells, s); }
-cudaError_t launch_build_maps(const PostArgs<float> &a, int dim, cudaStream_t s) { return launch_maps(a, dim, 0, a.ncells, s); }
+cudaError_t launch_build_maps(const PostArgs<double> &a, int dim, cudaStream_t s) { return launch_maps(a, dim, 0, a.res[2], s); }
+cudaError_t launch_build_maps(const PostArgs<float> &a, int dim, cudaStream_t s) { return launch_maps(a, dim, 0, a.res[2], s); }
+/* cells [c0, c1) must be whole z-planes of a 3D grid */
 cudaError_t launch_build_maps_range(const PostArgs<double> &a, int dim, int64_t c0, int64_t c1, cudaStream_t s)
 {
-    return launch_maps(a, dim, c0, c1, s);
+    const int64_t plane = (int64_t)a.res[0] * a.res[1];
+    return launch_maps(a, dim, c0 / plane, (c1 + plane - 1) / plane, s);
 }
 cudaError_t launch_build_maps_range(const PostArgs<float> &a, int dim, int64_t c0, int64_t c1, cudaStream_t s)
 {
-    return launch_maps(a, dim, c0, c1, s);
+    const int64_t plane = (int64_t)a.res[0] * a.res[1];
+    return launch_maps(a, dim, c0 / plane, (c1 + plane - 1) / plane, s);
 }
 
-/* batched: block k of the list belongs to the domain whose range holds k */
-template <typename R>
-__device__ __forceinline__ int batch_post_domain(const BatchPost<R> &b, int64_t k)
+/* batched: block k of a list belongs to the domain whose range holds k */
+__device__ __forceinline__ int batch_domain_of(const int64_t *start, int n, int64_t k)
 {
-    int lo = 0, hi = b.n - 1;
+    int lo = 0, hi = n - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(&b.block_start[mid]) <= k) lo = mid;
+        if (__ldg(&start[mid]) <= k) lo = mid;
         else hi = mid - 1;
     }
     return lo;
@@ -321,7 +521,7 @@ __device__ __forceinline__ int batch_post_domain(const BatchPost<R> &b, int64_t 
 template <int PM, typename R>
 __global__ void __launch_bounds__(256) k_post_prune_batched(const BatchPost<R> b)
 {
-    const int inst = batch_post_domain(b, blockIdx.x);
+    const int inst = batch_domain_of(b.block_start, b.n, blockIdx.x);
     if (!b.active[inst]) return;
     const PostArgs<R> &a = b.args[inst];
     const int64_t c = (int64_t)(blockIdx.x - b.block_start[inst]) * blockDim.x + threadIdx.x;
@@ -330,43 +530,45 @@ __global__ void __launch_bounds__(256) k_post_prune_batched(const BatchPost<R> b
 }
 
 template <int DIM, int PM, typename R>
-__global__ void __launch_bounds__(256) k_post_union_batched(const BatchPost<R> b)
+__global__ void __launch_bounds__(32 * kPostRowWarps) k_post_union_rows_batched(const BatchPost<R> b)
 {
-    const int inst = batch_post_domain(b, blockIdx.x);
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int inst = batch_domain_of(b.row_start, b.n, blockIdx.x);
     if (!b.active[inst]) return;
     const PostArgs<R> &a = b.args[inst];
-    const int64_t c = (int64_t)(blockIdx.x - b.block_start[inst]) * blockDim.x + threadIdx.x;
-    if (c >= a.ncells) return;
-    post_union_cell<DIM, PM, R>(a, c);
+    unsigned char *wsm = smem + (size_t)(threadIdx.x >> 5) * post_row_warp_bytes(b.pmax);
+    post_union_row<DIM, PM, R>(a, blockIdx.x - b.row_start[inst], wsm);
 }
 
 template <int DIM, typename R>
-__global__ void __launch_bounds__(256) k_build_maps_batched(const BatchPost<R> b)
+__global__ void __launch_bounds__(32 * kPostRowWarps) k_build_maps_rows_batched(const BatchPost<R> b)
 {
-    const int inst = batch_post_domain(b, blockIdx.x);
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int inst = batch_domain_of(b.row_start, b.n, blockIdx.x);
     if (!b.active[inst]) return;
     const PostArgs<R> &a = b.args[inst];
     if (!a.maps) return;
-    const int64_t c = (int64_t)(blockIdx.x - b.block_start[inst]) * blockDim.x + threadIdx.x;
-    if (c >= a.ncells) return;
-    build_maps_cell<DIM, R>(a, c);
+    unsigned char *wsm = smem + (size_t)(threadIdx.x >> 5) * post_row_warp_bytes(b.pmax);
+    build_maps_row<DIM, R>(a, blockIdx.x - b.row_start[inst], wsm);
 }
 
 template <typename R>
 static cudaError_t launch_post_batched(const BatchPost<R> &b, int dim, cudaStream_t s)
 {
     if (b.total < 1) return cudaSuccess;
-    dim3 grid((unsigned)b.total), block(256);
-    k_post_prune_batched<CIPHER_PMAX, R><<<grid, block, 0, s>>>(b);
+    k_post_prune_batched<CIPHER_PMAX, R><<<(unsigned)b.total, 256, 0, s>>>(b);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if (dim == 1) k_post_union_batched<1, CIPHER_PMAX, R><<<grid, block, 0, s>>>(b);
-    else if (dim == 2) k_post_union_batched<2, CIPHER_PMAX, R><<<grid, block, 0, s>>>(b);
-    else k_post_union_batched<3, CIPHER_PMAX, R><<<grid, block, 0, s>>>(b);
+    const size_t sm = kPostRowWarps * post_row_warp_bytes(b.pmax);
+    const unsigned rb = (unsigned)b.row_total;
+    const unsigned bs = 32 * kPostRowWarps;
+    if (dim == 1) k_post_union_rows_batched<1, CIPHER_PMAX, R><<<rb, bs, sm, s>>>(b);
+    else if (dim == 2) k_post_union_rows_batched<2, CIPHER_PMAX, R><<<rb, bs, sm, s>>>(b);
+    else k_post_union_rows_batched<3, CIPHER_PMAX, R><<<rb, bs, sm, s>>>(b);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (dim == 1) k_build_maps_batched<1, R><<<grid, block, 0, s>>>(b);
-    else if (dim == 2) k_build_maps_batched<2, R><<<grid, block, 0, s>>>(b);
-    else k_build_maps_batched<3, R><<<grid, block, 0, s>>>(b);
+    if (dim == 1) k_build_maps_rows_batched<1, R><<<rb, bs, sm, s>>>(b);
+    else if (dim == 2) k_build_maps_rows_batched<2, R><<<rb, bs, sm, s>>>(b);
+    else k_build_maps_rows_batched<3, R><<<rb, bs, sm, s>>>(b);
     return cudaGetLastError();
 }
 
@@ -376,16 +578,22 @@ cudaError_t launch_poststep_batched(const BatchPost<float> &b, int dim, cudaStre
 template <typename R>
 static cudaError_t launch_post(const PostArgs<R> &a, int dim, cudaStream_t s)
 {
-    int64_t blocks = (a.ncells + 255) / 256;
-    dim3 grid((unsigned)blocks), block(256);
-    k_post_prune<CIPHER_PMAX, R><<<grid, block, 0, s>>>(a);
+    const unsigned blocks = (unsigned)((a.ncells + 255) / 256);
+    k_post_prune<CIPHER_PMAX, R><<<blocks, 256, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if (dim == 1) k_post_union<1, CIPHER_PMAX, R><<<grid, block, 0, s>>>(a);
-    else if (dim == 2) k_post_union<2, CIPHER_PMAX, R><<<grid, block, 0, s>>>(a);
-    else k_post_union<3, CIPHER_PMAX, R><<<grid, block, 0, s>>>(a);
+    if (a.fl.start) {
+        /* adapted meshes: neighbours from the face lists, no face maps */
+        k_post_union_listed<CIPHER_PMAX, R><<<blocks, 256, 0, s>>>(a);
+        return cudaGetLastError();
+    }
+    const size_t sm = kPostRowWarps * post_row_warp_bytes(a.P);
+    const unsigned rb = (unsigned)row_blocks(a.res);
+    if (dim == 1) k_post_union_rows<1, CIPHER_PMAX, R><<<rb, 32 * kPostRowWarps, sm, s>>>(a, 0);
+    else if (dim == 2) k_post_union_rows<2, CIPHER_PMAX, R><<<rb, 32 * kPostRowWarps, sm, s>>>(a, 0);
+    else k_post_union_rows<3, CIPHER_PMAX, R><<<rb, 32 * kPostRowWarps, sm, s>>>(a, 0);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    return launch_maps(a, dim, 0, a.ncells, s);
+    return launch_maps(a, dim, 0, a.res[2], s);
 }
 
 cudaError_t launch_poststep(const PostArgs<double> &a, int dim, cudaStream_t s) { return launch_post(a, dim, s); }

@@ -86,7 +86,7 @@ cipher::PostArgs<R> noalloc_args(const cipher_grid_desc *g, void *X, const Noall
     a.npf = g->npf;
     a.as = (uint16_t *)(x + g->layout.as_offset);
     /* the face maps of the layout, when it has them, are rebuilt as well */
-    a.maps = g->layout.map_planes == 2 * g->dim ? (uint64_t *)(x + g->layout.map_offset) : nullptr;
+    a.maps = g->layout.map_planes == g->layout.pf_size ? (uint32_t *)(x + g->layout.map_offset) : nullptr;
     a.phi = (R *)(x + g->layout.pf_offset);
     a.ex = (double *)(x + g->layout.ex_offset);
     a.tm = (const R *)(x + g->layout.tm_offset);
@@ -117,8 +117,9 @@ extern "C" int cipher_poststep_noalloc(const cipher_grid_desc *g, void *X, void 
     }
     if (cells != g->layout.ncells) return CIPHER_E_ARG;
     if (g->npf < 1 || g->npf > 65535) return CIPHER_E_ARG;
-    /* the face maps are rebuilt when the layout has them; any other plane count is a foreign layout */
-    if (g->layout.map_planes != 0 && g->layout.map_planes != 2 * g->dim) return CIPHER_E_ARG;
+    /* the face maps (one word plane per slot) are rebuilt when the layout has
+     * them; any other plane count is a foreign layout */
+    if (g->layout.map_planes != 0 && g->layout.map_planes != P) return CIPHER_E_ARG;
     /* explicit site potentials: S per phase, at most two sublattices of ncp-1 potentials */
     const int S = g->ex_per_phase;
     if (S < 0 || S > 2 * CIPHER_MAXCP) return CIPHER_E_ARG;

@@ -48,13 +48,13 @@ constexpr int kIPP = CIPHER_MIXED_IPP;   /* items per lane and pass in the items
  * slice of shared memory, so warps never wait for one another.  The face
  * gather, the bulk of the work, runs over the row's (cell, slot) items, so a
  * lane never idles while a neighbour lane walks a larger set:
- *   1. lane = cell: active count and the cell's face-map words (as 32-bit
- *      halves, slots 0-7 and 8-15) into shared memory, one 16-bit tag (cell lane, slot) per item in slot-major
- *      order;
- *   2. lane = item: the slot's phase fraction and its Laplacian over the
- *      cell's 2*dim faces (absent or gated faces map every slot to 15);
- *      neighbour cells follow from the row's position (y and z offsets are
- *      the same for the whole row);
+ *   1. lane = cell: active count, and one 16-bit tag (cell lane, slot) per
+ *      item in slot-major order;
+ *   2. lane = item: the slot's phase fraction, its face-map word (one word
+ *      per slot: the neighbour's slot across each face, 15 for absent or
+ *      gated faces) and its Laplacian over the cell's 2*dim faces; neighbour
+ *      cells follow from the row's position (y and z offsets are the same
+ *      for the whole row);
  *   3. lane = cell: the O(n) closed forms of the cell terms and all P
  *      slots of F (coalesced plane by plane).
  * Laplacians pass from phase 2 to phase 3 in a slot-major table with row
@@ -64,16 +64,18 @@ constexpr int kIPP = CIPHER_MIXED_IPP;   /* items per lane and pass in the items
  * reference's face order: the difference is FP32 rounding.
  * IX is the index type of plane offsets: int when every offset of the
  * domain fits (max(P, 2*dim) * stride < 2^31, all benchmark and batch
- * sizes), int64_t otherwise.
+ * sizes), int64_t otherwise.  R is the real type: float for the mixed
+ * layout; double gives the same closed form on an FP64 state (the FP64
+ * closed-form path, within rounding of the reference-order kernel).
  */
-__host__ __device__ constexpr size_t items_warp_bytes(int dim, int P)
+__host__ __device__ constexpr size_t items_warp_bytes(int P, int rbytes)
 {
-    return ((size_t)32 * 2 * dim * 8 + (size_t)33 * P * 4 + (size_t)32 * P * 2 + 15) / 16 * 16;
+    return ((size_t)33 * P * rbytes + (size_t)32 * P * 2 + 15) / 16 * 16;
 }
 
-__host__ __device__ constexpr size_t items_tile_bytes(int dim, int T, int P, int ix_bytes)
+__host__ __device__ constexpr size_t items_tile_bytes(int T, int P, int rbytes)
 {
-    return (void)ix_bytes, (size_t)(T / 32) * items_warp_bytes(dim, P);
+    return (size_t)(T / 32) * items_warp_bytes(P, rbytes);
 }
 
 /* whether a domain's plane offsets fit the 32-bit kernels */
@@ -83,16 +85,41 @@ __host__ __device__ inline bool items_fit_i32(int64_t stride, int P, int dim)
     return planes * stride < ((int64_t)1 << 31) - 1;
 }
 
-template <int DIM, typename IX>
-__device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const CellIndex &cix, unsigned char *smem)
+/* the closed-form constants in the kernel's real type: FP32 forms computed on
+ * the host (with active-set thresholds equal to the double tests), or the
+ * FP64 values themselves */
+template <typename R>
+struct ItemConsts {
+    R coef, inv_w, w_pi2, sig, tjh, mob, tol_gt, tol1_lt, tol_lt, tol1_gt;
+};
+
+__device__ __forceinline__ ItemConsts<float> item_consts(const PfArgs<float> &a)
+{
+    return {a.coef_f, a.inv_w_f, a.w_pi2_f, a.sig_f, a.tjh_f, a.mob_f, a.tol_gt, a.tol1_lt, a.tol_lt, a.tol1_gt};
+}
+
+__device__ __forceinline__ ItemConsts<double> item_consts(const PfArgs<double> &a)
+{
+    const double pi2 = CIPHER_PI_D * CIPHER_PI_D;
+    return {a.face_coef, 1.0 / a.wid0, a.wid0 / pi2, a.sig0, 0.5 * a.tj0, a.mob0,
+            CIPHER_TOL, 1.0 - CIPHER_TOL, CIPHER_TOL, 1.0 - CIPHER_TOL};
+}
+
+__device__ __forceinline__ float item_rcp(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double item_rcp(double x) { return 1.0 / x; }
+__device__ __forceinline__ float item_fma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double item_fma(double a, double b, double c) { return fma(a, b, c); }
+
+template <int DIM, typename IX, typename R>
+__device__ __forceinline__ void items_tile(const PfArgs<R> &a, const CellIndex &cix, unsigned char *smem)
 {
     constexpr int ND = 2 * DIM;
     const int lane = threadIdx.x & 31, P = a.P;
     const IX S = (IX)a.stride;
-    const float *phi = a.phi;
-    unsigned char *ws = smem + (size_t)(threadIdx.x >> 5) * items_warp_bytes(DIM, P);
-    uint32_t *sw = (uint32_t *)ws;                                /* [ND][2][32] face-map word halves */
-    float *slap = (float *)(sw + ND * 64);                        /* [P][33] Laplacian, later the capillary force */
+    const R *phi = a.phi;
+    const ItemConsts<R> k = item_consts(a);
+    unsigned char *ws = smem + (size_t)(threadIdx.x >> 5) * items_warp_bytes(P, (int)sizeof(R));
+    R *slap = (R *)ws;                                            /* [P][33] Laplacian, later the capillary force */
     uint16_t *itag = (uint16_t *)(slap + 33 * P);                 /* [32*P] cell lane | slot << 5 */
 
     __syncwarp();                    /* the previous row's readers are done */
@@ -118,40 +145,26 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
             st *= (IX)a.res[d];
         }
     }
-    if (n > 0) {
-        const int co[3] = {cix.x, cix.y, cix.z};
-#pragma unroll
-        for (int d = 0; d < DIM; d++) {
-            const bool wrap = a.per[d] && a.res[d] > 1;
-            const bool lo = co[d] > 0 || wrap, hi = co[d] < a.res[d] - 1 || wrap;
-            const uint64_t wl = lo ? __ldg(&a.maps[(IX)(2 * d) * S + c]) : ~0ull;
-            const uint64_t wh = hi ? __ldg(&a.maps[(IX)(2 * d + 1) * S + c]) : ~0ull;
-            sw[(4 * d + 0) * 32 + lane] = (uint32_t)wl;
-            sw[(4 * d + 1) * 32 + lane] = (uint32_t)(wl >> 32);
-            sw[(4 * d + 2) * 32 + lane] = (uint32_t)wh;
-            sw[(4 * d + 3) * 32 + lane] = (uint32_t)(wh >> 32);
-        }
-    }
     /* items in slot-major order (slot 0 of every cell, then slot 1 of the
      * cells that have one, ...): consecutive lanes then gather neighbouring
      * cells of the same planes, which share sectors */
     const int maxn = __reduce_max_sync(0xffffffffu, n);
     const unsigned below = (1u << lane) - 1u;
     int total = 0;
-    for (int k = 0; k < maxn; k++) {
-        const unsigned m = __ballot_sync(0xffffffffu, n > k);
-        if (n > k) itag[total + __popc(m & below)] = (uint16_t)(lane | k << 5);
+    for (int kk = 0; kk < maxn; kk++) {
+        const unsigned m = __ballot_sync(0xffffffffu, n > kk);
+        if (n > kk) itag[total + __popc(m & below)] = (uint16_t)(lane | kk << 5);
         total += __popc(m);
     }
     __syncwarp();
 
-    /* 2. items, kIPP per pass so that their loads are in flight together */
-    const float coef = a.coef_f;
+    /* 2. items, kIPP per pass so that their loads are in flight together; an
+     * item's face-map word gives its neighbour slot across each face */
     const IX xlo_wrap = (IX)(a.res[0] - 1), xhi_wrap = -(IX)(a.res[0] - 1);
     for (int it = lane; it < total; it += 32 * kIPP) {
         int cl[kIPP], sl[kIPP];
         bool ok[kIPP];
-        float l[kIPP];
+        R l[kIPP];
 #pragma unroll
         for (int u = 0; u < kIPP; u++) {
             ok[u] = it + 32 * u < total;
@@ -163,23 +176,22 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
         for (int u = 0; u < kIPP; u++) {
             const IX cc = crow + (IX)cl[u];
             const int x = xrow + cl[u];
-            const float p = __ldg(&phi[(IX)sl[u] * S + cc]);
-            const unsigned sh = 4u * (unsigned)(sl[u] & 7);
-            const uint32_t *swh = sw + (sl[u] >> 3) * 32 + cl[u];   /* the word half holding slot sl */
-            float pn[ND];
+            const R p = __ldg(&phi[(IX)sl[u] * S + cc]);
+            const uint32_t w = __ldg(&a.maps[(IX)sl[u] * S + cc]);
+            R pn[ND];
 #pragma unroll
             for (int q = 0; q < ND; q++) {
-                const int j = (int)((swh[q * 64] >> sh) & 15u);
+                const int j = (int)((w >> (4 * q)) & 15u);
                 IX dq;
                 if (q == 0) dq = x > 0 ? (IX)-1 : xlo_wrap;
                 else if (q == 1) dq = x < a.res[0] - 1 ? (IX)1 : xhi_wrap;
                 else dq = (q & 1) ? dhi[q >> 1] : dlo[q >> 1];
                 pn[q] = j < P ? __ldg(&phi[(IX)j * S + cc + dq]) : p;
             }
-            float acc = 0.0f;
+            R acc = (R)0;
 #pragma unroll
             for (int q = 0; q < ND; q++) acc += pn[q] - p;
-            l[u] = coef * acc;
+            l[u] = k.coef * acc;
         }
 #pragma unroll
         for (int u = 0; u < kIPP; u++)
@@ -187,75 +199,74 @@ __device__ __forceinline__ void mixed_items_tile(const PfArgs<float> &a, const C
     }
     __syncwarp();
 
-    /* 3. cell terms in FP32.  The sum of the capillary forces over the
-     * cell's slots has a closed form in the slot sums:
+    /* 3. cell terms.  The sum of the capillary forces over the cell's slots
+     * has a closed form in the slot sums:
      *   C = 8 (-sigma (n-1) A - tj/2 (n-2)(S1^2 - S2)) + L,   L = sum of Laplacians,
      * so one pass gives the sums and a second the forces and the active set */
     if (!cix.live) return;
     uint32_t act = 0;
-    float nf = 0.0f, Caf = 0.0f;
-    float *cl3 = slap + lane;        /* slot k at cl3[33 * k] */
-    const float *cp3 = phi + c;      /* slot k at cp3[k * S] (cached since phase 2) */
+    R nf = (R)0, Caf = (R)0;
+    R *cl3 = slap + lane;            /* slot k at cl3[33 * k] */
+    const R *cp3 = phi + c;          /* slot k at cp3[k * S] (cached since phase 2) */
     if (n > 1) {
-        const float inv_w = a.inv_w_f, w_pi2 = a.w_pi2_f, sig = a.sig_f, tjh = a.tjh_f, mob = a.mob_f;
-        float A = 0.0f, S1 = 0.0f, S2 = 0.0f, L = 0.0f;
+        R A = (R)0, S1 = (R)0, S2 = (R)0, L = (R)0;
         {
-            const float *pp = cp3;
+            const R *pp = cp3;
 #pragma unroll 2
-            for (int k = 0; k < n; k++, pp += S) {
-                const float pk = __ldg(pp), lk = cl3[33 * k];
-                A += pk * inv_w + lk * w_pi2;
+            for (int kk = 0; kk < n; kk++, pp += S) {
+                const R pk = __ldg(pp), lk = cl3[33 * kk];
+                A += pk * k.inv_w + lk * k.w_pi2;
                 S1 += pk;
                 S2 += pk * pk;
                 L += lk;
             }
         }
-        const float fn = (float)n;
-        const float C = 8.0f * (-sig * (fn - 1.0f) * A - tjh * (fn - 2.0f) * (S1 * S1 - S2)) + L;
-        const float *pp = cp3;
+        const R fn = (R)n;
+        const R C = (R)8 * (-k.sig * (fn - (R)1) * A - k.tjh * (fn - (R)2) * (S1 * S1 - S2)) + L;
+        const R *pp = cp3;
 #pragma unroll 2
-        for (int k = 0; k < n; k++, pp += S) {
-            const float pk = __ldg(pp), lk = cl3[33 * k];
-            const float ak = pk * inv_w + lk * w_pi2;
-            const float o1 = S1 - pk, o2 = S2 - pk * pk;
-            const float cap = 8.0f * (-sig * (A - ak) - tjh * (o1 * o1 - o2)) + lk;
-            cl3[33 * k] = cap;
-            const float u = mob * (fn * cap - C);
-            const bool on = (pk > a.tol_gt && pk < a.tol1_lt) || (pk < a.tol_lt && u > 0.0f) ||
-                            (pk > a.tol1_gt && u < 0.0f);
-            act |= (uint32_t)on << k;
-            nf += on ? 1.0f : 0.0f;
-            Caf += on ? cap : 0.0f;
+        for (int kk = 0; kk < n; kk++, pp += S) {
+            const R pk = __ldg(pp), lk = cl3[33 * kk];
+            const R ak = pk * k.inv_w + lk * k.w_pi2;
+            const R o1 = S1 - pk, o2 = S2 - pk * pk;
+            const R cap = (R)8 * (-k.sig * (A - ak) - k.tjh * (o1 * o1 - o2)) + lk;
+            cl3[33 * kk] = cap;
+            const R u = k.mob * (fn * cap - C);
+            const bool on = (pk > k.tol_gt && pk < k.tol1_lt) || (pk < k.tol_lt && u > (R)0) ||
+                            (pk > k.tol1_gt && u < (R)0);
+            act |= (uint32_t)on << kk;
+            nf += on ? (R)1 : (R)0;
+            Caf += on ? cap : (R)0;
         }
     }
     /* F = m (nact cap - Ca) / nact on the active slots, 0 elsewhere; slots
      * at or above the row's largest count are 0 for every lane */
-    const float scale = act ? a.mob_f * __frcp_rn(nf) : 0.0f;
-    float *fp = a.fphi + c;
+    const R scale = act ? k.mob * item_rcp(nf) : (R)0;
+    R *fp = a.fphi + c;
     int m = 0;
 #pragma unroll 2
     for (; m < maxn; m++) {
-        float vv = 0.0f;
-        if (act >> m & 1u) vv = scale * fmaf(nf, cl3[33 * m], -Caf);
+        R vv = (R)0;
+        if (act >> m & 1u) vv = scale * item_fma(nf, cl3[33 * m], -Caf);
         *fp = vv;
         fp += S;
     }
 #pragma unroll 2
     for (; m < P; m++) {
-        *fp = 0.0f;
+        *fp = (R)0;
         fp += S;
     }
-    double tr = 0.0;
-    if (a.has_temp_rate) tr += a.temp_rate;
-    a.ftm[c] = (float)tr;
+    R tr = (R)0;
+    if (a.has_temp_rate) tr += (R)a.temp_rate;
+    a.ftm[c] = tr;
 }
 
-template <int DIM, typename IX>
-__global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_mixed_items(const PfArgs<float> a)
+template <int DIM, typename IX, typename R>
+__global__ void __launch_bounds__(kMixedBlock) k_rhs_pf_items(const PfArgs<R> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const CellIndex ci = cell_index<kBX, kBY>(a.res, a.zbase);
-    mixed_items_tile<DIM, IX>(a, ci, smem);
+    items_tile<DIM, IX, R>(a, ci, smem);
 }
 
 /* one cell of the mixed RHS, several interfaces (reference-order cell terms in FP32) */
@@ -291,7 +302,7 @@ __global__ void __launch_bounds__(kBX * BY) k_rhs_pf_mixed_batched(const BatchTi
         int inst;
         const CellIndex ci = batch_cell_index<kBX, BY>(b, t, inst);
         if (!b.active[inst]) continue;          /* uniform across the block */
-        if (SINGLE) mixed_items_tile<DIM, IX>(b.args[inst], ci, smem);
+        if (SINGLE) items_tile<DIM, IX, float>(b.args[inst], ci, smem);
         else pf_mixed_multi_cell<DIM, PM>(b.args[inst], ci, sc);
     }
 }
@@ -313,21 +324,33 @@ static cudaError_t allow_smem(K kernel, size_t bytes)
     return e;
 }
 
+template <typename R, int DIM>
+static cudaError_t launch_items(const PfArgs<R> &a, dim3 grid, cudaStream_t s)
+{
+    const size_t sm = items_tile_bytes(kMixedBlock, a.P, (int)sizeof(R));
+    cudaError_t e;
+    if (items_fit_i32(a.stride, a.P, DIM)) {
+        if ((e = allow_smem(k_rhs_pf_items<DIM, int, R>, sm)) != cudaSuccess) return e;
+        k_rhs_pf_items<DIM, int, R><<<grid, kMixedBlock, sm, s>>>(a);
+    } else {
+        if ((e = allow_smem(k_rhs_pf_items<DIM, int64_t, R>, sm)) != cudaSuccess) return e;
+        k_rhs_pf_items<DIM, int64_t, R><<<grid, kMixedBlock, sm, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+static dim3 items_grid(const int *res, int zcount)
+{
+    return dim3((unsigned)((res[0] + kBX - 1) / kBX), (unsigned)((res[1] + kBY - 1) / kBY),
+                (unsigned)(zcount > 0 ? zcount : res[2]));
+}
+
 template <int DIM, int PM>
 static void launch_pm(const PfArgs<float> &a, cudaStream_t s)
 {
-    dim3 grid((unsigned)((a.res[0] + kBX - 1) / kBX), (unsigned)((a.res[1] + kBY - 1) / kBY),
-              (unsigned)(a.zcount > 0 ? a.zcount : a.res[2]));
+    const dim3 grid = items_grid(a.res, a.zcount);
     if (a.single) {
-        if (items_fit_i32(a.stride, a.P, DIM)) {
-            const size_t sm = items_tile_bytes(DIM, kMixedBlock, a.P, 4);
-            if (allow_smem(k_rhs_pf_mixed_items<DIM, int>, sm) != cudaSuccess) return;
-            k_rhs_pf_mixed_items<DIM, int><<<grid, kMixedBlock, sm, s>>>(a);
-        } else {
-            const size_t sm = items_tile_bytes(DIM, kMixedBlock, a.P, 8);
-            if (allow_smem(k_rhs_pf_mixed_items<DIM, int64_t>, sm) != cudaSuccess) return;
-            k_rhs_pf_mixed_items<DIM, int64_t><<<grid, kMixedBlock, sm, s>>>(a);
-        }
+        launch_items<float, DIM>(a, grid, s);
     } else {
         size_t sm = slot_columns_bytes(a.P, kMixedBlock, 4, true);
         k_rhs_pf_mixed_multi<DIM, PM><<<grid, kMixedBlock, sm, s>>>(a);
@@ -346,8 +369,7 @@ static void launch_dim(const PfArgs<float> &a, cudaStream_t s)
 template <int DIM, int PM, bool SINGLE, typename IX>
 static cudaError_t launch_batched_ix(const BatchTiles<float> &b, int by, int grid, cudaStream_t s)
 {
-    const size_t sm = SINGLE ? items_tile_bytes(DIM, kBX * by, b.pmax, (int)sizeof(IX))
-                             : slot_columns_bytes(b.pmax, kBX * by, 4, true);
+    const size_t sm = SINGLE ? items_tile_bytes(kBX * by, b.pmax, 4) : slot_columns_bytes(b.pmax, kBX * by, 4, true);
     cudaError_t e;
     if (by == 1) {
         if ((e = allow_smem(k_rhs_pf_mixed_batched<DIM, PM, SINGLE, 1, IX>, sm)) != cudaSuccess) return e;
@@ -385,6 +407,15 @@ cudaError_t launch_rhs_pf_batched(const BatchTiles<float> &b, int dim, int singl
     if (dim == 1) return launch_batched_dim<1>(b, single, by, grid, s);
     if (dim == 2) return launch_batched_dim<2>(b, single, by, grid, s);
     return launch_batched_dim<3>(b, single, by, grid, s);
+}
+
+/* the closed-form single-interface kernel on an FP64 state (FP64 arithmetic) */
+cudaError_t launch_rhs_items_fp64(const PfArgs<double> &a, int dim, cudaStream_t s)
+{
+    const dim3 grid = items_grid(a.res, a.zcount);
+    if (dim == 1) return launch_items<double, 1>(a, grid, s);
+    if (dim == 2) return launch_items<double, 2>(a, grid, s);
+    return launch_items<double, 3>(a, grid, s);
 }
 
 cudaError_t launch_rhs_phasefield(const PfArgs<float> &a, int dim, cudaStream_t s)

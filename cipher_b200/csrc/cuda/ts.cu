@@ -51,6 +51,7 @@ constexpr int kMaxStages = 4;
 struct PlaneGroup {
     int64_t offset;
     int nplanes, esize;
+    int per_slot;                   /* planes per active-set slot (PF 1, EX S); 0: not slot planes */
 };
 
 struct CombineArgs {
@@ -59,6 +60,9 @@ struct CombineArgs {
     PlaneGroup groups[4];
     int nk;
     const char *x;                  /* base state */
+    const uint16_t *nact;           /* active counts of x (AS plane 0): slots at or past a cell's count are
+                                       skipped; their derivatives are zero, so they change nothing and
+                                       add exact zeros to the error sum */
     const char *k[kMaxStages];      /* stage derivatives */
     double w[kMaxStages];           /* h * b_j (or h * a_ij) */
     double we[kMaxStages];          /* h * bhat_j (norm only) */
@@ -84,7 +88,7 @@ __device__ __forceinline__ void store_real(char *base, int esize, int64_t i, dou
  * arrays); the operations and their order are those of the FP64 path. */
 template <bool NORM, typename E>
 __device__ __forceinline__ double combine_cells(const CombineArgs &a, int nk, const double *w, const double *we,
-                                                int64_t off, int64_t c0, int64_t c1)
+                                                int64_t off, int64_t c0, int64_t c1, int slot)
 {
     const E *x = (const E *)(a.x + off);
     E *y = (E *)(a.y + off);
@@ -93,6 +97,7 @@ __device__ __forceinline__ double combine_cells(const CombineArgs &a, int nk, co
     for (int j = 0; j < kMaxStages; j++) kp[j] = j < nk ? (const E *)(a.k[j] + off) : x;
     double sum = 0.0;
     for (int64_t c = c0 + threadIdx.x; c < c1; c += kTsThreads) {
+        if (slot >= 0 && slot >= (int)__ldg(&a.nact[c])) continue;
         const double xv = (double)x[c];
         double acc = 0.0, acce = 0.0;
 #pragma unroll
@@ -130,8 +135,9 @@ __device__ __forceinline__ void rk_combine_block(const CombineArgs &a, int nk, c
         const int64_t off = g.offset + (int64_t)plane * a.stride * g.esize;
         const int64_t c0 = bx * kTsCellsPerBlock;
         const int64_t c1 = c0 + kTsCellsPerBlock < a.ncells ? c0 + kTsCellsPerBlock : a.ncells;
-        sum = g.esize == 8 ? combine_cells<NORM, double>(a, nk, w, we, off, c0, c1)
-                           : combine_cells<NORM, float>(a, nk, w, we, off, c0, c1);
+        const int slot = g.per_slot > 0 ? plane / g.per_slot : -1;
+        sum = g.esize == 8 ? combine_cells<NORM, double>(a, nk, w, we, off, c0, c1, slot)
+                           : combine_cells<NORM, float>(a, nk, w, we, off, c0, c1, slot);
     }
     if (NORM) {
         /* fixed-order block reduction: shuffle tree per warp, then the warps in order */
@@ -373,12 +379,13 @@ static CombineArgs make_combine(const cipher_state_layout &L, const cipher_ts_op
     a.ncells = L.ncells;
     a.stride = L.stride;
     int g = 0;
-    a.groups[g++] = {L.pf_offset, L.pf_size, esize};
-    if (L.dp_size) a.groups[g++] = {L.dp_offset, L.dp_size, 8};
-    if (L.ex_size) a.groups[g++] = {L.ex_offset, L.ex_size, 8};
-    a.groups[g++] = {L.tm_offset, 1, esize};
+    a.groups[g++] = {L.pf_offset, L.pf_size, esize, 1};
+    if (L.dp_size) a.groups[g++] = {L.dp_offset, L.dp_size, 8, 0};
+    if (L.ex_size) a.groups[g++] = {L.ex_offset, L.ex_size, 8, L.ex_size / L.pf_size};
+    a.groups[g++] = {L.tm_offset, 1, esize, 0};
     a.ngroups = g;
     a.x = (const char *)X;
+    a.nact = (const uint16_t *)((const char *)X + L.as_offset);
     a.y = (char *)Y;
     for (int j = 0; j < ns; j++) a.k[j] = (const char *)K[j];
     a.atol = o.abstol;
@@ -677,6 +684,8 @@ struct cipher_batch {
     int64_t *d_as_units, *d_as_start, as_total;          /* active sets X -> Y */
     void *d_post;
     int64_t *d_post_start, post_total;
+    int64_t *d_post_rows, post_row_total;
+    int post_pmax;
     /* control block: double h[n] | int active[n] | int accept[n] | int gactive[sum m] */
     char *d_ctl, *h_ctl;
     size_t ctl_bytes;
@@ -772,6 +781,7 @@ static void free_tables(cipher_batch *b)
     b->d_as_units = b->d_as_start = nullptr;
     b->d_post = nullptr;
     b->d_post_start = nullptr;
+    b->d_post_rows = nullptr;
     if (b->graph) cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
     b->stable_steps = 0;
@@ -1163,10 +1173,19 @@ static int rebuild(cipher_batch *b)
     }
     /* PostStep */
     {
-        std::vector<int64_t> st(1, 0);
-        for (int i = 0; i < n; i++) st.push_back(st.back() + (b->slots[b->dense[i]].lay.ncells + 255) / 256);
+        std::vector<int64_t> st(1, 0), rows(1, 0);
+        int pmax = 1;
+        for (int i = 0; i < n; i++) {
+            const BatchSlot &sl = b->slots[b->dense[i]];
+            st.push_back(st.back() + (sl.lay.ncells + 255) / 256);
+            rows.push_back(rows.back() + post_row_blocks(sl.info.res));
+            if (sl.lay.pf_size > pmax) pmax = sl.lay.pf_size;
+        }
         b->post_total = st.back();
+        b->post_row_total = rows.back();
+        b->post_pmax = pmax;
         stage(b, &b->d_post_start, st);
+        stage(b, &b->d_post_rows, rows);
         if (b->precision == CIPHER_PREC_FP64) {
             std::vector<PostArgs<double>> v;
             for (int i = 0; i < n; i++) {
@@ -1219,10 +1238,12 @@ static int launch_step(cipher_batch *b)
             const int dim = b->slots[b->dense[0]].info.dim;
             cudaError_t e;
             if (b->precision == CIPHER_PREC_FP64) {
-                BatchPost<double> p = {(const PostArgs<double> *)b->d_post, b->d_post_start, accept, n, b->post_total};
+                BatchPost<double> p = {(const PostArgs<double> *)b->d_post, b->d_post_start, accept, n, b->post_total,
+                                       b->d_post_rows, b->post_row_total, b->post_pmax};
                 e = launch_poststep_batched(p, dim, s);
             } else {
-                BatchPost<float> p = {(const PostArgs<float> *)b->d_post, b->d_post_start, accept, n, b->post_total};
+                BatchPost<float> p = {(const PostArgs<float> *)b->d_post, b->d_post_start, accept, n, b->post_total,
+                                      b->d_post_rows, b->post_row_total, b->post_pmax};
                 e = launch_poststep_batched(p, dim, s);
             }
             TS_CUDA(e, "batched poststep");

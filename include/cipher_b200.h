@@ -182,12 +182,16 @@ enum { CIPHER_PREC_FP64 = 0,    /* plain FP64 drop-in */
 /*
  * Device state layout (structure of arrays, plane-major, one plane per slot):
  *   AS  uint16 [P+1][stride]   plane 0 = active count n, planes 1..P = sorted ids
- *   MAP uint64 [2*dim][stride] per cell and face direction (2d: lower, 2d+1:
- *                              upper neighbour along d): 4 bits per own slot,
- *                              the neighbour's slot of the same phase or 15;
- *                              all 15 where the reference's face gate is off.
- *                              Derived from AS: rebuilt by cipher_poststep,
- *                              cipher_state_from_aos and cipher_state_refresh
+ *   MAP uint32 [P][stride]     face maps (uniform grids): for each active slot k
+ *                              < n, bits 4q..4q+3 of word [k][cell] hold the
+ *                              slot of the same phase in the neighbour across
+ *                              face q (q = 2d: lower, 2d+1: upper neighbour
+ *                              along d), or 15 where the neighbour lacks it or
+ *                              the reference's face gate is off; words of
+ *                              slots >= n are unspecified.  Derived from AS:
+ *                              rebuilt by cipher_poststep,
+ *                              cipher_state_from_aos and cipher_state_refresh.
+ *                              Adapted meshes have none (map_planes 0).
  *   PF  real   [P][stride]     phase fractions of the active phases
  *   DP  double [D][stride]     diffusion potentials mu
  *   EX  double [P*S][stride]   explicit site potentials, slot g*S+s*D+c
@@ -205,7 +209,7 @@ typedef struct cipher_state_layout {
     int64_t as_offset, pf_offset, dp_offset, ex_offset, tm_offset;
     int64_t bytes;       /* total bytes of one state vector */
     int64_t map_offset;  /* MAP region (between AS and PF) */
-    int32_t map_planes;  /* 2*dim */
+    int32_t map_planes;  /* P (uniform grids) or 0 (adapted meshes) */
 } cipher_state_layout;
 
 /* create a context on `device` for problem p over mesh m (owned cells only;
@@ -217,6 +221,13 @@ int cipher_ctx_layout(const cipher_ctx *c, cipher_state_layout *out);
 
 /* F = RHS(t, X) over all owned cells; X and F are device state vectors */
 int cipher_rhs(cipher_ctx *c, double t, const void *X, void *F, void *stream);
+
+/* which kernel an FP64 grain-growth context with a single interface uses:
+ * the reference's operation order (default; bit-identical to the
+ * reference), or the O(n) closed form of the pair and triple sums that the
+ * mixed path uses, in FP64 (equal to the reference within rounding) */
+enum { CIPHER_RHS_REFERENCE_ORDER = 0, CIPHER_RHS_CLOSED_FORM = 1 };
+int cipher_ctx_set_rhs_form(cipher_ctx *c, int form);
 
 /* per-step active-set update of X in place: Gibbs-simplex projection, prune
  * phi <= TOL, union with the face neighbours' pruned sets, reorder PF/EX.
@@ -261,7 +272,7 @@ typedef struct cipher_grid_desc {
     int32_t periodic[3];
     int32_t ex_per_phase;        /* S: explicit site potentials per phase, 0..2*CIPHER_MAXCP;
                                     layout.ex_size must be pf_size*S */
-    cipher_state_layout layout;  /* offsets of the state planes (see above); map_planes 0 or 2*dim */
+    cipher_state_layout layout;  /* offsets of the state planes (see above); map_planes 0 or P */
     int32_t npf;                 /* phases of the problem: a set holding an id >= npf is a bad set */
     int32_t ncp, nmat;           /* components and materials (read when S > 0) */
     /* device copies of the problem's material[nmat] and phasematerialmapping[npf]

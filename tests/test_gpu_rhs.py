@@ -197,3 +197,20 @@ def test_full_size_config_properties():
     assert np.all(phi_rate[n == 1] == 0)
     Fo = oracle.port_rhs(P, M, X)
     assert np.array_equal(F, Fo)
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_rhs_fp64_closed_form_within_1e10(case):
+    """the closed-form single-interface kernel on an FP64 state: the pair and
+    triple sums of the reference summed in another order, so equal to the
+    reference within FP64 rounding: max|dF|/max|F| <= 1e-10"""
+    P, M, X = _build(*case[1:])
+    ctx = cb.Context(P, M, "fp64")
+    ctx.set_rhs_form("closed")
+    F = _device_rhs(ctx, X)
+    Fo = _oracle_rhs(P, M, X)
+    L = P.aos
+    sl = slice(L.pf_offset, L.pf_offset + P.s.pf_size)
+    err = np.abs(F[:, sl] - Fo[:, sl]).max() / np.abs(Fo[:, sl]).max()
+    assert err <= 1e-10, err
+    assert np.array_equal(F[:, L.tm_offset], Fo[:, L.tm_offset])

@@ -157,4 +157,4 @@ def test_noalloc_rejects_inconsistent_descriptions():
     assert rc(phasematerialmapping=None) == L.E_ARG
     assert rc(npf=0) == L.E_ARG
     assert rc(ncp=1) == L.E_ARG
-    assert rc(layout_map_planes=3) == L.E_ARG            # neither 0 nor 2*dim
+    assert rc(layout_map_planes=3) == L.E_ARG            # neither 0 nor P
