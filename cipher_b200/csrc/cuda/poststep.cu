@@ -17,6 +17,7 @@
  * phase sets are decided by the same arithmetic as the reference.
  */
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 #include "device_common.cuh"
 #include "kernels.h"
@@ -41,9 +42,15 @@ __device__ __forceinline__ void post_prune_cell(const PostArgs<R> &a, int64_t c)
         return;
     }
     double phi[PM], s[PM];
+    uint16_t ids[PM];
+    /* every load of the cell issued together */
 #pragma unroll
     for (int g = 0; g < PM; g++)
-        if (g < n) { phi[g] = (double)a.phi[(int64_t)g * S + c]; s[g] = phi[g]; }
+        if (g < n) {
+            phi[g] = (double)a.phi[(int64_t)g * S + c];
+            ids[g] = a.as[(int64_t)(1 + g) * S + c];
+            s[g] = phi[g];
+        }
     /* sort a copy in descending order (insertion sort; n <= 16) */
     for (int i = 1; i < n; i++) {
         double v = s[i];
@@ -66,7 +73,7 @@ __device__ __forceinline__ void post_prune_cell(const PostArgs<R> &a, int64_t c)
             double v = phi[g] - tmax > 0.0 ? phi[g] - tmax : 0.0;
             a.phi[(int64_t)g * S + c] = (R)v;
             if (v > CIPHER_TOL) {
-                a.pruned[(int64_t)(1 + np) * S + c] = a.as[(int64_t)(1 + g) * S + c];
+                a.pruned[(int64_t)(1 + np) * S + c] = ids[g];
                 np++;
             }
         }
@@ -75,7 +82,7 @@ __device__ __forceinline__ void post_prune_cell(const PostArgs<R> &a, int64_t c)
 }
 
 template <int PM, typename R>
-__global__ void __launch_bounds__(256) k_post_prune(const PostArgs<R> a)
+__global__ void __launch_bounds__(256, 4) k_post_prune(const PostArgs<R> a)
 {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= a.ncells) return;
@@ -208,12 +215,26 @@ constexpr int kPostRowWarps = 4;
  * count, 1..P ids; then two halo cells [2][P+1] */
 __host__ __device__ constexpr size_t post_stage_elems(int P) { return (size_t)5 * (P + 1) * 32 + 2 * (P + 1); }
 
-__host__ __device__ constexpr size_t post_row_warp_bytes(int P)
+/* a warp's slice of shared memory, each region on a 16-byte boundary:
+ * staged sets (uint16), then the per-lane work columns - two uint16
+ * superset columns [P][32] (union) or one uint32 map-word column [P][32]
+ * (maps) - then an 8-byte column [P][32] (the union's old phase fractions) */
+__host__ __device__ constexpr size_t post_stage_bytes(int P) { return (post_stage_elems(P) * 2 + 15) / 16 * 16; }
+__host__ __device__ constexpr size_t post_work_offset(int P) { return post_stage_bytes(P); }
+__host__ __device__ constexpr size_t post_old_offset(int P) { return post_stage_bytes(P) + (size_t)P * 32 * 4; }
+__host__ __device__ constexpr size_t post_row_warp_bytes(int P) { return post_old_offset(P) + (size_t)P * 32 * 8; }
+/* the face-map kernel needs no old-phase column */
+__host__ __device__ constexpr size_t maps_row_warp_bytes(int P) { return post_old_offset(P); }
+
+/* 16-byte asynchronous copies global -> shared (no registers held) */
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc)
 {
-    /* staged sets, then the per-lane work columns: two uint16 superset
-     * columns [P][32] each (union) or one uint32 map-word column [P][32]
-     * (maps) */
-    return (post_stage_elems(P) * 2 + (size_t)P * 32 * 4 + 15) / 16 * 16;
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
 struct RowCells {
@@ -267,13 +288,43 @@ __device__ __forceinline__ int x_nb(const int *res, const int *per, int x, int s
 }
 
 /* stage the sets held in planes (count plane, then P id planes, stride S) of
- * the row, its neighbour rows and its two outer x neighbours */
-template <int DIM>
+ * the row, its neighbour rows and its two outer x neighbours.  When rows are
+ * whole 32-cell segments (res[0] a multiple of 32, so every row segment of a
+ * plane is 64 bytes on a 16-byte boundary: planes start on 256-byte
+ * boundaries and strides are multiples of 128) every plane of every row is
+ * copied with 16-byte asynchronous copies, all in flight together;
+ * otherwise a row's loads are issued together (unrolled to PM) before they
+ * are stored.  Staged counts are the raw counts; readers clamp them to P. */
+template <int DIM, int PM>
 __device__ __forceinline__ void stage_row_sets(const uint16_t *planes, int64_t S, int P, const int *res, const int *per,
                                                const RowCells &r, uint16_t *st, bool *row_present)
 {
     const int lane = threadIdx.x & 31;
     const int P1 = P + 1;
+    /* whole 64-byte row segments on 16-byte boundaries (checked, not assumed) */
+    const bool bulk = (res[0] & 31) == 0 && ((uintptr_t)planes & 15) == 0 && (S & 7) == 0;
+    if (bulk) {
+        const int64_t crow = r.c - lane;          /* first cell of the row */
+        for (int row = 0; row < 5; row++) {
+            int64_t off = 0;
+            bool present = row == 0;
+            if (row > 0) {
+                const int d = (row + 1) >> 1;
+                if (d < DIM) {
+                    off = row_offset(res, per, r, d, (row + 1) & 1);
+                    present = off != INT64_MIN;
+                }
+            }
+            row_present[row] = present;
+            if (!present) continue;
+            uint16_t *rs = st + (size_t)row * P1 * 32;
+            const uint16_t *src = planes + crow + off;
+            for (int j = lane; j < P1 * 4; j += 32) {
+                const int k = j >> 2, ch = j & 3;
+                cp_async16(rs + k * 32 + ch * 8, src + (int64_t)k * S + ch * 8);
+            }
+        }
+    } else {
     for (int row = 0; row < 5; row++) {
         int64_t off = 0;
         bool present = row == 0;
@@ -291,9 +342,14 @@ __device__ __forceinline__ void stage_row_sets(const uint16_t *planes, int64_t S
         int n = r.live ? (int)planes[cc] : 0;
         if (n > P) n = P;
         rs[lane] = (uint16_t)n;
-        const int maxn = __reduce_max_sync(0xffffffffu, n);
-        for (int k = 0; k < maxn; k++)
-            if (k < n) rs[(1 + k) * 32 + lane] = planes[(int64_t)(1 + k) * S + cc];
+        uint16_t v[PM];
+#pragma unroll
+        for (int k = 0; k < PM; k++)
+            if (k < n) v[k] = planes[(int64_t)(1 + k) * S + cc];
+#pragma unroll
+        for (int k = 0; k < PM; k++)
+            if (k < n) rs[(1 + k) * 32 + lane] = v[k];
+    }
     }
     /* the lower x neighbour of the first lane and the upper one of the last
      * live lane, when they lie outside the row */
@@ -308,9 +364,16 @@ __device__ __forceinline__ void stage_row_sets(const uint16_t *planes, int64_t S
             int n = planes[cc];
             if (n > P) n = P;
             h[0] = (uint16_t)n;
-            for (int k = 0; k < n; k++) h[1 + k] = planes[(int64_t)(1 + k) * S + cc];
+            uint16_t v[PM];
+#pragma unroll
+            for (int k = 0; k < PM; k++)
+                if (k < n) v[k] = planes[(int64_t)(1 + k) * S + cc];
+#pragma unroll
+            for (int k = 0; k < PM; k++)
+                if (k < n) h[1 + k] = v[k];
         }
     }
+    if (bulk) cp_async_wait_all();
     __syncwarp();
 }
 
@@ -332,7 +395,7 @@ __device__ __forceinline__ int staged_nb(const uint16_t *st, int P, const int *r
             const uint16_t *rs = st + (xn - r.x0);
             ids = rs + 32;
             stride = 32;
-            return rs[0];
+            return rs[0] < P ? rs[0] : P;
         }
         const uint16_t *h = st + (size_t)5 * P1 * 32 + side * P1;   /* only the first / last lane gets here */
         ids = h + 1;
@@ -344,11 +407,14 @@ __device__ __forceinline__ int staged_nb(const uint16_t *st, int P, const int *r
     const uint16_t *rs = st + (size_t)row * P1 * 32 + lane;
     ids = rs + 32;
     stride = 32;
-    return rs[0];
+    return rs[0] < P ? rs[0] : P;
 }
 
-/* union of this lane's pruned set with its face neighbours' (all staged) */
-template <int DIM, int PM, typename R>
+/* union of this lane's pruned set with its face neighbours' (all staged).
+ * EX: the state has explicit site potentials to move or initialise (the
+ * per-cell form with its local tables); without them only phase fractions
+ * move, through this lane's shared columns. */
+template <int DIM, int PM, typename R, bool EX>
 __device__ __forceinline__ void post_union_row(const PostArgs<R> &a, int64_t rb, unsigned char *wsm)
 {
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -356,9 +422,9 @@ __device__ __forceinline__ void post_union_row(const PostArgs<R> &a, int64_t rb,
     if (!row_of<DIM>(a.res, rb, wib, r)) return;           /* whole warp */
     const int P = a.P;
     uint16_t *st = (uint16_t *)wsm;
-    uint16_t *supA = st + post_stage_elems(P), *supB = supA + P * 32;
+    uint16_t *supA = (uint16_t *)(wsm + post_work_offset(P)), *supB = supA + P * 32;
     bool present[5];
-    stage_row_sets<DIM>(a.pruned, a.stride, P, a.res, a.per, r, st, present);
+    stage_row_sets<DIM, PM>(a.pruned, a.stride, P, a.res, a.per, r, st, present);
     if (!r.live) return;
     const int n = a.as[r.c];
     int ns = st[lane];
@@ -391,17 +457,52 @@ __device__ __forceinline__ void post_union_row(const PostArgs<R> &a, int64_t rb,
         nxt = t;
         ns = m;
     }
-    uint16_t sup[PM];
-    for (int k = 0; k < ns; k++) sup[k] = cur[k * 32];
-    post_write_cell<PM, R>(a, r.c, n, ns, sup);
+    if (EX) {
+        uint16_t sup[PM];
+        for (int k = 0; k < ns; k++) sup[k] = cur[k * 32];
+        post_write_cell<PM, R>(a, r.c, n, ns, sup);
+        return;
+    }
+    /* phase fractions only: the cell's old ids and phi go to this lane's
+     * own shared columns (loads four at a time); then the superset is
+     * written slot by slot (survivors keep phi, new phases get 0) */
+    const int64_t S = a.stride;
+    uint16_t *oid = nxt;                                  /* the free superset column */
+    double *oph = (double *)(wsm + post_old_offset(P)) + lane;
+    for (int k0 = 0; k0 < n; k0 += 4) {
+        R v[4];
+        uint16_t id[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (k0 + j < n) { id[j] = a.as[(int64_t)(1 + k0 + j) * S + r.c]; v[j] = a.phi[(int64_t)(k0 + j) * S + r.c]; }
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (k0 + j < n) { oid[(k0 + j) * 32] = id[j]; oph[(k0 + j) * 32] = (double)v[j]; }
+    }
+    /* a superset equal to the old set changes nothing: every phase keeps its
+     * slot and its (projected) phase fraction */
+    if (ns == n) {
+        bool same = true;
+        for (int g = 0; g < ns && same; g++) same = cur[g * 32] == oid[g * 32];
+        if (same) return;
+    }
+    int i = 0;
+    for (int g = 0; g < ns; g++) {
+        const uint16_t idg = cur[g * 32];
+        while (i < n && oid[i * 32] < idg) i++;
+        const R v = (i < n && oid[i * 32] == idg) ? (R)oph[i * 32] : (R)0;
+        a.phi[(int64_t)g * S + r.c] = v;
+    }
+    a.as[r.c] = (uint16_t)ns;
+    for (int g = 0; g < ns; g++) a.as[(int64_t)(1 + g) * S + r.c] = cur[g * 32];
 }
 
-template <int DIM, int PM, typename R>
+template <int DIM, int PM, typename R, bool EX>
 __global__ void __launch_bounds__(32 * kPostRowWarps) k_post_union_rows(const PostArgs<R> a, int64_t rb0)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char *wsm = smem + (size_t)(threadIdx.x >> 5) * post_row_warp_bytes(a.P);
-    post_union_row<DIM, PM, R>(a, rb0 + blockIdx.x, wsm);
+    post_union_row<DIM, PM, R, EX>(a, rb0 + blockIdx.x, wsm);
 }
 
 /*
@@ -412,7 +513,7 @@ __global__ void __launch_bounds__(32 * kPostRowWarps) k_post_union_rows(const Po
  * fails the phase-flux gate of src/cipher.c:277.  Bad sets raise
  * ERR_BADSET.
  */
-template <int DIM, typename R>
+template <int DIM, int PM, typename R>
 __device__ __forceinline__ void build_maps_row(const PostArgs<R> &a, int64_t rb, unsigned char *wsm)
 {
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -421,9 +522,9 @@ __device__ __forceinline__ void build_maps_row(const PostArgs<R> &a, int64_t rb,
     const int P = a.P;
     const int64_t S = a.stride;
     uint16_t *st = (uint16_t *)wsm;
-    uint32_t *mw = (uint32_t *)(st + post_stage_elems(P));   /* 4-byte aligned: 324 (P+1) bytes of staging */
+    uint32_t *mw = (uint32_t *)(wsm + post_work_offset(P));
     bool present[5];
-    stage_row_sets<DIM>(a.as, S, P, a.res, a.per, r, st, present);
+    stage_row_sets<DIM, PM>(a.as, S, P, a.res, a.per, r, st, present);
     if (!r.live) return;
     const int n = a.as[r.c];
     bool ok = n >= 1 && n <= P;
@@ -463,12 +564,29 @@ __device__ __forceinline__ void build_maps_row(const PostArgs<R> &a, int64_t rb,
     for (int k = 0; k < n; k++) a.maps[(int64_t)k * S + r.c] = w[k * 32];
 }
 
-template <int DIM, typename R>
+template <int DIM, int PM, typename R>
 __global__ void __launch_bounds__(32 * kPostRowWarps) k_build_maps_rows(const PostArgs<R> a, int64_t rb0)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    unsigned char *wsm = smem + (size_t)(threadIdx.x >> 5) * post_row_warp_bytes(a.P);
-    build_maps_row<DIM, R>(a, rb0 + blockIdx.x, wsm);
+    unsigned char *wsm = smem + (size_t)(threadIdx.x >> 5) * maps_row_warp_bytes(a.P);
+    build_maps_row<DIM, PM, R>(a, rb0 + blockIdx.x, wsm);
+}
+
+/* the kernels' slot arrays are sized by a bucket of P: 4, 8, 12 or 16 */
+template <typename F>
+__host__ inline cudaError_t with_pm(int P, F f)
+{
+    if (P <= 4) return f(std::integral_constant<int, 4>());
+    if (P <= 8) return f(std::integral_constant<int, 8>());
+    if (P <= 12) return f(std::integral_constant<int, 12>());
+    return f(std::integral_constant<int, 16>());
+}
+template <typename F>
+__host__ inline cudaError_t with_dim(int dim, F f)
+{
+    if (dim == 1) return f(std::integral_constant<int, 1>());
+    if (dim == 2) return f(std::integral_constant<int, 2>());
+    return f(std::integral_constant<int, 3>());
 }
 
 /* row blocks of a grid (4 rows of 32 cells each) and of its z-planes [z0, z1) */
@@ -485,11 +603,13 @@ static cudaError_t launch_maps(const PostArgs<R> &a, int dim, int64_t z0, int64_
     if (!a.maps || z1 <= z0) return cudaSuccess;
     const int64_t per = row_blocks_per_plane(a.res);
     const unsigned blocks = (unsigned)((z1 - z0) * per);
-    const size_t sm = kPostRowWarps * post_row_warp_bytes(a.P);
-    if (dim == 1) k_build_maps_rows<1, R><<<blocks, 32 * kPostRowWarps, sm, s>>>(a, z0 * per);
-    else if (dim == 2) k_build_maps_rows<2, R><<<blocks, 32 * kPostRowWarps, sm, s>>>(a, z0 * per);
-    else k_build_maps_rows<3, R><<<blocks, 32 * kPostRowWarps, sm, s>>>(a, z0 * per);
-    return cudaGetLastError();
+    const size_t sm = kPostRowWarps * maps_row_warp_bytes(a.P);
+    return with_dim(dim, [&](auto D) {
+        return with_pm(a.P, [&](auto PMC) {
+            k_build_maps_rows<D(), PMC(), R><<<blocks, 32 * kPostRowWarps, sm, s>>>(a, z0 * per);
+            return cudaGetLastError();
+        });
+    });
 }
 
 cudaError_t launch_build_maps(const PostArgs<double> &a, int dim, cudaStream_t s) { return launch_maps(a, dim, 0, a.res[2], s); }
@@ -529,18 +649,19 @@ __global__ void __launch_bounds__(256) k_post_prune_batched(const BatchPost<R> b
     post_prune_cell<PM, R>(a, c);
 }
 
-template <int DIM, int PM, typename R>
+template <int DIM, int PM, typename R, bool EX>
 __global__ void __launch_bounds__(32 * kPostRowWarps) k_post_union_rows_batched(const BatchPost<R> b)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int inst = batch_domain_of(b.row_start, b.n, blockIdx.x);
     if (!b.active[inst]) return;
     const PostArgs<R> &a = b.args[inst];
+    if ((a.S > 0) != EX) return;                          /* the other kind's launch takes it */
     unsigned char *wsm = smem + (size_t)(threadIdx.x >> 5) * post_row_warp_bytes(b.pmax);
-    post_union_row<DIM, PM, R>(a, blockIdx.x - b.row_start[inst], wsm);
+    post_union_row<DIM, PM, R, EX>(a, blockIdx.x - b.row_start[inst], wsm);
 }
 
-template <int DIM, typename R>
+template <int DIM, int PM, typename R>
 __global__ void __launch_bounds__(32 * kPostRowWarps) k_build_maps_rows_batched(const BatchPost<R> b)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -549,27 +670,30 @@ __global__ void __launch_bounds__(32 * kPostRowWarps) k_build_maps_rows_batched(
     const PostArgs<R> &a = b.args[inst];
     if (!a.maps) return;
     unsigned char *wsm = smem + (size_t)(threadIdx.x >> 5) * post_row_warp_bytes(b.pmax);
-    build_maps_row<DIM, R>(a, blockIdx.x - b.row_start[inst], wsm);
+    build_maps_row<DIM, PM, R>(a, blockIdx.x - b.row_start[inst], wsm);
 }
 
 template <typename R>
 static cudaError_t launch_post_batched(const BatchPost<R> &b, int dim, cudaStream_t s)
 {
     if (b.total < 1) return cudaSuccess;
-    k_post_prune_batched<CIPHER_PMAX, R><<<(unsigned)b.total, 256, 0, s>>>(b);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = with_pm(b.pmax, [&](auto PMC) {
+        k_post_prune_batched<PMC(), R><<<(unsigned)b.total, 256, 0, s>>>(b);
+        return cudaGetLastError();
+    });
     if (e != cudaSuccess) return e;
     const size_t sm = kPostRowWarps * post_row_warp_bytes(b.pmax);
     const unsigned rb = (unsigned)b.row_total;
     const unsigned bs = 32 * kPostRowWarps;
-    if (dim == 1) k_post_union_rows_batched<1, CIPHER_PMAX, R><<<rb, bs, sm, s>>>(b);
-    else if (dim == 2) k_post_union_rows_batched<2, CIPHER_PMAX, R><<<rb, bs, sm, s>>>(b);
-    else k_post_union_rows_batched<3, CIPHER_PMAX, R><<<rb, bs, sm, s>>>(b);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (dim == 1) k_build_maps_rows_batched<1, R><<<rb, bs, sm, s>>>(b);
-    else if (dim == 2) k_build_maps_rows_batched<2, R><<<rb, bs, sm, s>>>(b);
-    else k_build_maps_rows_batched<3, R><<<rb, bs, sm, s>>>(b);
-    return cudaGetLastError();
+    return with_dim(dim, [&](auto D) {
+        return with_pm(b.pmax, [&](auto PMC) {
+            /* domains with and without site potentials: one launch each */
+            k_post_union_rows_batched<D(), PMC(), R, false><<<rb, bs, sm, s>>>(b);
+            k_post_union_rows_batched<D(), PMC(), R, true><<<rb, bs, sm, s>>>(b);
+            k_build_maps_rows_batched<D(), PMC(), R><<<rb, bs, sm, s>>>(b);
+            return cudaGetLastError();
+        });
+    });
 }
 
 cudaError_t launch_poststep_batched(const BatchPost<double> &b, int dim, cudaStream_t s) { return launch_post_batched(b, dim, s); }
@@ -579,8 +703,10 @@ template <typename R>
 static cudaError_t launch_post(const PostArgs<R> &a, int dim, cudaStream_t s)
 {
     const unsigned blocks = (unsigned)((a.ncells + 255) / 256);
-    k_post_prune<CIPHER_PMAX, R><<<blocks, 256, 0, s>>>(a);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = with_pm(a.P, [&](auto PMC) {
+        k_post_prune<PMC(), R><<<blocks, 256, 0, s>>>(a);
+        return cudaGetLastError();
+    });
     if (e != cudaSuccess) return e;
     if (a.fl.start) {
         /* adapted meshes: neighbours from the face lists, no face maps */
@@ -589,10 +715,14 @@ static cudaError_t launch_post(const PostArgs<R> &a, int dim, cudaStream_t s)
     }
     const size_t sm = kPostRowWarps * post_row_warp_bytes(a.P);
     const unsigned rb = (unsigned)row_blocks(a.res);
-    if (dim == 1) k_post_union_rows<1, CIPHER_PMAX, R><<<rb, 32 * kPostRowWarps, sm, s>>>(a, 0);
-    else if (dim == 2) k_post_union_rows<2, CIPHER_PMAX, R><<<rb, 32 * kPostRowWarps, sm, s>>>(a, 0);
-    else k_post_union_rows<3, CIPHER_PMAX, R><<<rb, 32 * kPostRowWarps, sm, s>>>(a, 0);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    e = with_dim(dim, [&](auto D) {
+        return with_pm(a.P, [&](auto PMC) {
+            if (a.S > 0) k_post_union_rows<D(), PMC(), R, true><<<rb, 32 * kPostRowWarps, sm, s>>>(a, 0);
+            else k_post_union_rows<D(), PMC(), R, false><<<rb, 32 * kPostRowWarps, sm, s>>>(a, 0);
+            return cudaGetLastError();
+        });
+    });
+    if (e != cudaSuccess) return e;
     return launch_maps(a, dim, 0, a.res[2], s);
 }
 
