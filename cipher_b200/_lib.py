@@ -133,6 +133,11 @@ class TSOpts(C.Structure):
                 ("dtmax", C.c_double), ("reltol", C.c_double), ("abstol", C.c_double), ("max_steps", C.c_int64)]
 
 
+class AMROpts(C.Structure):
+    _fields_ = [("nblocks", C.c_int32 * 3), ("lmin", C.c_int32), ("lmax", C.c_int32), ("initcoarsen", C.c_int32),
+                ("interval", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32), ("ts", TSOpts)]
+
+
 class TSStats(C.Structure):
     _fields_ = [("steps", C.c_int64), ("rejected", C.c_int64), ("rhs_calls", C.c_int64), ("t", C.c_double),
                 ("dt", C.c_double), ("last_norm", C.c_double)]
@@ -187,6 +192,11 @@ _SIGNATURES = [
     ("cipher_abi_sizes", C.c_int, [C.POINTER(C.c_int64), C.c_int]),
     ("cipher_pool_trim", C.c_int, [C.c_int]),
     ("cipher_ctx_set_rhs_form", C.c_int, [C.c_void_p, C.c_int]),
+    ("cipher_amr_create", C.c_int, [PP, C.POINTER(AMROpts), C.POINTER(C.c_void_p)]),
+    ("cipher_amr_destroy", None, [C.c_void_p]),
+    ("cipher_amr_solve", C.c_int, [C.c_void_p, C.c_double, C.c_int64, C.c_void_p]),
+    ("cipher_amr_state", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(MP),
+                                   C.POINTER(C.c_int64)]),
     ("cipher_forest_create", C.c_int, [C.c_int, C.POINTER(C.c_int32), C.c_int, C.c_int, C.c_int,
                                        C.POINTER(C.c_int32), C.POINTER(C.c_double), C.POINTER(C.c_void_p)]),
     ("cipher_forest_destroy", None, [C.c_void_p]),

@@ -229,6 +229,61 @@ class Forest:
             pass
 
 
+class AMR:
+    """Time stepping with adaptive refinement (cipher_amr_*): the reference's
+    main loop with its forest - initial coarsening of the SetUpProblem state,
+    then an adaptation every `interval` accepted steps, the state moved on the
+    device."""
+
+    def __init__(self, problem: Problem, nblocks, lmin: int, lmax: int, initcoarsen: int, interval: int,
+                 opts: L.TSOpts, precision: str = "fp64", device: int = 0):
+        self._lib = L.load()
+        o = L.AMROpts()
+        for d, v in enumerate(list(nblocks) + [1] * (3 - len(nblocks))):
+            o.nblocks[d] = v
+        o.lmin, o.lmax, o.initcoarsen, o.interval = lmin, lmax, initcoarsen, interval
+        o.precision = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}[precision]
+        o.device = device
+        o.ts = opts
+        out = C.c_void_p()
+        L.check(self._lib.cipher_amr_create(problem.ptr, C.byref(o), C.byref(out)), "cipher_amr_create")
+        self.ptr = out
+        self.problem = problem
+        self.device = device
+
+    def solve(self, t_end: float, max_steps: int = 0) -> L.TSStats:
+        st = L.TSStats()
+        L.check(self._lib.cipher_amr_solve(self.ptr, float(t_end), int(max_steps), C.byref(st)), "cipher_amr_solve")
+        return st
+
+    def state(self):
+        """(context pointer, device state pointer, mesh struct, adaptations)"""
+        ctx, X, m, n = C.c_void_p(), C.c_void_p(), L.MP(), C.c_int64()
+        L.check(self._lib.cipher_amr_state(self.ptr, C.byref(ctx), C.byref(X), C.byref(m), C.byref(n)),
+                "cipher_amr_state")
+        return ctx, X, m.contents, n.value
+
+    def state_aos(self) -> np.ndarray:
+        """the current state in the reference AoS layout (host)"""
+        import torch
+        ctx, X, m, _ = self.state()
+        out = torch.empty((int(m.ncells), self.problem.ndof), dtype=torch.float64, device=f"cuda:{self.device}")
+        L.check(self._lib.cipher_state_to_aos(ctx, X, C.c_void_p(out.data_ptr()), None), "cipher_state_to_aos")
+        torch.cuda.synchronize(self.device)
+        return out.cpu().numpy()
+
+    def close(self):
+        if self.ptr:
+            self._lib.cipher_amr_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def initial_state_aos(problem: Problem, mesh: Mesh) -> np.ndarray:
     """SetUpProblem's state (src/init.c:1721-1830) in the reference AoS layout."""
     lib = L.load()

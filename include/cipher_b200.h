@@ -349,6 +349,33 @@ int cipher_ts_set_dt(cipher_ts *ts, double dt);
 int cipher_ts_set_nucleation(cipher_ts *ts, struct cipher_nucleation *nu);
 
 /* ------------------------------------------------------------------ */
+/* time stepping with adaptive refinement (the reference's main loop     */
+/* with AMR, src/cipher.c:1365-1606 and 1607-1829)                      */
+/* ------------------------------------------------------------------ */
+
+typedef struct cipher_amr_opts {
+    int32_t nblocks[3];          /* forest blocks per direction (the brick of the reference's forest) */
+    int32_t lmin, lmax;          /* minnrefine / maxnrefine; lmax is the voxel grid's level */
+    int32_t initcoarsen;         /* adaptations of the initial state (initcoarsen) */
+    int32_t interval;            /* accepted steps between adaptations (amrinterval) */
+    int32_t precision, device;
+    cipher_ts_opts ts;           /* stepper options (max_steps is replaced by interval) */
+} cipher_amr_opts;
+
+typedef struct cipher_amr cipher_amr;
+
+/* the forest at the finest level, the SetUpProblem state (chemistry from c0
+ * on the device), `initcoarsen` adaptations by the reference's marks, then
+ * a device context and stepper over the adapted mesh.  p must outlive it. */
+int cipher_amr_create(const cipher_problem *p, const cipher_amr_opts *o, cipher_amr **out);
+void cipher_amr_destroy(cipher_amr *a);
+/* step to t_end (or max_steps accepted steps, 0 = no limit), adapting
+ * every `interval` accepted steps; stats accumulate over the adaptations */
+int cipher_amr_solve(cipher_amr *a, double t_end, int64_t max_steps, cipher_ts_stats *stats);
+/* the current context, device state, mesh and number of adaptations so far */
+int cipher_amr_state(const cipher_amr *a, cipher_ctx **ctx, void **X, const cipher_mesh **m, int64_t *adaptations);
+
+/* ------------------------------------------------------------------ */
 /* many independent domains stepped together                           */
 /* (no counterpart in the reference, which runs one domain per job)    */
 /* ------------------------------------------------------------------ */

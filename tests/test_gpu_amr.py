@@ -173,3 +173,81 @@ def test_adapt_loop_matches_cpu_restatement():
         m = n > k
         assert np.array_equal(Xd[m, 1 + k], Xo[m, 1 + k])
         assert np.array_equal(Xd[m, A.pf_offset + k], Xo[m, A.pf_offset + k])
+
+
+def _cpu_amr_loop(P, nblocks, lmin, lmax, initcoarsen, interval, opts, t_end):
+    """the same loop with the CPU restatement of the stepper and the host
+    forest: initial coarsening, then `interval` accepted steps between
+    adaptations, the step size carried over"""
+    from cipher_b200 import _lib as L
+    F = cb.Forest(P.s.dim, nblocks, lmin, lmax, periodic=tuple(P.s.periodic[d] for d in range(3)))
+    M = F.mesh(P)
+    X = cb.initial_state_aos(P, M)
+    for _ in range(initcoarsen):
+        F.adapt(F.mark_active(X), X, P.aos.pf_offset)
+        X = F.transfer_aos(X)
+        M = F.mesh(P)
+    X = np.ascontiguousarray(X)
+    t, steps, dt, nad = 0.0, 0, None, 0
+    while t < t_end:
+        o = L.TSOpts.from_buffer_copy(opts)
+        o.max_steps = interval
+        if dt is not None:
+            o.dt0 = dt
+        ts = oracle.PortTS(P, M, o)
+        st = ts.solve(X, t, t_end, L.TSStats())
+        t, dt = st.t, st.dt
+        steps += st.steps
+        ts.close()
+        if t < t_end and st.steps >= interval:
+            A = P.aos
+            sets = X[:, :A.pf_offset].copy()
+            n = sets[:, 0].astype(int)
+            for k in range(1, A.pf_offset):
+                sets[n < k, k] = 0.0
+            F.adapt(F.mark_active(sets), sets, A.pf_offset)
+            X = np.ascontiguousarray(F.transfer_aos(X))
+            M = F.mesh(P)
+            nad += 1
+    return X, steps, nad, F
+
+
+def test_amr_driver_matches_cpu_restatement():
+    """the device AMR loop (cipher_amr_*) equals the same loop run with the
+    CPU restatement of the stepper and the host forest, bit for bit (FP64,
+    grain growth: the same steps, adaptations and final state)"""
+    P = cb.Problem.grain_growth(2, [32, 32], 6, 8, 9)
+    o = cb.ts_options(P, "2a", dt0=1e-3, dtmin=1e-9, dtmax=1.0, reltol=1e-4, abstol=1e-4)
+    amr = cb.AMR(P, [1, 1], 2, 5, 3, 4, o, "fp64")
+    st = amr.solve(0.6)
+    _, _, m, nad = amr.state()
+    Xd = amr.state_aos()
+    Xo, steps, nad_o, F = _cpu_amr_loop(P, [1, 1], 2, 5, 3, 4, o, 0.6)
+    assert st.steps == steps and nad == nad_o and nad >= 2
+    assert Xd.shape == Xo.shape
+    A = P.aos
+    n = Xo[:, 0].astype(int)
+    assert np.array_equal(Xd[:, 0], Xo[:, 0])
+    for k in range(A.pf_size):
+        msk = n > k
+        assert np.array_equal(Xd[msk, 1 + k], Xo[msk, 1 + k])
+        assert np.array_equal(Xd[msk, A.pf_offset + k], Xo[msk, A.pf_offset + k])
+
+
+def test_amr_driver_alloy_runs_and_adapts():
+    """a chemistry problem (calphad2sl, walls) through the AMR driver: the
+    initial coarsening leaves fewer leaves than voxels, adaptations happen,
+    and the state stays finite with valid sets"""
+    P = cb.Problem.alloy(2, [64, 64], "calphad2sl", 3, 4, 8, 5, cb._lib.ALLOY_WALLS)
+    o = cb.ts_options(P, "2a", dt0=1e-6, dtmin=1e-12, dtmax=1e-2, reltol=1e-3, abstol=1e-3)
+    amr = cb.AMR(P, [1, 1], 3, 6, 3, 5, o, "fp64")
+    _, _, m0, _ = amr.state()
+    n0 = int(m0.ncells)
+    assert n0 < 64 * 64
+    st = amr.solve(1.0, max_steps=15)
+    _, _, m, nad = amr.state()
+    X = amr.state_aos()
+    assert st.steps == 15 and nad >= 2
+    assert np.isfinite(X).all()
+    n = X[:, 0].astype(int)
+    assert n.min() >= 1 and n.max() <= P.s.pf_size
