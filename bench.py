@@ -375,6 +375,58 @@ def run_config1_steps(dev: int, P, M, steps: int = 200):
     return out
 
 
+def run_chemistry_amr(dev: int, steps: int = 20):
+    """configuration 2 as specified: the 512^2 alloy (calphad2sl, 4
+    components, 2 grains + 20 precipitates, P = 15) on an adaptive forest,
+    levels 5-9 (the 512^2 grid is level 9), its SetUpProblem state coarsened
+    4 times by the reference's marks; the RHS timed on the adapted mesh
+    (cell-updates per leaf, and per effective 512^2 cell), then a solve with
+    an adaptation every 10 accepted steps"""
+    import ctypes as C
+    import torch
+    import cipher_b200 as cb
+    from cipher_b200 import _lib as L
+    from cipher_b200 import workloads as W
+    P = W.alloy_2d()
+    eff = int(np.prod([P.s.resolution[d] for d in range(2)]))
+    o = cb.ts_options(P, "2a", dt0=1e-6, dtmin=1e-12, dtmax=1e-2, reltol=1e-3, abstol=1e-3)
+    lib = L.load()
+    stream = torch.cuda.current_stream()
+    out = {"workload": "2D alloy, calphad2sl 4 components (D=3, S=6), 2 grains + 20 precipitates, P=15, "
+                       "forest levels 5-9 over a 512^2 effective grid (initial coarsening x4, adaptation every "
+                       "10 accepted steps)", "effective_cells": eff}
+    for prec in ("fp64", "mixed"):
+        amr = cb.AMR(P, [1, 1], 5, 9, 4, 10, o, prec, device=dev)
+        ctx, X, m, _ = amr.state()
+        lay = L.StateLayout()
+        L.check(lib.cipher_ctx_layout(ctx, C.byref(lay)), "cipher_ctx_layout")
+        F = torch.empty(int(lay.bytes), dtype=torch.uint8, device=f"cuda:{dev}")
+        leaves = int(m.ncells)
+
+        def rhs():
+            L.check(lib.cipher_rhs(ctx, 0.0, X, C.c_void_p(F.data_ptr()), C.c_void_p(stream.cuda_stream)),
+                    "cipher_rhs")
+        for _ in range(3):
+            rhs()
+        torch.cuda.synchronize()
+        tot, _ = time_launches(rhs, steps, stream)
+        ms = tot / steps
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = amr.solve(1.0, max_steps=30)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        _, _, m2, nad = amr.state()
+        out[prec] = {"leaves": leaves, "rhs_ms": ms, "value": leaves / (ms / 1e3), "unit": UNIT,
+                     "effective_value": eff / (ms / 1e3),
+                     "solve": {"steps": int(st.steps), "rejected": int(st.rejected), "rhs_calls": int(st.rhs_calls),
+                               "ms_total": e0.elapsed_time(e1), "adaptations": int(nad),
+                               "leaves_end": int(m2.ncells), "t_reached": float(st.t)}}
+        amr.close()
+    out["mixed_speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
+
+
 def _config1_only(dev: int, steps: int):
     import cipher_b200 as cb
     P = build_problem()
@@ -720,6 +772,7 @@ def run_cipher(args, rank, world, local_rank):
     }
     if not args.no_extra and world == 1:
         for key, fn in (("config1_steps", lambda: run_config1_steps(dev, P, M, 200)),
+                        ("chemistry_amr", lambda: run_chemistry_amr(dev, 20)),
                         ("chemistry", lambda: run_chemistry(dev, 20, peak)),
                         ("batched", lambda: run_batched(dev, 256, 50.0, 16)),
                         ("serving", lambda: run_serving(dev, 50.0, 4.0))):
@@ -743,7 +796,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the chemistry, batched and serving legs reported beside the headline")
-    ap.add_argument("--only", choices=["chemistry", "batched", "serving", "config1_steps"],
+    ap.add_argument("--only", choices=["chemistry", "batched", "serving", "config1_steps", "chemistry_amr"],
                     help="run one of the legs beside the headline alone (for profiling) and print its object")
     ap.add_argument("--batch-domains", type=int, default=256, help="--only batched: number of domains")
     ap.add_argument("--batch-t-end", type=float, default=50.0, help="--only batched: end time of every domain")
@@ -763,7 +816,8 @@ def main():
               "batched": lambda: run_batched(local_rank, args.batch_domains, args.batch_t_end, 16,
                                              tuple(args.batch_precisions.split(","))),
               "serving": lambda: run_serving(local_rank, 50.0, 4.0),
-              "config1_steps": lambda: _config1_only(local_rank, args.steps)}[args.only]
+              "config1_steps": lambda: _config1_only(local_rank, args.steps),
+              "chemistry_amr": lambda: run_chemistry_amr(local_rank, args.steps)}[args.only]
         print(json.dumps({args.only: fn()}), flush=True)
     elif args.impl == "reference":
         run_reference(args, rank, world)
