@@ -22,7 +22,7 @@ MAXRKTAB = 50
 MAXBIN = 10
 MAXSRC = 2
 MAXDIR = 8
-MAXLC = 8
+MAXLC = 64
 MAXBC = 6
 
 CHEM_QUADRATIC, CHEM_CALPHADDIS, CHEM_CALPHAD2SL, CHEM_NONE = 0, 1, 2, 3
@@ -178,6 +178,18 @@ class OutputField(C.Structure):
 
 
 OUT_PHASEID, OUT_MATID, OUT_INTERFACEID, OUT_CHEMPOT, OUT_COMP, OUT_PHI, OUT_TEMPERATURE = range(7)
+
+
+class ConfigStruct(C.Structure):
+    _fields_ = [("problem", C.POINTER(ProblemStruct)), ("ncomponents", C.c_int32),
+                ("componentname", (C.c_char * 64) * MAXCP), ("nsites", C.c_int32), ("nnuclei", C.c_int32),
+                ("voxelsite", C.POINTER(C.c_int32)), ("sitephase", C.POINTER(C.c_int32)),
+                ("sitenucleus", C.POINTER(C.c_int32)), ("nuclei", C.POINTER(Nucleus)), ("noutputs", C.c_int32),
+                ("outputs", C.POINTER(OutputField)), ("outputfreq", C.c_int32), ("outfile", C.c_char * 256),
+                ("petscoptions", C.c_char * 1024), ("rk_type", C.c_char * 16), ("has_random_seed", C.c_int32),
+                ("random_seed", C.c_int64), ("initblocksize", C.c_int32 * 3), ("initrefine", C.c_int32),
+                ("initcoarsen", C.c_int32), ("maxnrefine", C.c_int32), ("minnrefine", C.c_int32),
+                ("amrinterval", C.c_int32), ("max_phase_neighbours", C.c_int32)]
 INIT_SHARP, INIT_DIFFUSE = 0, 1
 TS_RK1FE, TS_RK2A, TS_RK3BS = 0, 1, 2
 BATCH_RUNNING, BATCH_FINISHED, BATCH_FAILED = 0, 1, 2
@@ -284,6 +296,11 @@ _SIGNATURES = [
     ("cipher_state_to_aos", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cipher_rhs_aos_host", C.c_int,
      [C.c_void_p, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
+    ("cipher_config_parse", C.c_int, [C.c_char_p, C.c_size_t, C.c_char_p, C.POINTER(C.POINTER(ConfigStruct))]),
+    ("cipher_config_load", C.c_int, [C.c_char_p, C.POINTER(C.POINTER(ConfigStruct))]),
+    ("cipher_config_free", None, [C.POINTER(ConfigStruct)]),
+    ("cipher_output_field_parse", C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), C.POINTER(OutputField)]),
+    ("cipher_yaml_to_json", C.c_int, [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
 ]
 
 EXPORTED = [s[0] for s in _SIGNATURES]

@@ -9,6 +9,7 @@ the arithmetic is the library's).
 from __future__ import annotations
 
 import ctypes as C
+import re
 from dataclasses import dataclass
 
 import numpy as np
@@ -19,9 +20,12 @@ from . import _lib as L
 class Problem:
     """Owns a ``cipher_problem`` (model parameters + initial voxel map)."""
 
-    def __init__(self, ptr):
+    def __init__(self, ptr, owner=None):
+        """owner: an object that owns the problem (a Config); the problem is
+        then freed with it, not by this wrapper"""
         self._lib = L.load()
         self.ptr = ptr
+        self._owner = owner
 
     @classmethod
     def grain_growth(cls, dim: int, res, ngrains: int, cap: int, seed: int, energy: float = 1.0,
@@ -79,8 +83,85 @@ class Problem:
         return np.ctypeslib.as_array(s.voxelphase, shape=(n,)).copy()
 
     def close(self):
-        if self.ptr:
+        if self.ptr and self._owner is None:
             self._lib.cipher_problem_free(self.ptr)
+        self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Config:
+    """A run read from the reference's YAML configuration format
+    (cipher_config_load / cipher_config_parse, SetUpConfig src/init.c:104-1716):
+    the problem, nucleation sites and nuclei, output fields and the solver,
+    AMR and output parameters."""
+
+    def __init__(self, ptr):
+        self._lib = L.load()
+        self.ptr = ptr
+        self.problem = Problem(self.s.problem, owner=self)
+
+    @classmethod
+    def load(cls, path: str) -> "Config":
+        lib = L.load()
+        out = C.POINTER(L.ConfigStruct)()
+        L.check(lib.cipher_config_load(path.encode(), C.byref(out)), f"cipher_config_load({path})")
+        return cls(out)
+
+    @classmethod
+    def parse(cls, text: str, basedir: str | None = None) -> "Config":
+        lib = L.load()
+        b = text.encode()
+        out = C.POINTER(L.ConfigStruct)()
+        L.check(lib.cipher_config_parse(b, len(b), basedir.encode() if basedir else None, C.byref(out)),
+                "cipher_config_parse")
+        return cls(out)
+
+    @property
+    def s(self) -> L.ConfigStruct:
+        return self.ptr.contents
+
+    @property
+    def components(self) -> list:
+        s = self.s
+        return [s.componentname[i].value.decode() for i in range(s.ncomponents)]
+
+    def nucleation_tables(self):
+        """(voxelsite, sitephase, sitenucleus, nuclei) or None without sites"""
+        s = self.s
+        if s.nsites == 0:
+            return None
+        P = self.problem.s
+        n = int(np.prod([P.resolution[d] for d in range(P.dim)]))
+        vs = np.ctypeslib.as_array(s.voxelsite, shape=(n,)).copy()
+        sp = np.ctypeslib.as_array(s.sitephase, shape=(s.nsites,)).copy()
+        sn = np.ctypeslib.as_array(s.sitenucleus, shape=(s.nsites,)).copy()
+        nz = (L.Nucleus * max(s.nnuclei, 1))()
+        C.memmove(nz, s.nuclei, C.sizeof(L.Nucleus) * s.nnuclei)
+        return vs, sp, sn, nz
+
+    def output_spec(self):
+        """the header's output fields as [(name, kind, index)]"""
+        s = self.s
+        inv = {v: k for k, v in OUTPUT_KINDS.items()}
+        return [(s.outputs[i].name.decode(), inv[s.outputs[i].kind], s.outputs[i].index) for i in range(s.noutputs)]
+
+    def ts_options(self, **over):
+        """stepper options of the configuration: the -ts_rk_type of its
+        petscoptions (PETSc's default 3bs), tolerances and step limits"""
+        rk = self.s.rk_type.decode()
+        if rk not in ("1fe", "2a", "3bs"):
+            raise ValueError(f"-ts_rk_type {rk}: the stepper has the 1fe, 2a and 3bs tableaux")
+        return ts_options(self.problem, rk, **over)
+
+    def close(self):
+        if self.ptr:
+            self.problem.ptr = None
+            self._lib.cipher_config_free(self.ptr)
             self.ptr = None
 
     def __del__(self):
@@ -88,6 +169,19 @@ class Problem:
             self.close()
         except Exception:
             pass
+
+
+def yaml_to_json(text: str):
+    """the configuration parser's reading of a YAML text, as Python objects
+    (dicts, lists, strings)"""
+    import json
+    lib = L.load()
+    b = text.encode()
+    need = C.c_size_t(0)
+    L.check(lib.cipher_yaml_to_json(b, len(b), None, 0, C.byref(need)), "cipher_yaml_to_json")
+    buf = C.create_string_buffer(need.value)
+    L.check(lib.cipher_yaml_to_json(b, len(b), buf, need.value, C.byref(need)), "cipher_yaml_to_json")
+    return json.loads(buf.value.decode())
 
 
 class Mesh:
@@ -647,6 +741,8 @@ class Server:
             pass
 
 
+CIPHER_MAXCP_PY = 1 << 20     # an index past every component: the field is zero
+
 OUTPUT_KINDS = {"phaseid": L.OUT_PHASEID, "matid": L.OUT_MATID, "interfaceid": L.OUT_INTERFACEID,
                 "chempot": L.OUT_CHEMPOT, "c": L.OUT_COMP, "phi": L.OUT_PHI, "temperature": L.OUT_TEMPERATURE}
 
@@ -661,6 +757,36 @@ def output_fields(spec):
         arr[k].index = int(index)
         arr[k].name = name.encode()[:47]
     return arr
+
+
+def _atoi(tok: str) -> int:
+    """C atoi: optional sign and leading digits, 0 when there are none"""
+    m = re.match(r"\s*([+-]?\d+)", tok)
+    return int(m.group(1)) if m else 0
+
+
+def output_spec(names, components):
+    """[(name, kind, index)] for the reference's output names, read as its
+    output step reads them (src/cipher.c:1005-1080): "phaseid", "matid",
+    "interfaceid" and "temperature" by name; a name holding "_chempot",
+    else "_c", else "_phi" takes the text before its first "_" as the
+    component (looked up in `components`; no match gives a zero field, as the
+    reference leaves the field at zero) or the phase id (C atoi)"""
+    spec = []
+    for name in names:
+        tok = name.lstrip("_").split("_", 1)[0]          # strtok_r(name, "_")
+        if name in ("phaseid", "matid", "interfaceid", "temperature"):
+            spec.append((name, name, 0))
+        elif "_chempot" in name or "_c" in name:
+            # the potentials hold the first ncp-1 components: the last one's
+            # position is past them and gives zero, as in the reference
+            idx = components.index(tok) if tok in components else CIPHER_MAXCP_PY
+            spec.append((name, "chempot" if "_chempot" in name else "c", idx))
+        elif "_phi" in name:
+            spec.append((name, "phi", _atoi(tok)))
+        else:
+            raise ValueError(f"unknown output field {name!r}")
+    return spec
 
 
 def compute_output(ctx: Context, X, spec, stream=None) -> np.ndarray:

@@ -44,6 +44,13 @@ int cipher_set_error(int code, const char *fmt, ...)
     return code;
 }
 
+/* the same, for the library's C host units (the message is already formatted) */
+extern "C" int cipher_host_set_error(int code, const char *msg)
+{
+    snprintf(g_errmsg, sizeof(g_errmsg), "%s", msg);
+    return code;
+}
+
 static int cuda_fail(cudaError_t e, const char *where)
 {
     return set_error(CIPHER_E_CUDA, "%s: %s", where, cudaGetErrorString(e));

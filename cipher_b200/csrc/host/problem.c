@@ -820,11 +820,13 @@ int cipher_initial_state_diffuse_aos(const cipher_problem *p, const cipher_mesh 
 
 int cipher_abi_sizes(int64_t *out, int n)
 {
-    const int64_t s[9] = {(int64_t)sizeof(cipher_tseries), (int64_t)sizeof(cipher_rk), (int64_t)sizeof(cipher_mobility),
-                          (int64_t)sizeof(cipher_source), (int64_t)sizeof(cipher_material),
-                          (int64_t)sizeof(cipher_interface), (int64_t)sizeof(cipher_bc),
-                          (int64_t)sizeof(cipher_problem), (int64_t)sizeof(cipher_mesh)};
-    int k = n < 9 ? n : 9;
+    const int64_t s[12] = {(int64_t)sizeof(cipher_tseries), (int64_t)sizeof(cipher_rk), (int64_t)sizeof(cipher_mobility),
+                           (int64_t)sizeof(cipher_source), (int64_t)sizeof(cipher_material),
+                           (int64_t)sizeof(cipher_interface), (int64_t)sizeof(cipher_bc),
+                           (int64_t)sizeof(cipher_problem), (int64_t)sizeof(cipher_mesh),
+                           (int64_t)sizeof(cipher_nucleus), (int64_t)sizeof(cipher_output_field),
+                           (int64_t)sizeof(cipher_config)};
+    int k = n < 12 ? n : 12;
     for (int i = 0; i < k; i++) out[i] = s[i];
     return k;
 }

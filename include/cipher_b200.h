@@ -48,8 +48,9 @@ const char *cipher_last_error(void);
 int cipher_pool_trim(int device);
 
 /* sizeof of the public structs, for binding generators to check their
- * mirrors: out[0..8] = tseries, rk, mobility, source, material, interface,
- * bc, problem, mesh; returns how many were written (at most n) */
+ * mirrors: out[0..11] = tseries, rk, mobility, source, material, interface,
+ * bc, problem, mesh, nucleus, output_field, config; returns how many were
+ * written (at most n) */
 int cipher_abi_sizes(int64_t *out, int n);
 
 /* ------------------------------------------------------------------ */
@@ -541,6 +542,53 @@ int cipher_state_to_aos(cipher_ctx *c, const void *X, double *aos, void *stream)
  * planes go through in z-slabs on the context's own streams, so that copies
  * out overlap copies in; pinned host buffers give full copy speed. */
 int cipher_rhs_aos_host(cipher_ctx *c, double t, const double *X_host, double *F_host, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* configuration files (the reference's YAML input, SetUpConfig,        */
+/* src/init.c:24-1716)                                                  */
+/* ------------------------------------------------------------------ */
+
+/* everything a configuration file sets: the problem, nucleation, output
+ * fields, and the solver / AMR / output parameters the problem does not hold */
+typedef struct cipher_config {
+    cipher_problem *problem;              /* owned; voxelphase from voxel_phase_mapping */
+    int32_t ncomponents;
+    char componentname[CIPHER_MAXCP][64];
+    /* nucleation: header n_sites / nuclei, nucleus/<name>, site mappings */
+    int32_t nsites, nnuclei;
+    int32_t *voxelsite;                   /* [prod(resolution)] site of each voxel, -1 for none; NULL without sites */
+    int32_t *sitephase, *sitenucleus;     /* [nsites] */
+    cipher_nucleus *nuclei;               /* [nnuclei] */
+    /* output fields (header outputs) and their cadence */
+    int32_t noutputs;
+    cipher_output_field *outputs;         /* [noutputs] */
+    int32_t outputfreq;
+    char outfile[256];
+    /* stepper and mesh parameters (solution_parameters) */
+    char petscoptions[1024];
+    char rk_type[16];                     /* -ts_rk_type of petscoptions, else PETSc's default "3bs" */
+    int32_t has_random_seed;
+    int64_t random_seed;
+    int32_t initblocksize[3], initrefine, initcoarsen, maxnrefine, minnrefine, amrinterval;
+    int32_t max_phase_neighbours;
+} cipher_config;
+
+/* parse a configuration held in memory; `basedir` (or NULL) is where
+ * mapping files named "*.txt" are looked for first (then the working
+ * directory, as the reference does).  Errors name the property at fault. */
+int cipher_config_parse(const char *text, size_t len, const char *basedir, cipher_config **out);
+/* read and parse a configuration file */
+int cipher_config_load(const char *path, cipher_config **out);
+void cipher_config_free(cipher_config *c);
+/* one output name of the configuration format ("phaseid", "matid",
+ * "interfaceid", "temperature", "<comp>_chempot", "<comp>_c", "<phase>_phi")
+ * as a field, read as the reference's output step reads it (src/cipher.c:
+ * 1005-1080); a component that is not listed gives a zero field */
+int cipher_output_field_parse(const char *name, int ncomponents, const char *const *components,
+                              cipher_output_field *out);
+/* the configuration parser's view of a YAML text as JSON (objects, arrays,
+ * strings), for checking a file; *needed = bytes including the final NUL */
+int cipher_yaml_to_json(const char *text, size_t len, char *out, size_t outlen, size_t *needed);
 
 #ifdef __cplusplus
 }

@@ -30,7 +30,7 @@ extern "C" {
 #define CIPHER_MAXBIN    10   /* C(5,2) */
 #define CIPHER_MAXSRC    2    /* sources per material / interface */
 #define CIPHER_MAXDIR    8    /* anisotropy directions */
-#define CIPHER_MAXLC     8    /* load cases */
+#define CIPHER_MAXLC     64   /* load cases */
 #define CIPHER_MAXBC     6    /* boundary conditions (src/init.c: assert <= 6) */
 
 #define CIPHER_TOL       1.0e-6     /* src/typedef.h:26 */

@@ -7,10 +7,11 @@ Two oracles:
 
 * ``port``: this project's C restatement (oracle/port/*.c), built into
   ``oracle/liboracle_port.so``.
-* ``ref``: the reference's own src/{typedef,utility,material,cipher}.c compiled
-  unmodified against the PETSc shim (oracle/shim) into
-  ``oracle/_ref/libcipher_ref.so``; built where the reference sources exist
-  and shipped as a prebuilt library elsewhere.
+* ``ref``: the reference's own src/{typedef,utility,material,init,cipher}.c
+  compiled unmodified against the PETSc shim (oracle/shim, with a replay of
+  libyaml's event API for init.c) into ``oracle/_ref/libcipher_ref.so``;
+  built where the reference sources exist and shipped as a prebuilt library
+  elsewhere.
 """
 from __future__ import annotations
 
@@ -26,6 +27,8 @@ REF_LIB = os.path.join(HERE, "_ref", "libcipher_ref.so")
 # the reference's src/ directory: CIPHER_REF_SRC, else the location the
 # build recipe (oracle/Makefile) assumes
 REF_SRC = os.environ.get("CIPHER_REF_SRC") or "/root/reference/src"
+# the reference's project root (its examples/ live there), when present
+REF_ROOT = os.path.dirname(REF_SRC) if os.path.isdir(REF_SRC) else None
 
 _port = None
 _ref = None
@@ -65,6 +68,8 @@ def port():
                                                C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                                C.c_void_p, C.c_double, C.c_double, C.POINTER(C.c_uint64),
                                                C.POINTER(C.c_int8), C.POINTER(C.c_double)]
+        lib.oracle_nucleation_threshold.restype = C.c_double
+        lib.oracle_nucleation_threshold.argtypes = [C.c_void_p, C.c_int] + [C.c_double] * 6 + [C.POINTER(C.c_int)]
         lib.oracle_ts_create.restype = C.c_void_p
         lib.oracle_ts_create.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         lib.oracle_ts_destroy.restype = None
@@ -102,6 +107,16 @@ def ref():
         lib.ref_poststep.restype = C.c_int
         lib.ref_poststep.argtypes = [C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_double), C.c_int,
                                      C.POINTER(C.c_double)]
+        lib.ref_set_nuclei.restype = C.c_int
+        lib.ref_set_nuclei.argtypes = [C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int, C.c_void_p]
+        lib.ref_nucleation_sites.restype = C.c_int
+        lib.ref_nucleation_sites.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_int8),
+                                             C.POINTER(C.c_double)]
+        lib.ref_nucleation_event.restype = C.c_int
+        lib.ref_nucleation_event.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_uint, C.POINTER(C.c_double)]
+        lib.ref_output_fields.restype = C.c_int
+        lib.ref_output_fields.argtypes = [C.POINTER(C.c_double), C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                          C.POINTER(C.c_double)]
         _ref = lib
     return _ref
 
@@ -149,6 +164,16 @@ def port_output_fields(problem, mesh, X: np.ndarray, kinds, idx) -> np.ndarray:
     if rc:
         raise RuntimeError(f"oracle_output_fields failed ({rc})")
     return out
+
+
+def port_nucleation_threshold(nucleus, dim, t, dt, T, volume, gv, diffusivity):
+    """(draws, threshold) of the event rule of a nucleus (a cipher_nucleus
+    structure): the event fires when a draw happens and the number drawn is
+    below the threshold"""
+    draw = C.c_int(0)
+    thr = port().oracle_nucleation_threshold(C.addressof(nucleus), dim, t, dt, T, volume, gv, diffusivity,
+                                              C.byref(draw))
+    return bool(draw.value), thr
 
 
 class PortNucleation:
@@ -235,8 +260,21 @@ class PortTS:
 class RefOracle:
     """The reference's RHSFunction/PostStep on one problem (one at a time)."""
 
-    def __init__(self, problem, mesh):
+    def __init__(self, problem, mesh, nucleation=None):
+        """nucleation = (sitephase, sitenucleus, nuclei) makes the reference's
+        nucleation helpers usable (nucleation_sites / nucleation_event)"""
         self.lib = ref()
+        self.nsites = 0
+        if nucleation is not None:
+            sp, sn, nz = nucleation
+            self._sp = np.ascontiguousarray(sp, dtype=np.int32)
+            self._sn = np.ascontiguousarray(sn, dtype=np.int32)
+            self.nsites = len(self._sp)
+            i32 = C.POINTER(C.c_int32)
+            rc = self.lib.ref_set_nuclei(self.nsites, self._sp.ctypes.data_as(i32), self._sn.ctypes.data_as(i32),
+                                         len(nz), C.cast(nz, C.c_void_p))
+            if rc:
+                raise RuntimeError(f"ref_set_nuclei failed ({rc})")
         rc = self.lib.ref_create(_addr(problem), _addr(mesh))
         if rc:
             raise RuntimeError(f"ref_create failed ({rc})")
@@ -260,6 +298,55 @@ class RefOracle:
         assert X.flags.c_contiguous and X.dtype == np.float64
         d = C.c_double(dt)
         return self.lib.ref_poststep(_dp(X), t, C.byref(d), step, None)
+
+    def setup_problem(self, cellphase) -> np.ndarray:
+        """the reference's SetUpProblem (src/init.c:1721-1830): the initial
+        state of the owned cells from the phase of each cell"""
+        cp = np.ascontiguousarray(cellphase, dtype=np.int32)
+        X = np.zeros((self.mesh.nowned, self.ndof))
+        self.lib.ref_setup_problem.restype = C.c_int
+        self.lib.ref_setup_problem.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_int32)]
+        rc = self.lib.ref_setup_problem(_dp(X), cp.ctypes.data_as(C.POINTER(C.c_int32)))
+        if rc:
+            raise RuntimeError(f"reference SetUpProblem failed ({rc})")
+        return X
+
+    def nucleation_sites(self, X: np.ndarray, cellsite, active=None):
+        """the reference's per-site (barrier, diffusivity, temperature,
+        volume) of state X, NaN rows for sites not evaluated; returns (out,
+        active) with retired sites cleared"""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        cs = np.ascontiguousarray(cellsite, dtype=np.int32)
+        act = np.ones(self.nsites, dtype=np.int8) if active is None else np.array(active, dtype=np.int8)
+        out = np.full((max(self.nsites, 1), 4), np.nan)
+        rc = self.lib.ref_nucleation_sites(_dp(X), cs.ctypes.data_as(C.POINTER(C.c_int32)),
+                                           act.ctypes.data_as(C.POINTER(C.c_int8)), _dp(out))
+        if rc:
+            raise RuntimeError(f"ref_nucleation_sites failed ({rc})")
+        return out[:self.nsites], act
+
+    def nucleation_event(self, site, t, dt, T, volume, gv, diffusivity, seed):
+        """(fired, first number the reference's generator gives for seed)"""
+        draw = C.c_double(0.0)
+        e = self.lib.ref_nucleation_event(site, t, dt, T, volume, gv, diffusivity, seed, C.byref(draw))
+        if e < 0:
+            raise RuntimeError("ref_nucleation_event failed")
+        return bool(e), draw.value
+
+    def output_fields(self, X: np.ndarray, names, components, t: float = 0.0, step: int = 0) -> np.ndarray:
+        """the reference's PostStep with its output step on X (in place):
+        the fields it writes, [len(names), nowned]"""
+        assert X.flags.c_contiguous and X.dtype == np.float64
+        nb = [n.encode() for n in names]
+        cb_ = [c.encode() for c in components]
+        na = (C.c_char_p * len(nb))(*nb)
+        ca = (C.c_char_p * max(len(cb_), 1))(*cb_)
+        out = np.zeros((self.mesh.nowned, len(nb)))
+        rc = self.lib.ref_output_fields(_dp(X), t, step, len(nb), C.cast(na, C.c_void_p), C.cast(ca, C.c_void_p),
+                                        _dp(out))
+        if rc:
+            raise RuntimeError(f"ref_output_fields failed ({rc})")
+        return np.ascontiguousarray(out.T)
 
     def close(self):
         if self.lib is not None:

@@ -100,25 +100,38 @@ static void cell_barrier(const cipher_problem *p, const cipher_nucleus *nz, int 
     }
 }
 
-static int nuc_event(const cipher_nucleus *nz, int dim, double t, double dt, double T, double volume, double gv,
-                     double diffusivity, uint64_t *rng)
+/* the event rule of NucleationEvent_* (src/material.c:47-135) up to the
+ * draw: *draw = 1 when the reference draws a number for this site, and the
+ * event fires when that number is below the returned threshold */
+double oracle_nucleation_threshold(const cipher_nucleus *nz, int dim, double t, double dt, double T, double volume,
+                                   double gv, double diffusivity, int *draw)
 {
+    *draw = 0;
     if (nz->model == CIPHER_NUC_CONSTANT) {
-        const double u = nuc_uniform(rng);
-        return u < dt * nz->nucleation_rate && t > nz->incubationtimemin;
+        *draw = 1;
+        return t > nz->incubationtimemin ? dt * nz->nucleation_rate : -1.0;
     }
-    if (nz->model != CIPHER_NUC_CNT && nz->model != CIPHER_NUC_THERMAL) return 0;
-    if (t < nz->incubationtimemin || T > nz->liquidus) return 0;
+    if (nz->model != CIPHER_NUC_CNT && nz->model != CIPHER_NUC_THERMAL) return -1.0;
+    if (t < nz->incubationtimemin || T > nz->liquidus) return -1.0;
     const double KbT = NUC_KBANGST2 * T;
     const double radius_c = 2.0 * nz->gamma / gv / NUC_ANGSTROM;
     if (radius_c < nz->lengthscale * pow(volume, 1.0 / dim) && radius_c > nz->minsize) {
         const double zeldovich = nz->atomicvolume * sqrt(nz->gamma / KbT) / (2.0 * NUC_PI * radius_c * radius_c);
         const double beta = 4.0 * NUC_PI * diffusivity * nz->lengthscale * nz->lengthscale * radius_c / nz->atomicvolume;
         const double prob = exp(-(4.0 * NUC_PI * nz->gamma * radius_c * radius_c) * nz->shapefactor / (3.0 * KbT));
-        const double u = nuc_uniform(rng);
-        if (u < dt * zeldovich * beta * prob) return 1;
+        *draw = 1;
+        return dt * zeldovich * beta * prob;
     }
-    return 0;
+    return -1.0;
+}
+
+static int nuc_event(const cipher_nucleus *nz, int dim, double t, double dt, double T, double volume, double gv,
+                     double diffusivity, uint64_t *rng)
+{
+    int draw;
+    const double thr = oracle_nucleation_threshold(nz, dim, t, dt, T, volume, gv, diffusivity, &draw);
+    if (!draw) return 0;
+    return nuc_uniform(rng) < thr;
 }
 
 /* one update of the whole-domain AoS state X; active[nsites] is updated,

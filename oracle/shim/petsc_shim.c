@@ -94,7 +94,17 @@ PetscErrorCode VecCopy(Vec x, Vec y)
 }
 PetscErrorCode VecDestroy(Vec *v) { shim_vec_free(*v); *v = NULL; return 0; }
 PetscErrorCode VecGetDM(Vec v, DM *dm) { *dm = v->dm; return 0; }
-PetscErrorCode VecView(Vec v, PetscViewer w) { (void)v; (void)w; return shim_unsupported("VecView"); }
+/* the output step's VecView: the bridge collects the vector (no file is
+ * written); any other VecView is not modelled */
+extern double *shim_capture;
+extern int shim_capture_n;
+PetscErrorCode VecView(Vec v, PetscViewer w)
+{
+    (void)w;
+    if (!shim_capture || v->n != shim_capture_n) return shim_unsupported("VecView");
+    memcpy(shim_capture, v->a, (size_t)v->n * sizeof(double));
+    return 0;
+}
 
 /* ---------------- DM: vectors ---------------- */
 static Vec pool_get(DM dm, int local)
@@ -329,9 +339,14 @@ SHIM_STUB(PetscSFBcastBegin(PetscSF s, MPI_Datatype t, const void *a, void *b, M
 SHIM_STUB(PetscSFBcastEnd(PetscSF s, MPI_Datatype t, const void *a, void *b, MPI_Op o), "PetscSFBcastEnd")
 SHIM_STUB(PetscFECreateDefault(MPI_Comm c, PetscInt a, PetscInt b, PetscBool x, const char *p, PetscInt q, PetscFE *f), "PetscFECreateDefault")
 SHIM_STUB(PetscFEDestroy(PetscFE *f), "PetscFEDestroy")
-SHIM_STUB(PetscViewerVTKOpen(MPI_Comm c, const char *n, PetscFileMode m, PetscViewer *v), "PetscViewerVTKOpen")
-SHIM_STUB(PetscViewerPushFormat(PetscViewer v, PetscViewerFormat f), "PetscViewerPushFormat")
-SHIM_STUB(PetscViewerDestroy(PetscViewer *v), "PetscViewerDestroy")
+PetscErrorCode PetscViewerVTKOpen(MPI_Comm c, const char *n, PetscFileMode m, PetscViewer *v)
+{
+    (void)c; (void)n; (void)m;
+    *v = NULL;
+    return shim_capture ? 0 : shim_unsupported("PetscViewerVTKOpen");
+}
+PetscErrorCode PetscViewerPushFormat(PetscViewer v, PetscViewerFormat f) { (void)v; (void)f; return 0; }
+PetscErrorCode PetscViewerDestroy(PetscViewer *v) { *v = NULL; return 0; }
 SHIM_STUB(TSCreate(MPI_Comm c, TS *t), "TSCreate")
 SHIM_STUB(TSSetType(TS t, TSType y), "TSSetType")
 SHIM_STUB(TSSetDM(TS t, DM d), "TSSetDM")

@@ -8,6 +8,22 @@ through the PETSc shim into oracle/_ref/libcipher_ref.so) produce the outputs:
   F      RHSFunction(X)
   Xpost  PostStep(X) (projection, pruning, neighbour union, reorder)
 
+Two more kinds pin the parts of PostStep around the active-set update:
+
+  nuc_ref.npz        the reference's per-site nucleation averages
+                     (NucleationBarrier, src/material.c:137-290, summed as
+                     src/cipher.c:733-815) and its event decisions
+                     (NucleationEvent, src/material.c:47-135) for seeded
+                     draws of the C library's generator
+  out_ref_*.npz      the fields of the reference's output step
+                     (src/cipher.c:976-1081) after its PostStep
+  configs/*.ref.npz  the reference's SetUpConfig (src/init.c:104-1716) on
+                     the configuration files configs/*.yaml (YAML events from
+                     PyYAML, see oracle/config_dump.py)
+  configs/*.state.npz its SetUpProblem state (src/init.c:1721-1830) and
+                     RHSFunction there (not for parse_* files, whose random
+                     sources the reference draws with rand())
+
 Run from the repository root where the reference sources exist:
     python tests/golden/make_golden.py [fixture names...]
 """
@@ -131,6 +147,107 @@ def build_multi(dim, res, ng, cap, seed, nitf, feats):
     return P, M, cb.diffuse_state_aos(P, M, 4.0)
 
 
+# nucleation fixture: the shared nucleation scenario with a CNT nucleus on
+# the two-phase site 3 and a thermal one on site 4, evolved by the
+# reference's own steps, with a temperature field that varies by cell
+NUC_SITENUCLEUS = [0, 1, 2, 0, 2, 3]
+NUC_STEPS = 4
+NUC_SEEDS = 48
+
+# output fixtures: (name, builder kind, args, steps, field names, component names)
+OUT_CASES = [
+    ("out_ref_alloy2d", "alloy", (2, [40, 32], "calphad2sl", 4, 6, 8, 9, 0x01), 3,
+     ["phaseid", "matid", "interfaceid", "al_chempot", "cu_chempot", "va_chempot", "al_c", "cu_c", "mg_c", "va_c",
+      "2_phi", "0_phi", "7_phi", "temperature"], ["al", "cu", "mg", "va"]),
+    ("out_ref_gg3d", "gg", (3, [12, 10, 8], 20, 8, 4), 0,
+     ["phaseid", "matid", "interfaceid", "3_phi", "11_phi", "temperature"], []),
+]
+
+
+def nucleation_fixture():
+    """the reference's nucleation averages on an evolved state, and its
+    event decisions at a step size that puts each site's threshold near one
+    half, for seeds 1..NUC_SEEDS"""
+    sys.path.insert(0, os.path.dirname(HERE))
+    from nucleation_case import build
+    P, voxelsite, sitephase, sitenucleus, nuclei, vox = build(sitenucleus=NUC_SITENUCLEUS)
+    M = cb.Mesh(P)
+    A = P.aos
+    X0 = oracle.port_initial_state(P, M)
+    with oracle.RefOracle(P, M, nucleation=(sitephase, sitenucleus, nuclei)) as R:
+        X = evolve_with_reference(P, M, R, X0, NUC_STEPS)
+        x = np.arange(M.nowned) % P.s.resolution[0]
+        X[:, A.tm_offset] = 690.0 + 0.75 * x
+        sites, active = R.nucleation_sites(X, voxelsite)
+        rows = []
+        for s in range(len(sitephase)):
+            if not active[s]:
+                continue
+            gv, diff, T, vol = sites[s]
+            nz = nuclei[sitenucleus[s]]
+            draws, thr1 = oracle.port_nucleation_threshold(nz, P.s.dim, 1.0, 1.0, T, vol, gv, diff)
+            dt = 0.5 / thr1 if draws and thr1 > 0 else 1e-3
+            for seed in range(1, NUC_SEEDS + 1):
+                fired, u = R.nucleation_event(s, 1.0, dt, T, vol, gv, diff, seed)
+                rows.append([s, 1.0, dt, seed, u, float(fired)])
+    np.savez_compressed(os.path.join(HERE, "nuc_ref.npz"), X=X, sites=sites, active=active,
+                        events=np.array(rows), sitenucleus=np.array(NUC_SITENUCLEUS))
+    n = X[:, 0].astype(int)
+    print("nuc_ref", X.shape, "active", active, "two-phase cells in sites",
+          int(((voxelsite >= 0) & (n > 1)).sum()), "fired", int(np.array(rows)[:, 5].sum()), "of", len(rows))
+
+
+def output_case(kind, args):
+    if kind == "alloy":
+        P, M = build_alloy(*args)
+    else:
+        dim, res, ng, cap, seed = args
+        P = cb.Problem.grain_growth(dim, res, ng, cap, seed)
+        M = cb.Mesh(P)
+    return P, M
+
+
+def output_fixture(name, kind, args, steps, names, comps):
+    """the reference's PostStep with its output step on an evolved state"""
+    P, M = output_case(kind, args)
+    with oracle.RefOracle(P, M) as R:
+        X0 = oracle.port_initial_state(P, M) if kind == "alloy" else cb.diffuse_state_aos(P, M, 4.0)
+        X = evolve_with_reference(P, M, R, X0, steps) if steps else X0
+        Xp = np.ascontiguousarray(X.copy())
+        O = R.output_fields(Xp, names, comps)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), X=X, Xpost=Xp, out=O, names=np.array(names),
+                        comps=np.array(comps if comps else [""]))
+    print(name, X.shape, "fields", O.shape, "two-phase cells", int((Xp[:, 0] > 1).sum()))
+
+
+CONFIG_DIR = os.path.join(HERE, "configs")
+
+
+def config_fixtures(name):
+    """for configs/<name>.yaml: the reference's SetUpConfig result
+    (<name>.ref.npz, by oracle.config_dump in its own process, since the
+    reference aborts on a file it rejects) and its SetUpProblem state with the
+    RHS there (<name>.state.npz)"""
+    import subprocess
+    path = os.path.join(CONFIG_DIR, name + ".yaml")
+    out = os.path.join(CONFIG_DIR, name + ".ref.npz")
+    r = subprocess.run([sys.executable, "-m", "oracle.config_dump", path, out], cwd=ROOT, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    if name.startswith("parse_"):
+        print(name, "config")
+        return
+    cfg = cb.Config.load(path)
+    P = cfg.problem
+    M = cb.Mesh(P)
+    cellphase = P.voxelphase()[np.ctypeslib.as_array(M.s.cell_global, shape=(M.nowned,))]
+    with oracle.RefOracle(P, M) as R:
+        X0 = R.setup_problem(cellphase)
+        F = R.rhs(X0)
+    np.savez_compressed(os.path.join(CONFIG_DIR, name + ".state.npz"), X0=X0, F=F)
+    print(name, "config and state", X0.shape, "max|F|", np.abs(F).max())
+
+
 def main(only=None):
     """regenerate every fixture, or only the named ones"""
     oracle.build(ref=True)
@@ -138,6 +255,14 @@ def main(only=None):
     def wanted(name):
         return not only or name in only
 
+    for f in sorted(os.listdir(CONFIG_DIR)):
+        if f.endswith(".yaml") and wanted("config_" + f[:-5]):
+            config_fixtures(f[:-5])
+    if wanted("nuc_ref"):
+        nucleation_fixture()
+    for name, kind, args, steps, names, comps in OUT_CASES:
+        if wanted(name):
+            output_fixture(name, kind, args, steps, names, comps)
     for name, kind, dim, res, a, ncp, npr, cap, seed, feats, lmin, lmax, iters, diffuse, steps in AMR_CASES:
         if not wanted(name):
             continue

@@ -7,7 +7,7 @@ import cipher_b200 as cb
 from cipher_b200 import _lib as L
 
 
-def build(seed: int = 5):
+def build(seed: int = 5, sitenucleus=None):
     P = cb.Problem.alloy(2, [32, 24], "calphad2sl", 4, 4, 8, seed, 0x01)
     vox = P.voxelphase()
     res = (32, 24)
@@ -29,14 +29,14 @@ def build(seed: int = 5):
             for x in range(x0, x0 + 3):
                 voxelsite[x + res[0] * y] = s
     sitephase = np.array([2, 3, 4, 5, 2, 3], dtype=np.int32)
-    sitenucleus = np.array([0, 1, 2, 3, 1, 0], dtype=np.int32)
+    sitenucleus = np.array([0, 1, 2, 3, 1, 0] if sitenucleus is None else sitenucleus, dtype=np.int32)
     common = dict(matrix=[0, 1], active_solutes=[1, 1, 1, 0], gamma=0.3, shapefactor=0.5, minsize=1e-3,
                   atomicvolume=1e-5, lengthscale=10.0, incubationtimemin=0.0, liquidus=2000.0)
     nuclei = cb.nuclei_array([
         dict(model=L.NUC_CNT, **common),
         dict(model=L.NUC_CONSTANT, nucleation_rate=1e30, **common),
-        dict(model=L.NUC_THERMAL, solvus_temperature_0=900.0, enthalpy_fusion_0=1e8, has_solvus_c=1,
-             solvus_temperature_c=[50.0, -20.0, 10.0, 0.0], **common),
+        dict(common, model=L.NUC_THERMAL, solvus_temperature_0=900.0, enthalpy_fusion_0=4e9, has_solvus_c=1,
+             solvus_temperature_c=[50.0, -20.0, 10.0, 0.0]),
         dict(model=L.NUC_CONSTANT, nucleation_rate=0.0, **common),
     ])
     return P, voxelsite, sitephase, sitenucleus, nuclei, vox

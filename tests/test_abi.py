@@ -32,10 +32,10 @@ def test_library_loads_and_exports_declared_symbols():
 
 def test_struct_sizes_match_mirrors():
     lib = L.load()
-    out = (C.c_int64 * 9)()
-    assert lib.cipher_abi_sizes(out, 9) == 9
+    out = (C.c_int64 * 12)()
+    assert lib.cipher_abi_sizes(out, 12) == 12
     mirrors = [L.TSeries, L.RK, L.Mobility, L.Source, L.Material, L.Interface, L.BC, L.ProblemStruct,
-               L.MeshStruct]
+               L.MeshStruct, L.Nucleus, L.OutputField, L.ConfigStruct]
     for size, m in zip(out, mirrors):
         assert size == C.sizeof(m), (m.__name__, size, C.sizeof(m))
 

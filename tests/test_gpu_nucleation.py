@@ -58,3 +58,27 @@ def test_stepper_restarts_from_dtmin_after_a_nucleus():
     st = ts.stats()
     assert st.dt == 1e-9                    # a constant-model site fired in the first update
     assert nu.sites()["active"][1] == 0
+
+
+def test_device_averages_match_reference_fixture():
+    """per-site averages on the device against the reference's own
+    NucleationBarrier sums (fixture made by the reference): 1e-12 (the site
+    fractions pass through exp and log on the device), the same sites
+    evaluated and retired"""
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "nuc_ref.npz"))
+    P, voxelsite, sitephase, sitenucleus, nuclei, vox = build(sitenucleus=list(g["sitenucleus"]))
+    M = cb.Mesh(P)
+    ctx = cb.Context(P, M, "fp64")
+    dX = ctx.alloc_state()
+    ctx.from_aos(g["X"], dX)
+    dev = cb.Nucleation(ctx, voxelsite, sitephase, sitenucleus, nuclei, seed=1)
+    assert dev.step(dX, 0.0, 0.0) == 0            # dt = 0: every threshold is zero
+    sd = dev.sites()
+    got = np.stack([sd["barrier"], sd["diffusivity"], sd["temperature"], sd["volume"]], axis=1)
+    ref = g["sites"]
+    ev = ~np.isnan(ref[:, 0])
+    assert np.array_equal(sd["active"], g["active"])
+    assert np.array_equal(np.isnan(got[:, 0]), ~ev)
+    scale = np.maximum(np.abs(ref[ev]), 1e-300)
+    assert (np.abs(got[ev] - ref[ev]) <= 1e-12 * scale).all()

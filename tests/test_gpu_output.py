@@ -44,3 +44,28 @@ def test_output_fields_match_restatement(precision, tmp_path):
     path = str(tmp_path / "alloy_0.vtu")
     cb.write_vtu(path, P, SPEC, D)
     assert open(path, "rb").read(5) == b"<?xml"
+
+
+def test_output_fields_match_reference_fixtures():
+    """the device's fields on the reference's post-step state against the
+    fields the reference's own output step wrote (fixtures): ids, phase
+    fractions, potentials and temperature exactly, compositions 1e-12"""
+    import glob
+    import os
+    from golden.make_golden import OUT_CASES, output_case
+    paths = sorted(glob.glob(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "out_ref_*.npz")))
+    assert len(paths) >= 2
+    for path in paths:
+        case = next(c for c in OUT_CASES if c[0] == os.path.basename(path)[:-4])
+        P, M = output_case(case[1], case[2])
+        g = np.load(path)
+        spec = cb.api.output_spec([str(n) for n in g["names"]], [str(c) for c in g["comps"] if str(c)])
+        ctx = cb.Context(P, M, "fp64")
+        dX = ctx.alloc_state()
+        ctx.from_aos(g["Xpost"], dX)
+        D = cb.compute_output(ctx, dX, spec)
+        for k, (name, kind, _) in enumerate(spec):
+            if kind == "c":
+                assert np.abs(D[k] - g["out"][k]).max() <= 1e-12, (path, name)
+            else:
+                assert np.array_equal(D[k], g["out"][k]), (path, name)

@@ -2,6 +2,7 @@
 VTU writer, on the CPU: the restatement's fields have the properties the
 reference's definitions imply, and a written file parses back to the same
 grid and arrays."""
+import glob
 import os
 import re
 import xml.etree.ElementTree as ET
@@ -80,3 +81,54 @@ def test_vtu_round_trip(tmp_path, dim, res):
     assert lo[0] == x and lo[1] == y and hi[0] == x + 1 and hi[1] == y + 1
     for name, row in zip([s[0] for s in spec], F):
         assert np.array_equal(d[name], row)
+
+
+# ---- pinned against the reference's own output step ----
+
+OUT_REF = sorted(glob.glob(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "out_ref_*.npz")))
+
+
+def _out_case(path):
+    from golden.make_golden import OUT_CASES, output_case
+    name = os.path.basename(path)[:-4]
+    case = next(c for c in OUT_CASES if c[0] == name)
+    P, M = output_case(case[1], case[2])
+    g = np.load(path)
+    names = [str(n) for n in g["names"]]
+    comps = [str(c) for c in g["comps"] if str(c)]
+    return P, M, g, cb.api.output_spec(names, comps)
+
+
+def test_reference_output_fixtures_present():
+    assert len(OUT_REF) >= 2
+
+
+@pytest.mark.parametrize("path", OUT_REF, ids=[os.path.basename(p) for p in OUT_REF])
+def test_restatement_equals_reference_output(path):
+    """the fields the reference's output step wrote after its PostStep
+    (fixture) equal the restatement's on the same post-step state: ids,
+    phase fractions, potentials and temperature exactly, compositions (site
+    fractions through exp) to 1e-14"""
+    P, M, g, spec = _out_case(path)
+    k, i = _kinds(spec)
+    O = oracle.port_output_fields(P, M, g["Xpost"], k, i)
+    for f, (name, kind, _) in enumerate(spec):
+        if kind == "c":
+            assert np.abs(O[f] - g["out"][f]).max() <= 1e-14, name
+        else:
+            assert np.array_equal(O[f], g["out"][f]), name
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference oracle not built")
+@pytest.mark.parametrize("path", OUT_REF, ids=[os.path.basename(p) for p in OUT_REF])
+def test_reference_output_step_reproduces_fixture(path):
+    """the reference run again here gives the fixture bit for bit (state
+    after PostStep and every field)"""
+    P, M, g, spec = _out_case(path)
+    X = np.ascontiguousarray(g["X"].copy())
+    names = [str(n) for n in g["names"]]
+    comps = [str(c) for c in g["comps"] if str(c)]
+    with oracle.RefOracle(P, M) as R:
+        O = R.output_fields(X, names, comps)
+    assert np.array_equal(X, g["Xpost"])
+    assert np.array_equal(O, g["out"])
