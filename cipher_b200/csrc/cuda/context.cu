@@ -92,6 +92,9 @@ struct cipher_ctx {
     cipher_state_layout lay;
     cipher_aos_layout aos;
     int general;                  /* 1: chemistry / heat / boundary kernels (rhs_general.cu) */
+    int aniso;                    /* gradient-based anisotropy: gradients of phi before the RHS */
+    double cw[3];                 /* cell width per axis (centroids of the gradient weights) */
+    double *d_grad;               /* [dim][P][stride] gradients (aniso) */
     int single;
     double sig0, mob0, wid0, tj0, ffactor, vol, junctionpenalty, delta;
     int has_temp_rate;
@@ -129,12 +132,11 @@ static constexpr int kAosSlabs = 32;
 
 static int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 
-/* problems the general kernels take: everything the reference's RHS does on
- * a uniform grid except gradient-based anisotropy and random sources (which
- * call rand() inside the RHS) */
+/* problems the general kernels take: everything the reference's RHS does
+ * except random sources (which call rand() inside the RHS) */
 static int problem_supported(const cipher_problem *p, char *why, size_t len)
 {
-    if (p->gradient_calculation) { snprintf(why, len, "gradient_calculation (anisotropy) is not implemented"); return 0; }
+    if (p->gradient_calculation < 0 || p->gradient_calculation > 1) { snprintf(why, len, "gradient_calculation is 0 or 1"); return 0; }
     if (p->ncp < 1 || p->ncp > CIPHER_MAXCP || p->ndp != p->ncp - 1) { snprintf(why, len, "bad component count"); return 0; }
     if (p->nbcs < 0 || p->nbcs > CIPHER_MAXBC) { snprintf(why, len, "bad boundary condition count"); return 0; }
     for (int m = 0; m < p->nmat; m++) {
@@ -155,6 +157,16 @@ static int problem_supported(const cipher_problem *p, char *why, size_t len)
     if (p->interpolation != CIPHER_INTERP_CUBIC && p->interpolation != CIPHER_INTERP_QUADRATIC &&
         p->interpolation != CIPHER_INTERP_LINEAR) { snprintf(why, len, "unknown interpolation"); return 0; }
     return 1;
+}
+
+/* gradient-based anisotropy changes results only where an interface has
+ * anisotropy values (src/cipher.c:427-460) */
+static int has_anisotropy(const cipher_problem *p)
+{
+    if (!p->gradient_calculation) return 0;
+    for (int i = 0; i < p->nf; i++)
+        if (p->interface[i].energy_naniso > 0 || p->interface[i].mobility_naniso > 0) return 1;
+    return 0;
 }
 
 /* problems the phase-field-only kernels take: no chemistry, no heat, no
@@ -197,6 +209,7 @@ static void free_ctx(cipher_ctx *c)
     dev_free(c->d_mob);
     dev_free(c->d_tcond);
     dev_free(c->d_pruned);
+    dev_free(c->d_grad);
     dev_free(c->d_err);
     pinned_word_free(c->h_err);
     dev_free(c->d_aos_x);
@@ -345,9 +358,15 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
     c->nmat = p->nmat;
     c->junctionpenalty = p->junctionpenalty;
     c->listed = !m->uniform;
-    /* the phase-field kernels walk uniform grids; adapted meshes take the
-     * general kernels over their face lists */
-    c->general = c->listed || !phasefield_only(p);
+    c->aniso = has_anisotropy(p);
+    if (c->aniso && (c->listed || m->nowned != m->ncells)) {
+        free_ctx(c);
+        return set_error(CIPHER_E_UNSUPPORTED, "gradient-based anisotropy needs a whole-domain uniform grid");
+    }
+    for (int d = 0; d < 3; d++) c->cw[d] = d < p->dim ? p->size[d] / p->resolution[d] : 1.0;
+    /* the phase-field kernels walk uniform grids; adapted meshes and
+     * anisotropy take the general kernels */
+    c->general = c->listed || !phasefield_only(p) || c->aniso;
     c->interp = p->interpolation;
     c->delta = m->cellgeom[0];
     c->nbcs = p->nbcs;
@@ -448,6 +467,13 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
             memcpy(h[i].mobilityc, s->mobilityc, sizeof(h[i].mobilityc));
             h[i].nsources = s->nsources;
             memcpy(h[i].sources, s->sources, sizeof(h[i].sources));
+            /* anisotropy acts only with gradient_calculation (src/cipher.c:427) */
+            h[i].energy_n = p->gradient_calculation ? s->energy_naniso : 0;
+            h[i].mobility_n = p->gradient_calculation ? s->mobility_naniso : 0;
+            memcpy(h[i].energy_dir, s->energy_aniso_dir, sizeof(h[i].energy_dir));
+            memcpy(h[i].energy_val, s->energy_aniso_val, sizeof(h[i].energy_val));
+            memcpy(h[i].mobility_dir, s->mobility_aniso_dir, sizeof(h[i].mobility_dir));
+            memcpy(h[i].mobility_val, s->mobility_aniso_val, sizeof(h[i].mobility_val));
         }
         e = dev_alloc(&c->d_itfs, (size_t)p->nf * sizeof(DevInterface));
         if (e == cudaSuccess) e = cudaMemcpy(c->d_itfs, h, (size_t)p->nf * sizeof(DevInterface), cudaMemcpyHostToDevice);
@@ -486,6 +512,10 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
         if (e != cudaSuccess) { free_ctx(c); return cuda_fail(e, "temperature table"); }
     }
     if ((e = dev_alloc(&c->d_pruned, (size_t)(c->P + 1) * c->stride * sizeof(uint16_t))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc pruned"); }
+    if (c->aniso && (e = dev_alloc(&c->d_grad, (size_t)c->dim * c->P * c->stride * sizeof(double))) != cudaSuccess) {
+        free_ctx(c);
+        return cuda_fail(e, "cudaMalloc gradients");
+    }
     if ((e = dev_alloc(&c->d_err, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc err"); }
     if ((e = cudaMemset(c->d_err, 0, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMemset err"); }
     if ((e = pinned_word_alloc(&c->h_err)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "pinned error word"); }
@@ -635,6 +665,8 @@ static GenArgs<R> gen_args(const cipher_ctx *c, const void *X, void *F)
     a.ex = (const double *)(x + c->lay.ex_offset);
     a.tm = (const R *)(x + c->lay.tm_offset);
     a.fl = face_lists(c);
+    a.grad = c->d_grad;
+    for (int d = 0; d < 3; d++) a.cw[d] = c->cw[d];
     a.comp = c->d_comp;
     a.mob = c->d_mob;
     a.tcond = c->d_tcond;

@@ -27,6 +27,10 @@ struct DevInterface {
     double mobilityc[CIPHER_MAXCP];
     int nsources;
     cipher_source sources[CIPHER_MAXSRC];
+    /* anisotropy (IENERGY / IMOBILITY dir, val, n): unit directions [n][dim] */
+    int energy_n, mobility_n;
+    double energy_dir[CIPHER_MAXDIR * 3], energy_val[CIPHER_MAXDIR];
+    double mobility_dir[CIPHER_MAXDIR * 3], mobility_val[CIPHER_MAXDIR];
 };
 
 /* material tables on the device: the host structs of cipher_problem.h
@@ -89,6 +93,32 @@ __device__ inline void interface_props(const DevInterface &itf, double T, double
 {
     sig = 1.0;
     mob = 1.0;
+    sig *= itf.energy_m0;
+    if (itf.energy_act.n) sig *= exp(tseries(T, itf.energy_act) / CIPHER_R_GAS / T);
+    mob *= itf.mobility_m0;
+    if (itf.mobility_act.n) mob *= exp(tseries(T, itf.mobility_act) / CIPHER_R_GAS / T);
+    wid = itf.width;
+}
+
+/* the same with the anisotropy of the pair's interface normal u (unit, or
+ * zero where the gradients cancel): sigma and m start from
+ * 1 + sum_dir (u . dir)^4 val_dir before the prefactor and the activation
+ * term (src/cipher.c:427-460) */
+__device__ inline void interface_props_aniso(const DevInterface &itf, double T, const double *u, int dim, double &sig,
+                                             double &mob, double &wid)
+{
+    sig = 1.0;
+    mob = 1.0;
+    for (int k = 0; k < itf.energy_n; k++) {
+        double dot = 0.0;
+        for (int d = 0; d < dim; d++) dot += u[d] * itf.energy_dir[dim * k + d];
+        sig += ipow(dot, 4) * itf.energy_val[k];
+    }
+    for (int k = 0; k < itf.mobility_n; k++) {
+        double dot = 0.0;
+        for (int d = 0; d < dim; d++) dot += u[d] * itf.mobility_dir[dim * k + d];
+        mob += ipow(dot, 4) * itf.mobility_val[k];
+    }
     sig *= itf.energy_m0;
     if (itf.energy_act.n) sig *= exp(tseries(T, itf.energy_act) / CIPHER_R_GAS / T);
     mob *= itf.mobility_m0;

@@ -130,6 +130,8 @@ struct GenArgs {
     const R *tm;
     double *comp, *mob, *tcond;   /* per-cell scratch: [ncp][stride], [ncp][stride], [stride] */
     FaceLists fl;                 /* face lists of an adapted mesh (fl.start == NULL: uniform grid) */
+    double *grad;                 /* [dim][P][stride] phase-field gradients, or NULL (no anisotropy) */
+    double cw[3];                 /* cell width along each axis: centroid = (i + 0.5) * cw */
     R *fphi;
     double *fdp, *fex;
     R *ftm;

@@ -193,6 +193,88 @@ __device__ __forceinline__ int64_t gen_face_nb(const int *res, const int *per, i
     return (co[d] == 0 && per[d] && res[d] > 1) ? c + (int64_t)(res[d] - 1) * st[d] : -1;
 }
 
+/* phase-field gradients of a cell's slots by least squares over its face
+ * neighbours (src/cipher.c:82-146), with the weights the reference builds
+ * once in main() (src/cipher.c:1232-1282) formed here per cell in the same
+ * operation order: centroid differences in the cell's face order, AtA,
+ * its closed-form inverse, (AtA)^-1 At.  grad[d][g] = sum_k w[d][k] (phi_k(g)
+ * - phi(g)), the phase taken as absent (0) in a neighbour that does not
+ * hold it; centroid differences across a periodic side are the raw ones, as
+ * the reference's cell centroids give them. */
+template <int PM, typename R>
+__global__ void __launch_bounds__(kGenBlock) k_gradients(const GenArgs<R> a, const int DIM)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.ncells) return;
+    const int64_t S = a.stride;
+    int co[3] = {0, 0, 0};
+    co[0] = (int)(c % a.res[0]);
+    co[1] = DIM > 1 ? (int)((c / a.res[0]) % a.res[1]) : 0;
+    co[2] = DIM > 2 ? (int)(c / ((int64_t)a.res[0] * a.res[1])) : 0;
+    uint16_t ids[PM];
+    double phi[PM];
+    const int n = load_set<PM>(a, c, ids, phi);
+    if (n == 0) return;
+    /* neighbours in the cell's face order, with their centroid offsets */
+    int64_t nbs[6];
+    double A[6 * 3];
+    int nls = 0;
+    for (int f = 0; f < 3 * DIM; f++) {
+        const int64_t nb = gen_face_nb(a.res, a.per, c, co, f, DIM);
+        if (nb < 0 || nb == c) continue;
+        const int64_t q[3] = {nb % a.res[0], DIM > 1 ? (nb / a.res[0]) % a.res[1] : 0,
+                              DIM > 2 ? nb / ((int64_t)a.res[0] * a.res[1]) : 0};
+        for (int d = 0; d < DIM; d++) {
+            const double xn = ((double)q[d] + 0.5) * a.cw[d], xc = ((double)co[d] + 0.5) * a.cw[d];
+            A[nls * DIM + d] = xn - xc;
+        }
+        nbs[nls++] = nb;
+    }
+    double ata[9], inv[9], w[3 * 6];
+    for (int i = 0; i < DIM; i++)
+        for (int j = i; j < DIM; j++) {
+            double v = 0.0;
+            for (int k = 0; k < nls; k++) v += A[k * DIM + i] * A[k * DIM + j];
+            ata[i * DIM + j] = v;
+            ata[j * DIM + i] = v;
+        }
+    invert_small(inv, ata, DIM);
+    for (int i = 0; i < DIM; i++)
+        for (int k = 0; k < nls; k++) {
+            double v = 0.0;
+            for (int d = 0; d < DIM; d++) v += inv[i * DIM + d] * A[k * DIM + d];
+            w[i * nls + k] = v;
+        }
+    double gr[3][PM];
+    for (int g = 0; g < n; g++)
+        for (int d = 0; d < DIM; d++) {
+            double t = 0.0;
+            for (int k = 0; k < nls; k++) t -= w[d * nls + k] * phi[g];
+            gr[d][g] = t;
+        }
+    for (int k = 0; k < nls; k++) {
+        const int64_t nb = nbs[k];
+        const int nn = a.as[nb];
+        if (nn < 1 || nn > a.P) continue;          /* that cell's own thread raises the flag */
+        int i = 0, j = 0;
+        while (i < n && j < nn) {
+            const uint16_t b = a.as[(int64_t)(1 + j) * S + nb];
+            if (ids[i] == b) {
+                const double pn = (double)a.phi[(int64_t)j * S + nb];
+                for (int d = 0; d < DIM; d++) gr[d][i] += w[d * nls + k] * pn;
+                i++;
+                j++;
+            } else if (ids[i] < b) {
+                i++;
+            } else {
+                j++;
+            }
+        }
+    }
+    for (int d = 0; d < DIM; d++)
+        for (int g = 0; g < n; g++) a.grad[((int64_t)d * a.P + g) * S + c] = gr[d][g];
+}
+
 /* ff*x/vol as the reference forms it (src/cipher.c:281-282) */
 template <typename R>
 __device__ __forceinline__ double face_div(const GenArgs<R> &a, double x)
@@ -393,6 +475,25 @@ __global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> 
     }
     for (int q = n * SP; q < a.P * SP; q++) a.fex[(int64_t)q * S + c] = 0.0;
 
+    /* pair properties; with anisotropy they depend on the pair's normal,
+     * the normalised difference of the two slots' gradients (src/cipher.c:
+     * 427-460) */
+    auto props = [&](int k, int j, double &s_, double &m_, double &w_) {
+        const DevInterface &itf = pair_itf(a, ids[k], ids[j]);
+        if (a.grad && (itf.energy_n || itf.mobility_n)) {
+            double u[3], nrm = 0.0;
+            for (int d = 0; d < DIM; d++) {
+                u[d] = a.grad[((int64_t)d * a.P + k) * S + c] - a.grad[((int64_t)d * a.P + j) * S + c];
+                nrm += u[d] * u[d];
+            }
+            nrm = sqrt(nrm);
+            if (nrm > 1e-16)
+                for (int d = 0; d < DIM; d++) u[d] /= nrm;
+            interface_props_aniso(itf, T, u, DIM, s_, m_, w_);
+        } else {
+            interface_props(itf, T, s_, m_, w_);
+        }
+    };
     for (int g = 0; g < PM; g++) pf[g] = 0.0;
     if (n > 1) {
         /* capillary force with the triple-junction penalty (src/cipher.c:474-497) */
@@ -401,15 +502,15 @@ __global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> 
         for (int k = 0; k < n; k++) {
             for (int j = k + 1; j < n; j++) {
                 double skj, mkj, wkj;
-                interface_props(pair_itf(a, ids[k], ids[j]), T, skj, mkj, wkj);
+                props(k, j, skj, mkj, wkj);
                 cap[k] -= skj * (phi[j] / wkj + lap[j] * wkj / PI / PI);
                 cap[j] -= skj * (phi[k] / wkj + lap[k] * wkj / PI / PI);
                 for (int i = j + 1; i < n; i++) {
                     double s_, m_, w_, tj = 0.0, v;
                     v = skj / wkj; tj = tj > v ? tj : v;
-                    interface_props(pair_itf(a, ids[k], ids[i]), T, s_, m_, w_);
+                    props(k, i, s_, m_, w_);
                     v = s_ / w_; tj = tj > v ? tj : v;
-                    interface_props(pair_itf(a, ids[j], ids[i]), T, s_, m_, w_);
+                    props(j, i, s_, m_, w_);
                     v = s_ / w_; tj = tj > v ? tj : v;
                     tj *= a.junctionpenalty;
                     cap[k] -= tj * phi[j] * phi[i];
@@ -439,7 +540,7 @@ __global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> 
         for (int k = 0; k < n; k++) {
             for (int j = k + 1; j < n; j++) {
                 double s_, m_, w_;
-                interface_props(pair_itf(a, ids[k], ids[j]), T, s_, m_, w_);
+                props(k, j, s_, m_, w_);
                 const double r = m_ * ((cap[k] - cap[j]) - (chem[k] - chem[j]) * 8.0 * sqrt(h[k] * h[j]) / PI);
                 unc[k] += r;
                 unc[j] -= r;
@@ -453,7 +554,7 @@ __global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> 
             for (int j = k + 1; j < n; j++) {
                 if (!(act >> j & 1u)) continue;
                 double s_, m_, w_;
-                interface_props(pair_itf(a, ids[k], ids[j]), T, s_, m_, w_);
+                props(k, j, s_, m_, w_);
                 const double r = m_ * ((cap[k] - cap[j]) - (chem[k] - chem[j]) * 8.0 * sqrt(h[k] * h[j]) / PI);
                 pf[k] += r;
                 pf[j] -= r;
@@ -920,6 +1021,7 @@ static cudaError_t launch_gen(const GenArgs<R> &a, int dim, cudaStream_t s)
         k_specialise<R><<<a.chem.nmat, 256, 0, s>>>(a.chem.mat, (cipher_material *)a.chem.spec, a.tm,
                                                      (double *)a.chem.tspec);
     if (a.ndp) k_chem_cell<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a);
+    if (a.grad) k_gradients<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a, dim);
     k_rhs_general<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a, dim);
     return cudaGetLastError();
 }

@@ -73,9 +73,9 @@ static void chem_source(const cipher_problem *p, const double *comp, const doubl
     }
 }
 
-static int check_supported(const cipher_problem *p)
+static int check_supported(const cipher_problem *p, const cipher_mesh *m)
 {
-    if (p->gradient_calculation) return 7;
+    if (p->gradient_calculation && !m->uniform) return 7;
     for (int m = 0; m < p->nmat; m++) {
         for (int s = 0; s < p->material[m].nsources; s++)
             if (p->material[m].sources[s].model != CIPHER_SOURCE_SINK) return 7;
@@ -88,10 +88,91 @@ static int check_supported(const cipher_problem *p)
     return 0;
 }
 
+/* phase-field gradients of the owned cells (src/cipher.c:82-146) with the
+ * least-squares weights of src/cipher.c:1232-1282: each owned cell's face
+ * neighbours in face order, centroid offsets ((i + 0.5) * size / resolution
+ * per axis of the grid index, raw across periodic sides), AtA, its inverse,
+ * (AtA)^-1 At; grad[(c*dim + d)*P + g] */
+static int gradients(const cipher_problem *p, const cipher_mesh *m, const double *X, const cipher_aos_layout *L,
+                     double *grad)
+{
+    const int dim = p->dim, P = p->pf_size, ndof = L->ndof;
+    const int nown = m->nowned;
+    int *cnt = (int *)calloc((size_t)nown, sizeof(int));
+    int *nbr = (int *)malloc((size_t)nown * 24 * sizeof(int));
+    if (!cnt || !nbr) { free(cnt); free(nbr); return 2; }
+    for (int f = 0; f < m->nfaces; f++) {
+        const int a = m->face_cells[2 * f], b = m->face_cells[2 * f + 1];
+        if (a == b) continue;
+        if (a < nown && cnt[a] < 24) nbr[a * 24 + cnt[a]++] = b;
+        if (b < nown && cnt[b] < 24) nbr[b * 24 + cnt[b]++] = a;
+    }
+    uint16_t ids[CIPHER_MAXAP], nids[CIPHER_MAXAP];
+    for (int c = 0; c < nown; c++) {
+        double xc[3], A[24 * 3], ata[9], inv[9], w[3 * 24];
+        const int nls = cnt[c];
+        int64_t g = m->cell_global[c];
+        for (int d = 0; d < dim; d++) {
+            xc[d] = ((double)(g % p->resolution[d]) + 0.5) * (p->size[d] / p->resolution[d]);
+            g /= p->resolution[d];
+        }
+        for (int k = 0; k < nls; k++) {
+            int64_t q = m->cell_global[nbr[c * 24 + k]];
+            for (int d = 0; d < dim; d++) {
+                A[k * dim + d] = ((double)(q % p->resolution[d]) + 0.5) * (p->size[d] / p->resolution[d]);
+                q /= p->resolution[d];
+                A[k * dim + d] -= xc[d];
+            }
+        }
+        for (int i = 0; i < dim; i++)
+            for (int j = i; j < dim; j++) {
+                double v = 0.0;
+                for (int k = 0; k < nls; k++) v += A[k * dim + i] * A[k * dim + j];
+                ata[i * dim + j] = v;
+                ata[j * dim + i] = v;
+            }
+        or_invert(inv, ata, dim);
+        for (int i = 0; i < dim; i++)
+            for (int k = 0; k < nls; k++) {
+                double v = 0.0;
+                for (int d = 0; d < dim; d++) v += inv[i * dim + d] * A[k * dim + d];
+                w[i * nls + k] = v;
+            }
+        const double *cell = &X[(size_t)c * ndof];
+        int n;
+        decode_set(&cell[L->as_offset], ids, &n);
+        const double *phi = &cell[L->pf_offset];
+        double *gc = &grad[(size_t)c * dim * P];
+        for (int q = 0; q < dim * P; q++) gc[q] = 0.0;
+        for (int s = 0; s < n; s++)
+            for (int d = 0; d < dim; d++) {
+                double v = 0.0;
+                for (int k = 0; k < nls; k++) v -= w[d * nls + k] * phi[s];
+                gc[d * P + s] = v;
+            }
+        for (int k = 0; k < nls; k++) {
+            const double *nc = &X[(size_t)nbr[c * 24 + k] * ndof];
+            int nn;
+            decode_set(&nc[L->as_offset], nids, &nn);
+            for (int i = 0, j = 0; i < n && j < nn;) {
+                if (ids[i] == nids[j]) {
+                    for (int d = 0; d < dim; d++) gc[d * P + i] += w[d * nls + k] * nc[L->pf_offset + j];
+                    i++;
+                    j++;
+                } else if (ids[i] < nids[j]) i++;
+                else j++;
+            }
+        }
+    }
+    free(cnt);
+    free(nbr);
+    return 0;
+}
+
 int oracle_rhs(const cipher_problem *p, const cipher_mesh *m, double t, const double *X, double *F)
 {
     (void)t;
-    int rc = check_supported(p);
+    int rc = check_supported(p, m);
     if (rc) return rc;
     cipher_aos_layout L = or_layout(p);
     const int ndof = L.ndof, P = p->pf_size, ncp = p->ncp, ndp = p->ndp;
@@ -237,6 +318,19 @@ int oracle_rhs(const cipher_problem *p, const cipher_mesh *m, double t, const do
         }
     }
 
+    /* ---- gradients for anisotropic interfaces (cipher.c:82-146) ---- */
+    double *grad = NULL;
+    int aniso = 0;
+    for (int i = 0; p->gradient_calculation && i < p->nf; i++)
+        if (p->interface[i].energy_naniso > 0 || p->interface[i].mobility_naniso > 0) aniso = 1;
+    if (aniso) {
+        grad = (double *)malloc((size_t)nowned * dim * P * sizeof(double));
+        if (!grad || gradients(p, m, X, &L, grad)) {
+            free(grad); free(lap); free(yall); free(comp); free(mob); free(tcond);
+            return 2;
+        }
+    }
+
     /* ---- per owned cell (cipher.c:391-664) ---- */
     for (int c = 0; c < nowned; c++) {
         const double *cell = &X[(size_t)c * ndof];
@@ -262,6 +356,27 @@ int oracle_rhs(const cipher_problem *p, const cipher_mesh *m, double t, const do
                     int kj = k * n + j;
                     sig[kj] = 1.0;
                     mij[kj] = 1.0;
+                    if (grad) {   /* anisotropy about the pair's normal (cipher.c:427-460) */
+                        const double *gc = &grad[(size_t)c * dim * P];
+                        double u[3], nrm = 0.0;
+                        for (int d = 0; d < dim; d++) {
+                            u[d] = gc[d * P + k] - gc[d * P + j];
+                            nrm += u[d] * u[d];
+                        }
+                        nrm = sqrt(nrm);
+                        if (nrm > 1e-16)
+                            for (int d = 0; d < dim; d++) u[d] /= nrm;
+                        for (int q = 0; q < itf->energy_naniso; q++) {
+                            double dot = 0.0;
+                            for (int d = 0; d < dim; d++) dot += u[d] * itf->energy_aniso_dir[dim * q + d];
+                            sig[kj] += or_ipow(dot, 4) * itf->energy_aniso_val[q];
+                        }
+                        for (int q = 0; q < itf->mobility_naniso; q++) {
+                            double dot = 0.0;
+                            for (int d = 0; d < dim; d++) dot += u[d] * itf->mobility_aniso_dir[dim * q + d];
+                            mij[kj] += or_ipow(dot, 4) * itf->mobility_aniso_val[q];
+                        }
+                    }
                     sig[kj] *= itf->energy_m0;
                     if (itf->energy_activation.n)
                         sig[kj] *= exp(or_tseries(T, &itf->energy_activation) / CIPHER_R_GAS / T);
@@ -422,7 +537,7 @@ int oracle_rhs(const cipher_problem *p, const cipher_mesh *m, double t, const do
             or_matvec(&fc[L.dp_offset], dmdc, wdp, DPn);
         }
     }
-    free(lap); free(yall); free(comp); free(mob); free(tcond);
+    free(grad); free(lap); free(yall); free(comp); free(mob); free(tcond);
     return 0;
 }
 

@@ -128,10 +128,6 @@ static int build_appctx(const cipher_problem *p)
     u->size = (PetscReal *)malloc(3 * sizeof(PetscReal));
     for (int d = 0; d < 3; d++) { u->resolution[d] = p->resolution[d]; u->size[d] = p->size[d]; }
     u->gradient_calculation = p->gradient_calculation;
-    if (p->gradient_calculation) {
-        fprintf(stderr, "ref_bridge: gradient_calculation needs the LSQ matrix of main(); not built\n");
-        return 1;
-    }
 
     /* field sizes (src/init.c:1330-1343) */
     MAXSITES = p->maxsites;
@@ -334,6 +330,69 @@ static int build_dm(const cipher_mesh *m, int ndof)
     return 0;
 }
 
+/* the least-squares gradient weights main() builds when gradient_calculation
+ * is set (src/cipher.c:1232-1282), restated over the shim DM: cell
+ * centroids of the uniform grid ((i + 0.5) * size / resolution per axis,
+ * from the cell's grid index), the neighbours of each owned cell in its cone
+ * order, the reference's Invertmatrix */
+static int build_gradient_matrix(const cipher_problem *p, const cipher_mesh *m)
+{
+    AppCtx *u = &g_user;
+    struct _p_DM *dm = &g_dm;
+    const int dim = p->dim;
+    if (!m->uniform) return 1;
+    dm->centroid = (double *)calloc((size_t)3 * m->ncells, sizeof(double));
+    if (!dm->centroid) return 1;
+    for (int c = 0; c < m->ncells; c++) {
+        int64_t g = m->cell_global[c];
+        for (int d = 0; d < dim; d++) {
+            const int64_t i = g % p->resolution[d];
+            g /= p->resolution[d];
+            dm->centroid[3 * c + d] = ((double)i + 0.5) * (p->size[d] / p->resolution[d]);
+        }
+    }
+    u->gradient_matrix = (PetscReal *)malloc((size_t)24 * dim * u->nlocalcells * sizeof(PetscReal));
+    u->gradient_nleastsq = (PetscInt *)malloc((size_t)u->nlocalcells * sizeof(PetscInt));
+    if (!u->gradient_matrix || !u->gradient_nleastsq) return 1;
+    for (PetscInt localcell = 0; localcell < u->nlocalcells; ++localcell) {
+        const PetscInt cell = u->localcells[localcell];
+        PetscReal centroid[3], a_mat[24 * 3], ata_mat[9], atainv_mat[9];
+        PetscInt conesize, nsupp;
+        const PetscInt *cone, *scells;
+        DMPlexComputeCellGeometryFVM(dm, cell, NULL, centroid, NULL);
+        DMPlexGetConeSize(dm, cell, &conesize);
+        DMPlexGetCone(dm, cell, &cone);
+        PetscInt nls = 0;
+        for (PetscInt face = 0; face < conesize; face++) {
+            DMPlexGetSupportSize(dm, cone[face], &nsupp);
+            DMPlexGetSupport(dm, cone[face], &scells);
+            for (PetscInt supp = 0; supp < nsupp; supp++) {
+                if (scells[supp] != cell && scells[supp] < u->ninteriorcells) {
+                    if (nls >= 24) return 1;
+                    DMPlexComputeCellGeometryFVM(dm, scells[supp], NULL, &a_mat[nls * dim], NULL);
+                    for (int d = 0; d < dim; ++d) a_mat[nls * dim + d] -= centroid[d];
+                    nls++;
+                }
+            }
+        }
+        u->gradient_nleastsq[localcell] = nls;
+        for (int i = 0; i < dim; ++i)
+            for (int j = i; j < dim; ++j) {
+                PetscReal val = 0.0;
+                for (PetscInt k = 0; k < nls; ++k) val += a_mat[k * dim + i] * a_mat[k * dim + j];
+                ata_mat[i * dim + j] = val;
+                ata_mat[j * dim + i] = val;
+            }
+        Invertmatrix(atainv_mat, ata_mat, dim);
+        PetscReal *gm = &u->gradient_matrix[24 * dim * localcell];
+        memset(gm, 0, (size_t)dim * nls * sizeof(PetscReal));
+        for (int i = 0; i < dim; ++i)
+            for (PetscInt j = 0; j < nls; ++j)
+                for (int d = 0; d < dim; ++d) gm[i * nls + j] += atainv_mat[i * dim + d] * a_mat[j * dim + d];
+    }
+    return 0;
+}
+
 int ref_create(const cipher_problem *p, const cipher_mesh *m)
 {
     if (g_ready) return 1;
@@ -349,6 +408,7 @@ int ref_create(const cipher_problem *p, const cipher_mesh *m)
     for (int f = 0; f < m->nfaces; f++) g_user.localfaces[f] = m->ncells + f;
     g_user.nlocalfaces = m->nfaces;
     g_user.cellgeom = m->cellgeom;
+    if (p->gradient_calculation && build_gradient_matrix(p, m)) return 4;
     memset(&g_ts, 0, sizeof(g_ts));
     g_ts.ctx = &g_user;
     g_ready = 1;
@@ -499,6 +559,11 @@ void ref_destroy(void)
     free(g_dm.cone_off);
     free(g_dm.cone);
     free(g_dm.support);
+    free(g_dm.centroid);
+    free(g_user.gradient_matrix);
+    free(g_user.gradient_nleastsq);
+    g_user.gradient_matrix = NULL;
+    g_user.gradient_nleastsq = NULL;
     for (int i = 0; i < g_dm.nlabels; i++) { free(g_dm.labels[i]->values); free(g_dm.labels[i]); }
     free(g_user.localcells);
     free(g_user.localfaces);

@@ -22,7 +22,8 @@ Two more kinds pin the parts of PostStep around the active-set update:
                      PyYAML, see oracle/config_dump.py)
   configs/*.state.npz its SetUpProblem state (src/init.c:1721-1830) and
                      RHSFunction there (not for parse_* files, whose random
-                     sources the reference draws with rand())
+                     sources the reference draws with rand()); aniso_* files
+                     also hold a state evolved by 3 reference steps (X1, F1)
 
 Run from the repository root where the reference sources exist:
     python tests/golden/make_golden.py [fixture names...]
@@ -125,9 +126,11 @@ def evolve_with_reference(P, M, R, X, steps):
     for _ in range(steps):
         F = R.rhs(X)
         fphi = np.abs(F[:, A.pf_offset:A.pf_offset + A.pf_size]).max()
-        fdp = np.abs(F[:, A.dp_offset:A.dp_offset + A.dp_size]).max()
-        mu = np.abs(X[:, A.dp_offset:A.dp_offset + A.dp_size]).max()
-        dt = min(0.05 / max(fphi, 1e-300), 0.02 * mu / max(fdp, 1e-300))
+        dt = 0.05 / max(fphi, 1e-300)
+        if A.dp_size:
+            fdp = np.abs(F[:, A.dp_offset:A.dp_offset + A.dp_size]).max()
+            mu = np.abs(X[:, A.dp_offset:A.dp_offset + A.dp_size]).max()
+            dt = min(dt, 0.02 * mu / max(fdp, 1e-300))
         X = X + dt * F
         assert R.poststep(X) == 0
     return X
@@ -241,10 +244,15 @@ def config_fixtures(name):
     P = cfg.problem
     M = cb.Mesh(P)
     cellphase = P.voxelphase()[np.ctypeslib.as_array(M.s.cell_global, shape=(M.nowned,))]
+    extra = {}
     with oracle.RefOracle(P, M) as R:
         X0 = R.setup_problem(cellphase)
         F = R.rhs(X0)
-    np.savez_compressed(os.path.join(CONFIG_DIR, name + ".state.npz"), X0=X0, F=F)
+        if name.startswith("aniso"):
+            # a state with diffuse interfaces for the gradient-based anisotropy
+            X1 = evolve_with_reference(P, M, R, X0, 3)
+            extra = dict(X1=X1, F1=R.rhs(X1))
+    np.savez_compressed(os.path.join(CONFIG_DIR, name + ".state.npz"), X0=X0, F=F, **extra)
     print(name, "config and state", X0.shape, "max|F|", np.abs(F).max())
 
 

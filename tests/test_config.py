@@ -39,7 +39,7 @@ def _ids(paths):
 
 
 def test_committed_configs_present():
-    assert len(CONFIGS) >= 4 and len(STATE_CONFIGS) >= 3
+    assert len(CONFIGS) >= 7 and len(STATE_CONFIGS) >= 6
 
 
 @pytest.mark.parametrize("path", CONFIGS + EXAMPLES, ids=_ids(CONFIGS + EXAMPLES))
@@ -95,6 +95,27 @@ def test_restatement_rhs_on_config_equals_reference(path):
     M = cb.Mesh(cfg.problem)
     g = np.load(path[:-5] + ".state.npz")
     assert np.array_equal(oracle.port_rhs(cfg.problem, M, g["X0"]), g["F"])
+
+
+ANISO = [p for p in STATE_CONFIGS if os.path.basename(p).startswith("aniso")]
+
+
+@pytest.mark.parametrize("path", ANISO, ids=_ids(ANISO))
+def test_restatement_anisotropy_equals_reference_on_evolved_state(path):
+    """gradient-based anisotropy (least-squares gradients, normals of each
+    pair, (u . dir)^4 terms on energy and mobility): the restatement equals
+    the reference's RHS bit for bit on a state evolved by the reference, and
+    the anisotropy changes the result"""
+    cfg = cb.Config.load(path)
+    M = cb.Mesh(cfg.problem)
+    g = np.load(path[:-5] + ".state.npz")
+    F = oracle.port_rhs(cfg.problem, M, g["X1"])
+    assert np.array_equal(F, g["F1"])
+    cfg.problem.s.gradient_calculation = 0
+    F0 = oracle.port_rhs(cfg.problem, M, g["X1"])
+    A = cfg.problem.aos
+    sl = slice(A.pf_offset, A.pf_offset + A.pf_size)
+    assert np.abs(F0[:, sl] - F[:, sl]).max() > 1e-3 * np.abs(F[:, sl]).max()
 
 
 def test_config_values():

@@ -230,9 +230,14 @@ def test_trajectory_fp64_vs_port():
 def test_unsupported_configurations_rejected():
     P = cb.Problem.alloy(2, [8, 8], "calphad2sl", 3, 2, 4, 1, 0)
     M = cb.Mesh(P)
+    # gradient-based anisotropy runs on whole-domain uniform grids only
     P.s.gradient_calculation = 1
+    P.s.interface[0].energy_naniso = 1
+    P.s.interface[0].energy_aniso_val[0] = 0.1
+    P.s.interface[0].energy_aniso_dir[0] = 1.0
+    Mf = cb.Forest(2, [1, 1], 2, 3).mesh(P)
     with pytest.raises(L.CipherError) as e:
-        cb.Context(P, M, "fp64")
+        cb.Context(P, Mf, "fp64")
     assert e.value.code == L.E_UNSUPPORTED
     P.s.gradient_calculation = 0
     P.s.material[1].nsources = 1
