@@ -775,7 +775,7 @@ def run_cipher(args, rank, world, local_rank):
                         ("chemistry_amr", lambda: run_chemistry_amr(dev, 20)),
                         ("chemistry", lambda: run_chemistry(dev, 20, peak)),
                         ("batched", lambda: run_batched(dev, 256, 50.0, 16)),
-                        ("serving", lambda: run_serving(dev, 50.0, 4.0))):
+                        ("serving", lambda: run_serving(dev, 50.0, args.serving_seconds))):
             t1 = time.time()
             try:
                 line[key] = fn()
@@ -801,6 +801,8 @@ def main():
     ap.add_argument("--batch-domains", type=int, default=256, help="--only batched: number of domains")
     ap.add_argument("--batch-t-end", type=float, default=50.0, help="--only batched: end time of every domain")
     ap.add_argument("--batch-precisions", default="fp64,mixed", help="--only batched: precisions to run")
+    ap.add_argument("--serving-seconds", type=float, default=60.0,
+                    help="length of the serving leg's arrival trace (Poisson, 50 requests/s)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -815,7 +817,7 @@ def main():
         fn = {"chemistry": lambda: run_chemistry(local_rank, args.steps, peak),
               "batched": lambda: run_batched(local_rank, args.batch_domains, args.batch_t_end, 16,
                                              tuple(args.batch_precisions.split(","))),
-              "serving": lambda: run_serving(local_rank, 50.0, 4.0),
+              "serving": lambda: run_serving(local_rank, 50.0, args.serving_seconds),
               "config1_steps": lambda: _config1_only(local_rank, args.steps),
               "chemistry_amr": lambda: run_chemistry_amr(local_rank, args.steps)}[args.only]
         print(json.dumps({args.only: fn()}), flush=True)

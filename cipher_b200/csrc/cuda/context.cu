@@ -95,6 +95,8 @@ struct cipher_ctx {
     int aniso;                    /* gradient-based anisotropy: gradients of phi before the RHS */
     double cw[3];                 /* cell width per axis (centroids of the gradient weights) */
     double *d_grad;               /* [dim][P][stride] gradients (aniso) */
+    int32_t *d_order, *d_order_cursor; /* general kernels' cell grouping (kOrderClasses cursors) */
+    int nclass;
     int single;
     double sig0, mob0, wid0, tj0, ffactor, vol, junctionpenalty, delta;
     int has_temp_rate;
@@ -210,6 +212,8 @@ static void free_ctx(cipher_ctx *c)
     dev_free(c->d_tcond);
     dev_free(c->d_pruned);
     dev_free(c->d_grad);
+    dev_free(c->d_order);
+    dev_free(c->d_order_cursor);
     dev_free(c->d_err);
     pinned_word_free(c->h_err);
     dev_free(c->d_aos_x);
@@ -516,6 +520,14 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
         free_ctx(c);
         return cuda_fail(e, "cudaMalloc gradients");
     }
+    if (c->general && c->nmat + 3 <= kOrderClasses) {
+        c->nclass = c->nmat + 3;
+        if ((e = dev_alloc(&c->d_order, (size_t)c->stride * sizeof(int32_t))) != cudaSuccess ||
+            (e = dev_alloc(&c->d_order_cursor, kOrderClasses * sizeof(int32_t))) != cudaSuccess) {
+            free_ctx(c);
+            return cuda_fail(e, "cudaMalloc cell order");
+        }
+    }
     if ((e = dev_alloc(&c->d_err, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc err"); }
     if ((e = cudaMemset(c->d_err, 0, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMemset err"); }
     if ((e = pinned_word_alloc(&c->h_err)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "pinned error word"); }
@@ -666,6 +678,9 @@ static GenArgs<R> gen_args(const cipher_ctx *c, const void *X, void *F)
     a.tm = (const R *)(x + c->lay.tm_offset);
     a.fl = face_lists(c);
     a.grad = c->d_grad;
+    a.order = c->d_order;
+    a.order_cursor = c->d_order_cursor;
+    a.nclass = c->nclass;
     for (int d = 0; d < 3; d++) a.cw[d] = c->cw[d];
     a.comp = c->d_comp;
     a.mob = c->d_mob;

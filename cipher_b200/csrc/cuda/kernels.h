@@ -105,6 +105,10 @@ struct DevBC {
 
 /* arguments of the general RHS on a uniform grid: chemistry, heat,
  * boundary faces, several interfaces and materials */
+/* classes of the general kernels' cell grouping: one per material for
+ * single-phase cells, then sets of 2, 3 and more phases */
+constexpr int kOrderClasses = 32;
+
 template <typename R>
 struct GenArgs {
     int64_t ncells, stride;
@@ -131,6 +135,9 @@ struct GenArgs {
     double *comp, *mob, *tcond;   /* per-cell scratch: [ncp][stride], [ncp][stride], [stride] */
     FaceLists fl;                 /* face lists of an adapted mesh (fl.start == NULL: uniform grid) */
     double *grad;                 /* [dim][P][stride] phase-field gradients, or NULL (no anisotropy) */
+    int32_t *order;               /* [ncells] cells grouped by class (single-phase material, set size), or NULL */
+    int32_t *order_cursor;        /* [kOrderClasses] placement cursors of the grouping */
+    int nclass;                   /* classes in use: nmat + 3 (0: no grouping) */
     double cw[3];                 /* cell width along each axis: centroid = (i + 0.5) * cw */
     R *fphi;
     double *fdp, *fex;
