@@ -520,8 +520,9 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
         free_ctx(c);
         return cuda_fail(e, "cudaMalloc gradients");
     }
-    if (c->general && c->nmat + 3 <= kOrderClasses) {
-        c->nclass = c->nmat + 3;
+    const bool order_pf = !c->general && c->precision == CIPHER_PREC_FP64 && c->P < kOrderClasses;
+    if ((c->general && c->nmat + 3 <= kOrderClasses) || order_pf) {
+        c->nclass = c->general ? c->nmat + 3 : c->P + 1;
         if ((e = dev_alloc(&c->d_order, (size_t)c->stride * sizeof(int32_t))) != cudaSuccess ||
             (e = dev_alloc(&c->d_order_cursor, kOrderClasses * sizeof(int32_t))) != cudaSuccess) {
             free_ctx(c);
@@ -593,6 +594,10 @@ static PfArgs<R> pf_args(const cipher_ctx *c, const void *X, void *F)
     memset(&a, 0, sizeof(a));
     const char *x = (const char *)X;
     char *f = (char *)F;
+    if (!c->general) {
+        a.order = c->d_order;
+        a.order_cursor = c->d_order_cursor;
+    }
     a.ncells = c->ncells;
     a.stride = c->stride;
     for (int d = 0; d < 3; d++) { a.res[d] = c->res[d]; a.per[d] = c->per[d]; }

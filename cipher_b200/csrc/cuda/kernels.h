@@ -39,6 +39,11 @@ struct FaceLists {
 constexpr int32_t FACE_SELF_L = (int32_t)0x80000000u;
 
 /* arguments of the phase-field-only RHS on a uniform grid */
+/* classes of the kernels' cell grouping (general kernels: one per material
+ * for single-phase cells, then sets of 2, 3 and more phases; FP64 phase-field
+ * kernel: the set size) */
+constexpr int kOrderClasses = 32;
+
 template <typename R>
 struct PfArgs {
     int64_t ncells, stride;
@@ -70,6 +75,9 @@ struct PfArgs {
     R *fphi;
     R *ftm;
     int *err;
+    /* FP64 reference-order kernel: cells grouped by set size (NULL: grid order) */
+    int32_t *order;               /* [ncells] */
+    int32_t *order_cursor;        /* [kOrderClasses] */
 };
 
 cudaError_t launch_rhs_phasefield(const PfArgs<double> &a, int dim, cudaStream_t s);
@@ -105,10 +113,6 @@ struct DevBC {
 
 /* arguments of the general RHS on a uniform grid: chemistry, heat,
  * boundary faces, several interfaces and materials */
-/* classes of the general kernels' cell grouping: one per material for
- * single-phase cells, then sets of 2, 3 and more phases */
-constexpr int kOrderClasses = 32;
-
 template <typename R>
 struct GenArgs {
     int64_t ncells, stride;

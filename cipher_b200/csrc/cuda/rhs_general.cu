@@ -434,8 +434,7 @@ __global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> 
         }
         /* chemical-potential flux with the Andersson-Agren frame (material.c:1125-1137) */
         if (ndp) {
-            double me[CIPHER_MAXCP], ca[CIPHER_MAXCP], MB[(CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1)];
-            double dmu[CIPHER_MAXCP], fl[CIPHER_MAXCP];
+            double me[CIPHER_MAXCP], ca[CIPHER_MAXCP];
             for (int d = 0; d < ncp; d++) {
                 const double ml = a.mob[(int64_t)d * S + cl], mr = a.mob[(int64_t)d * S + cr];
                 const double cL = a.comp[(int64_t)d * S + cl], cR = a.comp[(int64_t)d * S + cr];
@@ -443,25 +442,52 @@ __global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> 
                 else me[d] = 0.0;
                 ca[d] = 2.0 * cL * cR / (cL + cR);
             }
-            for (int i = 0; i < ndp; i++)
-                for (int j = 0; j < ndp; j++) {
-                    double acc = 0.0;
-                    for (int k = 0; k < ncp; k++)
-                        acc += ((j == k ? 1.0 : 0.0) - ca[j]) * ((k == i ? 1.0 : 0.0) - ca[i]) * me[k];
-                    MB[i * ndp + j] = acc;
+            if constexpr (sizeof(R) == 4) {
+                /* mixed: the flux stencil in FP32 - the Andersson-Agren matrix
+                 * and its product with the potential difference (formed in
+                 * FP64, then rounded) - accumulated into the FP64 divergence */
+                float MB[(CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1)], dmu[CIPHER_MAXCP];
+                for (int i = 0; i < ndp; i++)
+                    for (int j = 0; j < ndp; j++) {
+                        float acc = 0.0f;
+                        for (int k = 0; k < ncp; k++)
+                            acc += ((j == k ? 1.0f : 0.0f) - (float)ca[j]) * ((k == i ? 1.0f : 0.0f) - (float)ca[i]) *
+                                   (float)me[k];
+                        MB[i * ndp + j] = acc;
+                    }
+                for (int d = 0; d < ndp; d++) dmu[d] = (float)(a.dp[(int64_t)d * S + cr] - a.dp[(int64_t)d * S + cl]);
+                for (int d = 0; d < ndp; d++) {
+                    float f = 0.0f;
+                    for (int j = 0; j < ndp; j++) f += MB[d * ndp + j] * dmu[j];
+                    if (self_L) ldp[d] += fdiv((double)f);
+                    else ldp[d] -= fdiv((double)f);
                 }
-            for (int d = 0; d < ndp; d++) dmu[d] = a.dp[(int64_t)d * S + cr] - a.dp[(int64_t)d * S + cl];
-            matvec(fl, MB, dmu, ndp);
-            for (int d = 0; d < ndp; d++) {
-                if (self_L) ldp[d] += fdiv(fl[d]);
-                else ldp[d] -= fdiv(fl[d]);
+            } else {
+                double MB[(CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1)], dmu[CIPHER_MAXCP], fl[CIPHER_MAXCP];
+                for (int i = 0; i < ndp; i++)
+                    for (int j = 0; j < ndp; j++) {
+                        double acc = 0.0;
+                        for (int k = 0; k < ncp; k++)
+                            acc += ((j == k ? 1.0 : 0.0) - ca[j]) * ((k == i ? 1.0 : 0.0) - ca[i]) * me[k];
+                        MB[i * ndp + j] = acc;
+                    }
+                for (int d = 0; d < ndp; d++) dmu[d] = a.dp[(int64_t)d * S + cr] - a.dp[(int64_t)d * S + cl];
+                matvec(fl, MB, dmu, ndp);
+                for (int d = 0; d < ndp; d++) {
+                    if (self_L) ldp[d] += fdiv(fl[d]);
+                    else ldp[d] -= fdiv(fl[d]);
+                }
             }
         }
-        /* heat flux */
+        /* heat flux (mixed: the face product in FP32) */
         if (a.tcond) {
             const double tl = a.tcond[cl], tr = a.tcond[cr];
             if (fabs(tl) > 1e-32 && fabs(tr) > 1e-32) {
-                const double ft = 2.0 * tl * tr / (tl + tr) * ((double)a.tm[cr] - (double)a.tm[cl]);
+                double ft;
+                if constexpr (sizeof(R) == 4)
+                    ft = (double)((float)(2.0 * tl * tr / (tl + tr)) * ((float)a.tm[cr] - (float)a.tm[cl]));
+                else
+                    ft = 2.0 * tl * tr / (tl + tr) * ((double)a.tm[cr] - (double)a.tm[cl]);
                 if (self_L) ltm += fdiv(ft);
                 else ltm -= fdiv(ft);
             }
@@ -574,31 +600,38 @@ __global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> 
         }
     };
     for (int g = 0; g < PM; g++) pf[g] = 0.0;
-    if (n > 1) {
-        /* capillary force with the triple-junction penalty (src/cipher.c:474-497) */
-        double cap[PM], unc[PM];
-        for (int g = 0; g < n; g++) cap[g] = 0.0;
+    /* the interface terms (capillary force, active set, constrained rates)
+     * in the compute type RC: FP64 on the FP64 path (the reference's
+     * operations), FP32 on the mixed path; the chemical driving force comes
+     * from the FP64 model evaluation above */
+    auto interface_rates = [&](auto zero) {
+        using RC = decltype(zero);
+        const RC PIc = (RC)PI;
+        RC cap[PM], unc[PM], rate[PM];
+        for (int g = 0; g < n; g++) { cap[g] = (RC)0; rate[g] = (RC)0; }
         for (int k = 0; k < n; k++) {
             for (int j = k + 1; j < n; j++) {
-                double skj, mkj, wkj;
-                props(k, j, skj, mkj, wkj);
-                cap[k] -= skj * (phi[j] / wkj + lap[j] * wkj / PI / PI);
-                cap[j] -= skj * (phi[k] / wkj + lap[k] * wkj / PI / PI);
+                double skd, mkd, wkd;
+                props(k, j, skd, mkd, wkd);
+                const RC skj = (RC)skd, wkj = (RC)wkd;
+                cap[k] -= skj * ((RC)phi[j] / wkj + (RC)lap[j] * wkj / PIc / PIc);
+                cap[j] -= skj * ((RC)phi[k] / wkj + (RC)lap[k] * wkj / PIc / PIc);
                 for (int i = j + 1; i < n; i++) {
-                    double s_, m_, w_, tj = 0.0, v;
+                    double s_, m_, w_;
+                    RC tj = (RC)0, v;
                     v = skj / wkj; tj = tj > v ? tj : v;
                     props(k, i, s_, m_, w_);
-                    v = s_ / w_; tj = tj > v ? tj : v;
+                    v = (RC)s_ / (RC)w_; tj = tj > v ? tj : v;
                     props(j, i, s_, m_, w_);
-                    v = s_ / w_; tj = tj > v ? tj : v;
-                    tj *= a.junctionpenalty;
-                    cap[k] -= tj * phi[j] * phi[i];
-                    cap[j] -= tj * phi[k] * phi[i];
-                    cap[i] -= tj * phi[k] * phi[j];
+                    v = (RC)s_ / (RC)w_; tj = tj > v ? tj : v;
+                    tj *= (RC)a.junctionpenalty;
+                    cap[k] -= tj * (RC)phi[j] * (RC)phi[i];
+                    cap[j] -= tj * (RC)phi[k] * (RC)phi[i];
+                    cap[i] -= tj * (RC)phi[k] * (RC)phi[j];
                 }
             }
-            cap[k] *= 8.0;
-            cap[k] += lap[k];
+            cap[k] *= (RC)8;
+            cap[k] += (RC)lap[k];
         }
         /* chemical driving force (src/cipher.c:499-522) */
         for (int k = 0; k < n; k++)
@@ -613,20 +646,20 @@ __global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> 
             }
         interpolant_dT<PM>(a.interp, chem, phi, n);
         /* active set and constrained rate (src/cipher.c:524-555) */
-        double nact = 0.0;
+        RC nact = (RC)0;
         uint32_t act = 0;
-        for (int g = 0; g < n; g++) unc[g] = 0.0;
+        for (int g = 0; g < n; g++) unc[g] = (RC)0;
         for (int k = 0; k < n; k++) {
             for (int j = k + 1; j < n; j++) {
                 double s_, m_, w_;
                 props(k, j, s_, m_, w_);
-                const double r = m_ * ((cap[k] - cap[j]) - (chem[k] - chem[j]) * 8.0 * sqrt(h[k] * h[j]) / PI);
+                const RC r = (RC)m_ * ((cap[k] - cap[j]) - (RC)(chem[k] - chem[j]) * (RC)8 * (RC)sqrt(h[k] * h[j]) / PIc);
                 unc[k] += r;
                 unc[j] -= r;
             }
-            const bool on = (phi[k] > CIPHER_TOL && phi[k] < 1.0 - CIPHER_TOL) || (phi[k] < CIPHER_TOL && unc[k] > 0.0) ||
-                            (phi[k] > 1.0 - CIPHER_TOL && unc[k] < 0.0);
-            if (on) { act |= 1u << k; nact += 1.0; }
+            const bool on = (phi[k] > CIPHER_TOL && phi[k] < 1.0 - CIPHER_TOL) || (phi[k] < CIPHER_TOL && unc[k] > (RC)0) ||
+                            (phi[k] > 1.0 - CIPHER_TOL && unc[k] < (RC)0);
+            if (on) { act |= 1u << k; nact += (RC)1; }
         }
         for (int k = 0; k < n; k++) {
             if (!(act >> k & 1u)) continue;
@@ -634,12 +667,17 @@ __global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> 
                 if (!(act >> j & 1u)) continue;
                 double s_, m_, w_;
                 props(k, j, s_, m_, w_);
-                const double r = m_ * ((cap[k] - cap[j]) - (chem[k] - chem[j]) * 8.0 * sqrt(h[k] * h[j]) / PI);
-                pf[k] += r;
-                pf[j] -= r;
+                const RC r = (RC)m_ * ((cap[k] - cap[j]) - (RC)(chem[k] - chem[j]) * (RC)8 * (RC)sqrt(h[k] * h[j]) / PIc);
+                rate[k] += r;
+                rate[j] -= r;
             }
-            pf[k] /= nact;
+            rate[k] /= nact;
         }
+        for (int g = 0; g < n; g++) pf[g] = (double)rate[g];
+    };
+    if (n > 1) {
+        if constexpr (sizeof(R) == 4) interface_rates(0.0f);
+        else interface_rates(0.0);
     }
     for (int g = 0; g < a.P; g++) a.fphi[(int64_t)g * S + c] = (R)(g < PM ? pf[g] : 0.0);
 
