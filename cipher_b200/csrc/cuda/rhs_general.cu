@@ -20,9 +20,15 @@
  * kernel instead of stored: the same arithmetic gives the same bits, and a
  * few exponentials per phase cost less than 8*P*S bytes written and read.
  *
- * All arithmetic is FP64 in the reference's operation order (this unit is
- * compiled with --fmad=false); phi and T are read and written in the state's
- * storage type R (double, or float for the mixed layout).
+ * With an FP64 state (R = double) all arithmetic is FP64 in the reference's
+ * operation order (this unit is compiled with --fmad=false).  With the mixed
+ * layout (R = float: phi and T stored in FP32) the flux stencil (the
+ * Andersson-Agren matrix times the potential difference, the heat-flux
+ * product) and the interface terms (capillary force, active set, pair rates)
+ * run in FP32, each face flux summed into an FP64 divergence, while the
+ * model evaluations and the mu update stay FP64.  Gradient-based
+ * anisotropy adds k_gradients before the RHS; both kernels walk the cells
+ * grouped by class (k_order_*).
  */
 #include <cstdint>
 #include <cuda_runtime.h>
