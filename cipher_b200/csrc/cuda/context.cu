@@ -95,7 +95,8 @@ struct cipher_ctx {
     int aniso;                    /* gradient-based anisotropy: gradients of phi before the RHS */
     double cw[3];                 /* cell width per axis (centroids of the gradient weights) */
     double *d_grad;               /* [dim][P][stride] gradients (aniso) */
-    int32_t *d_order, *d_order_cursor; /* general kernels' cell grouping (kOrderClasses cursors) */
+    int32_t *d_order, *d_order_cursor; /* cell grouping: order, class totals */
+    int32_t *d_order_counts;      /* [kOrderClasses][blocks of 256 cells] */
     int nclass;
     int single;
     double sig0, mob0, wid0, tj0, ffactor, vol, junctionpenalty, delta;
@@ -214,6 +215,7 @@ static void free_ctx(cipher_ctx *c)
     dev_free(c->d_grad);
     dev_free(c->d_order);
     dev_free(c->d_order_cursor);
+    dev_free(c->d_order_counts);
     dev_free(c->d_err);
     pinned_word_free(c->h_err);
     dev_free(c->d_aos_x);
@@ -523,8 +525,10 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
     const bool order_pf = !c->general && c->precision == CIPHER_PREC_FP64 && c->P < kOrderClasses;
     if ((c->general && c->nmat + 3 <= kOrderClasses) || order_pf) {
         c->nclass = c->general ? c->nmat + 3 : c->P + 1;
+        const size_t nblk = (size_t)(c->ncells + 255) / 256;
         if ((e = dev_alloc(&c->d_order, (size_t)c->stride * sizeof(int32_t))) != cudaSuccess ||
-            (e = dev_alloc(&c->d_order_cursor, kOrderClasses * sizeof(int32_t))) != cudaSuccess) {
+            (e = dev_alloc(&c->d_order_cursor, kOrderClasses * sizeof(int32_t))) != cudaSuccess ||
+            (e = dev_alloc(&c->d_order_counts, kOrderClasses * nblk * sizeof(int32_t))) != cudaSuccess) {
             free_ctx(c);
             return cuda_fail(e, "cudaMalloc cell order");
         }
@@ -597,6 +601,7 @@ static PfArgs<R> pf_args(const cipher_ctx *c, const void *X, void *F)
     if (!c->general) {
         a.order = c->d_order;
         a.order_cursor = c->d_order_cursor;
+        a.order_counts = c->d_order_counts;
     }
     a.ncells = c->ncells;
     a.stride = c->stride;
@@ -685,6 +690,7 @@ static GenArgs<R> gen_args(const cipher_ctx *c, const void *X, void *F)
     a.grad = c->d_grad;
     a.order = c->d_order;
     a.order_cursor = c->d_order_cursor;
+    a.order_counts = c->d_order_counts;
     a.nclass = c->nclass;
     for (int d = 0; d < 3; d++) a.cw[d] = c->cw[d];
     a.comp = c->d_comp;

@@ -77,7 +77,8 @@ struct PfArgs {
     int *err;
     /* FP64 reference-order kernel: cells grouped by set size (NULL: grid order) */
     int32_t *order;               /* [ncells] */
-    int32_t *order_cursor;        /* [kOrderClasses] */
+    int32_t *order_cursor;        /* [kOrderClasses] class totals */
+    int32_t *order_counts;        /* [kOrderClasses][blocks of 256 cells] */
 };
 
 cudaError_t launch_rhs_phasefield(const PfArgs<double> &a, int dim, cudaStream_t s);
@@ -140,7 +141,8 @@ struct GenArgs {
     FaceLists fl;                 /* face lists of an adapted mesh (fl.start == NULL: uniform grid) */
     double *grad;                 /* [dim][P][stride] phase-field gradients, or NULL (no anisotropy) */
     int32_t *order;               /* [ncells] cells grouped by class (single-phase material, set size), or NULL */
-    int32_t *order_cursor;        /* [kOrderClasses] placement cursors of the grouping */
+    int32_t *order_cursor;        /* [kOrderClasses] class totals of the grouping */
+    int32_t *order_counts;        /* [kOrderClasses][blocks of 256 cells] per-block counts, then offsets */
     int nclass;                   /* classes in use: nmat + 3 (0: no grouping) */
     double cw[3];                 /* cell width along each axis: centroid = (i + 0.5) * cw */
     R *fphi;

@@ -36,6 +36,7 @@
 #include "device_common.cuh"
 #include "kernels.h"
 #include "models.cuh"
+#include "order.cuh"
 
 namespace cipher {
 
@@ -182,76 +183,28 @@ __global__ void __launch_bounds__(kGenBlock) k_chem_cell(const GenArgs<R> a)
 
 /* A warp of the general kernels runs one model per lane: cells whose single
  * phase belongs to different materials, and cells with several phases,
- * diverge.  The kernels therefore walk the cells in an order grouped by
- * class (the material of a single-phase cell; sets of 2, 3, >3 phases),
- * each class's cells in grid order within a block, so that warps mostly
- * hold one class.  Every cell's arithmetic is unchanged: the results do
- * not depend on the order. */
-template <typename R>
-__device__ __forceinline__ int cell_class(const GenArgs<R> &a, int64_t c)
-{
-    const int n = a.as[c];
-    if (n == 1) {
-        const int id = a.as[a.stride + c];
-        if (id >= 0 && id < a.npf) return a.chem.pmm[id];
+ * diverge.  The kernels therefore walk the cells grouped by class (the
+ * material of a single-phase cell; sets of 2, 3, more phases; order.cuh).
+ * Every cell's arithmetic is unchanged: the results do not depend on the
+ * order. */
+struct GeneralClassKey {
+    const uint16_t *as;
+    int64_t stride;
+    const int32_t *pmm;
+    int npf, nmat;
+    __device__ __forceinline__ int operator()(int64_t c) const
+    {
+        const int n = as[c];
+        if (n == 1) {
+            const int id = as[stride + c];
+            if (id >= 0 && id < npf) {
+                const int m = pmm[id];
+                if (m >= 0 && m < nmat) return m;
+            }
+        }
+        return nmat + (n <= 2 ? 0 : n == 3 ? 1 : 2);
     }
-    const int k = n <= 2 ? 0 : n == 3 ? 1 : 2;
-    return a.chem.nmat + k;
-}
-
-/* per-class counts (order_cursor[k] += count) */
-template <typename R>
-__global__ void __launch_bounds__(256) k_order_count(const GenArgs<R> a)
-{
-    __shared__ int cnt[kOrderClasses];
-    if (threadIdx.x < kOrderClasses) cnt[threadIdx.x] = 0;
-    __syncthreads();
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < a.ncells) atomicAdd(&cnt[cell_class(a, c)], 1);
-    __syncthreads();
-    if (threadIdx.x < a.nclass && cnt[threadIdx.x]) atomicAdd(&a.order_cursor[threadIdx.x], cnt[threadIdx.x]);
-}
-
-/* counts -> start of each class (exclusive prefix), one warp */
-__global__ void k_order_scan(int32_t *cursor, int nclass)
-{
-    if (threadIdx.x != 0) return;
-    int acc = 0;
-    for (int k = 0; k < nclass; k++) {
-        const int v = cursor[k];
-        cursor[k] = acc;
-        acc += v;
-    }
-}
-
-/* place every cell: within a block, each class's cells keep grid order */
-template <typename R>
-__global__ void __launch_bounds__(256) k_order_place(const GenArgs<R> a)
-{
-    __shared__ int wcnt[8][kOrderClasses];
-    __shared__ int base[kOrderClasses];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int key = c < a.ncells ? cell_class(a, c) : -1;
-    int rank = 0;
-    for (int k = 0; k < a.nclass; k++) {
-        const unsigned m = __ballot_sync(0xffffffffu, key == k);
-        if (key == k) rank = __popc(m & ((1u << lane) - 1u));
-        if (lane == 0) wcnt[warp][k] = __popc(m);
-    }
-    __syncthreads();
-    if (threadIdx.x < a.nclass) {
-        int tot = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += wcnt[w][threadIdx.x];
-        base[threadIdx.x] = tot ? atomicAdd(&a.order_cursor[threadIdx.x], tot) : 0;
-    }
-    __syncthreads();
-    if (key >= 0) {
-        int off = base[key];
-        for (int w = 0; w < warp; w++) off += wcnt[w][key];
-        a.order[off + rank] = (int32_t)c;
-    }
-}
+};
 
 /* ------------------------------------------------------------------ */
 /* the RHS                                                              */
@@ -1144,11 +1097,8 @@ static cudaError_t launch_gen(const GenArgs<R> &a, int dim, cudaStream_t s)
         k_specialise<R><<<a.chem.nmat, 256, 0, s>>>(a.chem.mat, (cipher_material *)a.chem.spec, a.tm,
                                                      (double *)a.chem.tspec);
     if (a.order) {
-        const unsigned ob = (unsigned)((a.ncells + 255) / 256);
-        cudaMemsetAsync(a.order_cursor, 0, kOrderClasses * sizeof(int32_t), s);
-        k_order_count<R><<<ob, 256, 0, s>>>(a);
-        k_order_scan<<<1, 32, 0, s>>>(a.order_cursor, a.nclass);
-        k_order_place<R><<<ob, 256, 0, s>>>(a);
+        const OrderBuf o = {a.order, a.order_counts, a.order_cursor, a.nclass, a.ncells};
+        launch_order(o, GeneralClassKey{a.as, a.stride, a.chem.pmm, a.npf, a.chem.nmat}, s);
     }
     if (a.ndp) k_chem_cell<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a);
     if (a.grad) k_gradients<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a, dim);

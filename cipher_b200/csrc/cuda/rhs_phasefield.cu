@@ -20,6 +20,7 @@
 #include "kernels.h"
 #include "pf_gather.cuh"
 #include "pf_cell.cuh"
+#include "order.cuh"
 
 namespace cipher {
 
@@ -55,61 +56,15 @@ __global__ void __launch_bounds__(kFp64Block) k_rhs_pf_fp64(const PfArgs<double>
  * with different sizes idle.  On full-grid launches the kernel walks the
  * cells grouped by set size (each size's cells in grid order within a
  * block); every cell's arithmetic is unchanged. */
-__global__ void __launch_bounds__(256) k_pf_order_count(const PfArgs<double> a)
-{
-    __shared__ int cnt[kOrderClasses];
-    if (threadIdx.x < kOrderClasses) cnt[threadIdx.x] = 0;
-    __syncthreads();
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < a.ncells) {
-        const int n = a.as[c];
-        atomicAdd(&cnt[(n >= 1 && n <= a.P) ? n : 0], 1);
+struct SetSizeKey {
+    const uint16_t *as;
+    int P;
+    __device__ __forceinline__ int operator()(int64_t c) const
+    {
+        const int n = as[c];
+        return (n >= 1 && n <= P) ? n : 0;
     }
-    __syncthreads();
-    if (threadIdx.x <= a.P && cnt[threadIdx.x]) atomicAdd(&a.order_cursor[threadIdx.x], cnt[threadIdx.x]);
-}
-
-__global__ void k_pf_order_scan(int32_t *cursor, int nclass)
-{
-    if (threadIdx.x != 0) return;
-    int acc = 0;
-    for (int k = 0; k < nclass; k++) {
-        const int v = cursor[k];
-        cursor[k] = acc;
-        acc += v;
-    }
-}
-
-__global__ void __launch_bounds__(256) k_pf_order_place(const PfArgs<double> a)
-{
-    __shared__ int wcnt[8][kOrderClasses];
-    __shared__ int base[kOrderClasses];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    int key = -1;
-    if (c < a.ncells) {
-        const int n = a.as[c];
-        key = (n >= 1 && n <= a.P) ? n : 0;
-    }
-    int rank = 0;
-    for (int k = 0; k <= a.P; k++) {
-        const unsigned m = __ballot_sync(0xffffffffu, key == k);
-        if (key == k) rank = __popc(m & ((1u << lane) - 1u));
-        if (lane == 0) wcnt[warp][k] = __popc(m);
-    }
-    __syncthreads();
-    if (threadIdx.x <= a.P) {
-        int tot = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += wcnt[w][threadIdx.x];
-        base[threadIdx.x] = tot ? atomicAdd(&a.order_cursor[threadIdx.x], tot) : 0;
-    }
-    __syncthreads();
-    if (key >= 0) {
-        int off = base[key];
-        for (int w = 0; w < warp; w++) off += wcnt[w][key];
-        a.order[off + rank] = (int32_t)c;
-    }
-}
+};
 
 template <int DIM, int PM, bool SINGLE>
 __global__ void __launch_bounds__(kFp64Block) k_rhs_pf_fp64_ordered(const PfArgs<double> a)
@@ -146,11 +101,8 @@ static void launch_pm(const PfArgs<double> &a, cudaStream_t s)
     size_t sm = slot_columns_bytes(a.P, kFp64Block, 8, true);
     const bool whole = a.zcount <= 0 || (a.zbase == 0 && a.zcount >= a.res[2]);
     if (a.order && whole && a.P < kOrderClasses) {
-        const unsigned ob = (unsigned)((a.ncells + 255) / 256);
-        cudaMemsetAsync(a.order_cursor, 0, kOrderClasses * sizeof(int32_t), s);
-        k_pf_order_count<<<ob, 256, 0, s>>>(a);
-        k_pf_order_scan<<<1, 32, 0, s>>>(a.order_cursor, a.P + 1);
-        k_pf_order_place<<<ob, 256, 0, s>>>(a);
+        const OrderBuf o = {a.order, a.order_counts, a.order_cursor, a.P + 1, a.ncells};
+        launch_order(o, SetSizeKey{a.as, a.P}, s);
         const unsigned blocks = (unsigned)((a.ncells + kFp64Block - 1) / kFp64Block);
         if (a.single) k_rhs_pf_fp64_ordered<DIM, PM, true><<<blocks, kFp64Block, sm, s>>>(a);
         else k_rhs_pf_fp64_ordered<DIM, PM, false><<<blocks, kFp64Block, sm, s>>>(a);
