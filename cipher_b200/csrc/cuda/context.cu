@@ -16,6 +16,8 @@
 #include "cipher_b200.h"
 #include "device_common.cuh"
 #include "kernels.h"
+#include "models.cuh"
+#include "general_common.cuh"
 
 using namespace cipher;
 
@@ -98,6 +100,12 @@ struct cipher_ctx {
     int32_t *d_order, *d_order_cursor; /* cell grouping: order, class totals */
     int32_t *d_order_counts;      /* [kOrderClasses][blocks of 256 cells] */
     int nclass;
+    uint32_t single_models;       /* GenArgs::single_models */
+    /* (cell, phase) items of the cells of several phases (rhs_items.cu) */
+    double *d_iscr;
+    int32_t *d_ibase, *d_icell, *d_icount;
+    int64_t icap;                 /* 0: no item path */
+    int item_model;               /* GenArgs::item_model */
     int single;
     double sig0, mob0, wid0, tj0, ffactor, vol, junctionpenalty, delta;
     int has_temp_rate;
@@ -115,6 +123,7 @@ struct cipher_ctx {
     cipher_material *d_mat;
     double *d_t0;                 /* [npf] temperature0 of each phase's material */
     cipher_material *d_mat_spec;  /* the materials specialised at one temperature */
+    MatV *d_matv;                 /* their CALPHAD tables evaluated (NULL: off) */
     double *d_tspec;
     int32_t *d_pmm;
     double *d_comp, *d_mob, *d_tcond;
@@ -206,6 +215,7 @@ static void free_ctx(cipher_ctx *c)
     dev_free(c->d_mat);
     dev_free(c->d_t0);
     dev_free(c->d_mat_spec);
+    dev_free(c->d_matv);
     dev_free(c->d_tspec);
     dev_free(c->d_pmm);
     dev_free(c->d_comp);
@@ -216,6 +226,10 @@ static void free_ctx(cipher_ctx *c)
     dev_free(c->d_order);
     dev_free(c->d_order_cursor);
     dev_free(c->d_order_counts);
+    dev_free(c->d_iscr);
+    dev_free(c->d_ibase);
+    dev_free(c->d_icell);
+    dev_free(c->d_icount);
     dev_free(c->d_err);
     pinned_word_free(c->h_err);
     dev_free(c->d_aos_x);
@@ -496,10 +510,17 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
         if ((e = dev_alloc(&c->d_mat, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc materials"); }
         if ((e = cudaMemcpy(c->d_mat, p->material, nb, cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy materials"); }
         if ((e = dev_alloc(&c->d_mat_spec, nb)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc materials"); }
-        if ((e = dev_alloc(&c->d_tspec, sizeof(double))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc materials"); }
+        /* [0] the copies' temperature, [1 + m] material m's copy, [1 + nmat + m] its evaluated tables */
+        if ((e = dev_alloc(&c->d_tspec, (size_t)(1 + 2 * p->nmat) * sizeof(double))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc materials"); }
+        const char *senv = getenv("CIPHER_B200_SPECIALISED_KERNELS");
+        if ((!senv || strcmp(senv, "0") != 0) &&
+            (e = dev_alloc(&c->d_matv, (size_t)p->nmat * sizeof(MatV))) != cudaSuccess) {
+            free_ctx(c);
+            return cuda_fail(e, "cudaMalloc evaluated materials");
+        }
         {
-            const double nan = std::nan("");
-            if ((e = cudaMemcpy(c->d_tspec, &nan, sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy"); }
+            std::vector<double> nan((size_t)(1 + 2 * p->nmat), std::nan(""));
+            if ((e = cudaMemcpy(c->d_tspec, nan.data(), nan.size() * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "copy"); }
         }
         if (c->ndp) {
             nb = (size_t)c->ncp * c->stride * sizeof(double);
@@ -532,6 +553,44 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
             free_ctx(c);
             return cuda_fail(e, "cudaMalloc cell order");
         }
+    }
+    /* Specialised chemistry kernels, each giving the same bits as the
+     * general kernels (CIPHER_B200_SPECIALISED_KERNELS=0 keeps every cell in
+     * the general kernels, to compare the two):
+     *  - single-phase cells, per model whose materials all have the model's
+     *    sublattice count, compiled for 2..5 components (rhs_single.cu);
+     *  - the phases of cells of several phases as (cell, phase) items, one
+     *    thread each (rhs_items.cu), compiled for the component count and
+     *    model when every material has the same model (not "none"). */
+    c->item_model = -1;
+    const char *spec_env = getenv("CIPHER_B200_SPECIALISED_KERNELS");
+    const bool spec_on = !spec_env || strcmp(spec_env, "0") != 0;
+    if (spec_on && c->general && c->d_order && c->ncp >= 2 && c->ncp <= 5) {
+        uint32_t present = 0, bad = 0;
+        for (int m = 0; m < p->nmat; m++) {
+            const int model = p->material[m].model;
+            if (model < 0 || model >= 32) { bad = ~0u; break; }
+            present |= 1u << model;
+            if (p->material[m].nsites != model_nsites(model)) bad |= 1u << model;
+        }
+        c->single_models = present & ~bad;
+        if (c->single_models == present && (present & (present - 1)) == 0 && present != (1u << CIPHER_CHEM_NONE))
+            c->item_model = __builtin_ctz(present);
+    }
+    if (spec_on && c->general && c->d_order && c->ndp > 0 && c->ncells < ((int64_t)1 << 27)) {
+        /* room for the items of a few cells in ten, else those cells are
+         * evaluated whole by the general kernel */
+        int64_t cap = c->ncells / 2 > 65536 ? c->ncells / 2 : 65536;
+        if (cap > c->ncells * c->P) cap = c->ncells * c->P;
+        const int nq = item_q(c->ndp, c->S).nq;
+        if ((e = dev_alloc(&c->d_ibase, (size_t)c->stride * sizeof(int32_t))) != cudaSuccess ||
+            (e = dev_alloc(&c->d_icell, (size_t)cap * sizeof(int32_t))) != cudaSuccess ||
+            (e = dev_alloc(&c->d_icount, sizeof(int32_t))) != cudaSuccess ||
+            (e = dev_alloc(&c->d_iscr, (size_t)nq * cap * sizeof(double))) != cudaSuccess) {
+            free_ctx(c);
+            return cuda_fail(e, "cudaMalloc phase items");
+        }
+        c->icap = cap;
     }
     if ((e = dev_alloc(&c->d_err, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc err"); }
     if ((e = cudaMemset(c->d_err, 0, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMemset err"); }
@@ -679,6 +738,7 @@ static GenArgs<R> gen_args(const cipher_ctx *c, const void *X, void *F)
     a.chem.nmat = c->nmat;
     a.chem.spec = c->d_mat_spec;
     a.chem.tspec = c->d_tspec;
+    a.chem.matv_tab = c->d_matv;
     a.nbcs = c->nbcs;
     for (int b = 0; b < c->nbcs; b++) a.bcs[b] = c->bcs[b];
     a.as = (const uint16_t *)(x + c->lay.as_offset);
@@ -692,6 +752,15 @@ static GenArgs<R> gen_args(const cipher_ctx *c, const void *X, void *F)
     a.order_cursor = c->d_order_cursor;
     a.order_counts = c->d_order_counts;
     a.nclass = c->nclass;
+    a.single_models = c->single_models;
+    if (c->icap) {
+        a.iscr = c->d_iscr;
+        a.ibase = c->d_ibase;
+        a.icell = c->d_icell;
+        a.icount = c->d_icount;
+        a.icap = c->icap;
+    }
+    a.item_model = c->item_model;
     for (int d = 0; d < 3; d++) a.cw[d] = c->cw[d];
     a.comp = c->d_comp;
     a.mob = c->d_mob;

@@ -33,6 +33,33 @@ struct DevInterface {
     double mobility_dir[CIPHER_MAXDIR * 3], mobility_val[CIPHER_MAXDIR];
 };
 
+/* A T-series evaluated at one temperature, and the CALPHAD model tables of
+ * a material with every series evaluated (rhs_general.cu: k_evaluate): the
+ * fields the calphaddis and calphad2sl model bodies read (models.cuh), laid
+ * out densely - a cipher_rk spends 568 bytes on what an order count and one
+ * value per order say here. */
+struct TsV {
+    double v;
+};
+struct RkV {
+    int32_t n;
+    int32_t i[CIPHER_MAXRK];
+    TsV h[CIPHER_MAXRK];
+};
+struct MobV {
+    double m0;
+    TsV unary[CIPHER_MAXCP];
+    RkV binary[CIPHER_MAXBIN];
+};
+struct MatV {
+    int32_t model;
+    double p, q, molarvolume, stoichiometry[2];
+    TsV ref, unary[CIPHER_MAXCP * CIPHER_MAXCP];
+    RkV binary[CIPHER_MAXRKTAB], ternary[CIPHER_MAXRKTAB], binaryq[CIPHER_MAXRKTAB], ternaryq[CIPHER_MAXRKTAB];
+    MobV mobilityc[CIPHER_MAXCP];
+    TsV quad_ceq[CIPHER_MAXCP], quad_binary[CIPHER_MAXCP];   /* for the quadratic branches; never read */
+};
+
 /* material tables on the device: the host structs of cipher_problem.h
  * copied unchanged, and the phase -> material map */
 struct ChemTables {
@@ -43,6 +70,11 @@ struct ChemTables {
      * *tspec (rhs_general.cu: k_specialise), or NULL */
     const cipher_material *spec;
     const double *tspec;
+    /* the same materials as MatV at *tspec (NULL: none) */
+    const MatV *matv_tab;
+    /* matv_tab in the tables chem_at returns for a cell at *tspec, else
+     * NULL: the model wrappers read the evaluated tables through this */
+    const MatV *matv;
 };
 
 /* the tables a cell at temperature T reads: the specialised copy when it
@@ -50,7 +82,11 @@ struct ChemTables {
 __device__ __forceinline__ ChemTables chem_at(const ChemTables &t, double T)
 {
     ChemTables r = t;
-    if (t.spec && T == *t.tspec) r.mat = t.spec;
+    r.matv = nullptr;
+    if (t.spec && T == *t.tspec) {
+        r.mat = t.spec;
+        r.matv = t.matv_tab;
+    }
     return r;
 }
 
@@ -86,6 +122,10 @@ __device__ inline double tseries(double T, const cipher_tseries &s)
     if (fabs(s.logcoeff) > 0.0) r += s.logcoeff * T * log(T);
     return r;
 }
+
+/* an evaluated series: tseries(T, s) of the specialised series it was made
+ * from, bit for bit */
+__device__ __forceinline__ double tseries(double, const TsV &s) { return s.v; }
 
 /* pair properties sigma, m, w of an interface at temperature T
  * (src/cipher.c:422-471 without anisotropy) */

@@ -38,12 +38,12 @@ struct FaceLists {
 };
 constexpr int32_t FACE_SELF_L = (int32_t)0x80000000u;
 
-/* arguments of the phase-field-only RHS on a uniform grid */
 /* classes of the kernels' cell grouping (general kernels: one per material
  * for single-phase cells, then sets of 2, 3 and more phases; FP64 phase-field
  * kernel: the set size) */
 constexpr int kOrderClasses = 32;
 
+/* arguments of the phase-field-only RHS on a uniform grid */
 template <typename R>
 struct PfArgs {
     int64_t ncells, stride;
@@ -144,6 +144,13 @@ struct GenArgs {
     int32_t *order_cursor;        /* [kOrderClasses] class totals of the grouping */
     int32_t *order_counts;        /* [kOrderClasses][blocks of 256 cells] per-block counts, then offsets */
     int nclass;                   /* classes in use: nmat + 3 (0: no grouping) */
+    uint32_t single_models;       /* bit m: single-phase cells of model m run in rhs_single.cu's kernels */
+    double *iscr;                 /* [ItemQ::nq][icap] model results of the (cell, phase) items (rhs_items.cu) */
+    int32_t *ibase;               /* [ncells] first item of a cell of several phases, or -1 (no items) */
+    int32_t *icell;               /* [icap] item -> cell * 16 + slot */
+    int32_t *icount;              /* [1] items asked for by this RHS (may exceed icap) */
+    int64_t icap;                 /* item capacity (0: no item path) */
+    int item_model;               /* >= 0: every material has this model (items compiled for it), else -1 */
     double cw[3];                 /* cell width along each axis: centroid = (i + 0.5) * cw */
     R *fphi;
     double *fdp, *fex;
@@ -178,6 +185,17 @@ cudaError_t launch_output_fields(const GenArgs<float> &a, const int32_t *kinds, 
                                  double *out, cudaStream_t s);
 cudaError_t launch_rhs_general(const GenArgs<double> &a, int dim, cudaStream_t s);
 cudaError_t launch_rhs_general(const GenArgs<float> &a, int dim, cudaStream_t s);
+/* the single-phase cells of the models in a.single_models (rhs_single.cu):
+ * their composition, mobility and conductivity, then their RHS */
+cudaError_t launch_chem_single(const GenArgs<double> &a, cudaStream_t s);
+cudaError_t launch_chem_single(const GenArgs<float> &a, cudaStream_t s);
+cudaError_t launch_rhs_single(const GenArgs<double> &a, int dim, cudaStream_t s);
+cudaError_t launch_rhs_single(const GenArgs<float> &a, int dim, cudaStream_t s);
+/* the (cell, phase) items of the cells of several phases (rhs_items.cu):
+ * list them (a.ibase, a.icell), then evaluate each phase's models into the
+ * item scratch; a.icap > 0 */
+cudaError_t launch_items(const GenArgs<double> &a, cudaStream_t s);
+cudaError_t launch_items(const GenArgs<float> &a, cudaStream_t s);
 /* EX of every listed phase and mu of the majority phase from the materials'
  * c0 at the cell temperature (src/init.c:1790-1823) */
 cudaError_t launch_chem_init(const GenArgs<double> &a, double *ex, double *dp, cudaStream_t s);

@@ -34,9 +34,13 @@ __device__ inline double tseries_dT(double T, const cipher_tseries &s)
     return r;
 }
 
+/* the evaluated tables serve the CALPHAD models only, whose bodies take no
+ * T-derivative; present so that the quadratic branches compile */
+__device__ __forceinline__ double tseries_dT(double, const TsV &) { return 0.0; }
+
 /* closed-form inverses for the symmetric matrices of the path (n <= 4,
  * src/utility.c:232-405; only the lower-triangle cofactors are formed) */
-__device__ inline void invert_small(double *dst, const double *src, int n)
+__device__ __forceinline__ void invert_small(double *dst, const double *src, int n)
 {
     if (n == 1) {
         dst[0] = 1.0 / src[0];
@@ -90,20 +94,58 @@ __device__ __forceinline__ void matvec(double *dst, const double *A, const doubl
     }
 }
 
+/* v[i] for a component index i read from a table: with a compile-time
+ * count NC a select over the components, so v can stay in registers */
+template <int NC>
+__device__ __forceinline__ double pick(const double *v, int i)
+{
+    if constexpr (NC > 0) {
+        double r = v[0];
+#pragma unroll
+        for (int k = 1; k < NC; k++) r = i == k ? v[k] : r;
+        return r;
+    } else {
+        return v[i];
+    }
+}
+
+template <int NC>
+__device__ __forceinline__ void add_at(double *v, int i, double x)
+{
+    if constexpr (NC > 0) {
+#pragma unroll
+        for (int k = 0; k < NC; k++)
+            if (i == k) v[k] += x;
+    } else {
+        v[i] += x;
+    }
+}
+
+/* sublattices of a chemical model (cipher_problem_finalize) */
+__host__ __device__ constexpr int model_nsites(int model)
+{
+    return model == CIPHER_CHEM_NONE ? 0 : model == CIPHER_CHEM_CALPHAD2SL ? 2 : 1;
+}
+
 /* ---------------- raw model functions (per mole) ---------------- */
 
-static __device__ __noinline__ double energy_raw(const cipher_material &m, const double *y, double T, int ncp)
+template <int NC, int MODEL, typename Mat>
+static __device__ __forceinline__ double energy_body(const Mat &m, const double *y, double T, int ncp_rt)
 {
-    if (m.model == CIPHER_CHEM_NONE) return tseries(T, m.ref);
-    if (m.model == CIPHER_CHEM_QUADRATIC) {
+    const int ncp = NC > 0 ? NC : ncp_rt;
+    const int model = MODEL >= 0 ? MODEL : m.model;
+
+    if (model == CIPHER_CHEM_NONE) return tseries(T, m.ref);
+    if (model == CIPHER_CHEM_QUADRATIC) {
         double G = tseries(T, m.ref);
         for (int c = 0; c < ncp; c++)
             G += tseries(T, m.unary[c]) * (y[c] - tseries(T, m.quad_ceq[c]))
                + tseries(T, m.quad_binary[c]) * (y[c] - tseries(T, m.quad_ceq[c])) * (y[c] - tseries(T, m.quad_ceq[c]));
         return G;
     }
-    if (m.model == CIPHER_CHEM_CALPHADDIS) {
-        const cipher_rk *bin = m.binary, *ter = m.ternary;
+    if (model == CIPHER_CHEM_CALPHADDIS) {
+        const auto *bin = m.binary;
+        const auto *ter = m.ternary;
         double G = tseries(T, m.ref);
         for (int k = 0; k < ncp; k++) {
             G += tseries(T, m.unary[k]) * y[k] + CIPHER_R_GAS * T * y[k] * log(y[k]);
@@ -112,7 +154,7 @@ static __device__ __noinline__ double energy_raw(const cipher_material &m, const
                     G += tseries(T, bin->h[r]) * y[k] * y[j] * ipow(y[k] - y[j], (unsigned)r);
                 for (int i = j + 1; i < ncp; i++, ter++)
                     for (int r = 0; r < ter->n; r++)
-                        G += tseries(T, ter->h[r]) * y[k] * y[j] * y[i] * (y[ter->i[r]] + (1.0 - y[k] - y[j] - y[i]) / 3.0);
+                        G += tseries(T, ter->h[r]) * y[k] * y[j] * y[i] * (pick<NC>(y, ter->i[r]) + (1.0 - y[k] - y[j] - y[i]) / 3.0);
             }
         }
         return G;
@@ -120,45 +162,65 @@ static __device__ __noinline__ double energy_raw(const cipher_material &m, const
     const double *yp = y, *yq = y + ncp;
     double G = 0.0;
     for (int c = 0; c < ncp; c++) G += CIPHER_R_GAS * T * (m.p * yp[c] * log(yp[c]) + m.q * yq[c] * log(yq[c]));
-    for (int a = 0; a < ncp; a++)
+    for (int a = 0; a < ncp; a++) {
         for (int b = 0; b < ncp; b++) G += tseries(T, m.unary[a * ncp + b]) * yp[a] * yq[b];
-    const cipher_rk *rk = m.binary;
-    for (int i = 0; i < ncp; i++)
-        for (int j = i + 1; j < ncp; j++)
+    }
+    const auto *rk = m.binary;
+    for (int i = 0; i < ncp; i++) {
+        for (int j = i + 1; j < ncp; j++) {
             for (int q = 0; q < ncp; q++, rk++)
                 for (int r = 0; r < rk->n; r++)
                     G += tseries(T, rk->h[r]) * yp[i] * yp[j] * yq[q] * ipow(yp[i] - yp[j], (unsigned)r);
+        }
+    }
     rk = m.binaryq;
-    for (int p = 0; p < ncp; p++)
-        for (int i = 0; i < ncp; i++)
+    for (int p = 0; p < ncp; p++) {
+        for (int i = 0; i < ncp; i++) {
             for (int j = i + 1; j < ncp; j++, rk++)
                 for (int r = 0; r < rk->n; r++)
                     G += tseries(T, rk->h[r]) * yp[p] * yq[i] * yq[j] * ipow(yq[i] - yq[j], (unsigned)r);
+        }
+    }
     rk = m.ternary;
-    for (int i = 0; i < ncp; i++)
-        for (int j = i + 1; j < ncp; j++)
-            for (int k = j + 1; k < ncp; k++)
+    for (int i = 0; i < ncp; i++) {
+        for (int j = i + 1; j < ncp; j++) {
+            for (int k = j + 1; k < ncp; k++) {
                 for (int q = 0; q < ncp; q++, rk++)
                     for (int r = 0; r < rk->n; r++) G += tseries(T, rk->h[r]) * yp[i] * yp[j] * yp[k] * yq[q];
+            }
+        }
+    }
     rk = m.ternaryq;
-    for (int p = 0; p < ncp; p++)
-        for (int i = 0; i < ncp; i++)
-            for (int j = i + 1; j < ncp; j++)
+    for (int p = 0; p < ncp; p++) {
+        for (int i = 0; i < ncp; i++) {
+            for (int j = i + 1; j < ncp; j++) {
                 for (int k = j + 1; k < ncp; k++, rk++)
                     for (int r = 0; r < rk->n; r++) G += tseries(T, rk->h[r]) * yq[i] * yq[j] * yq[k] * yp[p];
+            }
+        }
+    }
     return G;
 }
 
-static __device__ __noinline__ void explicit_raw(const cipher_material &m, const double *y, double T, int ncp, double *mu)
+static __device__ __noinline__ double energy_raw(const cipher_material &m, const double *y, double T, int ncp)
 {
-    if (m.model == CIPHER_CHEM_NONE || m.model == CIPHER_CHEM_QUADRATIC) {
+    return energy_body<0, -1>(m, y, T, ncp);
+}
+
+template <int NC, int MODEL, typename Mat>
+static __device__ __forceinline__ void explicit_body(const Mat &m, const double *y, double T, int ncp_rt, double *mu)
+{
+    const int ncp = NC > 0 ? NC : ncp_rt;
+    const int model = MODEL >= 0 ? MODEL : m.model;
+
+    if (model == CIPHER_CHEM_NONE || model == CIPHER_CHEM_QUADRATIC) {
         for (int c = 0; c < ncp; c++) mu[c] = 0.0;
         return;
     }
-    if (m.model == CIPHER_CHEM_CALPHADDIS) {
+    if (model == CIPHER_CHEM_CALPHADDIS) {
         for (int i = 0; i < ncp; i++) mu[i] = tseries(T, m.unary[i]);
-        const cipher_rk *bin = m.binary;
-        for (int i = 0; i < ncp; i++)
+        const auto *bin = m.binary;
+        for (int i = 0; i < ncp; i++) {
             for (int j = i + 1; j < ncp; j++, bin++)
                 for (int r = 0; r < bin->n; r++) {
                     double a = tseries(T, bin->h[r]);
@@ -167,32 +229,36 @@ static __device__ __noinline__ void explicit_raw(const cipher_material &m, const
                     mu[i] += a * y[j] * (b + c * y[i]);
                     mu[j] += a * y[i] * (b - c * y[j]);
                 }
-        const cipher_rk *ter = m.ternary;
-        for (int i = 0; i < ncp; i++)
-            for (int j = i + 1; j < ncp; j++)
+        }
+        const auto *ter = m.ternary;
+        for (int i = 0; i < ncp; i++) {
+            for (int j = i + 1; j < ncp; j++) {
                 for (int k = j + 1; k < ncp; k++, ter++)
                     for (int r = 0; r < ter->n; r++) {
                         double a = tseries(T, ter->h[r]);
-                        double b = y[ter->i[r]] + (1.0 - y[k] - y[j] - y[i]) / 3.0;
+                        double b = pick<NC>(y, ter->i[r]) + (1.0 - y[k] - y[j] - y[i]) / 3.0;
                         mu[i] += a * y[j] * y[k] * (b - y[i] / 3.0);
                         mu[j] += a * y[k] * y[i] * (b - y[j] / 3.0);
                         mu[k] += a * y[i] * y[j] * (b - y[k] / 3.0);
-                        mu[ter->i[r]] += a * y[i] * y[j] * y[k];
+                        add_at<NC>(mu, ter->i[r], a * y[i] * y[j] * y[k]);
                     }
+            }
+        }
         return;
     }
     const double *yp = y, *yq = y + ncp;
     double *mp = mu, *mq = mu + ncp;
     for (int c = 0; c < 2 * ncp; c++) mu[c] = 0.0;
-    for (int a = 0; a < ncp; a++)
+    for (int a = 0; a < ncp; a++) {
         for (int b = 0; b < ncp; b++) {
             double w = tseries(T, m.unary[a * ncp + b]);
             mp[a] += w * yq[b];
             mq[b] += w * yp[a];
         }
-    const cipher_rk *rk = m.binary;
-    for (int i = 0; i < ncp; i++)
-        for (int j = i + 1; j < ncp; j++)
+    }
+    const auto *rk = m.binary;
+    for (int i = 0; i < ncp; i++) {
+        for (int j = i + 1; j < ncp; j++) {
             for (int q = 0; q < ncp; q++, rk++)
                 for (int r = 0; r < rk->n; r++) {
                     double a = tseries(T, rk->h[r]);
@@ -202,9 +268,11 @@ static __device__ __noinline__ void explicit_raw(const cipher_material &m, const
                     mp[j] += a * yp[i] * yq[q] * (b - c * yp[j]);
                     mq[q] += a * yp[i] * b * yp[j];
                 }
+        }
+    }
     rk = m.binaryq;
-    for (int p = 0; p < ncp; p++)
-        for (int i = 0; i < ncp; i++)
+    for (int p = 0; p < ncp; p++) {
+        for (int i = 0; i < ncp; i++) {
             for (int j = i + 1; j < ncp; j++, rk++)
                 for (int r = 0; r < rk->n; r++) {
                     double a = tseries(T, rk->h[r]);
@@ -214,10 +282,12 @@ static __device__ __noinline__ void explicit_raw(const cipher_material &m, const
                     mq[j] += a * yq[i] * yp[p] * (b - c * yq[j]);
                     mp[p] += a * yq[i] * b * yq[j];
                 }
+        }
+    }
     rk = m.ternary;
-    for (int i = 0; i < ncp; i++)
-        for (int j = i + 1; j < ncp; j++)
-            for (int k = j + 1; k < ncp; k++)
+    for (int i = 0; i < ncp; i++) {
+        for (int j = i + 1; j < ncp; j++) {
+            for (int k = j + 1; k < ncp; k++) {
                 for (int q = 0; q < ncp; q++, rk++)
                     for (int r = 0; r < rk->n; r++) {
                         double a = tseries(T, rk->h[r]);
@@ -226,10 +296,13 @@ static __device__ __noinline__ void explicit_raw(const cipher_material &m, const
                         mp[k] += a * yp[i] * yp[j] * yq[q];
                         mq[q] += a * yp[i] * yp[j] * yp[k];
                     }
+            }
+        }
+    }
     rk = m.ternaryq;
-    for (int p = 0; p < ncp; p++)
-        for (int i = 0; i < ncp; i++)
-            for (int j = i + 1; j < ncp; j++)
+    for (int p = 0; p < ncp; p++) {
+        for (int i = 0; i < ncp; i++) {
+            for (int j = i + 1; j < ncp; j++) {
                 for (int k = j + 1; k < ncp; k++, rk++)
                     for (int r = 0; r < rk->n; r++) {
                         double a = tseries(T, rk->h[r]);
@@ -238,16 +311,28 @@ static __device__ __noinline__ void explicit_raw(const cipher_material &m, const
                         mq[k] += a * yq[i] * yq[j] * yp[p];
                         mp[p] += a * yq[i] * yq[j] * yq[k];
                     }
+            }
+        }
+    }
 }
 
-static __device__ __noinline__ void implicit_raw(const cipher_material &m, const double *y, double T, int ncp, double *mu)
+static __device__ __noinline__ void explicit_raw(const cipher_material &m, const double *y, double T, int ncp, double *mu)
 {
-    if (m.model == CIPHER_CHEM_NONE) {
+    explicit_body<0, -1>(m, y, T, ncp, mu);
+}
+
+template <int NC, int MODEL, typename Mat>
+static __device__ __forceinline__ void implicit_body(const Mat &m, const double *y, double T, int ncp_rt, double *mu)
+{
+    const int ncp = NC > 0 ? NC : ncp_rt;
+    const int model = MODEL >= 0 ? MODEL : m.model;
+
+    if (model == CIPHER_CHEM_NONE) {
         for (int c = 0; c < ncp; c++) mu[c] = 0.0;
-    } else if (m.model == CIPHER_CHEM_QUADRATIC) {
+    } else if (model == CIPHER_CHEM_QUADRATIC) {
         for (int c = 0; c < ncp; c++)
             mu[c] = tseries(T, m.unary[c]) + 2.0 * tseries(T, m.quad_binary[c]) * (y[c] - tseries(T, m.quad_ceq[c]));
-    } else if (m.model == CIPHER_CHEM_CALPHADDIS) {
+    } else if (model == CIPHER_CHEM_CALPHADDIS) {
         for (int c = 0; c < ncp; c++) mu[c] = CIPHER_R_GAS * T * log(y[c]);
     } else {
         for (int c = 0; c < ncp; c++) {
@@ -257,18 +342,27 @@ static __device__ __noinline__ void implicit_raw(const cipher_material &m, const
     }
 }
 
-static __device__ __noinline__ void sitefrac_raw(const cipher_material &m, const double *pot, double T, int ncp, double *y)
+static __device__ __noinline__ void implicit_raw(const cipher_material &m, const double *y, double T, int ncp, double *mu)
 {
+    implicit_body<0, -1>(m, y, T, ncp, mu);
+}
+
+template <int NC, int MODEL, typename Mat>
+static __device__ __forceinline__ void sitefrac_body(const Mat &m, const double *pot, double T, int ncp_rt, double *y)
+{
+    const int ncp = NC > 0 ? NC : ncp_rt;
+    const int model = MODEL >= 0 ? MODEL : m.model;
+
     const int nd = ncp - 1;
-    if (m.model == CIPHER_CHEM_NONE) {
+    if (model == CIPHER_CHEM_NONE) {
         for (int c = 0; c < ncp; c++) y[c] = 0.0;
         y[ncp - 1] = 1.0;
-    } else if (m.model == CIPHER_CHEM_CALPHADDIS) {
+    } else if (model == CIPHER_CHEM_CALPHADDIS) {
         double RT = CIPHER_R_GAS * T, sum = 1.0;
         for (int c = 0; c < nd; c++) { y[c] = exp(pot[c] / RT); sum += y[c]; }
         y[nd] = 1.0;
         for (int c = 0; c < nd; c++) { y[c] /= sum; y[nd] -= y[c]; }
-    } else if (m.model == CIPHER_CHEM_CALPHAD2SL) {
+    } else if (model == CIPHER_CHEM_CALPHAD2SL) {
         double RT = CIPHER_R_GAS * T, sp = 1.0, sq = 1.0;
         double *yp = y, *yq = y + ncp;
         const double *pp = pot, *pq = pot + nd;
@@ -302,14 +396,23 @@ static __device__ __noinline__ void sitefrac_raw(const cipher_material &m, const
     }
 }
 
-static __device__ __noinline__ void tangent_raw(const cipher_material &m, const double *y, const double *pot, double T, int ncp,
-                                   double *tpot, double *tex, double *tT)
+static __device__ __noinline__ void sitefrac_raw(const cipher_material &m, const double *pot, double T, int ncp, double *y)
 {
+    sitefrac_body<0, -1>(m, pot, T, ncp, y);
+}
+
+template <int NC, int MODEL, typename Mat>
+static __device__ __forceinline__ void tangent_body(const Mat &m, const double *y, const double *pot, double T, int ncp_rt,
+                                         double *tpot, double *tex, double *tT)
+{
+    const int ncp = NC > 0 ? NC : ncp_rt;
+    const int model = MODEL >= 0 ? MODEL : m.model;
+
     const int nd = ncp - 1, nd2 = nd * nd;
-    if (m.model == CIPHER_CHEM_NONE) {
+    if (model == CIPHER_CHEM_NONE) {
         for (int c = 0; c < nd2; c++) { tpot[c] = 0.0; tex[c] = 0.0; }
         for (int c = 0; c < nd; c++) tT[c] = 0.0;
-    } else if (m.model == CIPHER_CHEM_CALPHADDIS) {
+    } else if (model == CIPHER_CHEM_CALPHADDIS) {
         double RT = CIPHER_R_GAS * T, t[16];
         for (int k = 0; k < 16; k++) t[k] = 0.0;
         for (int j = 0; j < nd; j++) {
@@ -318,9 +421,10 @@ static __device__ __noinline__ void tangent_raw(const cipher_material &m, const 
         }
         for (int c = 0; c < nd2; c++) { tpot[c] = t[c]; tex[c] = -t[c]; }
         for (int j = 0; j < nd; j++) tT[j] = 0.0;
-        for (int j = 0; j < nd; j++)
+        for (int j = 0; j < nd; j++) {
             for (int i = 0; i < nd; i++) tT[j] -= t[j * nd + i] * pot[i] / T;
-    } else if (m.model == CIPHER_CHEM_CALPHAD2SL) {
+        }
+    } else if (model == CIPHER_CHEM_CALPHAD2SL) {
         double RT = CIPHER_R_GAS * T, tp[16], tq[16];
         const double *yp = y, *yq = y + ncp, *pp = pot, *pq = pot + nd;
         for (int k = 0; k < 16; k++) { tp[k] = 0.0; tq[k] = 0.0; }
@@ -337,11 +441,12 @@ static __device__ __noinline__ void tangent_raw(const cipher_material &m, const 
             tex[c] = -tp[c]; tex[nd2 + c] = -tq[c];
         }
         for (int j = 0; j < 2 * nd; j++) tT[j] = 0.0;
-        for (int j = 0; j < nd; j++)
+        for (int j = 0; j < nd; j++) {
             for (int i = 0; i < nd; i++) {
                 tT[j] -= tp[j * nd + i] * pp[i] / T;
                 tT[nd + j] -= tq[j * nd + i] * pq[i] / T;
             }
+        }
     } else {
         double delta[CIPHER_MAXCP], ceqT[CIPHER_MAXCP], unT[CIPHER_MAXCP], biT[CIPHER_MAXCP];
         double ceq[CIPHER_MAXCP], bi[CIPHER_MAXCP], mat[16], inv[16];
@@ -367,15 +472,24 @@ static __device__ __noinline__ void tangent_raw(const cipher_material &m, const 
     }
 }
 
-static __device__ __noinline__ void mobility_raw(const cipher_material &m, const double *y, double T, int ncp, double *M)
+static __device__ __noinline__ void tangent_raw(const cipher_material &m, const double *y, const double *pot, double T, int ncp,
+                                   double *tpot, double *tex, double *tT)
 {
-    if (m.model == CIPHER_CHEM_NONE) {
+    tangent_body<0, -1>(m, y, pot, T, ncp, tpot, tex, tT);
+}
+
+template <int NC, int MODEL, typename Mat>
+static __device__ __forceinline__ void mobility_body(const Mat &m, const double *y, double T, int ncp_rt, double *M)
+{
+    const int ncp = NC > 0 ? NC : ncp_rt;
+    const int model = MODEL >= 0 ? MODEL : m.model;
+
+    if (model == CIPHER_CHEM_NONE) {
         for (int c = 0; c < ncp; c++) M[c] = 0.0;
-        return;
-    }
+    } else {
     for (int k = 0; k < ncp; k++) {
-        const cipher_mobility &mob = m.mobilityc[k];
-        const cipher_rk *bin = mob.binary;
+        const auto &mob = m.mobilityc[k];
+        const auto *bin = mob.binary;
         double mig = 0.0;
         for (int j = 0; j < ncp; j++) {
             mig += y[j] * tseries(T, mob.unary[j]);
@@ -385,6 +499,36 @@ static __device__ __noinline__ void mobility_raw(const cipher_material &m, const
         }
         M[k] = y[k] * mob.m0 / CIPHER_R_GAS / T * exp(mig / CIPHER_R_GAS / T);
     }
+    }
+}
+
+static __device__ __noinline__ void mobility_raw(const cipher_material &m, const double *y, double T, int ncp, double *M)
+{
+    mobility_body<0, -1>(m, y, T, ncp, M);
+}
+
+/* the same over the evaluated tables (calphaddis, calphad2sl) */
+static __device__ __noinline__ double energy_raw_v(const MatV &m, const double *y, double T, int ncp)
+{
+    return energy_body<0, -1>(m, y, T, ncp);
+}
+
+static __device__ __noinline__ void explicit_raw_v(const MatV &m, const double *y, double T, int ncp, double *mu)
+{
+    explicit_body<0, -1>(m, y, T, ncp, mu);
+}
+
+static __device__ __noinline__ void mobility_raw_v(const MatV &m, const double *y, double T, int ncp, double *M)
+{
+    mobility_body<0, -1>(m, y, T, ncp, M);
+}
+
+/* the evaluated tables of the material of `phase`, or NULL where the
+ * phase's cell is at another temperature or its model is not CALPHAD */
+__device__ __forceinline__ const MatV *matv_of(const ChemTables &t, int phase, int model)
+{
+    return (t.matv && (model == CIPHER_CHEM_CALPHADDIS || model == CIPHER_CHEM_CALPHAD2SL)) ? &t.matv[t.pmm[phase]]
+                                                                                           : nullptr;
 }
 
 /* ---------------- per-phase wrappers with the molar-volume scaling ---------------- */
@@ -393,7 +537,8 @@ static __device__ __noinline__ void mobility_raw(const cipher_material &m, const
 __device__ inline double chemenergy(const ChemTables &t, int phase, const double *y, const double *mu, double T)
 {
     const cipher_material &m = material_of(t, phase);
-    double G = energy_raw(m, y, T, t.ncp) / m.molarvolume;
+    const MatV *mv = matv_of(t, phase, m.model);
+    double G = (mv ? energy_raw_v(*mv, y, T, t.ncp) : energy_raw(m, y, T, t.ncp)) / m.molarvolume;
     for (int s = 0; s < m.nsites; s++)
         for (int c = 0; c < t.ndp; c++) G -= mu[c] * m.stoichiometry[s] * y[s * t.ncp + c];
     return G;
@@ -403,7 +548,9 @@ __device__ inline void sitepot_explicit(const ChemTables &t, int phase, const do
 {
     const cipher_material &m = material_of(t, phase);
     double full[2 * CIPHER_MAXCP];
-    explicit_raw(m, y, T, t.ncp, full);
+    const MatV *mv = matv_of(t, phase, m.model);
+    if (mv) explicit_raw_v(*mv, y, T, t.ncp, full);
+    else explicit_raw(m, y, T, t.ncp, full);
     for (int s = 0; s < m.nsites; s++)
         for (int c = 0; c < t.ndp; c++)
             out[s * t.ndp + c] = (full[s * t.ncp + c] - full[s * t.ncp + t.ndp]) / m.molarvolume;
@@ -445,8 +592,127 @@ __device__ inline void sitefrac_tangent(const ChemTables &t, int phase, const do
 __device__ inline void mobility(const ChemTables &t, int phase, const double *y, double T, double *M)
 {
     const cipher_material &m = material_of(t, phase);
-    mobility_raw(m, y, T, t.ncp, M);
+    const MatV *mv = matv_of(t, phase, m.model);
+    if (mv) mobility_raw_v(*mv, y, T, t.ncp, M);
+    else mobility_raw(m, y, T, t.ncp, M);
     for (int c = 0; c < t.ncp; c++) M[c] *= m.molarvolume;
 }
+
+/* ---------------- the wrappers for one component count and model ---------------- */
+/* The same operations as the wrappers above, with NC components and the
+ * model's sublattice count model_nsites(MODEL) fixed at compile time and
+ * the model bodies inlined: the single-phase kernels keep every array in
+ * registers.  m is a material of that model. */
+
+template <int NC, int MODEL, typename Mat>
+__device__ __forceinline__ void sitefrac_m(const Mat &m, const double *pot, double T, double *y)
+{
+    constexpr int ND = NC - 1, NS = model_nsites(MODEL);
+    double scaled[2 * CIPHER_MAXCP];
+    for (int s = 0; s < NS; s++) {
+        for (int c = 0; c < ND; c++) scaled[s * ND + c] = m.molarvolume * pot[s * ND + c];
+    }
+    sitefrac_body<NC, MODEL>(m, scaled, T, NC, y);
+}
+
+template <int NC, int MODEL, typename Mat>
+__device__ __forceinline__ double chemenergy_m(const Mat &m, const double *y, const double *mu, double T)
+{
+    constexpr int ND = NC - 1, NS = model_nsites(MODEL);
+    double G = energy_body<NC, MODEL>(m, y, T, NC) / m.molarvolume;
+    for (int s = 0; s < NS; s++) {
+        for (int c = 0; c < ND; c++) G -= mu[c] * m.stoichiometry[s] * y[s * NC + c];
+    }
+    return G;
+}
+
+template <int NC, int MODEL, typename Mat>
+__device__ __forceinline__ void sitepot_explicit_m(const Mat &m, const double *y, double T, double *out)
+{
+    constexpr int ND = NC - 1, NS = model_nsites(MODEL);
+    double full[2 * CIPHER_MAXCP];
+    explicit_body<NC, MODEL>(m, y, T, NC, full);
+    for (int s = 0; s < NS; s++) {
+        for (int c = 0; c < ND; c++) out[s * ND + c] = (full[s * NC + c] - full[s * NC + ND]) / m.molarvolume;
+    }
+}
+
+template <int NC, int MODEL, typename Mat>
+__device__ __forceinline__ void sitefrac_tangent_m(const Mat &m, const double *y, const double *pot,
+                                                   double T, double *tpot, double *tex, double *tT)
+{
+    constexpr int ND = NC - 1, NS = model_nsites(MODEL);
+    tangent_body<NC, MODEL>(m, y, pot, T, NC, tpot, tex, tT);
+    for (int c = 0; c < NS * ND * ND; c++) tpot[c] *= m.molarvolume;
+    for (int c = 0; c < NS * ND * ND; c++) tex[c] *= m.molarvolume;
+    for (int c = 0; c < NS * ND; c++) tT[c] *= m.molarvolume;
+}
+
+template <int NC, int MODEL, typename Mat>
+__device__ __forceinline__ void mobility_m(const Mat &m, const double *y, double T, double *M)
+{
+    mobility_body<NC, MODEL>(m, y, T, NC, M);
+    for (int c = 0; c < NC; c++) M[c] *= m.molarvolume;
+}
+
+/* the model calls of one phase: with NC > 0 and MODEL >= 0 the wrappers
+ * above for that count and model (every material of the problem has the
+ * model), reading the evaluated tables where the cell's temperature has
+ * them (the CALPHAD energy, explicit potentials and mobility: the only
+ * bodies that read T-series); else the general wrappers */
+template <int NC, int MODEL>
+struct PhaseModel {
+    static constexpr bool kFixed = NC > 0 && MODEL >= 0;
+    static constexpr bool kCalphad = MODEL == CIPHER_CHEM_CALPHADDIS || MODEL == CIPHER_CHEM_CALPHAD2SL;
+    static __device__ __forceinline__ int nsites(const cipher_material &m)
+    {
+        if constexpr (kFixed) return model_nsites(MODEL);
+        else return m.nsites;
+    }
+    static __device__ __forceinline__ void sitefrac(const ChemTables &t, int phase, const double *pot, double T, double *y)
+    {
+        if constexpr (kFixed) sitefrac_m<NC, MODEL>(material_of(t, phase), pot, T, y);
+        else cipher::sitefrac(t, phase, pot, T, y);
+    }
+    static __device__ __forceinline__ double chemenergy(const ChemTables &t, int phase, const double *y, const double *mu,
+                                                        double T)
+    {
+        if constexpr (kFixed) {
+            if constexpr (kCalphad)
+                if (t.matv) return chemenergy_m<NC, MODEL>(t.matv[t.pmm[phase]], y, mu, T);
+            return chemenergy_m<NC, MODEL>(material_of(t, phase), y, mu, T);
+        } else {
+            return cipher::chemenergy(t, phase, y, mu, T);
+        }
+    }
+    static __device__ __forceinline__ void sitepot_explicit(const ChemTables &t, int phase, const double *y, double T,
+                                                            double *out)
+    {
+        if constexpr (kFixed) {
+            if constexpr (kCalphad)
+                if (t.matv) { sitepot_explicit_m<NC, MODEL>(t.matv[t.pmm[phase]], y, T, out); return; }
+            sitepot_explicit_m<NC, MODEL>(material_of(t, phase), y, T, out);
+        } else {
+            cipher::sitepot_explicit(t, phase, y, T, out);
+        }
+    }
+    static __device__ __forceinline__ void sitefrac_tangent(const ChemTables &t, int phase, const double *y,
+                                                            const double *pot, double T, double *tpot, double *tex,
+                                                            double *tT)
+    {
+        if constexpr (kFixed) sitefrac_tangent_m<NC, MODEL>(material_of(t, phase), y, pot, T, tpot, tex, tT);
+        else cipher::sitefrac_tangent(t, phase, y, pot, T, tpot, tex, tT);
+    }
+    static __device__ __forceinline__ void mobility(const ChemTables &t, int phase, const double *y, double T, double *M)
+    {
+        if constexpr (kFixed) {
+            if constexpr (kCalphad)
+                if (t.matv) { mobility_m<NC, MODEL>(t.matv[t.pmm[phase]], y, T, M); return; }
+            mobility_m<NC, MODEL>(material_of(t, phase), y, T, M);
+        } else {
+            cipher::mobility(t, phase, y, T, M);
+        }
+    }
+};
 
 }  // namespace cipher

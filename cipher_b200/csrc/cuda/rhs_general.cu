@@ -35,200 +35,16 @@
 #include "cipher_b200.h"
 #include "device_common.cuh"
 #include "kernels.h"
+#include "general_common.cuh"
+#include "general_kernels.cuh"
 #include "models.cuh"
 #include "order.cuh"
 
 namespace cipher {
 
-constexpr int kGenBlock = 128;
-
-/* phase interpolant h and its transposed derivative (src/utility.c:470-557) */
-__device__ inline void interpolant(int kind, const double *phi, int n, double *h)
-{
-    if (kind == CIPHER_INTERP_LINEAR) {
-        for (int g = 0; g < n; g++) h[g] = phi[g];
-        return;
-    }
-    if (n == 1) { h[0] = 1.0; return; }
-    double sum = 0.0;
-    for (int g = 0; g < n; g++) {
-        h[g] = kind == CIPHER_INTERP_QUADRATIC ? phi[g] * phi[g] : phi[g] * phi[g] * (3.0 - 2.0 * phi[g]);
-        sum += h[g];
-    }
-    for (int g = 0; g < n; g++) h[g] /= sum;
-}
-
-template <int PM>
-__device__ inline void interpolant_dT(int kind, double *v, const double *phi, int n)
-{
-    if (kind == CIPHER_INTERP_LINEAR) return;
-    if (n == 1) { v[0] = 0.0; return; }
-    double avg = 0.0, sum = 0.0;
-    for (int g = 0; g < n; g++) {
-        double w = kind == CIPHER_INTERP_QUADRATIC ? phi[g] * phi[g] : phi[g] * phi[g] * (3.0 - 2.0 * phi[g]);
-        sum += w;
-        avg += w * v[g];
-    }
-    for (int g = 0; g < n; g++) {
-        if (kind == CIPHER_INTERP_QUADRATIC) v[g] = 2.0 * phi[g] * (v[g] - avg / sum) / sum;
-        else v[g] = 6.0 * phi[g] * (1.0 - phi[g]) * (v[g] - avg / sum) / sum;
-    }
-}
-
-template <typename R>
-__device__ __forceinline__ const DevInterface &pair_itf(const GenArgs<R> &a, int ia, int ib)
-{
-    return a.itfs[a.itflist[ia * a.npf + ib]];
-}
-
-/* implicit site potentials of slot g: stoichiometry*(mu - ci) - EX */
-template <typename R>
-__device__ __forceinline__ void slot_potential(const GenArgs<R> &a, const cipher_material &mat, const double *mu,
-                                               const double *ci, int64_t c, int g, double *pot)
-{
-    const int64_t S = a.stride;
-    for (int s = 0; s < mat.nsites; s++)
-        for (int d = 0; d < a.ndp; d++)
-            pot[s * a.ndp + d] = mat.stoichiometry[s] * (mu[d] - ci[d]) -
-                                 a.ex[(int64_t)(g * a.SP + s * a.ndp + d) * S + c];
-}
-
-/* segregation potential of the cell, sum_{k<j} h_k h_j V_kj (src/cipher.c:160-172) */
-template <typename R>
-__device__ __forceinline__ void segregation(const GenArgs<R> &a, const uint16_t *ids, const double *h, int n,
-                                            double *ci)
-{
-    for (int d = 0; d < CIPHER_MAXCP; d++) ci[d] = 0.0;
-    for (int k = 0; k < n; k++)
-        for (int j = k + 1; j < n; j++) {
-            const DevInterface &itf = pair_itf(a, ids[k], ids[j]);
-            if (itf.has_potential)
-                for (int d = 0; d < a.ndp; d++) ci[d] += h[k] * h[j] * itf.potential[d];
-        }
-}
-
-/* read a cell's set; returns n, or 0 (and raises ERR_BADSET) if invalid */
-template <int PM, typename R>
-__device__ __forceinline__ int load_set(const GenArgs<R> &a, int64_t c, uint16_t *ids, double *phi)
-{
-    const int64_t S = a.stride;
-    int n = a.as[c];
-    if (n < 1 || n > a.P || n > PM) {
-        atomicOr(a.err, ERR_BADSET);
-        return 0;
-    }
-    for (int g = 0; g < n; g++) {
-        ids[g] = a.as[(int64_t)(1 + g) * S + c];
-        phi[g] = (double)a.phi[(int64_t)g * S + c];
-        if (ids[g] >= a.npf) {
-            atomicOr(a.err, ERR_BADSET);
-            return 0;
-        }
-    }
-    return n;
-}
-
 /* ------------------------------------------------------------------ */
-/* per-cell composition, mobility and conductivity                      */
+/* phase-field gradients (anisotropy)                                   */
 /* ------------------------------------------------------------------ */
-
-template <int PM, typename R>
-__global__ void __launch_bounds__(kGenBlock) k_chem_cell(const GenArgs<R> a)
-{
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.ncells) return;
-    const int64_t c = a.order ? (int64_t)a.order[t] : t;
-    const int64_t S = a.stride;
-    const int ncp = a.ncp, ndp = a.ndp;
-    uint16_t ids[PM];
-    double phi[PM], h[PM];
-    const int n = load_set<PM>(a, c, ids, phi);
-    double mu[CIPHER_MAXCP], ci[CIPHER_MAXCP], mm[CIPHER_MAXCP], cc[CIPHER_MAXCP];
-    for (int d = 0; d < CIPHER_MAXCP; d++) { mm[d] = 0.0; cc[d] = 0.0; }
-    double tc = 0.0;
-    if (n > 0) {
-        const double T = (double)a.tm[c];
-        const ChemTables ch = chem_at(a.chem, T);
-        for (int d = 0; d < ndp; d++) mu[d] = a.dp[(int64_t)d * S + c];
-        interpolant(a.interp, phi, n, h);
-        segregation(a, ids, h, n, ci);
-        for (int g = 0; g < n; g++) {
-            const cipher_material &mat = material_of(ch, ids[g]);
-            double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP], me[CIPHER_MAXCP];
-            slot_potential(a, mat, mu, ci, c, g, pot);
-            sitefrac(ch, ids[g], pot, T, y);
-            mobility(ch, ids[g], y, T, me);
-            for (int d = 0; d < ncp; d++) mm[d] += h[g] * me[d];
-            for (int s = 0; s < mat.nsites; s++)
-                for (int d = 0; d < ncp; d++) cc[d] += h[g] * mat.stoichiometry[s] * y[s * ncp + d];
-            if (mat.tconductivity.n) tc += h[g] * tseries(T, mat.tconductivity);
-        }
-        for (int k = 0; k < n; k++)
-            for (int j = k + 1; j < n; j++) {
-                const DevInterface &itf = pair_itf(a, ids[k], ids[j]);
-                if (itf.has_mobilityc)
-                    for (int d = 0; d < ncp; d++) mm[d] *= exp(itf.mobilityc[d] / CIPHER_R_GAS / T);
-            }
-    }
-    for (int d = 0; d < ncp; d++) {
-        a.comp[(int64_t)d * S + c] = cc[d];
-        a.mob[(int64_t)d * S + c] = mm[d];
-    }
-    a.tcond[c] = tc;
-}
-
-/* ------------------------------------------------------------------ */
-/* cell grouping: the general kernels process cells grouped by class    */
-/* ------------------------------------------------------------------ */
-
-/* A warp of the general kernels runs one model per lane: cells whose single
- * phase belongs to different materials, and cells with several phases,
- * diverge.  The kernels therefore walk the cells grouped by class (the
- * material of a single-phase cell; sets of 2, 3, more phases; order.cuh).
- * Every cell's arithmetic is unchanged: the results do not depend on the
- * order. */
-struct GeneralClassKey {
-    const uint16_t *as;
-    int64_t stride;
-    const int32_t *pmm;
-    int npf, nmat;
-    __device__ __forceinline__ int operator()(int64_t c) const
-    {
-        const int n = as[c];
-        if (n == 1) {
-            const int id = as[stride + c];
-            if (id >= 0 && id < npf) {
-                const int m = pmm[id];
-                if (m >= 0 && m < nmat) return m;
-            }
-        }
-        return nmat + (n <= 2 ? 0 : n == 3 ? 1 : 2);
-    }
-};
-
-/* ------------------------------------------------------------------ */
-/* the RHS                                                              */
-/* ------------------------------------------------------------------ */
-
-/* neighbour at face position f in the reference's face order: [0,DIM)
- * below without wrap (descending d), [DIM,2DIM) own faces (ascending d),
- * [2DIM,3DIM) wrapped around from above (ascending d); -1 if absent */
-__device__ __forceinline__ int64_t gen_face_nb(const int *res, const int *per, int64_t c, const int *co, int f,
-                                               const int DIM)
-{
-    const int64_t st[3] = {1, (int64_t)res[0], (int64_t)res[0] * res[1]};
-    if (f < DIM) {
-        const int e = DIM - 1 - f;
-        return co[e] > 0 ? c - st[e] : -1;
-    }
-    if (f < 2 * DIM) {
-        const int d = f - DIM;
-        if (co[d] < res[d] - 1) return c + st[d];
-        return (per[d] && res[d] > 1) ? c - (int64_t)(res[d] - 1) * st[d] : -1;
-    }
-    const int d = f - 2 * DIM;
-    return (co[d] == 0 && per[d] && res[d] > 1) ? c + (int64_t)(res[d] - 1) * st[d] : -1;
-}
 
 /* phase-field gradients of a cell's slots by least squares over its face
  * neighbours (src/cipher.c:82-146), with the weights the reference builds
@@ -310,416 +126,6 @@ __global__ void __launch_bounds__(kGenBlock) k_gradients(const GenArgs<R> a, con
     }
     for (int d = 0; d < DIM; d++)
         for (int g = 0; g < n; g++) a.grad[((int64_t)d * a.P + g) * S + c] = gr[d][g];
-}
-
-/* ff*x/vol as the reference forms it (src/cipher.c:281-282) */
-template <typename R>
-__device__ __forceinline__ double face_div(const GenArgs<R> &a, double x)
-{
-    if (a.geom_mode == 2) return x;
-    if (a.geom_mode == 1) return (a.ffactor * x) * a.inv_vol;
-    return (a.ffactor * x) / a.vol;
-}
-
-template <int PM, typename R>
-__global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> a, const int DIM)
-{
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.ncells) return;
-    const int64_t c = a.order ? (int64_t)a.order[t] : t;
-    const int64_t S = a.stride;
-    const int ncp = a.ncp, ndp = a.ndp, SP = a.SP;
-    const double PI = CIPHER_PI_D;
-    const bool listed = a.fl.start != nullptr;   /* an adapted mesh: faces from the lists */
-    int co[3] = {0, 0, 0};
-    if (!listed) {
-        co[0] = (int)(c % a.res[0]);
-        co[1] = DIM > 1 ? (int)((c / a.res[0]) % a.res[1]) : 0;
-        co[2] = DIM > 2 ? (int)(c / ((int64_t)a.res[0] * a.res[1])) : 0;
-    }
-
-    uint16_t ids[PM];
-    double phi[PM], h[PM], lap[PM], pf[PM];
-    const int n = load_set<PM>(a, c, ids, phi);
-    if (n == 0) return;
-    const double T = (double)a.tm[c];
-    const ChemTables ch = chem_at(a.chem, T);
-    double mu[CIPHER_MAXCP], ldp[CIPHER_MAXCP];
-    for (int d = 0; d < ndp; d++) { mu[d] = a.dp[(int64_t)d * S + c]; ldp[d] = 0.0; }
-    double ltm = 0.0;
-    for (int g = 0; g < n; g++) lap[g] = 0.0;
-
-    /* ---- faces in the reference's face order (src/cipher.c:235-317) ---- */
-    const int f0 = listed ? a.fl.start[c] : 0, f1 = listed ? a.fl.start[c + 1] : 3 * DIM;
-    const double vol_c = listed ? a.fl.vol[c] : 0.0;
-#pragma unroll 1
-    for (int f = f0; f < f1; f++) {
-        int64_t nb;
-        bool self_L;
-        double ffv = 0.0;
-        if (listed) {
-            const int32_t v = a.fl.nbr[f];
-            nb = v & 0x7fffffff;
-            self_L = (v & FACE_SELF_L) != 0;
-            ffv = a.fl.ff[a.fl.face[f]];
-        } else {
-            nb = gen_face_nb(a.res, a.per, c, co, f, DIM);
-            if (nb < 0) continue;
-            self_L = f >= DIM && f < 2 * DIM;
-        }
-        /* ff*x/vol of this cell, as the reference forms it (src/cipher.c:281-282) */
-        auto fdiv = [&](double x) { return listed ? (ffv * x) / vol_c : face_div(a, x); };
-        const int64_t cl = self_L ? c : nb, cr = self_L ? nb : c;
-        const int nn = a.as[nb];
-        if (nn < 1 || nn > a.P) continue;          /* that cell's own thread raises the flag */
-        /* phase flux, gated on the L cell only (src/cipher.c:277) */
-        const bool gate = self_L ? (n > 1 || ids[0] > 1) : (nn > 1 || a.as[S + nb] > 1);
-        if (gate) {
-            int i = 0, j = 0;
-            while (i < n && j < nn) {
-                const uint16_t b = a.as[(int64_t)(1 + j) * S + nb];
-                if (ids[i] == b) {
-                    const double pn = (double)a.phi[(int64_t)j * S + nb];
-                    if (self_L) lap[i] += fdiv(pn - phi[i]);
-                    else lap[i] -= fdiv(phi[i] - pn);
-                    i++;
-                    j++;
-                } else if (ids[i] < b) {
-                    i++;
-                } else {
-                    j++;
-                }
-            }
-        }
-        /* chemical-potential flux with the Andersson-Agren frame (material.c:1125-1137) */
-        if (ndp) {
-            double me[CIPHER_MAXCP], ca[CIPHER_MAXCP];
-            for (int d = 0; d < ncp; d++) {
-                const double ml = a.mob[(int64_t)d * S + cl], mr = a.mob[(int64_t)d * S + cr];
-                const double cL = a.comp[(int64_t)d * S + cl], cR = a.comp[(int64_t)d * S + cr];
-                if (fabs(ml) > 1e-32 && fabs(mr) > 1e-32) me[d] = 2.0 * ml * mr / (ml + mr);
-                else me[d] = 0.0;
-                ca[d] = 2.0 * cL * cR / (cL + cR);
-            }
-            if constexpr (sizeof(R) == 4) {
-                /* mixed: the flux stencil in FP32 - the Andersson-Agren matrix
-                 * and its product with the potential difference (formed in
-                 * FP64, then rounded) - accumulated into the FP64 divergence */
-                float MB[(CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1)], dmu[CIPHER_MAXCP];
-                for (int i = 0; i < ndp; i++)
-                    for (int j = 0; j < ndp; j++) {
-                        float acc = 0.0f;
-                        for (int k = 0; k < ncp; k++)
-                            acc += ((j == k ? 1.0f : 0.0f) - (float)ca[j]) * ((k == i ? 1.0f : 0.0f) - (float)ca[i]) *
-                                   (float)me[k];
-                        MB[i * ndp + j] = acc;
-                    }
-                for (int d = 0; d < ndp; d++) dmu[d] = (float)(a.dp[(int64_t)d * S + cr] - a.dp[(int64_t)d * S + cl]);
-                for (int d = 0; d < ndp; d++) {
-                    float f = 0.0f;
-                    for (int j = 0; j < ndp; j++) f += MB[d * ndp + j] * dmu[j];
-                    if (self_L) ldp[d] += fdiv((double)f);
-                    else ldp[d] -= fdiv((double)f);
-                }
-            } else {
-                double MB[(CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1)], dmu[CIPHER_MAXCP], fl[CIPHER_MAXCP];
-                for (int i = 0; i < ndp; i++)
-                    for (int j = 0; j < ndp; j++) {
-                        double acc = 0.0;
-                        for (int k = 0; k < ncp; k++)
-                            acc += ((j == k ? 1.0 : 0.0) - ca[j]) * ((k == i ? 1.0 : 0.0) - ca[i]) * me[k];
-                        MB[i * ndp + j] = acc;
-                    }
-                for (int d = 0; d < ndp; d++) dmu[d] = a.dp[(int64_t)d * S + cr] - a.dp[(int64_t)d * S + cl];
-                matvec(fl, MB, dmu, ndp);
-                for (int d = 0; d < ndp; d++) {
-                    if (self_L) ldp[d] += fdiv(fl[d]);
-                    else ldp[d] -= fdiv(fl[d]);
-                }
-            }
-        }
-        /* heat flux (mixed: the face product in FP32) */
-        if (a.tcond) {
-            const double tl = a.tcond[cl], tr = a.tcond[cr];
-            if (fabs(tl) > 1e-32 && fabs(tr) > 1e-32) {
-                double ft;
-                if constexpr (sizeof(R) == 4)
-                    ft = (double)((float)(2.0 * tl * tr / (tl + tr)) * ((float)a.tm[cr] - (float)a.tm[cl]));
-                else
-                    ft = 2.0 * tl * tr / (tl + tr) * ((double)a.tm[cr] - (double)a.tm[cl]);
-                if (self_L) ltm += fdiv(ft);
-                else ltm -= fdiv(ft);
-            }
-        }
-    }
-
-    /* ---- boundary faces (src/cipher.c:319-389) ---- */
-    if (a.nbcs) {
-        const double dc = listed ? a.fl.delta[c] : a.delta;
-        const double cf = 1.0 / ipow(dc, 2);
-        const double tcc = a.tcond ? a.tcond[c] : 0.0;
-        const int q0 = listed ? a.fl.bstart[c] : 0, q1 = listed ? a.fl.bstart[c + 1] : 2 * DIM;
-        for (int b = 0; b < a.nbcs; b++) {
-            const DevBC &bc = a.bcs[b];
-#pragma unroll 1
-            for (int q = q0; q < q1; q++) {
-                if (listed) {
-                    if (bc.label != a.fl.blabel[q]) continue;
-                } else {
-                    const int d = q >> 1;
-                    if (a.per[d]) continue;
-                    const bool on = (q & 1) ? co[d] == a.res[d] - 1 : co[d] == 0;
-                    if (!on || bc.label != 2 * d + 1 + (q & 1)) continue;
-                }
-                double fd[CIPHER_MAXCP];
-                for (int k = 0; k < CIPHER_MAXCP; k++) fd[k] = 0.0;
-                if (bc.chem_type != CIPHER_BC_NONE) {
-                    if (bc.chem_type == CIPHER_BC_NEUMANN) {
-                        for (int k = 0; k < ndp; k++) if (bc.chem_on[k]) fd[k] = bc.chem_val[k] * dc;
-                    } else {
-                        for (int k = 0; k < ndp; k++)
-                            if (bc.chem_on[k]) fd[k] = a.mob[(int64_t)k * S + c] * (bc.chem_val[k] - mu[k]);
-                    }
-                }
-                double fluxt = 0.0;
-                if (bc.thermal_type == CIPHER_BC_NEUMANN) fluxt = tcc * bc.thermal_val * dc;
-                else if (bc.thermal_type == CIPHER_BC_DIRICHLET) fluxt = tcc * (bc.thermal_val - T);
-                if (bc.chem_type != CIPHER_BC_NONE)
-                    for (int k = 0; k < ndp; k++) ldp[k] += cf * fd[k];
-                if (bc.thermal_type != CIPHER_BC_NONE) ltm += cf * fluxt;
-            }
-        }
-    }
-
-    /* ---- cell terms (src/cipher.c:391-664) ---- */
-    interpolant(a.interp, phi, n, h);
-    double ci[CIPHER_MAXCP];
-    if (ndp) segregation(a, ids, h, n, ci);
-
-    /* pass over the phases: driving force, dEX/dt and the tangent sum */
-    double chem[PM], yw[PM * (CIPHER_MAXCP - 1)];
-    double cbar[CIPHER_MAXCP], dcdm[(CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1)];
-    for (int d = 0; d < CIPHER_MAXCP; d++) cbar[d] = 0.0;
-    for (int q = 0; q < (CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1); q++) dcdm[q] = 0.0;
-    /* tangent of the last phase evaluated: reused by the composition rate
-     * below when the cell has a single phase (same arguments, same bits) */
-    double tpot[2 * 16], tex[2 * 16], tT[2 * CIPHER_MAXCP];
-    for (int g = 0; g < n; g++) {
-        const cipher_material &mat = material_of(ch, ids[g]);
-        double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP];
-        if (ndp) {
-            slot_potential(a, mat, mu, ci, c, g, pot);
-            sitefrac(ch, ids[g], pot, T, y);
-        }
-        if (n > 1) {
-            chem[g] = chemenergy(ch, ids[g], y, mu, T);
-            for (int s = 0; s < mat.nsites; s++)
-                for (int d = 0; d < ndp; d++) cbar[d] += h[g] * mat.stoichiometry[s] * y[s * ncp + d];
-        }
-        if (ndp) {
-            for (int d = 0; d < ndp; d++) {
-                double w = 0.0;
-                for (int s = 0; s < mat.nsites; s++) w += mat.stoichiometry[s] * y[s * ncp + d];
-                yw[g * (CIPHER_MAXCP - 1) + d] = w;
-            }
-            /* explicit potential relaxation (src/cipher.c:570-581) */
-            double spx[2 * CIPHER_MAXCP];
-            sitepot_explicit(ch, ids[g], y, T, spx);
-            for (int s = 0; s < mat.nsites; s++)
-                for (int d = 0; d < ndp; d++) {
-                    const int64_t pl = (int64_t)(g * SP + s * ndp + d) * S + c;
-                    a.fex[pl] = mat.chempot_ex_kineticcoeff * (spx[s * ndp + d] - a.ex[pl]);
-                }
-            for (int q = mat.nsites * ndp; q < SP; q++) a.fex[(int64_t)(g * SP + q) * S + c] = 0.0;
-            sitefrac_tangent(ch, ids[g], y, pot, T, tpot, tex, tT);
-            for (int s = 0; s < mat.nsites; s++)
-                for (int q = 0; q < ndp * ndp; q++)
-                    dcdm[q] += h[g] * mat.stoichiometry[s] * mat.stoichiometry[s] * tpot[s * ndp * ndp + q];
-        }
-    }
-    for (int q = n * SP; q < a.P * SP; q++) a.fex[(int64_t)q * S + c] = 0.0;
-
-    /* pair properties; with anisotropy they depend on the pair's normal,
-     * the normalised difference of the two slots' gradients (src/cipher.c:
-     * 427-460) */
-    auto props = [&](int k, int j, double &s_, double &m_, double &w_) {
-        const DevInterface &itf = pair_itf(a, ids[k], ids[j]);
-        if (a.grad && (itf.energy_n || itf.mobility_n)) {
-            double u[3], nrm = 0.0;
-            for (int d = 0; d < DIM; d++) {
-                u[d] = a.grad[((int64_t)d * a.P + k) * S + c] - a.grad[((int64_t)d * a.P + j) * S + c];
-                nrm += u[d] * u[d];
-            }
-            nrm = sqrt(nrm);
-            if (nrm > 1e-16)
-                for (int d = 0; d < DIM; d++) u[d] /= nrm;
-            interface_props_aniso(itf, T, u, DIM, s_, m_, w_);
-        } else {
-            interface_props(itf, T, s_, m_, w_);
-        }
-    };
-    for (int g = 0; g < PM; g++) pf[g] = 0.0;
-    /* the interface terms (capillary force, active set, constrained rates)
-     * in the compute type RC: FP64 on the FP64 path (the reference's
-     * operations), FP32 on the mixed path; the chemical driving force comes
-     * from the FP64 model evaluation above */
-    auto interface_rates = [&](auto zero) {
-        using RC = decltype(zero);
-        const RC PIc = (RC)PI;
-        RC cap[PM], unc[PM], rate[PM];
-        for (int g = 0; g < n; g++) { cap[g] = (RC)0; rate[g] = (RC)0; }
-        for (int k = 0; k < n; k++) {
-            for (int j = k + 1; j < n; j++) {
-                double skd, mkd, wkd;
-                props(k, j, skd, mkd, wkd);
-                const RC skj = (RC)skd, wkj = (RC)wkd;
-                cap[k] -= skj * ((RC)phi[j] / wkj + (RC)lap[j] * wkj / PIc / PIc);
-                cap[j] -= skj * ((RC)phi[k] / wkj + (RC)lap[k] * wkj / PIc / PIc);
-                for (int i = j + 1; i < n; i++) {
-                    double s_, m_, w_;
-                    RC tj = (RC)0, v;
-                    v = skj / wkj; tj = tj > v ? tj : v;
-                    props(k, i, s_, m_, w_);
-                    v = (RC)s_ / (RC)w_; tj = tj > v ? tj : v;
-                    props(j, i, s_, m_, w_);
-                    v = (RC)s_ / (RC)w_; tj = tj > v ? tj : v;
-                    tj *= (RC)a.junctionpenalty;
-                    cap[k] -= tj * (RC)phi[j] * (RC)phi[i];
-                    cap[j] -= tj * (RC)phi[k] * (RC)phi[i];
-                    cap[i] -= tj * (RC)phi[k] * (RC)phi[j];
-                }
-            }
-            cap[k] *= (RC)8;
-            cap[k] += (RC)lap[k];
-        }
-        /* chemical driving force (src/cipher.c:499-522) */
-        for (int k = 0; k < n; k++)
-            for (int j = k + 1; j < n; j++) {
-                const DevInterface &itf = pair_itf(a, ids[k], ids[j]);
-                if (itf.has_potential) {
-                    double v = 0.0;
-                    for (int d = 0; d < ndp; d++) v += itf.potential[d] * cbar[d];
-                    chem[k] += v * h[j];
-                    chem[j] += v * h[k];
-                }
-            }
-        interpolant_dT<PM>(a.interp, chem, phi, n);
-        /* active set and constrained rate (src/cipher.c:524-555) */
-        RC nact = (RC)0;
-        uint32_t act = 0;
-        for (int g = 0; g < n; g++) unc[g] = (RC)0;
-        for (int k = 0; k < n; k++) {
-            for (int j = k + 1; j < n; j++) {
-                double s_, m_, w_;
-                props(k, j, s_, m_, w_);
-                const RC r = (RC)m_ * ((cap[k] - cap[j]) - (RC)(chem[k] - chem[j]) * (RC)8 * (RC)sqrt(h[k] * h[j]) / PIc);
-                unc[k] += r;
-                unc[j] -= r;
-            }
-            const bool on = (phi[k] > CIPHER_TOL && phi[k] < 1.0 - CIPHER_TOL) || (phi[k] < CIPHER_TOL && unc[k] > (RC)0) ||
-                            (phi[k] > 1.0 - CIPHER_TOL && unc[k] < (RC)0);
-            if (on) { act |= 1u << k; nact += (RC)1; }
-        }
-        for (int k = 0; k < n; k++) {
-            if (!(act >> k & 1u)) continue;
-            for (int j = k + 1; j < n; j++) {
-                if (!(act >> j & 1u)) continue;
-                double s_, m_, w_;
-                props(k, j, s_, m_, w_);
-                const RC r = (RC)m_ * ((cap[k] - cap[j]) - (RC)(chem[k] - chem[j]) * (RC)8 * (RC)sqrt(h[k] * h[j]) / PIc);
-                rate[k] += r;
-                rate[j] -= r;
-            }
-            rate[k] /= nact;
-        }
-        for (int g = 0; g < n; g++) pf[g] = (double)rate[g];
-    };
-    if (n > 1) {
-        if constexpr (sizeof(R) == 4) interface_rates(0.0f);
-        else interface_rates(0.0);
-    }
-    for (int g = 0; g < a.P; g++) a.fphi[(int64_t)g * S + c] = (R)(g < PM ? pf[g] : 0.0);
-
-    /* temperature rate (src/cipher.c:558-568) */
-    double cp = 0.0, tr = ltm;
-    for (int g = 0; g < n; g++) {
-        const cipher_material &mat = material_of(ch, ids[g]);
-        if (mat.specific_heat.n) cp += h[g] * tseries(T, mat.specific_heat);
-        if (mat.latent_heat.n) tr += pf[g] * tseries(T, mat.latent_heat);
-    }
-    if (cp != 0.0) tr /= cp;
-    if (a.has_temp_rate) tr += a.temp_rate;
-    a.ftm[c] = (R)tr;
-
-    if (!ndp) return;
-    /* composition rate and dmu/dt (src/cipher.c:583-662) */
-    const int DN = CIPHER_MAXCP - 1;
-    double cpv[PM * (CIPHER_MAXCP - 1)];
-    for (int q = 0; q < n * DN; q++) cpv[q] = 0.0;
-    for (int k = 0; k < n; k++)
-        for (int j = k + 1; j < n; j++) {
-            const DevInterface &itf = pair_itf(a, ids[k], ids[j]);
-            if (itf.has_potential)
-                for (int d = 0; d < ndp; d++) {
-                    cpv[k * DN + d] += itf.potential[d] * h[j];
-                    cpv[j * DN + d] += itf.potential[d] * h[k];
-                }
-        }
-    for (int g = 0; g < n; g++) {
-        double tmp[CIPHER_MAXCP];
-        for (int d = 0; d < ndp; d++) tmp[d] = cpv[g * DN + d];
-        matvec(&cpv[g * DN], dcdm, tmp, ndp);
-    }
-    double wdp[CIPHER_MAXCP];
-    for (int d = 0; d < CIPHER_MAXCP; d++) wdp[d] = 0.0;
-    if (n > 1) {
-        for (int d = 0; d < ndp; d++) {
-            double wpf[PM];
-            for (int g = 0; g < n; g++) wpf[g] = yw[g * DN + d] - cpv[g * DN + d];
-            interpolant_dT<PM>(a.interp, wpf, phi, n);
-            for (int g = 0; g < n; g++) wdp[d] -= pf[g] * wpf[g];
-        }
-    }
-    /* solute sources (material.c:295-351; sink model) */
-    double src[CIPHER_MAXCP], comp[CIPHER_MAXCP];
-    for (int d = 0; d < ncp; d++) { src[d] = 0.0; comp[d] = a.comp[(int64_t)d * S + c]; }
-    for (int k = 0; k < n; k++) {
-        const cipher_material &mat = material_of(ch, ids[k]);
-        for (int s = 0; s < mat.nsources; s++) {
-            double tmp[CIPHER_MAXCP];
-            for (int d = 0; d < ncp; d++) tmp[d] = mat.sources[s].rate[d] * (mat.sources[s].ceq[d] - comp[d]);
-            for (int d = 0; d < ncp; d++) src[d] += h[k] * h[k] * tmp[d];
-        }
-        for (int j = k + 1; j < n; j++) {
-            const DevInterface &itf = pair_itf(a, ids[k], ids[j]);
-            for (int s = 0; s < itf.nsources; s++) {
-                double tmp[CIPHER_MAXCP];
-                for (int d = 0; d < ncp; d++) tmp[d] = itf.sources[s].rate[d] * (itf.sources[s].ceq[d] - comp[d]);
-                for (int d = 0; d < ncp; d++) src[d] += 2.0 * h[k] * h[j] * tmp[d];
-            }
-        }
-    }
-    for (int d = 0; d < ndp; d++) wdp[d] += (ldp[d] + src[d]);
-    for (int g = 0; g < n; g++) {
-        const cipher_material &mat = material_of(ch, ids[g]);
-        if (n > 1) {
-            double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP];
-            slot_potential(a, mat, mu, ci, c, g, pot);
-            sitefrac(ch, ids[g], pot, T, y);
-            sitefrac_tangent(ch, ids[g], y, pot, T, tpot, tex, tT);
-        }
-        for (int s = 0; s < mat.nsites; s++) {
-            double dex[CIPHER_MAXCP];
-            for (int d = 0; d < ndp; d++) dex[d] = a.fex[(int64_t)(g * SP + s * ndp + d) * S + c];
-            matvec(&cpv[g * DN], &tex[s * ndp * ndp], dex, ndp);
-            for (int d = 0; d < ndp; d++)
-                wdp[d] -= h[g] * mat.stoichiometry[s] * (cpv[g * DN + d] + tT[s * ndp + d] * tr);
-        }
-    }
-    double dmdc[(CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1)], out[CIPHER_MAXCP];
-    invert_small(dmdc, dcdm, ndp);
-    matvec(out, dmdc, wdp, ndp);
-    for (int d = 0; d < ndp; d++) a.fdp[(int64_t)d * S + c] = out[d];
 }
 
 /* ------------------------------------------------------------------ */
@@ -1058,12 +464,16 @@ __device__ inline cipher_tseries *spec_slot(cipher_material &m, int k)
  * constant series {n = 1, T^0: tseries(T, s)} at T = the first cell's
  * temperature.  A constant series evaluates to 0.0 + v = v, so every model
  * function returns the same bits from either copy; cells at another
- * temperature keep reading the original. */
+ * temperature keep reading the original.  tspec[0]: the temperature of the
+ * copies; tspec[1 + m]: of material m's copy, which is kept when T has not
+ * changed (the materials are fixed for the context's life). */
 template <typename R>
 __global__ void __launch_bounds__(256) k_specialise(const cipher_material *mat, cipher_material *spec, const R *tm,
                                                     double *tspec)
 {
     const double T = (double)tm[0];
+    if (blockIdx.x == 0 && threadIdx.x == 0) tspec[0] = T;
+    if (tspec[1 + blockIdx.x] == T) return;
     const double *src = (const double *)&mat[blockIdx.x];
     double *dst = (double *)&spec[blockIdx.x];
     for (size_t i = threadIdx.x; i < sizeof(cipher_material) / sizeof(double); i += blockDim.x) dst[i] = src[i];
@@ -1082,7 +492,64 @@ __global__ void __launch_bounds__(256) k_specialise(const cipher_material *mat, 
         ts->coeff[0] = v;
         ts->logcoeff = 0.0;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) *tspec = T;
+    __syncthreads();
+    if (threadIdx.x == 0) tspec[1 + blockIdx.x] = T;
+}
+
+/* one block per material: the evaluated tables (MatV) of the specialised
+ * copy, each value tseries(T, s) of the specialised series s at the
+ * specialisation temperature - the value the model bodies compute from
+ * that series, bit for bit.  tspec[1 + nmat + m]: the temperature of
+ * material m's tables, kept while it has not changed. */
+__global__ void __launch_bounds__(256) k_evaluate(const cipher_material *spec, MatV *mv, double *tspec)
+{
+    const double T = tspec[0];
+    double *done = &tspec[1 + gridDim.x + blockIdx.x];
+    if (*done == T) return;
+    const cipher_material &m = spec[blockIdx.x];
+    MatV &v = mv[blockIdx.x];
+    const int t = threadIdx.x, nt = blockDim.x;
+    if (t == 0) {
+        v.model = m.model;
+        v.p = m.p;
+        v.q = m.q;
+        v.molarvolume = m.molarvolume;
+        v.stoichiometry[0] = m.stoichiometry[0];
+        v.stoichiometry[1] = m.stoichiometry[1];
+        v.ref.v = tseries(T, m.ref);
+    }
+    for (int k = t; k < CIPHER_MAXCP * CIPHER_MAXCP; k += nt) v.unary[k].v = tseries(T, m.unary[k]);
+    for (int k = t; k < CIPHER_MAXCP; k += nt) {
+        v.quad_ceq[k].v = 0.0;
+        v.quad_binary[k].v = 0.0;
+    }
+    auto rk = [&](RkV &o, const cipher_rk &r) {
+        o.n = r.n;
+        for (int j = 0; j < CIPHER_MAXRK; j++) {
+            o.i[j] = r.i[j];
+            o.h[j].v = tseries(T, r.h[j]);
+        }
+    };
+    for (int k = t; k < 4 * CIPHER_MAXRKTAB; k += nt) {
+        const int tab = k / CIPHER_MAXRKTAB, e = k % CIPHER_MAXRKTAB;
+        if (tab == 0) rk(v.binary[e], m.binary[e]);
+        else if (tab == 1) rk(v.ternary[e], m.ternary[e]);
+        else if (tab == 2) rk(v.binaryq[e], m.binaryq[e]);
+        else rk(v.ternaryq[e], m.ternaryq[e]);
+    }
+    for (int k = t; k < CIPHER_MAXCP * (1 + CIPHER_MAXBIN); k += nt) {
+        const int c = k / (1 + CIPHER_MAXBIN), e = k % (1 + CIPHER_MAXBIN);
+        const cipher_mobility &mo = m.mobilityc[c];
+        MobV &vo = v.mobilityc[c];
+        if (e == 0) {
+            vo.m0 = mo.m0;
+            for (int j = 0; j < CIPHER_MAXCP; j++) vo.unary[j].v = tseries(T, mo.unary[j]);
+        } else {
+            rk(vo.binary[e - 1], mo.binary[e - 1]);
+        }
+    }
+    __syncthreads();
+    if (t == 0) *done = T;
 }
 
 /* ------------------------------------------------------------------ */
@@ -1093,15 +560,27 @@ template <typename R>
 static cudaError_t launch_gen(const GenArgs<R> &a, int dim, cudaStream_t s)
 {
     const unsigned blocks = (unsigned)((a.ncells + kGenBlock - 1) / kGenBlock);
-    if (a.chem.spec)
+    if (a.chem.spec) {
         k_specialise<R><<<a.chem.nmat, 256, 0, s>>>(a.chem.mat, (cipher_material *)a.chem.spec, a.tm,
                                                      (double *)a.chem.tspec);
+        if (a.chem.matv_tab)
+            k_evaluate<<<a.chem.nmat, 256, 0, s>>>(a.chem.spec, (MatV *)a.chem.matv_tab, (double *)a.chem.tspec);
+    }
     if (a.order) {
         const OrderBuf o = {a.order, a.order_counts, a.order_cursor, a.nclass, a.ncells};
         launch_order(o, GeneralClassKey{a.as, a.stride, a.chem.pmm, a.npf, a.chem.nmat}, s);
     }
-    if (a.ndp) k_chem_cell<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a);
+    /* composition, mobility and conductivity of every cell before any face
+     * flux reads them; the phase items of the cells of several phases; then
+     * the RHS of the single-phase cells and of the rest */
+    cudaError_t e;
+    if (a.ndp) {
+        if (a.single_models && (e = launch_chem_single(a, s)) != cudaSuccess) return e;
+        k_chem_cell<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a);
+    }
     if (a.grad) k_gradients<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a, dim);
+    if (a.icap && (e = launch_items(a, s)) != cudaSuccess) return e;
+    if (a.single_models && (e = launch_rhs_single(a, dim, s)) != cudaSuccess) return e;
     k_rhs_general<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a, dim);
     return cudaGetLastError();
 }

@@ -195,6 +195,39 @@ def test_rhs_live_vs_port(case):
     assert max(errm.values()) <= TOLMIX, errm
 
 
+SPECIALISED_CASES = LIVE + [("3d_2sl_ncp5", 3, [16, 14, 12], "calphad2sl", 5, 8, 8, 45, 0x7F),
+                            ("2d_quad_ncp2", 2, [36, 30], "quadratic", 2, 8, 8, 46, 0x7F),
+                            ("2d_2sl_ncp3_mixedmodels", 2, [40, 36], "calphad2sl", 3, 10, 8, 47, 0xFF)]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", SPECIALISED_CASES, ids=[c[0] for c in SPECIALISED_CASES])
+def test_specialised_kernels_same_bits(case, prec, monkeypatch):
+    """cells evaluated by the kernels compiled for one component count and
+    model (single-phase cells; cells of 2 and 3 phases when every material
+    shares the model) give the same bits as the general kernels"""
+    _, dim, res, model, ncp, npr, cap, seed, feats = case
+    P = cb.Problem.alloy(dim, res, model, ncp, npr, cap, seed, feats)
+    M = cb.Mesh(P)
+    X = _evolve_port(P, M, oracle.port_initial_state(P, M), 2)
+    if prec == "mixed":
+        X = _round32(P, X)
+    assert (X[:, 0] == 1).mean() > 0.3
+    F_single = _device_rhs(cb.Context(P, M, prec), X)
+    monkeypatch.setenv("CIPHER_B200_SPECIALISED_KERNELS", "0")
+    F_general = _device_rhs(cb.Context(P, M, prec), X)
+    assert np.array_equal(F_single, F_general)
+
+
+@pytest.mark.parametrize("path", ALLOY_GOLDEN, ids=[os.path.basename(p) for p in ALLOY_GOLDEN])
+def test_specialised_kernels_same_bits_fixtures(path, monkeypatch):
+    P, M, g = _fixture(path)
+    F_single = _device_rhs(cb.Context(P, M, "fp64"), g["X"])
+    monkeypatch.setenv("CIPHER_B200_SPECIALISED_KERNELS", "0")
+    F_general = _device_rhs(cb.Context(P, M, "fp64"), g["X"])
+    assert np.array_equal(F_single, F_general)
+
+
 def test_trajectory_fp64_vs_port():
     """explicit steps on the device (waxpy + PostStep) against the oracle:
     identical sets at every step, fields within the accumulated tolerance"""
