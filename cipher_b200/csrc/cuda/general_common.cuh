@@ -22,6 +22,10 @@
 namespace cipher {
 
 constexpr int kGenBlock = 128;
+/* one warp per block for the kernels whose work sits in few cells (the
+ * cells of several phases, clustered where the grouping puts them): the
+ * block scheduler then spreads those warps over all SMs */
+constexpr int kWarpBlock = 32;
 
 /* phase interpolant h and its transposed derivative (src/utility.c:470-557) */
 __device__ __forceinline__ void interpolant(int kind, const double *phi, int n, double *h)

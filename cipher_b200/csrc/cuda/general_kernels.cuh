@@ -27,7 +27,7 @@ namespace cipher {
 /* ------------------------------------------------------------------ */
 
 template <int PM, typename R>
-__global__ void __launch_bounds__(kGenBlock) k_chem_cell(const GenArgs<R> a)
+__global__ void __launch_bounds__(kWarpBlock) k_chem_cell(const GenArgs<R> a)
 {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= a.ncells) return;
@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(kGenBlock) k_chem_cell(const GenArgs<R> a)
 /* ------------------------------------------------------------------ */
 
 template <int PM, typename R>
-__global__ void __launch_bounds__(kGenBlock, 12) k_rhs_general(const GenArgs<R> a, const int DIM)
+__global__ void __launch_bounds__(kWarpBlock, 32) k_rhs_general(const GenArgs<R> a, const int DIM)
 {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= a.ncells) return;

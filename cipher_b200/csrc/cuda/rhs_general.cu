@@ -560,6 +560,7 @@ template <typename R>
 static cudaError_t launch_gen(const GenArgs<R> &a, int dim, cudaStream_t s)
 {
     const unsigned blocks = (unsigned)((a.ncells + kGenBlock - 1) / kGenBlock);
+    const unsigned wblocks = (unsigned)((a.ncells + kWarpBlock - 1) / kWarpBlock);
     if (a.chem.spec) {
         k_specialise<R><<<a.chem.nmat, 256, 0, s>>>(a.chem.mat, (cipher_material *)a.chem.spec, a.tm,
                                                      (double *)a.chem.tspec);
@@ -576,12 +577,12 @@ static cudaError_t launch_gen(const GenArgs<R> &a, int dim, cudaStream_t s)
     cudaError_t e;
     if (a.ndp) {
         if (a.single_models && (e = launch_chem_single(a, s)) != cudaSuccess) return e;
-        k_chem_cell<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a);
+        k_chem_cell<CIPHER_PMAX, R><<<wblocks, kWarpBlock, 0, s>>>(a);
     }
     if (a.grad) k_gradients<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a, dim);
-    if (a.icap && (e = launch_items(a, s)) != cudaSuccess) return e;
     if (a.single_models && (e = launch_rhs_single(a, dim, s)) != cudaSuccess) return e;
-    k_rhs_general<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a, dim);
+    if (a.icap && (e = launch_items(a, s)) != cudaSuccess) return e;
+    k_rhs_general<CIPHER_PMAX, R><<<wblocks, kWarpBlock, 0, s>>>(a, dim);
     return cudaGetLastError();
 }
 

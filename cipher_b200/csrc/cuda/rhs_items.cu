@@ -34,7 +34,7 @@
 
 namespace cipher {
 
-constexpr int kItemBlock = 128;
+constexpr int kItemBlock = 64;
 
 template <typename R>
 __global__ void __launch_bounds__(kGenBlock) k_item_list(const GenArgs<R> a)
@@ -151,7 +151,7 @@ static cudaError_t launch_items_t(const GenArgs<R> &a, cudaStream_t s)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int64_t need = (a.icap + kItemBlock - 1) / kItemBlock;
-    const unsigned grid = (unsigned)(need < (int64_t)sms * 8 ? need : (int64_t)sms * 8);
+    const unsigned grid = (unsigned)(need < (int64_t)sms * 16 ? need : (int64_t)sms * 16);
     switch (a.item_model >= 0 ? a.ncp : 0) {
     case 2: launch_items_nc<2>(a, grid, s); break;
     case 3: launch_items_nc<3>(a, grid, s); break;
