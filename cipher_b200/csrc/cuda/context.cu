@@ -543,7 +543,11 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
         free_ctx(c);
         return cuda_fail(e, "cudaMalloc gradients");
     }
-    const bool order_pf = !c->general && c->precision == CIPHER_PREC_FP64 && c->P < kOrderClasses;
+    /* the FP64 reference-order kernel groups cells by set size above a
+     * 128^2 grid (on smaller domains the grouping's launches cost more than
+     * the lane activity gains) */
+    const bool order_pf = !c->general && c->precision == CIPHER_PREC_FP64 && c->P < kOrderClasses &&
+                          c->ncells > kSpecialisedMinCells;
     if ((c->general && c->nmat + 3 <= kOrderClasses) || order_pf) {
         c->nclass = c->general ? c->nmat + 3 : c->P + 1;
         const size_t nblk = (size_t)(c->ncells + 255) / 256;
@@ -556,15 +560,20 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
     }
     /* Specialised chemistry kernels, each giving the same bits as the
      * general kernels (CIPHER_B200_SPECIALISED_KERNELS=0 keeps every cell in
-     * the general kernels, to compare the two):
+     * the general kernels, =1 uses the specialised ones at any size, to
+     * compare the two):
      *  - single-phase cells, per model whose materials all have the model's
      *    sublattice count, compiled for 2..5 components (rhs_single.cu);
      *  - the phases of cells of several phases as (cell, phase) items, one
      *    thread each (rhs_items.cu), compiled for the component count and
      *    model when every material has the same model (not "none"). */
     c->item_model = -1;
+    /* by default only above a 128^2 grid: on smaller domains the extra
+     * launches cost more than the specialised kernels save */
     const char *spec_env = getenv("CIPHER_B200_SPECIALISED_KERNELS");
-    const bool spec_on = !spec_env || strcmp(spec_env, "0") != 0;
+    const bool spec_on = spec_env && strcmp(spec_env, "1") == 0 ? true
+                         : spec_env && strcmp(spec_env, "0") == 0 ? false
+                                                                   : c->ncells > kSpecialisedMinCells;
     if (spec_on && c->general && c->d_order && c->ncp >= 2 && c->ncp <= 5) {
         uint32_t present = 0, bad = 0;
         for (int m = 0; m < p->nmat; m++) {

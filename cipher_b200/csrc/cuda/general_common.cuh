@@ -26,6 +26,8 @@ constexpr int kGenBlock = 128;
  * cells of several phases, clustered where the grouping puts them): the
  * block scheduler then spreads those warps over all SMs */
 constexpr int kWarpBlock = 32;
+/* the single-phase and item kernels serve contexts of more cells than this */
+constexpr int64_t kSpecialisedMinCells = 16384;
 
 /* phase interpolant h and its transposed derivative (src/utility.c:470-557) */
 __device__ __forceinline__ void interpolant(int kind, const double *phi, int n, double *h)

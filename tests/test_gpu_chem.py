@@ -213,6 +213,7 @@ def test_specialised_kernels_same_bits(case, prec, monkeypatch):
     if prec == "mixed":
         X = _round32(P, X)
     assert (X[:, 0] == 1).mean() > 0.3
+    monkeypatch.setenv("CIPHER_B200_SPECIALISED_KERNELS", "1")     # at any domain size
     F_single = _device_rhs(cb.Context(P, M, prec), X)
     monkeypatch.setenv("CIPHER_B200_SPECIALISED_KERNELS", "0")
     F_general = _device_rhs(cb.Context(P, M, prec), X)
@@ -222,6 +223,7 @@ def test_specialised_kernels_same_bits(case, prec, monkeypatch):
 @pytest.mark.parametrize("path", ALLOY_GOLDEN, ids=[os.path.basename(p) for p in ALLOY_GOLDEN])
 def test_specialised_kernels_same_bits_fixtures(path, monkeypatch):
     P, M, g = _fixture(path)
+    monkeypatch.setenv("CIPHER_B200_SPECIALISED_KERNELS", "1")
     F_single = _device_rhs(cb.Context(P, M, "fp64"), g["X"])
     monkeypatch.setenv("CIPHER_B200_SPECIALISED_KERNELS", "0")
     F_general = _device_rhs(cb.Context(P, M, "fp64"), g["X"])
