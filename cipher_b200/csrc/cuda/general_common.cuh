@@ -168,18 +168,23 @@ struct GeneralClassKey {
 __device__ __forceinline__ int64_t gen_face_nb(const int *res, const int *per, int64_t c, const int *co, int f,
                                                const int DIM)
 {
-    const int64_t st[3] = {1, (int64_t)res[0], (int64_t)res[0] * res[1]};
+    /* the axis-indexed values as selects rather than indexed arrays, so that
+     * they stay in registers (a runtime index would place them in local
+     * memory) */
+    auto sel3 = [](const int *v, int d) { return d == 0 ? v[0] : d == 1 ? v[1] : v[2]; };
+    const int64_t r0 = res[0], r01 = (int64_t)res[0] * res[1];
+    auto st = [&](int d) -> int64_t { return d == 0 ? 1 : d == 1 ? r0 : r01; };
     if (f < DIM) {
         const int e = DIM - 1 - f;
-        return co[e] > 0 ? c - st[e] : -1;
+        return sel3(co, e) > 0 ? c - st(e) : -1;
     }
     if (f < 2 * DIM) {
-        const int d = f - DIM;
-        if (co[d] < res[d] - 1) return c + st[d];
-        return (per[d] && res[d] > 1) ? c - (int64_t)(res[d] - 1) * st[d] : -1;
+        const int d = f - DIM, rd = sel3(res, d);
+        if (sel3(co, d) < rd - 1) return c + st(d);
+        return (sel3(per, d) && rd > 1) ? c - (int64_t)(rd - 1) * st(d) : -1;
     }
-    const int d = f - 2 * DIM;
-    return (co[d] == 0 && per[d] && res[d] > 1) ? c + (int64_t)(res[d] - 1) * st[d] : -1;
+    const int d = f - 2 * DIM, rd = sel3(res, d);
+    return (sel3(co, d) == 0 && sel3(per, d) && rd > 1) ? c + (int64_t)(rd - 1) * st(d) : -1;
 }
 
 /* ff*x/vol as the reference forms it (src/cipher.c:281-282) */
@@ -337,8 +342,11 @@ __device__ __forceinline__ void boundary_faces(const GenArgs<R> &a, int64_t c, c
                 if (bc.label != a.fl.blabel[q]) continue;
             } else {
                 const int d = q >> 1;
-                if (a.per[d]) continue;
-                const bool on = (q & 1) ? co[d] == a.res[d] - 1 : co[d] == 0;
+                const int per_d = d == 0 ? a.per[0] : d == 1 ? a.per[1] : a.per[2];
+                const int res_d = d == 0 ? a.res[0] : d == 1 ? a.res[1] : a.res[2];
+                const int co_d = d == 0 ? co[0] : d == 1 ? co[1] : co[2];
+                if (per_d) continue;
+                const bool on = (q & 1) ? co_d == res_d - 1 : co_d == 0;
                 if (!on || bc.label != 2 * d + 1 + (q & 1)) continue;
             }
             double fd[CIPHER_MAXCP];
