@@ -591,6 +591,10 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
          * evaluated whole by the general kernel */
         int64_t cap = c->ncells / 2 > 65536 ? c->ncells / 2 : 65536;
         if (cap > c->ncells * c->P) cap = c->ncells * c->P;
+        /* CIPHER_B200_ITEM_CAPACITY=N caps the items (less device memory;
+         * the cells that do not fit are evaluated whole) */
+        const char *cap_env = getenv("CIPHER_B200_ITEM_CAPACITY");
+        if (cap_env && atoll(cap_env) > 0 && atoll(cap_env) < cap) cap = atoll(cap_env);
         const int nq = item_q(c->ndp, c->S).nq;
         if ((e = dev_alloc(&c->d_ibase, (size_t)c->stride * sizeof(int32_t))) != cudaSuccess ||
             (e = dev_alloc(&c->d_icell, (size_t)cap * sizeof(int32_t))) != cudaSuccess ||

@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(kGenBlock, 3) k_chem_single(const GenArgs<R> a
 }
 
 template <int NC, int MODEL, typename R>
-__global__ void __launch_bounds__(kGenBlock, 3) k_rhs_single(const GenArgs<R> a, const int DIM)
+__global__ void __launch_bounds__(kGenBlock, 5) k_rhs_single(const GenArgs<R> a, const int DIM)
 {
     constexpr int ND = NC - 1, NS = model_nsites(MODEL);
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;

@@ -230,6 +230,32 @@ def test_specialised_kernels_same_bits_fixtures(path, monkeypatch):
     assert np.array_equal(F_single, F_general)
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_item_capacity_overflow_same_bits(prec, monkeypatch):
+    """with room for only some items (the rest of the cells of several phases
+    evaluated whole, a cell's items straddling the capacity included) and a
+    second listing over a different state in the same context (entries of
+    the first listing left in the item table), the RHS keeps the general
+    kernels' bits"""
+    P = cb.Problem.alloy(2, [48, 40], "calphad2sl", 4, 12, 8, 52, 0)
+    M = cb.Mesh(P)
+    X1 = _evolve_port(P, M, oracle.port_initial_state(P, M), 2)
+    X2 = _evolve_port(P, M, X1, 2)
+    if prec == "mixed":
+        X1, X2 = _round32(P, X1), _round32(P, X2)
+    n1 = X1[:, 0].astype(int)
+    assert ((n1 >= 2) * n1).sum() > 101
+    monkeypatch.setenv("CIPHER_B200_SPECIALISED_KERNELS", "1")
+    monkeypatch.setenv("CIPHER_B200_ITEM_CAPACITY", "101")
+    ctx = cb.Context(P, M, prec)
+    Fs = [_device_rhs(ctx, X) for X in (X2, X1)]
+    monkeypatch.setenv("CIPHER_B200_SPECIALISED_KERNELS", "0")
+    monkeypatch.delenv("CIPHER_B200_ITEM_CAPACITY")
+    ctxg = cb.Context(P, M, prec)
+    for X, F in zip((X2, X1), Fs):
+        assert np.array_equal(F, _device_rhs(ctxg, X))
+
+
 def test_trajectory_fp64_vs_port():
     """explicit steps on the device (waxpy + PostStep) against the oracle:
     identical sets at every step, fields within the accumulated tolerance"""
