@@ -603,6 +603,12 @@ extern "C" int cipher_ctx_create(const cipher_problem *p, const cipher_mesh *m, 
             free_ctx(c);
             return cuda_fail(e, "cudaMalloc phase items");
         }
+        /* every entry names no item until a listing writes it */
+        if ((e = cudaMemset(c->d_icell, 0xff, (size_t)cap * sizeof(int32_t))) != cudaSuccess ||
+            (e = cudaStreamSynchronize(0)) != cudaSuccess) {
+            free_ctx(c);
+            return cuda_fail(e, "cudaMemset phase items");
+        }
         c->icap = cap;
     }
     if ((e = dev_alloc(&c->d_err, sizeof(int))) != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaMalloc err"); }

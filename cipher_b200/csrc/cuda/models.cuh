@@ -677,9 +677,12 @@ struct PhaseModel {
     static __device__ __forceinline__ double chemenergy(const ChemTables &t, int phase, const double *y, const double *mu,
                                                         double T)
     {
-        if constexpr (kFixed) {
-            if constexpr (kCalphad)
-                if (t.matv) return chemenergy_m<NC, MODEL>(t.matv[t.pmm[phase]], y, mu, T);
+        if constexpr (kFixed && kCalphad) {
+            /* the evaluated tables inline; a cell at another temperature
+             * calls the general wrapper (the same operations) */
+            if (t.matv) return chemenergy_m<NC, MODEL>(t.matv[t.pmm[phase]], y, mu, T);
+            return cipher::chemenergy(t, phase, y, mu, T);
+        } else if constexpr (kFixed) {
             return chemenergy_m<NC, MODEL>(material_of(t, phase), y, mu, T);
         } else {
             return cipher::chemenergy(t, phase, y, mu, T);
@@ -688,9 +691,10 @@ struct PhaseModel {
     static __device__ __forceinline__ void sitepot_explicit(const ChemTables &t, int phase, const double *y, double T,
                                                             double *out)
     {
-        if constexpr (kFixed) {
-            if constexpr (kCalphad)
-                if (t.matv) { sitepot_explicit_m<NC, MODEL>(t.matv[t.pmm[phase]], y, T, out); return; }
+        if constexpr (kFixed && kCalphad) {
+            if (t.matv) sitepot_explicit_m<NC, MODEL>(t.matv[t.pmm[phase]], y, T, out);
+            else cipher::sitepot_explicit(t, phase, y, T, out);
+        } else if constexpr (kFixed) {
             sitepot_explicit_m<NC, MODEL>(material_of(t, phase), y, T, out);
         } else {
             cipher::sitepot_explicit(t, phase, y, T, out);
@@ -705,9 +709,10 @@ struct PhaseModel {
     }
     static __device__ __forceinline__ void mobility(const ChemTables &t, int phase, const double *y, double T, double *M)
     {
-        if constexpr (kFixed) {
-            if constexpr (kCalphad)
-                if (t.matv) { mobility_m<NC, MODEL>(t.matv[t.pmm[phase]], y, T, M); return; }
+        if constexpr (kFixed && kCalphad) {
+            if (t.matv) mobility_m<NC, MODEL>(t.matv[t.pmm[phase]], y, T, M);
+            else cipher::mobility(t, phase, y, T, M);
+        } else if constexpr (kFixed) {
             mobility_m<NC, MODEL>(material_of(t, phase), y, T, M);
         } else {
             cipher::mobility(t, phase, y, T, M);

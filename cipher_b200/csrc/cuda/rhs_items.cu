@@ -63,6 +63,9 @@ __global__ void __launch_bounds__(kGenBlock) k_item_list(const GenArgs<R> a)
         for (int g = 0; g < n; g++) a.icell[first + g] = (int32_t)(c * 16 + g);
     } else {
         a.ibase[c] = -1;
+        /* a cell whose items straddle the capacity: its entries below it
+         * name no item */
+        for (int64_t q = first; n && q < first + n && q < a.icap; q++) a.icell[q] = -1;
     }
 }
 
@@ -77,6 +80,7 @@ __global__ void __launch_bounds__(kItemBlock) k_items(const GenArgs<R> a)
     for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < nitems;
          it += (int64_t)gridDim.x * blockDim.x) {
         const int32_t code = a.icell[it];
+        if (code < 0 || (int64_t)(code >> 4) >= a.ncells) continue;
         const int64_t c = code >> 4;
         const int g = code & 15;
         if (a.ibase[c] != it - g) continue;       /* an entry of an earlier listing */
