@@ -88,6 +88,19 @@ def test_rhs_mixed_on_adapted_mesh(path):
     assert err["pf"] <= TOLMIX, err
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("path", AMR_GOLDEN, ids=[os.path.basename(p) for p in AMR_GOLDEN])
+def test_specialised_kernels_same_bits_on_adapted_mesh(path, prec, monkeypatch):
+    """on face lists (hanging faces included) the single-phase and item
+    kernels give the general kernels' bits"""
+    P, F, M, g, kind = _fixture(path)
+    X = g["X"] if prec == "fp64" else _round32(P, g["X"])
+    monkeypatch.setenv("CIPHER_B200_SPECIALISED_KERNELS", "1")
+    Fs = _device_rhs(cb.Context(P, M, prec), X)
+    monkeypatch.setenv("CIPHER_B200_SPECIALISED_KERNELS", "0")
+    assert np.array_equal(Fs, _device_rhs(cb.Context(P, M, prec), X))
+
+
 @pytest.mark.parametrize("path", AMR_GOLDEN, ids=[os.path.basename(p) for p in AMR_GOLDEN])
 def test_poststep_on_adapted_mesh(path):
     P, F, M, g, kind = _fixture(path)
