@@ -5,20 +5,26 @@
  * potentials, interface mobility factors, solute sources, heat conduction,
  * latent and specific heat, boundary faces, several interfaces).
  *
- * Replaces RHSFunction (src/cipher.c:27-681) in two launches:
- *   k_chem_cell : per cell (src/cipher.c:148-233): site fractions of every
- *                 active phase at the cell's potentials, the interpolated
+ * Replaces RHSFunction (src/cipher.c:27-681) with, in launch order
+ * (launch_gen below):
+ *   k_specialise, k_evaluate : the materials' T-series at the cells'
+ *                 temperature (kept while it does not change);
+ *   k_order_*   : the cells grouped by class (order.cuh);
+ *   k_chem_single / k_chem_cell (general_kernels.cuh): per cell
+ *                 (src/cipher.c:148-233): site fractions of every active
+ *                 phase at the cell's potentials, the interpolated
  *                 composition, lattice mobility (with the interface factors)
  *                 and conductivity, stored in scratch planes that the face
  *                 terms of both neighbours read;
- *   k_rhs_general: per cell: the cell's faces gathered in the reference's
- *                 face order (phase, mu and heat fluxes, 235-317), its
- *                 boundary faces (319-389), then the cell terms (391-664):
- *                 capillary and chemical driving forces, active set and
- *                 constrained rate, dT/dt, dEX/dt and dmu/dt.
- * Site fractions of the cell's own phases are recomputed in the second
- * kernel instead of stored: the same arithmetic gives the same bits, and a
- * few exponentials per phase cost less than 8*P*S bytes written and read.
+ *   k_rhs_single (rhs_single.cu): the single-phase cells;
+ *   k_item_list, k_items (rhs_items.cu): the model evaluations of each
+ *                 phase of the cells of several phases, one thread each;
+ *   k_rhs_general (general_kernels.cuh): the other cells: faces in the
+ *                 reference's face order (phase, mu and heat fluxes,
+ *                 235-317), boundary faces (319-389), then the cell terms
+ *                 (391-664): capillary and chemical driving forces, active
+ *                 set and constrained rate, dT/dt, dEX/dt and dmu/dt.
+ * Every cell gives the same bits whichever kernel takes it.
  *
  * With an FP64 state (R = double) all arithmetic is FP64 in the reference's
  * operation order (this unit is compiled with --fmad=false).  With the mixed
@@ -27,8 +33,8 @@
  * product) and the interface terms (capillary force, active set, pair rates)
  * run in FP32, each face flux summed into an FP64 divergence, while the
  * model evaluations and the mu update stay FP64.  Gradient-based
- * anisotropy adds k_gradients before the RHS; both kernels walk the cells
- * grouped by class (k_order_*).
+ * anisotropy adds k_gradients before the RHS.  This unit also holds the
+ * initial chemistry, nucleation and output-field kernels.
  */
 #include <cstdint>
 #include <cuda_runtime.h>
