@@ -330,7 +330,8 @@ def run_chemistry(dev: int, steps: int, peak: float):
         ms = tot / steps
         out[name] = {"value": M.ncells / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
                      "bytes_per_cell_update": B, "roofline_frac": B * M.ncells / (ms / 1e3) / 1e9 / peak,
-                     "kernels": ["k_chem_cell", "k_rhs_general"]}
+                     "kernels": ["k_chem_single", "k_chem_cell", "k_rhs_single", "k_item_list", "k_items",
+                                 "k_rhs_general"]}
     errs = {}
     for nm, off, size in (("pf", A.pf_offset, A.pf_size), ("dp", A.dp_offset, A.dp_size),
                           ("ex", A.ex_offset, A.ex_size), ("tm", A.tm_offset, 1)):
