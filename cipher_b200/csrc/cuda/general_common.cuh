@@ -397,13 +397,16 @@ __device__ __forceinline__ int single_model(const GenArgs<R> &a, int64_t c)
 /* (cell, phase) items of the cells of several phases                   */
 /* ------------------------------------------------------------------ */
 
-/* per item, the model results the general kernel combines (rhs_items.cu
+/* per item, the model results the general kernels combine (rhs_items.cu
  * writes them): the phase's chemical energy, its weighted site fractions
  * yw[d] = sum_s stoichiometry_s y_s,d, its site fractions y[s][d] (d < ndp),
- * and the tangent blocks tpot[s], tex[s] (ndp x ndp) and tT[s] (ndp), for
- * s below the largest sublattice count; stored as planes q of icap items */
+ * the tangent blocks tpot[s], tex[s] (ndp x ndp) and tT[s] (ndp), for s
+ * below the largest sublattice count, and for the cell's composition and
+ * mobility (k_chem_cell) its site fractions of every component yc[s][d]
+ * (d < ncp = ndp + 1) and its component mobilities me[d]; stored as planes
+ * q of icap items */
 struct ItemQ {
-    int yw, y, tpot, tex, tt, nq;
+    int yw, y, tpot, tex, tt, yc, me, nq;
 };
 
 __host__ __device__ inline ItemQ item_q(int ndp, int SP)
@@ -415,7 +418,9 @@ __host__ __device__ inline ItemQ item_q(int ndp, int SP)
     q.tpot = q.y + ns * ndp;
     q.tex = q.tpot + ns * ndp * ndp;
     q.tt = q.tex + ns * ndp * ndp;
-    q.nq = q.tt + ns * ndp;
+    q.yc = q.tt + ns * ndp;
+    q.me = q.yc + ns * (ndp + 1);
+    q.nq = q.me + (ndp + 1);
     return q;
 }
 

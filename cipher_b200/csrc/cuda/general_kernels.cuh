@@ -38,6 +38,9 @@ __global__ void __launch_bounds__(kWarpBlock) k_chem_cell(const GenArgs<R> a)
     uint16_t ids[PM];
     double phi[PM], h[PM];
     const int n = load_set<PM>(a, c, ids, phi);
+    /* >= 0: the phases' site fractions and mobilities are items ib .. ib+n-1 */
+    const int32_t ib = a.ibase ? a.ibase[c] : -1;
+    const ItemQ iq = item_q(ndp, a.SP);
     double mu[CIPHER_MAXCP], ci[CIPHER_MAXCP], mm[CIPHER_MAXCP], cc[CIPHER_MAXCP];
     for (int d = 0; d < CIPHER_MAXCP; d++) { mm[d] = 0.0; cc[d] = 0.0; }
     double tc = 0.0;
@@ -50,9 +53,17 @@ __global__ void __launch_bounds__(kWarpBlock) k_chem_cell(const GenArgs<R> a)
         for (int g = 0; g < n; g++) {
             const cipher_material &mat = material_of(ch, ids[g]);
             double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP], me[CIPHER_MAXCP];
-            slot_potential(a, mat, mu, ci, c, g, pot);
-            sitefrac(ch, ids[g], pot, T, y);
-            mobility(ch, ids[g], y, T, me);
+            if (ib >= 0) {
+                const int64_t it = (int64_t)ib + g;
+                for (int d = 0; d < ncp; d++) me[d] = a.iscr[(int64_t)(iq.me + d) * a.icap + it];
+                for (int s = 0; s < mat.nsites; s++)
+                    for (int d = 0; d < ncp; d++)
+                        y[s * ncp + d] = a.iscr[(int64_t)(iq.yc + s * ncp + d) * a.icap + it];
+            } else {
+                slot_potential(a, mat, mu, ci, c, g, pot);
+                sitefrac(ch, ids[g], pot, T, y);
+                mobility(ch, ids[g], y, T, me);
+            }
             for (int d = 0; d < ncp; d++) mm[d] += h[g] * me[d];
             for (int s = 0; s < mat.nsites; s++) {
                 for (int d = 0; d < ncp; d++) cc[d] += h[g] * mat.stoichiometry[s] * y[s * ncp + d];

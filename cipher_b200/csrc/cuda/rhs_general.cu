@@ -10,6 +10,10 @@
  *   k_specialise, k_evaluate : the materials' T-series at the cells'
  *                 temperature (kept while it does not change);
  *   k_order_*   : the cells grouped by class (order.cuh);
+ *   k_item_list, k_items (rhs_items.cu): the model evaluations of each
+ *                 phase of the cells of several phases, one thread per
+ *                 phase and part (energy; explicit potentials and tangent;
+ *                 mobilities);
  *   k_chem_single / k_chem_cell (general_kernels.cuh): per cell
  *                 (src/cipher.c:148-233): site fractions of every active
  *                 phase at the cell's potentials, the interpolated
@@ -17,8 +21,6 @@
  *                 and conductivity, stored in scratch planes that the face
  *                 terms of both neighbours read;
  *   k_rhs_single (rhs_single.cu): the single-phase cells;
- *   k_item_list, k_items (rhs_items.cu): the model evaluations of each
- *                 phase of the cells of several phases, one thread each;
  *   k_rhs_general (general_kernels.cuh): the other cells: faces in the
  *                 reference's face order (phase, mu and heat fluxes,
  *                 235-317), boundary faces (319-389), then the cell terms
@@ -577,17 +579,18 @@ static cudaError_t launch_gen(const GenArgs<R> &a, int dim, cudaStream_t s)
         const OrderBuf o = {a.order, a.order_counts, a.order_cursor, a.nclass, a.ncells};
         launch_order(o, GeneralClassKey{a.as, a.stride, a.chem.pmm, a.npf, a.chem.nmat}, s);
     }
-    /* composition, mobility and conductivity of every cell before any face
-     * flux reads them; the phase items of the cells of several phases; then
-     * the RHS of the single-phase cells and of the rest */
+    /* the phase items of the cells of several phases (they read only the
+     * state); composition, mobility and conductivity of every cell before
+     * any face flux reads them (k_chem_cell combines the items' mobilities);
+     * then the RHS of the single-phase cells and of the rest */
     cudaError_t e;
+    if (a.icap && (e = launch_items(a, s)) != cudaSuccess) return e;
     if (a.ndp) {
         if (a.single_models && (e = launch_chem_single(a, s)) != cudaSuccess) return e;
         k_chem_cell<CIPHER_PMAX, R><<<wblocks, kWarpBlock, 0, s>>>(a);
     }
     if (a.grad) k_gradients<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a, dim);
     if (a.single_models && (e = launch_rhs_single(a, dim, s)) != cudaSuccess) return e;
-    if (a.icap && (e = launch_items(a, s)) != cudaSuccess) return e;
     k_rhs_general<CIPHER_PMAX, R><<<wblocks, kWarpBlock, 0, s>>>(a, dim);
     return cudaGetLastError();
 }

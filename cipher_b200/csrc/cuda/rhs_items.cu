@@ -19,8 +19,9 @@
  *                  the whole cell, the slot potential, sitefrac, energy,
  *                  explicit potentials, tangent), writing the phase's dEX/dt
  *                  planes of F and its results into the item scratch
- *                  (general_common.cuh: ItemQ); the energy and the explicit
- *                  potentials with the tangent run on two warps.
+ *                  (general_common.cuh: ItemQ), and the phase's mobilities
+ *                  for k_chem_cell; the energy, the explicit potentials with
+ *                  the tangent, and the mobilities run on three warps.
  * The general kernel then combines each cell's items in the reference's
  * order.  When every material has one model, k_items is compiled for the
  * component count and model (the model bodies inline, models.cuh).
@@ -35,7 +36,7 @@
 
 namespace cipher {
 
-constexpr int kItemBlock = 64;
+constexpr int kItemBlock = 96;     /* three warps: the three parts of 32 items */
 
 template <typename R>
 __global__ void __launch_bounds__(kGenBlock) k_item_list(const GenArgs<R> a)
@@ -78,17 +79,17 @@ __global__ void __launch_bounds__(kItemBlock) k_items(const GenArgs<R> a)
     const int ncp = NC > 0 ? NC : a.ncp, ndp = NC > 0 ? NC - 1 : a.ndp, SP = a.SP;
     const ItemQ iq = item_q(ndp, SP);
     const int64_t nitems = *a.icount < a.icap ? (int64_t)*a.icount : a.icap;
-    /* two warps per 32 items: the even warp evaluates the energy (and the
-     * site-fraction results), the odd one the explicit potentials and the
-     * tangent, so that the two long model chains of an item run side by
-     * side; both evaluate the site fractions (the same bits).  The grid
-     * stride is a multiple of 64 threads, so a thread's warp parity, and
-     * with it its part, stays the same along the loop. */
-    const int64_t nv = 2 * ((nitems + 31) / 32) * 32;
+    /* three warps per 32 items: part 0 evaluates the energy (and the
+     * site-fraction results), part 1 the explicit potentials and the
+     * tangent, part 2 the mobilities (for k_chem_cell), so that the long
+     * model chains of an item run side by side; each evaluates the site
+     * fractions (the same bits).  The grid stride is a multiple of 96
+     * threads, so a thread's part stays the same along the loop. */
+    const int64_t nv = 3 * ((nitems + 31) / 32) * 32;
     for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (int64_t)gridDim.x * blockDim.x) {
         const int64_t w = v >> 5;
-        const int part = (int)(w & 1);
-        const int64_t it = (w >> 1) * 32 + (v & 31);
+        const int part = (int)(w % 3);
+        const int64_t it = (w / 3) * 32 + (v & 31);
         if (it >= nitems) continue;
         const int32_t code = a.icell[it];
         if (code < 0 || (int64_t)(code >> 4) >= a.ncells) continue;
@@ -111,6 +112,16 @@ __global__ void __launch_bounds__(kItemBlock) k_items(const GenArgs<R> a)
         double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP];
         slot_potential<NC, MODEL>(a, mat, mu, ci, c, g, pot);
         PMod::sitefrac(ch, ids[g], pot, T, y);
+        if (part == 2) {
+            /* the phase's share of the cell's composition and mobility
+             * (src/cipher.c:148-233) */
+            double me[CIPHER_MAXCP];
+            PMod::mobility(ch, ids[g], y, T, me);
+            for (int d = 0; d < ncp; d++) put(iq.me + d, me[d]);
+            for (int s = 0; s < ns; s++)
+                for (int d = 0; d < ncp; d++) put(iq.yc + s * ncp + d, y[s * ncp + d]);
+            continue;
+        }
         if (part == 0) {
             put(0, PMod::chemenergy(ch, ids[g], y, mu, T));
             for (int s = 0; s < ns; s++)
@@ -168,7 +179,7 @@ static cudaError_t launch_items_t(const GenArgs<R> &a, cudaStream_t s)
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int64_t need = (2 * a.icap + kItemBlock - 1) / kItemBlock;   /* two threads per item */
+    const int64_t need = (3 * a.icap + kItemBlock - 1) / kItemBlock;   /* three threads per item */
     const unsigned grid = (unsigned)(need < (int64_t)sms * 16 ? need : (int64_t)sms * 16);
     switch (a.item_model >= 0 ? a.ncp : 0) {
     case 2: launch_items_nc<2>(a, grid, s); break;
