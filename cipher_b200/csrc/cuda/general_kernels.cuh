@@ -239,22 +239,24 @@ __global__ void __launch_bounds__(kWarpBlock, 32) k_rhs_general(const GenArgs<R>
         using RC = decltype(zero);
         const RC PIc = (RC)PI;
         RC cap[PM], unc[PM], rate[PM];
+        /* the pair properties once per pair, as the reference forms them
+         * (src/cipher.c:420-472), for the capillary, triple-junction,
+         * active-set and rate terms below */
+        double psig[PM * (PM - 1) / 2], pmob[PM * (PM - 1) / 2], pwid[PM * (PM - 1) / 2];
+        auto pi = [&](int k, int j) { return k * (2 * n - k - 1) / 2 + (j - k - 1); };
+        for (int k = 0; k < n; k++)
+            for (int j = k + 1; j < n; j++) props(k, j, psig[pi(k, j)], pmob[pi(k, j)], pwid[pi(k, j)]);
         for (int g = 0; g < n; g++) { cap[g] = (RC)0; rate[g] = (RC)0; }
         for (int k = 0; k < n; k++) {
             for (int j = k + 1; j < n; j++) {
-                double skd, mkd, wkd;
-                props(k, j, skd, mkd, wkd);
-                const RC skj = (RC)skd, wkj = (RC)wkd;
+                const RC skj = (RC)psig[pi(k, j)], wkj = (RC)pwid[pi(k, j)];
                 cap[k] -= skj * ((RC)phi[j] / wkj + (RC)lap[j] * wkj / PIc / PIc);
                 cap[j] -= skj * ((RC)phi[k] / wkj + (RC)lap[k] * wkj / PIc / PIc);
                 for (int i = j + 1; i < n; i++) {
-                    double s_, m_, w_;
                     RC tj = (RC)0, v;
                     v = skj / wkj; tj = tj > v ? tj : v;
-                    props(k, i, s_, m_, w_);
-                    v = (RC)s_ / (RC)w_; tj = tj > v ? tj : v;
-                    props(j, i, s_, m_, w_);
-                    v = (RC)s_ / (RC)w_; tj = tj > v ? tj : v;
+                    v = (RC)psig[pi(k, i)] / (RC)pwid[pi(k, i)]; tj = tj > v ? tj : v;
+                    v = (RC)psig[pi(j, i)] / (RC)pwid[pi(j, i)]; tj = tj > v ? tj : v;
                     tj *= (RC)a.junctionpenalty;
                     cap[k] -= tj * (RC)phi[j] * (RC)phi[i];
                     cap[j] -= tj * (RC)phi[k] * (RC)phi[i];
@@ -283,9 +285,8 @@ __global__ void __launch_bounds__(kWarpBlock, 32) k_rhs_general(const GenArgs<R>
         for (int g = 0; g < n; g++) unc[g] = (RC)0;
         for (int k = 0; k < n; k++) {
             for (int j = k + 1; j < n; j++) {
-                double s_, m_, w_;
-                props(k, j, s_, m_, w_);
-                const RC r = (RC)m_ * ((cap[k] - cap[j]) - (RC)(chem[k] - chem[j]) * (RC)8 * (RC)sqrt(h[k] * h[j]) / PIc);
+                const RC r = (RC)pmob[pi(k, j)] *
+                             ((cap[k] - cap[j]) - (RC)(chem[k] - chem[j]) * (RC)8 * (RC)sqrt(h[k] * h[j]) / PIc);
                 unc[k] += r;
                 unc[j] -= r;
             }
@@ -297,9 +298,8 @@ __global__ void __launch_bounds__(kWarpBlock, 32) k_rhs_general(const GenArgs<R>
             if (!(act >> k & 1u)) continue;
             for (int j = k + 1; j < n; j++) {
                 if (!(act >> j & 1u)) continue;
-                double s_, m_, w_;
-                props(k, j, s_, m_, w_);
-                const RC r = (RC)m_ * ((cap[k] - cap[j]) - (RC)(chem[k] - chem[j]) * (RC)8 * (RC)sqrt(h[k] * h[j]) / PIc);
+                const RC r = (RC)pmob[pi(k, j)] *
+                             ((cap[k] - cap[j]) - (RC)(chem[k] - chem[j]) * (RC)8 * (RC)sqrt(h[k] * h[j]) / PIc);
                 rate[k] += r;
                 rate[j] -= r;
             }
