@@ -90,13 +90,21 @@ __global__ void __launch_bounds__(kWarpBlock) k_chem_cell(const GenArgs<R> a)
 /* the RHS                                                              */
 /* ------------------------------------------------------------------ */
 
+/* two warps per 32 cells (one warp's worth of cells per block): the first
+ * gathers the faces (phase, mu and heat fluxes, boundary faces) while the
+ * second runs the cell terms that do not depend on them (interpolant,
+ * segregation, the pass over the phases); the face sums then pass to the
+ * second warp through shared memory.  The operations are the same. */
 template <int PM, typename R>
-__global__ void __launch_bounds__(kWarpBlock, 32) k_rhs_general(const GenArgs<R> a, const int DIM)
+__global__ void __launch_bounds__(2 * kWarpBlock, 16) k_rhs_general(const GenArgs<R> a, const int DIM)
 {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.ncells) return;
-    const int64_t c = a.order ? (int64_t)a.order[t] : t;
-    if (single_model(a, c) >= 0) return;           /* rhs_single.cu's kernels */
+    __shared__ double sh_lap[PM][kWarpBlock], sh_ldp[CIPHER_MAXCP][kWarpBlock], sh_ltm[kWarpBlock];
+    const int lane = threadIdx.x & 31;
+    const bool face_warp = threadIdx.x < kWarpBlock;
+    const int64_t t = (int64_t)blockIdx.x * kWarpBlock + lane;
+    bool active = t < a.ncells;
+    const int64_t c = active ? (a.order ? (int64_t)a.order[t] : t) : 0;
+    if (active && single_model(a, c) >= 0) active = false;   /* rhs_single.cu's kernels */
     const int64_t S = a.stride;
     const int ncp = a.ncp, ndp = a.ndp, SP = a.SP;
     const double PI = CIPHER_PI_D;
@@ -110,24 +118,25 @@ __global__ void __launch_bounds__(kWarpBlock, 32) k_rhs_general(const GenArgs<R>
 
     uint16_t ids[PM];
     double phi[PM], h[PM], lap[PM], pf[PM];
-    const int n = load_set<PM>(a, c, ids, phi);
-    if (n == 0) return;
+    const int n = active ? load_set<PM>(a, c, ids, phi) : 0;
+    if (n == 0) active = false;
     /* >= 0: the phases' model results are items ib .. ib+n-1 of the scratch */
-    const int32_t ib = a.ibase ? a.ibase[c] : -1;
+    const int32_t ib = active && a.ibase ? a.ibase[c] : -1;
     const ItemQ iq = item_q(ndp, SP);
     auto item = [&](int q, int g) { return a.iscr[(int64_t)q * a.icap + ib + g]; };
-    const double T = (double)a.tm[c];
+    const double T = active ? (double)a.tm[c] : 0.0;
     const ChemTables ch = chem_at(a.chem, T);
     double mu[CIPHER_MAXCP], ldp[CIPHER_MAXCP];
-    for (int d = 0; d < ndp; d++) { mu[d] = a.dp[(int64_t)d * S + c]; ldp[d] = 0.0; }
+    for (int d = 0; d < ndp; d++) { mu[d] = active ? a.dp[(int64_t)d * S + c] : 0.0; ldp[d] = 0.0; }
     double ltm = 0.0;
     for (int g = 0; g < n; g++) lap[g] = 0.0;
 
-    /* ---- faces in the reference's face order (src/cipher.c:235-317) ---- */
-    walk_faces(a, c, co, DIM, [&](int64_t nb, bool self_L, int nn, const auto &fdiv) {
-        /* phase flux, gated on the L cell only (src/cipher.c:277) */
-        const bool gate = self_L ? (n > 1 || ids[0] > 1) : (nn > 1 || a.as[S + nb] > 1);
-        if (gate) {
+    if (active && face_warp) {
+        /* ---- faces in the reference's face order (src/cipher.c:235-317) ---- */
+        walk_faces(a, c, co, DIM, [&](int64_t nb, bool self_L, int nn, const auto &fdiv) {
+            /* phase flux, gated on the L cell only (src/cipher.c:277) */
+            const bool gate = self_L ? (n > 1 || ids[0] > 1) : (nn > 1 || a.as[S + nb] > 1);
+            if (gate) {
                 int i = 0, j = 0;
                 while (i < n && j < nn) {
                     const uint16_t b = a.as[(int64_t)(1 + j) * S + nb];
@@ -143,73 +152,84 @@ __global__ void __launch_bounds__(kWarpBlock, 32) k_rhs_general(const GenArgs<R>
                         j++;
                     }
                 }
-        }
-        const int64_t cl = self_L ? c : nb, cr = self_L ? nb : c;
-        chem_heat_face<0>(a, cl, cr, self_L, fdiv, ldp, ltm);
-    });
-    boundary_faces<0>(a, c, co, DIM, T, mu, ldp, ltm);
+            }
+            const int64_t cl = self_L ? c : nb, cr = self_L ? nb : c;
+            chem_heat_face<0>(a, cl, cr, self_L, fdiv, ldp, ltm);
+        });
+        boundary_faces<0>(a, c, co, DIM, T, mu, ldp, ltm);
+        for (int g = 0; g < n; g++) sh_lap[g][lane] = lap[g];
+        for (int d = 0; d < ndp; d++) sh_ldp[d][lane] = ldp[d];
+        sh_ltm[lane] = ltm;
+    }
 
-    /* ---- cell terms (src/cipher.c:391-664) ---- */
-    interpolant(a.interp, phi, n, h);
     double ci[CIPHER_MAXCP];
-    if (ndp) segregation(a, ids, h, n, ci);
-
-    /* pass over the phases: driving force, dEX/dt and the tangent sum */
     double chem[PM], yw[PM * (CIPHER_MAXCP - 1)];
     double cbar[CIPHER_MAXCP], dcdm[(CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1)];
-    for (int d = 0; d < CIPHER_MAXCP; d++) cbar[d] = 0.0;
-    for (int q = 0; q < (CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1); q++) dcdm[q] = 0.0;
     /* tangent of the last phase evaluated: reused by the composition rate
      * below when the cell has a single phase (same arguments, same bits) */
     double tpot[2 * 16], tex[2 * 16], tT[2 * CIPHER_MAXCP];
-    for (int g = 0; g < n; g++) {
-        const cipher_material &mat = material_of(ch, ids[g]);
-        if (ib >= 0) {
-            /* the same sums over the item's stored results (n > 1, ndp > 0) */
-            chem[g] = item(0, g);
-            for (int s = 0; s < mat.nsites; s++)
-                for (int d = 0; d < ndp; d++) cbar[d] += h[g] * mat.stoichiometry[s] * item(iq.y + s * ndp + d, g);
-            for (int d = 0; d < ndp; d++) yw[g * (CIPHER_MAXCP - 1) + d] = item(iq.yw + d, g);
-            for (int s = 0; s < mat.nsites; s++)
-                for (int q = 0; q < ndp * ndp; q++)
-                    dcdm[q] += h[g] * mat.stoichiometry[s] * mat.stoichiometry[s] * item(iq.tpot + s * ndp * ndp + q, g);
-            continue;
-        }
-        double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP];
-        if (ndp) {
-            slot_potential(a, mat, mu, ci, c, g, pot);
-            sitefrac(ch, ids[g], pot, T, y);
-        }
-        if (n > 1) {
-            chem[g] = chemenergy(ch, ids[g], y, mu, T);
-            for (int s = 0; s < mat.nsites; s++) {
-                for (int d = 0; d < ndp; d++) cbar[d] += h[g] * mat.stoichiometry[s] * y[s * ncp + d];
+    if (active && !face_warp) {
+        /* ---- cell terms (src/cipher.c:391-664) ---- */
+        interpolant(a.interp, phi, n, h);
+        if (ndp) segregation(a, ids, h, n, ci);
+
+        /* pass over the phases: driving force, dEX/dt and the tangent sum */
+        for (int d = 0; d < CIPHER_MAXCP; d++) cbar[d] = 0.0;
+        for (int q = 0; q < (CIPHER_MAXCP - 1) * (CIPHER_MAXCP - 1); q++) dcdm[q] = 0.0;
+        for (int g = 0; g < n; g++) {
+            const cipher_material &mat = material_of(ch, ids[g]);
+            if (ib >= 0) {
+                /* the same sums over the item's stored results (n > 1, ndp > 0) */
+                chem[g] = item(0, g);
+                for (int s = 0; s < mat.nsites; s++)
+                    for (int d = 0; d < ndp; d++) cbar[d] += h[g] * mat.stoichiometry[s] * item(iq.y + s * ndp + d, g);
+                for (int d = 0; d < ndp; d++) yw[g * (CIPHER_MAXCP - 1) + d] = item(iq.yw + d, g);
+                for (int s = 0; s < mat.nsites; s++)
+                    for (int q = 0; q < ndp * ndp; q++)
+                        dcdm[q] += h[g] * mat.stoichiometry[s] * mat.stoichiometry[s] * item(iq.tpot + s * ndp * ndp + q, g);
+                continue;
             }
-        }
-        if (ndp) {
-            for (int d = 0; d < ndp; d++) {
-                double w = 0.0;
-                for (int s = 0; s < mat.nsites; s++) w += mat.stoichiometry[s] * y[s * ncp + d];
-                yw[g * (CIPHER_MAXCP - 1) + d] = w;
+            double pot[2 * CIPHER_MAXCP], y[2 * CIPHER_MAXCP];
+            if (ndp) {
+                slot_potential(a, mat, mu, ci, c, g, pot);
+                sitefrac(ch, ids[g], pot, T, y);
             }
-            /* explicit potential relaxation (src/cipher.c:570-581) */
-            double spx[2 * CIPHER_MAXCP];
-            sitepot_explicit(ch, ids[g], y, T, spx);
-            for (int s = 0; s < mat.nsites; s++) {
-                for (int d = 0; d < ndp; d++) {
-                    const int64_t pl = (int64_t)(g * SP + s * ndp + d) * S + c;
-                    a.fex[pl] = mat.chempot_ex_kineticcoeff * (spx[s * ndp + d] - a.ex[pl]);
+            if (n > 1) {
+                chem[g] = chemenergy(ch, ids[g], y, mu, T);
+                for (int s = 0; s < mat.nsites; s++) {
+                    for (int d = 0; d < ndp; d++) cbar[d] += h[g] * mat.stoichiometry[s] * y[s * ncp + d];
                 }
             }
-            for (int q = mat.nsites * ndp; q < SP; q++) a.fex[(int64_t)(g * SP + q) * S + c] = 0.0;
-            sitefrac_tangent(ch, ids[g], y, pot, T, tpot, tex, tT);
-            for (int s = 0; s < mat.nsites; s++) {
-                for (int q = 0; q < ndp * ndp; q++)
-                    dcdm[q] += h[g] * mat.stoichiometry[s] * mat.stoichiometry[s] * tpot[s * ndp * ndp + q];
+            if (ndp) {
+                for (int d = 0; d < ndp; d++) {
+                    double w = 0.0;
+                    for (int s = 0; s < mat.nsites; s++) w += mat.stoichiometry[s] * y[s * ncp + d];
+                    yw[g * (CIPHER_MAXCP - 1) + d] = w;
+                }
+                /* explicit potential relaxation (src/cipher.c:570-581) */
+                double spx[2 * CIPHER_MAXCP];
+                sitepot_explicit(ch, ids[g], y, T, spx);
+                for (int s = 0; s < mat.nsites; s++) {
+                    for (int d = 0; d < ndp; d++) {
+                        const int64_t pl = (int64_t)(g * SP + s * ndp + d) * S + c;
+                        a.fex[pl] = mat.chempot_ex_kineticcoeff * (spx[s * ndp + d] - a.ex[pl]);
+                    }
+                }
+                for (int q = mat.nsites * ndp; q < SP; q++) a.fex[(int64_t)(g * SP + q) * S + c] = 0.0;
+                sitefrac_tangent(ch, ids[g], y, pot, T, tpot, tex, tT);
+                for (int s = 0; s < mat.nsites; s++) {
+                    for (int q = 0; q < ndp * ndp; q++)
+                        dcdm[q] += h[g] * mat.stoichiometry[s] * mat.stoichiometry[s] * tpot[s * ndp * ndp + q];
+                }
             }
         }
+        for (int q = n * SP; q < a.P * SP; q++) a.fex[(int64_t)q * S + c] = 0.0;
     }
-    for (int q = n * SP; q < a.P * SP; q++) a.fex[(int64_t)q * S + c] = 0.0;
+    __syncthreads();
+    if (!active || face_warp) return;
+    for (int g = 0; g < n; g++) lap[g] = sh_lap[g][lane];
+    for (int d = 0; d < ndp; d++) ldp[d] = sh_ldp[d][lane];
+    ltm = sh_ltm[lane];
 
     /* pair properties; with anisotropy they depend on the pair's normal,
      * the normalised difference of the two slots' gradients (src/cipher.c:

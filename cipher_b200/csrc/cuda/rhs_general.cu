@@ -591,7 +591,7 @@ static cudaError_t launch_gen(const GenArgs<R> &a, int dim, cudaStream_t s)
     }
     if (a.grad) k_gradients<CIPHER_PMAX, R><<<blocks, kGenBlock, 0, s>>>(a, dim);
     if (a.single_models && (e = launch_rhs_single(a, dim, s)) != cudaSuccess) return e;
-    k_rhs_general<CIPHER_PMAX, R><<<wblocks, kWarpBlock, 0, s>>>(a, dim);
+    k_rhs_general<CIPHER_PMAX, R><<<wblocks, 2 * kWarpBlock, 0, s>>>(a, dim);   /* a face and a cell warp */
     return cudaGetLastError();
 }
 
